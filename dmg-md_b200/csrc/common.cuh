@@ -1,0 +1,208 @@
+// common.cuh -- shared device-side definitions of the nepx engine.
+//
+// Box and minimum image, NEP constants, cutoff and Chebyshev radial basis,
+// and the real solid harmonics used by the descriptor and force kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace nepx {
+
+constexpr int kMaxTypes = 16;
+constexpr int kMaxBasis = 17;   // basis_size + 1
+constexpr int kMaxN = 13;       // n_max + 1
+constexpr int kNumLM = 24;      // (L_max + 1)^2 - 1 at L_max = 4
+constexpr int kMaxDim = 128;
+constexpr int kMaxInv = 6;      // q_222, q_1111, q_112, q_123, q_233, q_134
+constexpr double kBoltzmann = 8.617343e-5;           // eV/K, GPUMD natural units
+constexpr double kTimeUnit = 1.018051e+1;            // natural time unit in fs
+constexpr double kPressureUnit = 1.602177e+2;        // eV/A^3 in GPa
+constexpr float kCoulomb = 14.399645f;               // e^2/(4 pi eps0) in eV A
+
+// Device-resident periodic box.  h is row-major with the cell vectors a, b, c
+// as columns (the layout of the reference's Box::cpu_h[0..8]); hinv its
+// inverse; fh the float copy (h then hinv) the FP32 kernels use.
+struct Box {
+  double h[9];
+  double hinv[9];
+  float fh[18];
+  int pbc[3];
+  int ortho;
+};
+
+// Cell grid and rebuild bookkeeping of the Verlet list, device resident.
+struct NeighborState {
+  int rebuild;         // 1: rebuild the Verlet list before the next filter
+  int overflow;        // bit 0 Verlet row, bit 1 radial row, bit 2 angular row
+  int nc[3];           // cells per direction
+  int ncell;
+  int max_nn[3];       // largest Verlet / radial / angular row of the last build
+  int nonfinite;       // a force or energy came out NaN/Inf
+};
+
+// Minimum image of a float displacement, the arithmetic of the large-box
+// path (reference box.cuh:84-127): half-box shortcut for orthogonal boxes,
+// fractional nearbyint otherwise.
+__device__ __forceinline__ void mic_f32(const Box& b, float& x, float& y, float& z)
+{
+  if (b.ortho) {
+    const float lx2 = b.fh[0] * 0.5f, ly2 = b.fh[4] * 0.5f, lz2 = b.fh[8] * 0.5f;
+    if (b.pbc[0] == 1) {
+      if (x < -lx2) x += b.fh[0];
+      else if (x > +lx2) x -= b.fh[0];
+    }
+    if (b.pbc[1] == 1) {
+      if (y < -ly2) y += b.fh[4];
+      else if (y > +ly2) y -= b.fh[4];
+    }
+    if (b.pbc[2] == 1) {
+      if (z < -lz2) z += b.fh[8];
+      else if (z > +lz2) z -= b.fh[8];
+    }
+  } else {
+    float sx = b.fh[9] * x + b.fh[10] * y + b.fh[11] * z;
+    float sy = b.fh[12] * x + b.fh[13] * y + b.fh[14] * z;
+    float sz = b.fh[15] * x + b.fh[16] * y + b.fh[17] * z;
+    if (b.pbc[0] == 1) sx -= nearbyintf(sx);
+    if (b.pbc[1] == 1) sy -= nearbyintf(sy);
+    if (b.pbc[2] == 1) sz -= nearbyintf(sz);
+    x = b.fh[0] * sx + b.fh[1] * sy + b.fh[2] * sz;
+    y = b.fh[3] * sx + b.fh[4] * sy + b.fh[5] * sz;
+    z = b.fh[6] * sx + b.fh[7] * sy + b.fh[8] * sz;
+  }
+}
+
+// Displacement r_j - r_i: the double difference rounded to float, then the
+// float minimum image -- the operand order of the reference's filter
+// (nep.cu:542-549), so neighbour predicates agree bit for bit.
+__device__ __forceinline__ void displacement(const Box& b, const double* __restrict__ x,
+                                             const double* __restrict__ y,
+                                             const double* __restrict__ z, double xi, double yi,
+                                             double zi, int j, float& dx, float& dy, float& dz)
+{
+  dx = __ldg(x + j) - xi;
+  dy = __ldg(y + j) - yi;
+  dz = __ldg(z + j) - zi;
+  mic_f32(b, dx, dy, dz);
+}
+
+// Cutoff function fc = (1 + cos(pi d / rc)) / 2 and its d-derivative.
+__device__ __forceinline__ void cutoff_fc(float rc, float rcinv, float d, float& fc, float& fcp)
+{
+  if (d < rc) {
+    float s, c;
+    sincospif(d * rcinv, &s, &c);
+    fc = 0.5f * c + 0.5f;
+    fcp = -1.5707963f * s * rcinv;
+  } else {
+    fc = 0.0f;
+    fcp = 0.0f;
+  }
+}
+
+// Shifted Chebyshev radial basis f_k(d) = (T_k(x) + 1) / 2 * fc (f_0 = fc)
+// with x = 2 (d/rc - 1)^2 - 1, k = 0..kmax-1.
+template <int KMAX>
+__device__ __forceinline__ void radial_basis(int kmax, float rcinv, float d, float fc, float* fn)
+{
+  const float u = d * rcinv - 1.0f;
+  const float x = 2.0f * u * u - 1.0f;
+  const float half_fc = 0.5f * fc;
+  float t0 = 1.0f, t1 = x;
+  fn[0] = fc;
+#pragma unroll
+  for (int k = 1; k < KMAX; ++k) {
+    if (k < kmax) fn[k] = (t1 + 1.0f) * half_fc;
+    const float t2 = 2.0f * x * t1 - t0;
+    t0 = t1;
+    t1 = t2;
+  }
+}
+
+// Basis values and their d-derivatives.
+template <int KMAX>
+__device__ __forceinline__ void radial_basis_d(int kmax, float rcinv, float d, float fc,
+                                               float fcp, float* fn, float* fnp)
+{
+  const float u = d * rcinv - 1.0f;
+  const float x = 2.0f * u * u - 1.0f;
+  const float dxdd = 4.0f * u * rcinv;
+  float t0 = 1.0f, t1 = x;       // T_{k-1}, T_k
+  float dt0 = 0.0f, dt1 = 1.0f;  // dT/dx
+  fn[0] = fc;
+  fnp[0] = fcp;
+#pragma unroll
+  for (int k = 1; k < KMAX; ++k) {
+    if (k < kmax) {
+      fn[k] = 0.5f * (t1 + 1.0f) * fc;
+      fnp[k] = 0.5f * (dt1 * dxdd * fc + (t1 + 1.0f) * fcp);
+    }
+    const float t2 = 2.0f * x * t1 - t0;
+    const float dt2 = 2.0f * t1 + 2.0f * x * dt1 - dt0;
+    t0 = t1;
+    t1 = t2;
+    dt0 = dt1;
+    dt1 = dt2;
+  }
+}
+
+// Real solid harmonics of degree L = 1..4 at the unit vector (x, y, z):
+// Y = P_L^m(z) * Re/Im (x + i y)^m with the z-polynomials below, in the
+// component order of the reference's blm moments (L^2 - 1 + {0, 2m-1, 2m}).
+// ZP[L][m] holds the coefficients of z^0..z^4.
+__device__ __forceinline__ float zpoly(int L, int m, const float* zp, float* dzf)
+{
+  // coefficients of the reference's Z_COEFFICIENT_L tables (nep_utilities.cuh:89-117)
+  float f = 0.0f, df = 0.0f;
+  switch (L * 8 + m) {
+    case 8 + 0: f = zp[1]; df = 1.0f; break;
+    case 8 + 1: f = 1.0f; df = 0.0f; break;
+    case 16 + 0: f = 3.0f * zp[2] - 1.0f; df = 6.0f * zp[1]; break;
+    case 16 + 1: f = zp[1]; df = 1.0f; break;
+    case 16 + 2: f = 1.0f; df = 0.0f; break;
+    case 24 + 0: f = 5.0f * zp[3] - 3.0f * zp[1]; df = 15.0f * zp[2] - 3.0f; break;
+    case 24 + 1: f = 5.0f * zp[2] - 1.0f; df = 10.0f * zp[1]; break;
+    case 24 + 2: f = zp[1]; df = 1.0f; break;
+    case 24 + 3: f = 1.0f; df = 0.0f; break;
+    case 32 + 0: f = 35.0f * zp[4] - 30.0f * zp[2] + 3.0f; df = 140.0f * zp[3] - 60.0f * zp[1]; break;
+    case 32 + 1: f = 7.0f * zp[3] - 3.0f * zp[1]; df = 21.0f * zp[2] - 3.0f; break;
+    case 32 + 2: f = 7.0f * zp[2] - 1.0f; df = 14.0f * zp[1]; break;
+    case 32 + 3: f = zp[1]; df = 1.0f; break;
+    case 32 + 4: f = 1.0f; df = 0.0f; break;
+    default: break;
+  }
+  *dzf = df;
+  return f;
+}
+
+// Harmonics Y[0..nlm) at unit vector u.
+__device__ __forceinline__ void harmonics(int L_max, float ux, float uy, float uz, float* Y)
+{
+  float zp[5];
+  zp[0] = 1.0f;
+#pragma unroll
+  for (int k = 1; k < 5; ++k) zp[k] = zp[k - 1] * uz;
+  int idx = 0;
+#pragma unroll
+  for (int L = 1; L <= 4; ++L) {
+    if (L > L_max) break;
+    float re = ux, im = uy;
+#pragma unroll
+    for (int m = 0; m <= L; ++m) {
+      float dzf;
+      const float zf = zpoly(L, m, zp, &dzf);
+      if (m == 0) {
+        Y[idx++] = zf;
+      } else {
+        Y[idx++] = zf * re;
+        Y[idx++] = zf * im;
+        const float r2 = ux * re - uy * im;
+        im = ux * im + uy * re;
+        re = r2;
+      }
+    }
+  }
+}
+
+}  // namespace nepx

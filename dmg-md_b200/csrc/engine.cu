@@ -1,0 +1,171 @@
+// engine.cu -- handle construction, device uploads and box handling.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "engine.h"
+
+namespace nepx {
+
+void upload_invariant_tables();
+size_t descriptor_smem_bytes(const ModelParams& p);
+void set_descriptor_smem_limit(size_t bytes);
+
+namespace {
+
+__global__ void k_set_box(Box* dst, Box src) { *dst = src; }
+
+template <typename T>
+cudaError_t dalloc(T*& ptr, size_t count)
+{
+  return cudaMalloc(reinterpret_cast<void**>(&ptr), std::max<size_t>(count, 1) * sizeof(T));
+}
+
+}  // namespace
+
+std::string make_box(const double* h, const int* pbc, Box& b)
+{
+  std::memcpy(b.h, h, sizeof(double) * 9);
+  for (int d = 0; d < 3; ++d) b.pbc[d] = pbc[d] ? 1 : 0;
+  // inverse with the cofactor order of the reference (box.cu:101-118)
+  b.hinv[0] = h[4] * h[8] - h[5] * h[7];
+  b.hinv[1] = h[2] * h[7] - h[1] * h[8];
+  b.hinv[2] = h[1] * h[5] - h[2] * h[4];
+  b.hinv[3] = h[5] * h[6] - h[3] * h[8];
+  b.hinv[4] = h[0] * h[8] - h[2] * h[6];
+  b.hinv[5] = h[2] * h[3] - h[0] * h[5];
+  b.hinv[6] = h[3] * h[7] - h[4] * h[6];
+  b.hinv[7] = h[1] * h[6] - h[0] * h[7];
+  b.hinv[8] = h[0] * h[4] - h[1] * h[3];
+  const double det = h[0] * (h[4] * h[8] - h[5] * h[7]) + h[1] * (h[5] * h[6] - h[3] * h[8]) +
+                     h[2] * (h[3] * h[7] - h[4] * h[6]);
+  if (!std::isfinite(det) || det == 0.0) return "singular or non-finite box";
+  for (int k = 0; k < 9; ++k) b.hinv[k] /= det;
+  b.ortho = h[1] == 0 && h[2] == 0 && h[3] == 0 && h[5] == 0 && h[6] == 0 && h[7] == 0;
+  for (int k = 0; k < 9; ++k) {
+    b.fh[k] = static_cast<float>(b.h[k]);
+    b.fh[9 + k] = static_cast<float>(b.hinv[k]);
+  }
+  return "";
+}
+
+void launch_set_box(Engine& e, const Box& b, cudaStream_t stream)
+{
+  k_set_box<<<1, 1, 0, stream>>>(e.d_box, b);
+}
+
+std::string engine_create(Engine& e, const std::string& nep_path, int max_atoms)
+{
+  std::string err = load_nep(nep_path, e.model);
+  if (!err.empty()) return err;
+  const NepModel& m = e.model;
+  ModelParams& p = e.params;
+  std::memset(&p, 0, sizeof(p));
+  p.version = m.version;
+  p.T = m.num_types;
+  p.nR = m.n_max_radial + 1;
+  p.nA = m.n_max_angular + 1;
+  p.kR = m.basis_radial + 1;
+  p.kA = m.basis_angular + 1;
+  p.L_max = m.L_max;
+  p.nlm = (m.L_max + 1) * (m.L_max + 1) - 1;
+  p.num_L = m.num_L;
+  p.dim = m.dim;
+  p.H = m.H;
+  p.num_inv = 0;
+  for (int v = 0; v < kMaxInv; ++v)
+    if (m.has_inv[v]) p.inv_id[p.num_inv++] = v;
+  for (int t = 0; t < m.num_types; ++t) {
+    p.rc_r[t] = m.rc_radial[t];
+    p.rc_a[t] = m.rc_angular[t];
+    p.Z[t] = m.Z[t];
+  }
+  p.zbl = m.zbl;
+  p.zbl_flexible = m.zbl_flexible;
+  p.typewise_zbl = m.typewise_zbl;
+  p.zbl_rc_inner = m.zbl_rc_inner;
+  p.zbl_rc_outer = m.zbl_rc_outer;
+  p.typewise_factor = m.typewise_factor;
+  p.num_c_radial = p.T * p.T * p.nR * p.kR;
+  if (p.T * p.T * (p.nR * p.kR + p.nA * p.kA) > 12288)
+    return "descriptor coefficient table too large for shared memory";
+
+  upload_invariant_tables();
+  // one parameter allocation: c_pair | w0 | b0 | w1 | out_bias | q_scaler | zbl | rc_r | rc_a
+  std::vector<float> blob;
+  auto append = [&blob](const std::vector<float>& v) {
+    const size_t at = blob.size();
+    blob.insert(blob.end(), v.begin(), v.end());
+    while (blob.size() % 4) blob.push_back(0.0f);   // 16-byte aligned blocks
+    return at;
+  };
+  const size_t o_c = append(m.c_pair), o_w0 = append(m.w0), o_b0 = append(m.b0);
+  const size_t o_w1 = append(m.w1), o_ob = append(m.out_bias), o_qs = append(m.q_scaler);
+  const size_t o_z = append(m.zbl_para.empty() ? std::vector<float>(1, 0.0f) : m.zbl_para);
+  const size_t o_rr = append(std::vector<float>(m.rc_radial, m.rc_radial + kMaxTypes));
+  const size_t o_ra = append(std::vector<float>(m.rc_angular, m.rc_angular + kMaxTypes));
+  if (dalloc(e.d_params, blob.size()) != cudaSuccess) return "cudaMalloc failed (parameters)";
+  if (cudaMemcpy(e.d_params, blob.data(), blob.size() * sizeof(float), cudaMemcpyHostToDevice) !=
+      cudaSuccess)
+    return "cudaMemcpy failed (parameters)";
+  p.c_pair = e.d_params + o_c;
+  p.w0 = e.d_params + o_w0;
+  p.b0 = e.d_params + o_b0;
+  p.w1 = e.d_params + o_w1;
+  p.out_bias = e.d_params + o_ob;
+  p.q_scaler = e.d_params + o_qs;
+  p.zbl_para = e.d_params + o_z;
+  e.d_rc_r = e.d_params + o_rr;
+  e.d_rc_a = e.d_params + o_ra;
+
+  // neighbour rows: the reference's MN_radial*1.25 scaled by ((rc+skin)/rc)^3
+  const int N = std::max(max_atoms, 1);
+  e.capacity = N;
+  NeighborBuffers& nb = e.nbr;
+  nb.mn_r = m.MN_radial;
+  nb.mn_a = m.MN_angular;
+  const double rc = m.rc_max, rv = rc + e.skin;
+  nb.mn_v = static_cast<int>(m.MN_radial * rv * rv * rv / (rc * rc * rc));
+  nb.mn_v = std::max(nb.mn_v, nb.mn_r);
+  if (nb.mn_v > 2048) return "Verlet row capacity above 2048 is not supported";
+  nb.pow2_v = 32;
+  while (nb.pow2_v < nb.mn_v) nb.pow2_v <<= 1;
+  nb.cell_cap = std::max(N, 4096);
+  bool ok = true;
+  ok &= dalloc(nb.nn_v, N) == cudaSuccess;
+  ok &= dalloc(nb.nl_v, static_cast<size_t>(N) * nb.mn_v) == cudaSuccess;
+  ok &= dalloc(nb.nn_r, N) == cudaSuccess;
+  ok &= dalloc(nb.nl_r, static_cast<size_t>(N) * nb.mn_r) == cudaSuccess;
+  ok &= dalloc(nb.nn_a, N) == cudaSuccess;
+  ok &= dalloc(nb.nl_a, static_cast<size_t>(N) * nb.mn_a) == cudaSuccess;
+  ok &= dalloc(nb.cell_count, nb.cell_cap) == cudaSuccess;
+  ok &= dalloc(nb.cell_start, nb.cell_cap) == cudaSuccess;
+  ok &= dalloc(nb.cell_atoms, N) == cudaSuccess;
+  ok &= dalloc(nb.cell_of, N) == cudaSuccess;
+  ok &= dalloc(nb.x0, 3 * static_cast<size_t>(N)) == cudaSuccess;
+  ok &= dalloc(e.scratch.fp_rad, static_cast<size_t>(N) * p.nR) == cudaSuccess;
+  ok &= dalloc(e.scratch.f12, static_cast<size_t>(N) * nb.mn_a) == cudaSuccess;
+  ok &= dalloc(e.scratch.pe_ann, N) == cudaSuccess;
+  ok &= dalloc(e.d_box, 1) == cudaSuccess;
+  ok &= dalloc(e.d_nstate, 1) == cudaSuccess;
+  if (!ok) return "cudaMalloc failed (per-atom buffers)";
+  if (cudaMemset(e.d_nstate, 0, sizeof(NeighborState)) != cudaSuccess) return "cudaMemset failed";
+  if (cudaMemset(nb.nn_a, 0, sizeof(int) * N) != cudaSuccess) return "cudaMemset failed";
+  e.smem_desc = descriptor_smem_bytes(p);
+  if (e.smem_desc > 227 * 1024) return "descriptor kernel needs more shared memory than a CTA has";
+  set_descriptor_smem_limit(e.smem_desc);
+  if (cudaGetLastError() != cudaSuccess) return "CUDA error during setup";
+  return "";
+}
+
+void engine_destroy(Engine& e)
+{
+  NeighborBuffers& nb = e.nbr;
+  void* ptrs[] = {e.d_params, e.d_box, e.d_nstate, nb.nn_v, nb.nl_v, nb.nn_r, nb.nl_r,
+                  nb.nn_a, nb.nl_a, nb.cell_count, nb.cell_start, nb.cell_atoms, nb.cell_of,
+                  nb.x0, e.scratch.fp_rad, e.scratch.f12, e.scratch.pe_ann, e.scratch.q};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+}
+
+}  // namespace nepx

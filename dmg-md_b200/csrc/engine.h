@@ -1,0 +1,78 @@
+// engine.h -- state of one nepx handle: the potential on the device, the
+// neighbour lists, per-atom scratch, and the launch entry points.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "common.cuh"
+#include "model.h"
+
+namespace nepx {
+
+struct NeighborBuffers {
+  int mn_v = 0, mn_r = 0, mn_a = 0, pow2_v = 0;
+  int* nn_v = nullptr;
+  int* nl_v = nullptr;   // [N][mn_v] row-major
+  int* nn_r = nullptr;
+  int* nl_r = nullptr;   // [N][mn_r]
+  int* nn_a = nullptr;
+  int* nl_a = nullptr;   // [N][mn_a]
+  int* cell_count = nullptr;
+  int* cell_start = nullptr;
+  int* cell_atoms = nullptr;
+  int* cell_of = nullptr;
+  int cell_cap = 0;
+  double* x0 = nullptr;  // positions at the last Verlet build (3N SoA)
+};
+
+struct ForceScratch {
+  float* fp_rad = nullptr;   // [N][nR] dE/dq of the radial descriptors (scaled)
+  float4* f12 = nullptr;     // [N][mn_a] directed angular partial forces
+  double* pe_ann = nullptr;  // [N] site energy of the ANN
+  float* q = nullptr;        // [N][dim] descriptors (mixed-precision path)
+};
+
+struct Engine {
+  NepModel model;
+  ModelParams params{};
+  int capacity = 0;          // atoms the buffers are sized for
+  double skin = 1.0;         // Verlet skin (A), the reference's default
+  // device copies of the model
+  float* d_params = nullptr; // one allocation holding all parameter blocks
+  float* d_rc_r = nullptr;
+  float* d_rc_a = nullptr;
+  Box* d_box = nullptr;
+  NeighborState* d_nstate = nullptr;
+  NeighborBuffers nbr;
+  ForceScratch scratch;
+  // host-side bookkeeping
+  Box last_box{};
+  bool have_box = false;
+  bool force_rebuild = true;
+  int last_n = -1;
+  size_t smem_desc = 0;      // dynamic shared memory of the descriptor kernel
+  std::string error;
+};
+
+// Loads the potential, uploads it and sizes every buffer for max_atoms.
+std::string engine_create(Engine& e, const std::string& nep_path, int max_atoms);
+void engine_destroy(Engine& e);
+
+// Host-side box: fills hinv, the float copy and the orthogonality flag.
+std::string make_box(const double* h, const int* pbc, Box& b);
+
+// Writes the box to the device copy in stream order.
+void launch_set_box(Engine& e, const Box& b, cudaStream_t stream);
+
+// Skin check, conditional Verlet rebuild and typewise filter.
+void launch_neighbor_update(Engine& e, int N, const double* pos, const int* type, bool force,
+                            cudaStream_t stream);
+
+// Descriptor + ANN + angular partial forces, then the force/virial gather.
+// accumulate = add into pe/force/virial instead of overwriting them.
+void launch_force(Engine& e, int N, const double* pos, const int* type, double* pe,
+                  double* force, double* virial, bool accumulate, cudaStream_t stream);
+
+}  // namespace nepx

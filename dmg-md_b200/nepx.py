@@ -1,0 +1,172 @@
+"""Python binding of the nepx C ABI (include/nepx.h) over ctypes.
+
+The engine is lib/libnepx.so (C++ host code + sm_100a CUDA kernels).  This
+module only marshals pointers: device buffers are torch CUDA tensors, and
+every call goes straight to the shared library.  There is no CPU fallback:
+loading fails loudly when the library is missing.
+
+    pot = Potential("nep.txt", max_atoms=4096)
+    pe, force, virial = pot.compute(types, box_h, positions)   # torch CUDA tensors
+
+Names follow the reference's potential interface (Potential::compute,
+src/gpumd_compat/potential.cuh:82-88): types 0-based in potential-file order,
+positions SoA (3, n) in Angstrom, virial (9, n) in the order
+xx yy zz xy xz yz yx zx zy.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libnepx.so")
+
+NEPX_ACCUMULATE = 1
+NEPX_SYNC_CHECK = 2
+
+ERRORS = {1: "NEPX_ERR_ARG", 2: "NEPX_ERR_FILE", 3: "NEPX_ERR_UNSUPPORTED", 4: "NEPX_ERR_CUDA",
+          5: "NEPX_ERR_CAPACITY", 6: "NEPX_ERR_OVERFLOW", 7: "NEPX_ERR_NONFINITE",
+          8: "NEPX_ERR_BOX"}
+
+# every symbol include/nepx.h declares (checked by tests/test_capi_symbols.py)
+EXPORTED = ["nepx_create", "nepx_destroy", "nepx_last_error", "nepx_info", "nepx_compute",
+            "nepx_notify_box_changed", "nepx_set_skin", "nepx_neighbors", "nepx_neighbor_stats"]
+
+
+class NepxError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__("%s: %s" % (ERRORS.get(code, code), message))
+        self.code = code
+
+
+class Box(ctypes.Structure):
+    _fields_ = [("h", ctypes.c_double * 9), ("pbc", ctypes.c_int * 3)]
+
+
+_lib = None
+
+
+def build():
+    import subprocess
+    subprocess.run(["make", "-s", "-j8", "-C", HERE], check=True)
+
+
+def lib():
+    """Load lib/libnepx.so (raises if it is missing: no fallback path)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError("nepx engine library not built: %s (run make -C dmg-md_b200)" % LIB_PATH)
+        L = ctypes.CDLL(LIB_PATH)
+        vp, ip, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
+        L.nepx_create.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(vp)]
+        L.nepx_destroy.argtypes = [vp]
+        L.nepx_last_error.argtypes = [vp]
+        L.nepx_last_error.restype = ctypes.c_char_p
+        L.nepx_info.argtypes = [vp, ip, dp]
+        L.nepx_compute.argtypes = [vp, ctypes.POINTER(Box), ctypes.c_int, vp, vp, vp, vp, vp,
+                                   ctypes.c_uint, vp]
+        L.nepx_notify_box_changed.argtypes = [vp]
+        L.nepx_set_skin.argtypes = [vp, ctypes.c_double]
+        L.nepx_neighbors.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp, ctypes.c_int, vp]
+        L.nepx_neighbor_stats.argtypes = [vp, ip, ip, ip, vp]
+        for name in EXPORTED:
+            if name != "nepx_last_error":
+                getattr(L, name).restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def make_box(h, pbc=(1, 1, 1)):
+    b = Box()
+    flat = [float(v) for v in (h.reshape(-1).tolist() if hasattr(h, "reshape") else h)]
+    if len(flat) != 9:
+        raise ValueError("box needs 9 numbers")
+    for k in range(9):
+        b.h[k] = flat[k]
+    for k in range(3):
+        b.pbc[k] = int(pbc[k])
+    return b
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        import torch
+        stream = torch.cuda.current_stream()
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+class Potential:
+    """A NEP potential on the current CUDA device (one nepx handle)."""
+
+    def __init__(self, path, max_atoms):
+        self._h = ctypes.c_void_p()
+        rc = lib().nepx_create(os.fsencode(path), int(max_atoms), ctypes.byref(self._h))
+        if rc:
+            raise NepxError(rc, "nepx_create(%s) failed" % path)
+        info = (ctypes.c_int * 16)()
+        rcs = (ctypes.c_double * 32)()
+        lib().nepx_info(self._h, info, rcs)
+        keys = ["version", "num_types", "zbl", "zbl_flexible", "n_max_r", "n_max_a", "basis_r",
+                "basis_a", "L_max", "num_L", "dim", "H", "MN_r", "MN_a", "has_q", "typewise_zbl"]
+        self.info = dict(zip(keys, list(info)))
+        self.max_atoms = int(max_atoms)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().nepx_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc:
+            raise NepxError(rc, lib().nepx_last_error(self._h).decode())
+
+    def compute(self, types, h, pos, pbc=(1, 1, 1), out=None, accumulate=False, sync_check=False,
+                stream=None):
+        """Energy (n,), force (3, n), virial (9, n) as float64 CUDA tensors."""
+        import torch
+        n = types.numel()
+        if out is None:
+            pe = torch.empty(n, dtype=torch.float64, device=pos.device)
+            force = torch.empty(3, n, dtype=torch.float64, device=pos.device)
+            virial = torch.empty(9, n, dtype=torch.float64, device=pos.device)
+        else:
+            pe, force, virial = out
+        assert types.dtype == torch.int32 and pos.dtype == torch.float64
+        assert types.is_contiguous() and pos.is_contiguous()
+        flags = (NEPX_ACCUMULATE if accumulate else 0) | (NEPX_SYNC_CHECK if sync_check else 0)
+        box = make_box(h, pbc)
+        self._check(lib().nepx_compute(self._h, ctypes.byref(box), n, _ptr(types), _ptr(pos),
+                                       _ptr(pe), _ptr(force), _ptr(virial), flags,
+                                       _stream_ptr(stream)))
+        return pe, force, virial
+
+    def neighbors(self, which, n, stream=None):
+        """Rows of the last compute as a list of CPU numpy arrays (ascending)."""
+        import torch
+        mn = self.info["MN_r"] if which == 0 else self.info["MN_a"]
+        nn = torch.empty(n, dtype=torch.int32, device="cuda")
+        nl = torch.empty(n, mn, dtype=torch.int32, device="cuda")
+        self._check(lib().nepx_neighbors(self._h, which, n, _ptr(nn), _ptr(nl), mn,
+                                         _stream_ptr(stream)))
+        torch.cuda.synchronize()
+        nn = nn.cpu().numpy()
+        nl = nl.cpu().numpy()
+        return [nl[i, :nn[i]].copy() for i in range(n)]
+
+    def neighbor_stats(self, stream=None):
+        r, a, v = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(lib().nepx_neighbor_stats(self._h, ctypes.byref(r), ctypes.byref(a),
+                                              ctypes.byref(v), _stream_ptr(stream)))
+        return r.value, a.value, v.value
+
+    def notify_box_changed(self):
+        self._check(lib().nepx_notify_box_changed(self._h))

@@ -1,0 +1,115 @@
+/*
+ * nepx.h -- C ABI of the B200-native NEP molecular-dynamics engine.
+ *
+ * Plain pointers and sizes only.  Device pointers are CUDA device memory of
+ * the calling process's current device; `stream` is a cudaStream_t (NULL =
+ * legacy default stream).  Every function returns 0 (NEPX_OK) or a positive
+ * NEPX_ERR_* code; nepx_last_error() gives the message.  No function exits
+ * the process.
+ *
+ * Each entry point names the reference (DMG-MD, zhangfeifan21/DMG-MD)
+ * interface it replaces.  INTEGRATION.md shows the bindings a maintainer of
+ * the reference adds (a NepForce adapter in C++ and a ctypes stub).
+ */
+#ifndef NEPX_H
+#define NEPX_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NEPX_OK 0
+#define NEPX_ERR_ARG 1          /* bad argument (null pointer, n out of range, ...) */
+#define NEPX_ERR_FILE 2         /* potential file missing or malformed */
+#define NEPX_ERR_UNSUPPORTED 3  /* valid input outside what the engine implements */
+#define NEPX_ERR_CUDA 4         /* a CUDA call failed */
+#define NEPX_ERR_CAPACITY 5     /* n above the capacity the handle was created with */
+#define NEPX_ERR_OVERFLOW 6     /* a neighbour row exceeded MN (raise MN in nep.txt) */
+#define NEPX_ERR_NONFINITE 7    /* an energy or force came out NaN/Inf */
+#define NEPX_ERR_BOX 8          /* box too thin for the large-box path, or singular */
+
+/* compute flags */
+#define NEPX_ACCUMULATE 1u      /* add into pe/force/virial (the reference's += contract) */
+#define NEPX_SYNC_CHECK 2u      /* synchronise the stream and report device-side errors */
+
+typedef struct nepx_handle nepx_t;
+
+/* Periodic box: h is row-major 3x3 with the cell vectors a, b, c as COLUMNS,
+ * i.e. h = {ax, bx, cx, ay, by, cy, az, bz, cz} (the reference's
+ * Box::cpu_h[0..8], src/gpumd_compat/box.cuh:53-70); pbc[d] = 1 periodic. */
+typedef struct nepx_box {
+  double h[9];
+  int pbc[3];
+} nepx_box;
+
+/*
+ * Parse a GPUMD-format nep.txt (nep4, nep4_zbl, nep5, nep5_zbl) and size the
+ * per-atom scratch for up to max_atoms atoms.
+ * Replaces NEP::NEP(const char*, int) (src/gpumd_compat/nep.cu:135-385) and
+ * NEP::allocate_workspace (nep.cu:432-451).
+ */
+int nepx_create(const char* nep_path, int max_atoms, nepx_t** out);
+
+/* Frees the handle and its device memory.  Replaces NEP::~NEP (nep.cu:397). */
+int nepx_destroy(nepx_t* handle);
+
+/* Message of the last error of this handle (never NULL). */
+const char* nepx_last_error(const nepx_t* handle);
+
+/*
+ * Model metadata. info[16]: version, num_types, zbl, zbl_flexible, n_max_radial,
+ * n_max_angular, basis_radial, basis_angular, l_max, num_L, dim, H,
+ * MN_radial, MN_angular (both x1.25 like the reference), has_q bitmask
+ * (bit0 q_222 .. bit5 q_134), typewise_zbl.  rc[2*T]: rc_radial[t],
+ * rc_angular[t].  Replaces NEP::params() (nep.cuh:200-201).
+ */
+int nepx_info(const nepx_t* handle, int* info, double* rc);
+
+/*
+ * Per-atom energy, force and virial of n atoms in a periodic box.
+ *   d_type   n ints, 0-based in potential-file order
+ *   d_pos    3n doubles SoA (x[0..n), y[0..n), z[0..n)), Angstrom
+ *   d_pe     n doubles, eV
+ *   d_force  3n doubles SoA, eV/Angstrom
+ *   d_virial 9n doubles SoA, order xx yy zz xy xz yz yx zx zy, eV
+ * Outputs are overwritten unless flags has NEPX_ACCUMULATE (then added, the
+ * reference's += contract).  The call is asynchronous on `stream`; device
+ * errors (row overflow, non-finite output) surface at the next call or
+ * immediately with NEPX_SYNC_CHECK.
+ * Replaces Potential::compute (src/gpumd_compat/potential.cuh:82-88) as
+ * implemented by NEP::compute (nep.cu:2071-2100), large-box path
+ * (nep.cu:1120-1280).  Boxes thinner than 2.5 (rc + skin) in a periodic
+ * direction take the reference's small-box path (nep.cu:1844-2064).
+ */
+int nepx_compute(nepx_t* handle, const nepx_box* box, int n, const int* d_type,
+                 const double* d_pos, double* d_pe, double* d_force, double* d_virial,
+                 unsigned flags, void* stream);
+
+/* Forces a Verlet rebuild at the next compute.  Replaces
+ * NEP::notify_box_changed (src/gpumd_compat/nep.cuh:170). */
+int nepx_notify_box_changed(nepx_t* handle);
+
+/* Verlet skin in Angstrom (reference default 1.0, neighbor.cuh). */
+int nepx_set_skin(nepx_t* handle, double skin);
+
+/*
+ * Copies the typewise neighbour rows of the last compute (which = 0 radial,
+ * 1 angular) into device buffers: d_nn[n] counts, d_nl[n*mn] row-major, rows
+ * ascending.  Test and diagnostics hook; the reference exposes the same rows
+ * through NEP::get_NN_radial_ptr / get_NL_radial_ptr (nep.cuh:254-256) in
+ * ordinal-major layout.
+ */
+int nepx_neighbors(nepx_t* handle, int which, int n, int* d_nn, int* d_nl, int mn, void* stream);
+
+/*
+ * Largest row seen since the last call (radial, angular, Verlet) and device
+ * error bits; synchronises `stream`.  Replaces the neighbor.out occupancy
+ * record (nep.cu:1156-1176).
+ */
+int nepx_neighbor_stats(nepx_t* handle, int* max_radial, int* max_angular, int* max_verlet,
+                        void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,145 @@
+"""Seeded synthetic inputs: NEP potential files and periodic structures.
+
+Shared by the tests and bench.py.  Nothing here reads the reference tree; the
+shapes, sizes and value distributions are those of the benchmark configs:
+
+  * NEP files with weights N(0, std^2) in the GPUMD nep.txt format that both
+    the reference GPU loader (nep.cu:135-415) and its CPU evaluator
+    (nep_cpu.cpp:1957-2250) accept: a 5-token cutoff line and a 4-token
+    l_max line;
+  * diamond carbon, FCC copper with vacancies, liquid water boxes at a given
+    density, random-packed multi-species boxes, and Maxwell-Boltzmann
+    velocities.
+"""
+import math
+import os
+
+import numpy as np
+
+MASS = {"H": 1.008, "C": 12.011, "N": 14.007, "O": 15.999, "Cu": 63.546, "Si": 28.085,
+        "Ba": 137.327, "Ti": 47.867}
+K_B = 8.617343e-5
+
+
+def write_nep(path, version=4, symbols=("C",), zbl=None, rc=(4.2, 3.7), mn=(100, 60),
+              n_max=(4, 4), basis=(8, 8), l_max=(4, 2, 1), H=30, seed=0, std=0.1,
+              q_scaler=1.0):
+    """Write a synthetic NEP file; returns its path.
+
+    zbl: None, (rc_inner, rc_outer) or (rc_inner, rc_outer, factor).
+    """
+    T = len(symbols)
+    nR, nA = n_max[0] + 1, n_max[1] + 1
+    kR, kA = basis[0] + 1, basis[1] + 1
+    num_L = l_max[0] + (1 if l_max[1] else 0) + (1 if l_max[2] else 0)
+    dim = nR + nA * num_L
+    if version == 4:
+        num_ann = (dim + 2) * H * T + 1
+    else:
+        num_ann = ((dim + 2) * H + 1) * T + 1
+    num_desc = T * T * (nR * kR + nA * kA)
+    rng = np.random.default_rng(seed)
+    params = rng.normal(0.0, std, num_ann + num_desc)
+    tag = "nep%d%s" % (version, "_zbl" if zbl else "")
+    lines = ["%s %d %s" % (tag, T, " ".join(symbols))]
+    if zbl:
+        lines.append("zbl " + " ".join("%g" % v for v in zbl))
+    lines.append("cutoff %g %g %d %d" % (rc[0], rc[1], mn[0], mn[1]))
+    lines.append("n_max %d %d" % n_max)
+    lines.append("basis_size %d %d" % basis)
+    lines.append("l_max %d %d %d" % tuple(l_max))
+    lines.append("ANN %d 0" % H)
+    lines += ["%.8e" % v for v in params]
+    qs = np.full(dim, q_scaler) if np.isscalar(q_scaler) else np.asarray(q_scaler)
+    lines += ["%.8e" % v for v in qs]
+    os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+    return path
+
+
+def _cubic_h(L):
+    return np.array([L, 0, 0, 0, L, 0, 0, 0, L], dtype=np.float64)
+
+
+def diamond(a=3.567, ncell=8, jitter=0.05, seed=0):
+    """Diamond supercell: (types, h, pos (3, n))."""
+    base = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0],
+                     [.25, .25, .25], [.25, .75, .75], [.75, .25, .75], [.75, .75, .25]])
+    g = np.stack(np.meshgrid(*[np.arange(ncell)] * 3, indexing="ij"), -1).reshape(-1, 3)
+    frac = (g[:, None, :] + base[None, :, :]).reshape(-1, 3) / ncell
+    L = a * ncell
+    rng = np.random.default_rng(seed)
+    pos = frac * L + rng.normal(0.0, jitter, frac.shape)
+    return np.zeros(len(pos), dtype=np.int32), _cubic_h(L), np.ascontiguousarray(pos.T % L)
+
+
+def fcc(a=3.615, ncell=8, vacancy=0.0, jitter=0.0, seed=0):
+    base = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0]])
+    g = np.stack(np.meshgrid(*[np.arange(ncell)] * 3, indexing="ij"), -1).reshape(-1, 3)
+    frac = (g[:, None, :] + base[None, :, :]).reshape(-1, 3) / ncell
+    rng = np.random.default_rng(seed)
+    if vacancy > 0:
+        keep = rng.random(len(frac)) >= vacancy
+        frac = frac[keep]
+    L = a * ncell
+    pos = frac * L
+    if jitter:
+        pos = pos + rng.normal(0.0, jitter, pos.shape)
+    return np.zeros(len(pos), dtype=np.int32), _cubic_h(L), np.ascontiguousarray(pos.T % L)
+
+
+def water(n_mol=8000, density=1.0, seed=0, roh=0.96, angle=104.5):
+    """Liquid-water box (types O=0, H=1) at density g/cm^3, random orientations.
+
+    Molecules sit on a jittered cubic lattice so no two oxygens overlap.
+    """
+    amu_per_A3 = density * 0.60221408
+    L = (n_mol * 18.015 / amu_per_A3) ** (1.0 / 3.0)
+    m = int(math.ceil(n_mol ** (1.0 / 3.0)))
+    rng = np.random.default_rng(seed)
+    sites = np.stack(np.meshgrid(*[np.arange(m)] * 3, indexing="ij"), -1).reshape(-1, 3)
+    sites = sites[rng.permutation(len(sites))[:n_mol]]
+    spacing = L / m
+    O = (sites + 0.5) * spacing + rng.uniform(-0.15, 0.15, (n_mol, 3)) * spacing
+    th = math.radians(angle)
+    local = np.array([[roh, 0, 0], [roh * math.cos(th), roh * math.sin(th), 0]])
+    # random rotations from normalised quaternions
+    q = rng.normal(size=(n_mol, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    w, x, y, z = q.T
+    R = np.stack([
+        np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)], -1),
+        np.stack([2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)], -1),
+        np.stack([2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], -1)], 1)
+    Hs = O[:, None, :] + np.einsum("mij,kj->mki", R, local)
+    pos = np.concatenate([O[:, None, :], Hs], 1).reshape(-1, 3) % L
+    types = np.tile(np.array([0, 1, 1], dtype=np.int32), n_mol)
+    return types, _cubic_h(L), np.ascontiguousarray(pos.T)
+
+
+def random_packed(n, num_types, density=0.08, min_dist=0.9, seed=0):
+    """Random-packed box at `density` atoms/A^3 with a soft minimum distance."""
+    L = (n / density) ** (1.0 / 3.0)
+    rng = np.random.default_rng(seed)
+    m = int(math.ceil(n ** (1.0 / 3.0)))
+    sites = np.stack(np.meshgrid(*[np.arange(m)] * 3, indexing="ij"), -1).reshape(-1, 3)
+    sites = sites[rng.permutation(len(sites))[:n]]
+    sp = L / m
+    pos = (sites + 0.5) * sp + rng.uniform(-0.25, 0.25, (n, 3)) * max(sp - min_dist, 0.0)
+    types = rng.integers(0, num_types, n).astype(np.int32)
+    return types, _cubic_h(L), np.ascontiguousarray((pos % L).T)
+
+
+def maxwell_boltzmann(masses, T, seed=0):
+    """Velocities (3, n) in A/fs with zero total momentum, scaled to T exactly."""
+    rng = np.random.default_rng(seed)
+    masses = np.asarray(masses, dtype=np.float64)
+    # natural units: v in A / (natural time); 1 natural time = 10.18051 fs
+    sigma = np.sqrt(K_B * T / masses)
+    v = rng.normal(size=(3, len(masses))) * sigma
+    p = (v * masses).sum(axis=1) / masses.sum()
+    v -= p[:, None]
+    ek = 0.5 * (masses * (v * v).sum(axis=0)).sum()
+    v *= math.sqrt(1.5 * len(masses) * K_B * T / ek)
+    return v / 10.18051
