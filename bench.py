@@ -1,0 +1,360 @@
+#!/usr/bin/env python3
+"""Benchmark of the nepx NEP molecular-dynamics engine on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload water|carbon|copper]
+
+Default workload (the headline config): liquid water, 8000 molecules = 24,000
+atoms at 1.0 g/cm^3, synthetic two-type NEP4 (O/H, rc 6.0/4.0 A, n_max 4/4,
+basis 8/8, l_max 4 2 0, 50 hidden units, weights N(0, 0.1^2), seeded),
+Bussi NVT (nvt_bdp) at 300 K, dt 0.5 fs.  One "step" is one full MD step:
+neighbour update, NEP energy/force/virial, FP64 velocity Verlet, thermo
+reduction and thermostat.  Metric: atom-steps/s, whole job (sum over ranks).
+
+value  -- device time (CUDA events on the MD stream) of K steps queued in
+          chunks of `--chunk` steps, each chunk preceded by a 512 MiB write
+          that flushes the 126 MB L2; max over ranks.
+e2e    -- the same K steps driven through the public C API one step per call
+          (nepx_md_run: host draws H2D, graph launch, thermo row D2H,
+          synchronisation), host wall clock.
+roofline -- the dominant kernel (fused descriptor/ANN/angular-force kernel),
+          its FP32 work per launch (the operation count of the algorithm it
+          runs, see flops_per_atom) over its CUDA-event time, against the FP32
+          FMA peak of B200 (148 SMs x 128 lanes x 2 FLOP x max SM clock).
+cpu_baseline -- the reference's own FP64 CPU NEP evaluator (NEP3_CPU,
+          oracle/_ref) over the full system on all host cores, force call.
+
+--impl reference times that same reference CPU evaluator alone (rank 0).
+Multi-GPU: one independent replica per GPU (the reference's one-rank path
+does not shard; replicas only), no collective on the data path.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "dmg-md_b200"))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+import numpy as np  # noqa: E402
+
+import workloads  # noqa: E402
+
+K_B = 8.617343e-5
+FP32_LANES = 148 * 128          # B200: SMs x FP32 lanes
+SM_MAX_MHZ = 1965.0
+
+WORKLOADS = {
+    # name: (builder, nep kwargs, ensemble kwargs, dt_fs)
+    "water": dict(
+        nep=dict(version=4, symbols=("O", "H"), rc=(6.0, 4.0), mn=(150, 60), n_max=(4, 4),
+                 basis=(8, 8), l_max=(4, 2, 0), H=50, seed=2024, std=0.1),
+        ens=dict(kind="nvt_bdp", T0=300.0, Tdamp=100.0), dt=0.5, T=300.0,
+        desc="water_8000mol_24000atoms_nep4_O-H_rc6.0-4.0_H50_nvt_bdp_300K_dt0.5fs"),
+    "carbon": dict(
+        nep=dict(version=4, symbols=("C",), rc=(4.2, 3.7), mn=(100, 60), n_max=(4, 4),
+                 basis=(8, 8), l_max=(4, 2, 1), H=30, seed=2025, std=0.1),
+        ens=dict(kind="nve"), dt=1.0, T=300.0,
+        desc="diamond_8x8x8_4096atoms_nep4_C_rc4.2-3.7_H30_nve_dt1fs"),
+    "copper": dict(
+        nep=dict(version=4, symbols=("Cu",), zbl=(1.0, 2.0), rc=(5.0, 4.0), mn=(100, 60),
+                 n_max=(4, 4), basis=(8, 8), l_max=(4, 2, 1), H=40, seed=2026, std=0.1),
+        ens=dict(kind="npt_ber", T0=300.0, Tdamp=100.0, p_gpa=0.0, bulk_gpa=140.0,
+                 tau_p=1000.0), dt=1.0, T=300.0,
+        desc="cu_fcc_63x63x63_1pct_vacancies_nepzbl_rc5.0-4.0_H40_npt_ber_dt1fs"),
+}
+
+MASSES = {"O": 15.999, "H": 1.008, "C": 12.011, "Cu": 63.546}
+
+
+def build_system(name, seed):
+    if name == "water":
+        t, h, p = workloads.water(n_mol=8000, seed=seed)
+    elif name == "carbon":
+        t, h, p = workloads.diamond(a=3.567, ncell=8, jitter=0.05, seed=seed)
+    else:
+        t, h, p = workloads.fcc(a=3.615, ncell=63, vacancy=0.01, seed=seed)
+    return t, h, p
+
+
+def flops_per_atom(info, nr, na):
+    """FP32 operations per atom of the fused descriptor/ANN/angular-force kernel.
+
+    Counts the algorithm the kernel runs (FMA = 2): per radial edge geometry
+    (~20), cutoff (~12), Chebyshev basis (4 kR) and the type-pair contraction
+    (2 nR kR); per angular edge the same with kA, nA plus harmonics (~3 nlm)
+    and the moment update (2 nA nlm); per center invariants, the ANN forward
+    and backward (4 dim H + 12 H) and the moment derivatives (4 nA nlm); per
+    angular edge of the force sweep geometry, cutoff and basis with
+    derivatives (8 kA), g and g' (4 nA kA), the A/B coefficients (4 nA nlm)
+    and the harmonic-gradient walk (~10 nlm).
+    """
+    nR, nA = info["n_max_r"] + 1, info["n_max_a"] + 1
+    kR, kA = info["basis_r"] + 1, info["basis_a"] + 1
+    nlm = (info["L_max"] + 1) ** 2 - 1
+    dim, H = info["dim"], info["H"]
+    radial = nr * (20 + 12 + 4 * kR + 2 * nR * kR)
+    angular_desc = na * (20 + 12 + 4 * kA + 2 * nA * kA + 3 * nlm + 2 * nA * nlm)
+    center = nA * (3 * nlm + 60) + 4 * dim * H + 12 * H + 4 * nA * nlm
+    angular_force = na * (20 + 14 + 8 * kA + 4 * nA * kA + 4 * nA * nlm + 10 * nlm + 10)
+    return radial + angular_desc + center + angular_force
+
+
+class ClockSampler:
+    """nvidia-smi SM clock / throttle-reason sampling during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu_id), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "50"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = float(parts[1])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[4:8]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_rate(nep_path, t, h, p, budget_s=8.0, max_reps=5):
+    """The reference's NEP3_CPU over all atoms on all host cores: atom-steps/s."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    if not oracle.ref_cpu_available():
+        return None
+    threads = os.cpu_count() or 1
+    ref = oracle.RefCpuModel(nep_path)
+    ref.compute(t, h, p, threads=threads)           # warm (thread pool, pages)
+    times = []
+    t_end = time.perf_counter() + budget_s
+    while len(times) < max_reps and time.perf_counter() < t_end:
+        t0 = time.perf_counter()
+        ref.compute(t, h, p, threads=threads)
+        times.append(time.perf_counter() - t0)
+    sec = statistics.median(times)
+    return {"value": len(t) / sec, "unit": "atom-steps/s", "cores": threads, "kind": "reference",
+            "sample": "NEP3_CPU (reference FP64 CPU evaluator) force call on all %d atoms, "
+                      "median of %d calls, %d threads" % (len(t), len(times), threads)}
+
+
+def run_reference_arm(args, rank):
+    if rank != 0:
+        return 0
+    spec = WORKLOADS[args.workload]
+    with tempfile.TemporaryDirectory() as tmp:
+        path = workloads.write_nep(os.path.join(tmp, "nep.txt"), **spec["nep"])
+        t, h, p = build_system(args.workload, seed=1)
+        base = cpu_reference_rate(path, t, h, p, budget_s=max(4.0, 0.5 * args.steps))
+    if base is None:
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "reference NEP3_CPU library oracle/_ref not built"}))
+        return 0
+    line = {"impl": "reference", "metric": "atom-steps/s", "value": base["value"],
+            "unit": "atom-steps/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * len(t) / base["value"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
+            "data": "synthetic", "config": {"workload": spec["desc"], "atoms": len(t)},
+            "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": "atom-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="water", choices=sorted(WORKLOADS))
+    ap.add_argument("--chunk", type=int, default=10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference_arm(args, rank)
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    import nepx
+
+    spec = WORKLOADS[args.workload]
+    tmp = tempfile.mkdtemp()
+    path = workloads.write_nep(os.path.join(tmp, "nep.txt"), **spec["nep"])
+    t, h, p = build_system(args.workload, seed=1 + rank)
+    n = len(t)
+    syms = spec["nep"]["symbols"]
+    masses = np.array([MASSES[syms[k]] for k in t])
+    v = workloads.maxwell_boltzmann(masses, spec["T"], seed=7 + rank)
+    pot = nepx.Potential(path, max_atoms=n)
+    md = nepx.MD(pot, t, masses, p, v, h)
+    ens = dict(spec["ens"])
+    kind = ens.pop("kind")
+    md.set_ensemble(kind, seed=12345678 + rank, **ens)
+    dt = spec["dt"]
+    md.run(args.warmup, dt)
+
+    d_pos, d_vel, d_force, d_type, stream_ptr = md.device_state()
+    stream = torch.cuda.ExternalStream(stream_ptr)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    K, chunk = args.steps, max(1, min(args.chunk, args.steps))
+    chunks = [chunk] * (K // chunk) + ([K % chunk] if K % chunk else [])
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in chunks]
+    props = torch.cuda.get_device_properties(local)
+    gpu_id = getattr(props, "uuid", None)
+    gpu_id = ("GPU-" + str(gpu_id)) if gpu_id is not None else local
+    clocks = ClockSampler(gpu_id)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.2)
+    for c, steps in enumerate(chunks):
+        with torch.cuda.stream(stream):
+            flush.fill_(c & 0xFF)
+        ev[c][0].record(stream)
+        md.run_async(steps, dt)
+        ev[c][1].record(stream)
+    md.sync()
+    torch.cuda.synchronize()
+    clock_info = clocks.stop()
+    if dist:
+        dist.barrier()
+    dev_ms = sum(a.elapsed_time(b) for a, b in ev)
+    atoms_total = n * world
+    if dist:
+        tt = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        dev_ms = float(tt.item())
+    value = atoms_total * K / (dev_ms / 1e3)
+    kernels_per_step = 13 + (2 if kind == "nvt_nhc" else 0)
+    launches = K * kernels_per_step + len(chunks)
+
+    # end to end through the public API: one nepx_md_run per step
+    rows = np.zeros((1, len(nepx.THERMO_COLUMNS)))
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(K):
+        rows = md.run(1, dt, thermo_every=1)
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        tt = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    e2e = {"value": atoms_total * K / e2e_s, "unit": "atom-steps/s",
+           "h2d_bytes_per_step": 3 * 8,           # the step's stochastic draws
+           "d2h_bytes_per_step": 20 * 8 + 4 + 232 + 56,   # thermo row, status, box, flags
+           "api": "nepx_md_run(steps=1, thermo_every=1) per step"}
+
+    # per-kernel profile of the force path on the final state
+    st = md.state()
+    tt_ = torch.as_tensor(np.asarray(t, dtype=np.int32), device="cuda")
+    pp_ = torch.as_tensor(np.ascontiguousarray(st["pos"]), device="cuda")
+    prof = pot.profile(tt_, st["h"], pp_, reps=50)
+    nr, na, nv = pot.neighbor_stats()
+    # mean neighbour counts of the final state
+    rr = pot.neighbors(0, n)
+    ra = pot.neighbors(1, n)
+    mean_r = float(np.mean([len(x) for x in rr]))
+    mean_a = float(np.mean([len(x) for x in ra]))
+    fpa = flops_per_atom(pot.info, mean_r, mean_a)
+    desc_flops = fpa * n
+    achieved = desc_flops / (prof["descriptor"] * 1e-3) / 1e12
+    peak = FP32_LANES * 2 * SM_MAX_MHZ * 1e6 / 1e12
+    roofline = {"bound": "fp32", "kernel": "k_descriptor_ann_f12",
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": None,
+                "peak_source": "B200 FP32 FMA peak: 148 SMs x 128 lanes x 2 FLOP x 1965 MHz "
+                               "(not in MEASURED_PEAKS.json, which holds HBM and bf16 only)",
+                "flops_per_atom": fpa, "mean_radial_neighbors": mean_r,
+                "mean_angular_neighbors": mean_a,
+                "stage_ms": prof}
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            cpu = cpu_reference_rate(path, t, h, p)
+        T_last = float(rows[-1, 0]) if rows is not None else None
+        line = {"metric": "atom-steps/s", "value": value, "unit": "atom-steps/s",
+                "n_gpus": world, "steps": K, "warmup": args.warmup,
+                "ms_per_step": dev_ms / K, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "fp32 (descriptors, ANN, forces) + fp64 "
+                                              "(integration, thermo reductions)",
+                "data": "synthetic (seeded structure, velocities and NEP weights)",
+                "config": {"workload": spec["desc"], "atoms_per_gpu": n, "ensemble": kind,
+                           "dt_fs": dt, "parallelism": "replicas x%d" % world,
+                           "l2": "flushed by a 512 MiB write before every %d-step chunk" % chunk,
+                           "final_temperature_K": T_last},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": launches, "clocks": clock_info}
+        print(json.dumps(line))
+    md.close()
+    pot.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -7,13 +7,7 @@
 #include "../../include/nepx.h"
 #include "engine.h"
 
-struct nepx_handle {
-  nepx::Engine engine;
-  nepx::NeighborState* h_state = nullptr;   // pinned mirror of the device flags
-  cudaEvent_t state_ready = nullptr;
-  bool state_pending = false;
-  std::string error;
-};
+#include "handle.h"
 
 namespace {
 
@@ -50,20 +44,6 @@ int check_state(nepx_handle* h, bool wait)
   }
   if (s.nonfinite) return fail(h, NEPX_ERR_NONFINITE, "non-finite energy or force");
   return NEPX_OK;
-}
-
-bool large_box_ok(const nepx::Engine& e, const nepx::Box& b)
-{
-  // small-box criterion of the reference (nep.cu:2002-2030): a periodic
-  // thickness <= 2.5 (rc + 1)
-  const double rc = e.model.rc_max;
-  for (int d = 0; d < 3; ++d) {
-    if (!b.pbc[d]) continue;
-    const double* r = b.hinv + 3 * d;
-    const double thick = 1.0 / std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
-    if (thick <= 2.5 * (rc + e.skin)) return false;
-  }
-  return true;
 }
 
 }  // namespace
@@ -151,13 +131,14 @@ int nepx_compute(nepx_t* h, const nepx_box* box, int n, const int* d_type, const
   nepx::Box b;
   std::string err = nepx::make_box(box->h, box->pbc, b);
   if (!err.empty()) return fail(h, NEPX_ERR_BOX, err);
-  if (!large_box_ok(e, b))
+  if (!nepx::large_box_ok(e, b))
     return fail(h, NEPX_ERR_BOX,
                 "box thinner than 2.5 (rc + skin) in a periodic direction (small-box path)");
   const bool changed = !e.have_box || std::memcmp(&b, &e.last_box, sizeof(nepx::Box)) != 0;
   const bool rebuild = e.force_rebuild || changed || n != e.last_n;
   auto s = static_cast<cudaStream_t>(stream);
   nepx::launch_set_box(e, b, s);
+  e.box_owner = nullptr;
   nepx::launch_neighbor_update(e, n, d_pos, d_type, rebuild, s);
   nepx::launch_force(e, n, d_pos, d_type, d_pe, d_force, d_virial,
                      (flags & NEPX_ACCUMULATE) != 0, s);
@@ -175,6 +156,42 @@ int nepx_compute(nepx_t* h, const nepx_box* box, int n, const int* d_type, const
     if (cudaStreamSynchronize(s) != cudaSuccess) return cuda_fail(h, "stream sync");
   }
   return NEPX_OK;
+}
+
+int nepx_profile(nepx_t* h, const nepx_box* box, int n, const int* d_type, const double* d_pos,
+                 double* d_pe, double* d_force, double* d_virial, int reps, double* ms,
+                 void* stream)
+{
+  if (!h || !ms || reps < 1) return NEPX_ERR_ARG;
+  nepx::Engine& e = h->engine;
+  // first call settles the lists (and validates the arguments)
+  int rc = nepx_compute(h, box, n, d_type, d_pos, d_pe, d_force, d_virial, NEPX_SYNC_CHECK, stream);
+  if (rc) return rc;
+  auto s = static_cast<cudaStream_t>(stream);
+  cudaEvent_t ev[5];
+  for (auto& x : ev) cudaEventCreate(&x);
+  double acc[4] = {0, 0, 0, 0};
+  for (int r = 0; r < reps; ++r) {
+    cudaEventRecord(ev[0], s);
+    nepx::launch_neighbor_update(e, n, d_pos, d_type, false, s);
+    cudaEventRecord(ev[1], s);
+    nepx::launch_descriptor(e, n, d_pos, d_type, s);
+    cudaEventRecord(ev[2], s);
+    nepx::launch_gather(e, n, d_pos, d_type, d_pe, d_force, d_virial, false, s);
+    cudaEventRecord(ev[3], s);
+    cudaEventSynchronize(ev[3]);
+    float t;
+    for (int k = 0; k < 3; ++k) {
+      cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+      acc[k] += t;
+    }
+    cudaEventElapsedTime(&t, ev[0], ev[3]);
+    acc[3] += t;
+  }
+  for (auto& x : ev) cudaEventDestroy(x);
+  for (int k = 0; k < 4; ++k) ms[k] = acc[k] / reps;
+  if (cudaPeekAtLastError() != cudaSuccess) return cuda_fail(h, "profile");
+  return check_state(h, true);
 }
 
 int nepx_notify_box_changed(nepx_t* h)

@@ -39,6 +39,7 @@ struct NeighborState {
   int ncell;
   int max_nn[3];       // largest Verlet / radial / angular row of the last build
   int nonfinite;       // a force or energy came out NaN/Inf
+  double box_scale;    // product of isotropic box factors since the last build (1 = none)
 };
 
 // Minimum image of a float displacement, the arithmetic of the large-box

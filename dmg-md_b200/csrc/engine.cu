@@ -49,6 +49,20 @@ std::string make_box(const double* h, const int* pbc, Box& b)
   return "";
 }
 
+bool large_box_ok(const Engine& e, const Box& b)
+{
+  // small-box criterion of the reference (nep.cu:2002-2030): a periodic
+  // thickness <= 2.5 (rc + 1) takes the image-expansion path
+  const double rc = e.model.rc_max;
+  for (int d = 0; d < 3; ++d) {
+    if (!b.pbc[d]) continue;
+    const double* r = b.hinv + 3 * d;
+    const double thick = 1.0 / std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    if (thick <= 2.5 * (rc + e.skin)) return false;
+  }
+  return true;
+}
+
 void launch_set_box(Engine& e, const Box& b, cudaStream_t stream)
 {
   k_set_box<<<1, 1, 0, stream>>>(e.d_box, b);
@@ -149,7 +163,10 @@ std::string engine_create(Engine& e, const std::string& nep_path, int max_atoms)
   ok &= dalloc(e.d_box, 1) == cudaSuccess;
   ok &= dalloc(e.d_nstate, 1) == cudaSuccess;
   if (!ok) return "cudaMalloc failed (per-atom buffers)";
-  if (cudaMemset(e.d_nstate, 0, sizeof(NeighborState)) != cudaSuccess) return "cudaMemset failed";
+  NeighborState init{};
+  init.box_scale = 1.0;
+  if (cudaMemcpy(e.d_nstate, &init, sizeof(init), cudaMemcpyHostToDevice) != cudaSuccess)
+    return "cudaMemcpy failed (neighbour state)";
   if (cudaMemset(nb.nn_a, 0, sizeof(int) * N) != cudaSuccess) return "cudaMemset failed";
   e.smem_desc = descriptor_smem_bytes(p);
   if (e.smem_desc > 227 * 1024) return "descriptor kernel needs more shared memory than a CTA has";

@@ -51,6 +51,7 @@ struct Engine {
   Box last_box{};
   bool have_box = false;
   bool force_rebuild = true;
+  const void* box_owner = nullptr;   // md whose box the device copy holds (nullptr: none)
   int last_n = -1;
   size_t smem_desc = 0;      // dynamic shared memory of the descriptor kernel
   std::string error;
@@ -63,6 +64,9 @@ void engine_destroy(Engine& e);
 // Host-side box: fills hinv, the float copy and the orthogonality flag.
 std::string make_box(const double* h, const int* pbc, Box& b);
 
+// True when the box is thick enough for the Verlet-list (large-box) path.
+bool large_box_ok(const Engine& e, const Box& b);
+
 // Writes the box to the device copy in stream order.
 void launch_set_box(Engine& e, const Box& b, cudaStream_t stream);
 
@@ -74,5 +78,8 @@ void launch_neighbor_update(Engine& e, int N, const double* pos, const int* type
 // accumulate = add into pe/force/virial instead of overwriting them.
 void launch_force(Engine& e, int N, const double* pos, const int* type, double* pe,
                   double* force, double* virial, bool accumulate, cudaStream_t stream);
+void launch_descriptor(Engine& e, int N, const double* pos, const int* type, cudaStream_t stream);
+void launch_gather(Engine& e, int N, const double* pos, const int* type, double* pe,
+                   double* force, double* virial, bool accumulate, cudaStream_t stream);
 
 }  // namespace nepx

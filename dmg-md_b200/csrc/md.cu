@@ -1,0 +1,697 @@
+// md.cu -- device-resident molecular dynamics: velocity Verlet in FP64 with
+// the reference's ensembles (NVE, Berendsen / Nose-Hoover chain / Bussi
+// NVT, isotropic Berendsen and stochastic-cell-rescaling NPT).
+//
+// Step order of the reference's single-rank loop (src/runtime.cu:747-848):
+//   [NHC: scale v by the pre-force chain factor]
+//   half kick + drift + wrap -> NEP force -> half kick -> thermo reduction
+//   -> thermostat velocity factor -> barostat box factor -> scale v (and x, box)
+// Every stage is a kernel on one stream; the thermostat / barostat scalars
+// are computed on the device from the FP64 thermo sums, with the stochastic
+// draws generated ahead on the host from the reference's random stream
+// (svr_rng.h).  A step therefore never synchronises with the host, and a run
+// is a CUDA graph of captured steps replayed back to back.
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/nepx.h"
+#include "handle.h"
+#include "md.h"
+
+struct MdMirror {
+  nepx::Box box;
+  int status;
+  nepx::NeighborState nstate;
+};
+
+struct nepx_md {
+  nepx::Md md;
+  MdMirror* mirror = nullptr;   // pinned host copy of the device status
+  nepx_handle* pot = nullptr;
+  double* h_noise = nullptr;   // pinned staging of the stochastic draws
+  cudaEvent_t noise_copied = nullptr;
+  bool own_stream = false;
+  std::string error;
+};
+
+namespace nepx {
+
+void launch_force(Engine& e, int N, const double* pos, const int* type, double* pe,
+                  double* force, double* virial, bool accumulate, cudaStream_t stream);
+
+namespace {
+
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ double box_volume(const Box& b)
+{
+  return fabs(b.h[0] * (b.h[4] * b.h[8] - b.h[5] * b.h[7]) +
+              b.h[1] * (b.h[5] * b.h[6] - b.h[3] * b.h[8]) +
+              b.h[2] * (b.h[3] * b.h[7] - b.h[4] * b.h[6]));
+}
+
+// block sum of 8 doubles per thread into partials[blockIdx.x * 8 + q]
+__device__ __forceinline__ void block_reduce8(double* v, double* partials)
+{
+  __shared__ double s[kThreads / 32][8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < 8; ++q)
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], off);
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < 8; ++q) s[warp][q] = v[q];
+  __syncthreads();
+  if (threadIdx.x < 8) {
+    double acc = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) acc += s[w][threadIdx.x];
+    partials[blockIdx.x * 8 + threadIdx.x] = acc;
+  }
+}
+
+// Pre-force kinetic sum (NHC only): partials[b*8 + 0] = sum m v^2.
+__global__ void k_ke_partials(int N, const double* __restrict__ mass,
+                              const double* __restrict__ vel, double* partials)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (i < N) {
+    const double vx = vel[i], vy = vel[N + i], vz = vel[2 * N + i];
+    v[0] = mass[i] * (vx * vx + vy * vy + vz * vz);
+  }
+  block_reduce8(v, partials);
+}
+
+// Nose-Hoover chain half step (Martyna-Tuckerman-Klein; Suzuki-Yoshida order
+// 7 x 4 RESPA substeps), the integrator of thermostat_nhc.cpp:47-116.
+__device__ double nhc_half_step(MdScalars& sc, double ek2, double kT, double dN, double dt_half)
+{
+  const double w[7] = {0.784513610477560,  0.235573213359357, -1.17767998417887,
+                       1.31518632068391,  -1.17767998417887,  0.235573213359357,
+                       0.784513610477560};
+  const int M = kChain;
+  double factor = 1.0;
+  for (int a = 0; a < 7; ++a) {
+    const double dt2 = dt_half * w[a] / 4;
+    const double dt4 = dt2 * 0.5;
+    const double dt8 = dt4 * 0.5;
+    for (int b = 0; b < 4; ++b) {
+      double G = sc.nhc_mom[M - 2] * sc.nhc_mom[M - 2] / sc.nhc_mass[M - 2] - kT;
+      sc.nhc_mom[M - 1] += dt4 * G;
+      for (int m = M - 2; m >= 0; --m) {
+        const double t = exp(-dt8 * sc.nhc_mom[m + 1] / sc.nhc_mass[m + 1]);
+        G = m == 0 ? ek2 - dN * kT
+                   : sc.nhc_mom[m - 1] * sc.nhc_mom[m - 1] / sc.nhc_mass[m - 1] - kT;
+        sc.nhc_mom[m] = t * (t * sc.nhc_mom[m] + dt4 * G);
+      }
+      for (int m = M - 1; m >= 0; --m) sc.nhc_pos[m] += dt2 * sc.nhc_mom[m] / sc.nhc_mass[m];
+      const double f = exp(-dt2 * sc.nhc_mom[0] / sc.nhc_mass[0]);
+      ek2 *= f * f;
+      factor *= f;
+      for (int m = 0; m < M - 1; ++m) {
+        const double t = exp(-dt8 * sc.nhc_mom[m + 1] / sc.nhc_mass[m + 1]);
+        G = m == 0 ? ek2 - dN * kT
+                   : sc.nhc_mom[m - 1] * sc.nhc_mom[m - 1] / sc.nhc_mass[m - 1] - kT;
+        sc.nhc_mom[m] = t * (t * sc.nhc_mom[m] + dt4 * G);
+      }
+      G = sc.nhc_mom[M - 2] * sc.nhc_mom[M - 2] / sc.nhc_mass[M - 2] - kT;
+      sc.nhc_mom[M - 1] += dt4 * G;
+    }
+  }
+  return factor;
+}
+
+__device__ __forceinline__ double target_temperature(const StepParams& p, long long step)
+{
+  const double fraction = static_cast<double>(step) / static_cast<double>(p.steps);
+  return p.T0 + (p.T1 - p.T0) * fraction;
+}
+
+__global__ void k_nhc_pre(StepParams p, MdScalars* sc, const double* __restrict__ partials,
+                          int nblocks)
+{
+  double ek2 = 0.0;
+  for (int b = 0; b < nblocks; ++b) ek2 += partials[b * 8];
+  const double kT = kBoltzmann * target_temperature(p, sc->step);
+  // before_force hands over the kinetic energy (ek2/2) and doubles it again
+  // (ensemble_control.cpp:186-198)
+  sc->vfactor_pre = nhc_half_step(*sc, ek2 * 0.5 * 2.0, kT, 3.0 * p.N, p.dt * 0.5);
+}
+
+// v = v * f_pre + F/m dt/2 ; x += v dt ; wrap into the cell
+// (runtime.cu:392-421, runtime_internal.hpp:648-681)
+__global__ void k_vv1(StepParams p, const Box* __restrict__ box, const double* __restrict__ mass,
+                      const double* __restrict__ force, double* pos, double* vel,
+                      const MdScalars* __restrict__ sc)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.N) return;
+  const int N = p.N;
+  const double f = sc->vfactor_pre;
+  const double half = p.dt * 0.5;
+  const double im = 1.0 / mass[i];
+  double r[3];
+  for (int d = 0; d < 3; ++d) {
+    const double v = vel[d * N + i] * f + force[d * N + i] * im * half;
+    vel[d * N + i] = v;
+    r[d] = pos[d * N + i] + v * p.dt;
+  }
+  const Box& b = *box;
+  double s[3];
+  for (int d = 0; d < 3; ++d) {
+    s[d] = b.hinv[3 * d] * r[0] + b.hinv[3 * d + 1] * r[1] + b.hinv[3 * d + 2] * r[2];
+    if (b.pbc[d] == 1) {
+      if (s[d] < 0.0) s[d] += 1.0;
+      else if (s[d] > 1.0) s[d] -= 1.0;
+    }
+  }
+  for (int d = 0; d < 3; ++d)
+    pos[d * N + i] = b.h[3 * d] * s[0] + b.h[3 * d + 1] * s[1] + b.h[3 * d + 2] * s[2];
+}
+
+// second half kick and the FP64 thermo partial sums (runtime.cu:442-493)
+__global__ void k_vv2_thermo(StepParams p, const double* __restrict__ mass,
+                             const double* __restrict__ force, double* vel,
+                             const double* __restrict__ pe, const double* __restrict__ virial,
+                             double* partials)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int N = p.N;
+  double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (i < N) {
+    const double half = p.dt * 0.5;
+    const double m = mass[i];
+    const double im = 1.0 / m;
+    double vv[3];
+    for (int d = 0; d < 3; ++d) {
+      vv[d] = vel[d * N + i] + force[d * N + i] * im * half;
+      vel[d * N + i] = vv[d];
+    }
+    v[0] = m * (vv[0] * vv[0] + vv[1] * vv[1] + vv[2] * vv[2]);
+    v[1] = pe[i];
+    v[2] = virial[i] + m * vv[0] * vv[0];
+    v[3] = virial[N + i] + m * vv[1] * vv[1];
+    v[4] = virial[2 * N + i] + m * vv[2] * vv[2];
+    v[5] = virial[3 * N + i] + m * vv[0] * vv[1];
+    v[6] = virial[4 * N + i] + m * vv[0] * vv[2];
+    v[7] = virial[5 * N + i] + m * vv[1] * vv[2];
+  }
+  block_reduce8(v, partials);
+}
+
+// Thermo normalisation, thermostat and barostat scalars, box update and the
+// thermo row of this step (ensemble_control.cpp:180-306, npt_scr.cpp:21-33,
+// box_control.cpp:9-68).  One block: 8 threads reduce the partials in a
+// fixed order, thread 0 does the scalar work.
+__global__ void k_ensemble(StepParams p, Box* box, MdScalars* sc, const double* __restrict__ partials,
+                           int nblocks, const double* __restrict__ noise, double* rows,
+                           int rows_cap, NeighborState* nstate, int* status)
+{
+  __shared__ double s_sum[8];
+  if (threadIdx.x < 8) {
+    double acc = 0.0;
+    for (int b = 0; b < nblocks; ++b) acc += partials[b * 8 + threadIdx.x];
+    s_sum[threadIdx.x] = acc;
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  const long long step = sc->step;
+  Box& b = *box;
+  const double V = box_volume(b);
+  double th[8];
+  th[0] = s_sum[0] / (3.0 * p.N * kBoltzmann);
+  th[1] = s_sum[1];
+  for (int q = 2; q < 8; ++q) th[q] = s_sum[q] / V;
+  for (int q = 0; q < 8; ++q) sc->thermo[q] = th[q];
+  const double Tt = target_temperature(p, step);
+  double vf = 1.0, bf = 1.0;
+  const double* nz = noise + 3 * step;
+  switch (p.kind) {
+    case kNvtBer:
+    case kNptBer: {
+      const double coupling = 1.0 / p.Tdamp;
+      if (coupling > 1.0e-5) vf = sqrt(1.0 + coupling * (Tt / th[0] - 1.0));
+      break;
+    }
+    case kNvtNhc: {
+      const double ek2 = th[0] * (3.0 * p.N * kBoltzmann);
+      vf = nhc_half_step(*sc, ek2, kBoltzmann * Tt, 3.0 * p.N, p.dt * 0.5);
+      break;
+    }
+    case kNvtBdp:
+    case kNptScr: {
+      const int ndeg = 3 * p.N;
+      const double old_ke = th[0] * ndeg * kBoltzmann * 0.5;
+      const double sigma = ndeg * kBoltzmann * Tt * 0.5;
+      const double new_ke = resample_kinetic(old_ke, sigma, ndeg, p.bdp_factor, nz[0], nz[1]);
+      vf = sqrt(new_ke / old_ke);
+      break;
+    }
+    default:
+      break;
+  }
+  if (p.kind == kNptBer || p.kind == kNptScr) {
+    const double p_inst = (th[2] + th[3] + th[4]) * 0.3333333333333333;
+    bf = 1.0 - p.pc * (p.p_target - p_inst);
+    if (p.kind == kNptScr)
+      bf += sqrt(0.666666666666667 * p.pc * kBoltzmann * Tt / V) * nz[2];
+    if (!(bf > 0.0) || !isfinite(bf)) {
+      *status |= 2;
+      bf = 1.0;
+    } else if (bf != 1.0) {
+      b.h[0] *= bf;
+      b.h[4] *= bf;
+      b.h[8] *= bf;
+      const double det = b.h[0] * b.h[4] * b.h[8];
+      b.hinv[0] = b.h[4] * b.h[8] / det;
+      b.hinv[4] = b.h[0] * b.h[8] / det;
+      b.hinv[8] = b.h[0] * b.h[4] / det;
+      for (int k = 0; k < 9; ++k) {
+        b.fh[k] = static_cast<float>(b.h[k]);
+        b.fh[9 + k] = static_cast<float>(b.hinv[k]);
+      }
+      nstate->box_scale *= bf;
+    }
+  }
+  if (!(vf > 0.0) || !isfinite(vf)) {
+    *status |= 1;
+    vf = 1.0;
+  }
+  sc->vfactor = vf;
+  sc->bfactor = bf;
+  if (p.thermo_every > 0 && (step + 1) % p.thermo_every == 0) {
+    const long long row = (step + 1) / p.thermo_every - 1;
+    if (row < rows_cap) {
+      double* r = rows + row * kThermoCols;
+      r[0] = th[0];
+      r[1] = 1.5 * p.N * kBoltzmann * th[0];
+      r[2] = th[1];
+      r[3] = th[2] * kPressureUnit;
+      r[4] = th[3] * kPressureUnit;
+      r[5] = th[4] * kPressureUnit;
+      r[6] = th[7] * kPressureUnit;
+      r[7] = th[6] * kPressureUnit;
+      r[8] = th[5] * kPressureUnit;
+      const int cols[9] = {0, 3, 6, 1, 4, 7, 2, 5, 8};
+      for (int k = 0; k < 9; ++k) r[9 + k] = b.h[cols[k]];
+      r[18] = vf;
+      r[19] = bf;
+    }
+  }
+  sc->step = step + 1;
+  sc->vfactor_pre = 1.0;
+}
+
+// v *= velocity factor; under a box change x and the Verlet reference x0
+// scale with the box
+__global__ void k_scale(int N, double* vel, double* pos, double* x0,
+                        const MdScalars* __restrict__ sc)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const double vf = sc->vfactor, bf = sc->bfactor;
+  if (vf != 1.0)
+    for (int d = 0; d < 3; ++d) vel[d * N + i] *= vf;
+  if (bf != 1.0)
+    for (int d = 0; d < 3; ++d) {
+      pos[d * N + i] *= bf;
+      x0[d * N + i] *= bf;
+    }
+}
+
+__global__ void k_init_scalars(MdScalars* sc, StepParams p, double T0, double tau)
+{
+  sc->step = 0;
+  sc->vfactor_pre = 1.0;
+  sc->vfactor = 1.0;
+  sc->bfactor = 1.0;
+  // Nose-Hoover chain start (thermostat_nhc.cpp:25-41)
+  const double kT = kBoltzmann * T0;
+  for (int m = 0; m < kChain; ++m) {
+    sc->nhc_pos[m] = 0.0;
+    sc->nhc_mom[m] = (m % 2 == 0) ? 1.0 : -1.0;
+    sc->nhc_mass[m] = kT * tau * tau;
+  }
+  sc->nhc_mass[0] *= 3.0 * p.N;
+}
+
+}  // namespace
+
+// One MD step on the md's stream (captured into a graph by md_run).
+void md_enqueue_step(Md& md, const StepParams& p, int* d_status)
+{
+  Engine& e = *md.engine;
+  const int N = md.N;
+  const int blocks = (N + kThreads - 1) / kThreads;
+  cudaStream_t s = md.stream;
+  if (p.kind == kNvtNhc) {
+    k_ke_partials<<<blocks, kThreads, 0, s>>>(N, md.d_mass, md.d_vel, md.d_partials);
+    k_nhc_pre<<<1, 1, 0, s>>>(p, md.d_sc, md.d_partials, blocks);
+  }
+  k_vv1<<<blocks, kThreads, 0, s>>>(p, e.d_box, md.d_mass, md.d_force, md.d_pos, md.d_vel, md.d_sc);
+  launch_neighbor_update(e, N, md.d_pos, md.d_type, false, s);
+  launch_force(e, N, md.d_pos, md.d_type, md.d_pe, md.d_force, md.d_virial, false, s);
+  k_vv2_thermo<<<blocks, kThreads, 0, s>>>(p, md.d_mass, md.d_force, md.d_vel, md.d_pe,
+                                          md.d_virial, md.d_partials);
+  k_ensemble<<<1, 32, 0, s>>>(p, e.d_box, md.d_sc, md.d_partials, blocks, md.d_noise, md.d_rows,
+                              md.rows_cap, e.d_nstate, d_status);
+  k_scale<<<blocks, kThreads, 0, s>>>(N, md.d_vel, md.d_pos, e.nbr.x0, md.d_sc);
+}
+
+void md_init_scalars(Md& md, const StepParams& p, double T0, double tau)
+{
+  k_init_scalars<<<1, 1, 0, md.stream>>>(md.d_sc, p, T0, tau);
+}
+
+}  // namespace nepx
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+
+namespace {
+
+int md_fail(nepx_md* m, int code, const std::string& msg)
+{
+  if (m) m->error = msg;
+  return code;
+}
+
+int md_cuda(nepx_md* m, const char* what)
+{
+  const cudaError_t err = cudaGetLastError();
+  return md_fail(m, NEPX_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(err));
+}
+
+template <typename T>
+bool dalloc(T*& p, size_t n)
+{
+  return cudaMalloc(reinterpret_cast<void**>(&p), std::max<size_t>(n, 1) * sizeof(T)) ==
+         cudaSuccess;
+}
+
+int* status_buffer(nepx_md* m)
+{
+  // one int of device status behind the partials (allocated with them)
+  return reinterpret_cast<int*>(m->md.d_partials + 8 * static_cast<size_t>(m->md.partial_blocks));
+}
+
+}  // namespace
+
+extern "C" {
+
+int nepx_md_create(nepx_t* pot, int n, const int* h_type, const double* h_mass,
+                   const double* h_pos, const double* h_vel, const nepx_box* box, void* stream,
+                   nepx_md_t** out)
+{
+  if (!pot || !h_type || !h_mass || !h_pos || !h_vel || !box || !out || n < 1)
+    return NEPX_ERR_ARG;
+  *out = nullptr;
+  nepx::Engine& e = pot->engine;
+  if (n > e.capacity) return NEPX_ERR_CAPACITY;
+  for (int i = 0; i < n; ++i)
+    if (h_type[i] < 0 || h_type[i] >= e.model.num_types || !(h_mass[i] > 0.0))
+      return NEPX_ERR_ARG;
+  auto* m = new (std::nothrow) nepx_md();
+  if (!m) return NEPX_ERR_ARG;
+  nepx::Md& md = m->md;
+  md.engine = &e;
+  md.N = n;
+  m->pot = pot;
+  if (!nepx::make_box(box->h, box->pbc, md.box).empty() || !nepx::large_box_ok(e, md.box)) {
+    delete m;
+    return NEPX_ERR_BOX;
+  }
+  if (stream) {
+    md.stream = static_cast<cudaStream_t>(stream);
+  } else if (cudaStreamCreateWithFlags(&md.stream, cudaStreamNonBlocking) == cudaSuccess) {
+    m->own_stream = true;
+  }
+  md.partial_blocks = (n + 255) / 256;
+  bool ok = md.stream != nullptr;
+  ok = ok && dalloc(md.d_type, n) && dalloc(md.d_mass, n) && dalloc(md.d_pos, 3 * size_t(n)) &&
+       dalloc(md.d_vel, 3 * size_t(n)) && dalloc(md.d_force, 3 * size_t(n)) &&
+       dalloc(md.d_pe, n) && dalloc(md.d_virial, 9 * size_t(n)) &&
+       dalloc(md.d_partials, 8 * size_t(md.partial_blocks) + 2) && dalloc(md.d_sc, 1);
+  ok = ok && cudaEventCreateWithFlags(&m->noise_copied, cudaEventDisableTiming) == cudaSuccess;
+  ok = ok && cudaMallocHost(reinterpret_cast<void**>(&m->mirror), sizeof(MdMirror)) == cudaSuccess;
+  if (ok) {
+    std::memset(m->mirror, 0, sizeof(MdMirror));
+    m->mirror->box = md.box;
+  }
+  if (ok) {
+    // velocities arrive in A/fs; the engine integrates in natural units
+    std::vector<double> v(h_vel, h_vel + 3 * size_t(n));
+    for (double& x : v) x *= nepx::kTimeUnit;
+    ok = cudaMemcpy(md.d_type, h_type, sizeof(int) * n, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(md.d_mass, h_mass, sizeof(double) * n, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(md.d_pos, h_pos, sizeof(double) * 3 * n, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemcpy(md.d_vel, v.data(), sizeof(double) * 3 * n, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaMemset(status_buffer(m), 0, sizeof(int)) == cudaSuccess;
+  }
+  if (!ok) {
+    nepx_md_destroy(m);
+    return NEPX_ERR_CUDA;
+  }
+  *out = m;
+  return NEPX_OK;
+}
+
+int nepx_md_destroy(nepx_md_t* m)
+{
+  if (!m) return NEPX_ERR_ARG;
+  nepx::Md& md = m->md;
+  if (md.stream) cudaStreamSynchronize(md.stream);
+  if (md.graph) cudaGraphExecDestroy(md.graph);
+  void* ptrs[] = {md.d_type, md.d_mass, md.d_pos, md.d_vel, md.d_force, md.d_pe, md.d_virial,
+                  md.d_partials, md.d_sc, md.d_noise, md.d_rows};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (m->h_noise) cudaFreeHost(m->h_noise);
+  if (m->mirror) cudaFreeHost(m->mirror);
+  if (m->noise_copied) cudaEventDestroy(m->noise_copied);
+  if (md.engine && md.engine->box_owner == &md) md.engine->box_owner = nullptr;
+  if (m->own_stream && md.stream) cudaStreamDestroy(md.stream);
+  delete m;
+  return NEPX_OK;
+}
+
+const char* nepx_md_last_error(const nepx_md_t* m) { return m ? m->error.c_str() : "null handle"; }
+
+int nepx_md_set_ensemble(nepx_md_t* m, int kind, const double* params, unsigned seed)
+{
+  if (!m || kind < nepx::kNVE || kind > nepx::kNptScr) return NEPX_ERR_ARG;
+  nepx::EnsembleConfig c;
+  c.kind = kind;
+  if (kind != nepx::kNVE) {
+    if (!params) return md_fail(m, NEPX_ERR_ARG, "ensemble parameters missing");
+    c.T0 = params[0];
+    c.T1 = params[1];
+    c.Tdamp = params[2];
+    if (!(c.T0 > 0.0) || !(c.T1 > 0.0) || !(c.Tdamp >= 1.0))
+      return md_fail(m, NEPX_ERR_ARG, "ensemble needs T0 > 0, T1 > 0 and Tdamp >= 1");
+    if (kind == nepx::kNptBer || kind == nepx::kNptScr) {
+      c.p_gpa = params[3];
+      c.bulk_gpa = params[4];
+      c.tau_p = params[5];
+      if (!std::isfinite(c.p_gpa) || !(c.bulk_gpa > 0.0) || !(c.tau_p >= 1.0))
+        return md_fail(m, NEPX_ERR_ARG, "NPT needs finite P, B > 0 and tau_p >= 1");
+      const nepx::Box& b = m->md.box;
+      if (!b.ortho || !b.pbc[0] || !b.pbc[1] || !b.pbc[2])
+        return md_fail(m, NEPX_ERR_UNSUPPORTED,
+                       "isotropic NPT needs an orthogonal box periodic in all directions");
+    }
+  }
+  c.seed = seed;
+  m->md.ens = c;
+  m->md.rng = nepx::SvrRng(seed);
+  return NEPX_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Enqueues `steps` steps on the md stream; nothing waits for the device.
+int md_enqueue_run(nepx_md* m, int steps, double dt_fs, int thermo_every, double* h_thermo)
+{
+  if (!m || steps < 1 || !(dt_fs >= 0.0) || thermo_every < 0) return NEPX_ERR_ARG;
+  nepx::Md& md = m->md;
+  nepx::Engine& e = *md.engine;
+  const nepx::EnsembleConfig& c = md.ens;
+  const int N = md.N;
+  nepx::StepParams p{};
+  p.N = N;
+  p.kind = c.kind;
+  p.steps = steps;
+  p.thermo_every = thermo_every;
+  p.dt = dt_fs / nepx::kTimeUnit;
+  p.T0 = c.T0;
+  p.T1 = c.T1;
+  p.Tdamp = c.Tdamp;
+  p.rc_v = e.model.rc_max + e.skin;
+  p.skin = e.skin;
+  if (c.kind == nepx::kNptBer || c.kind == nepx::kNptScr) {
+    p.p_target = c.p_gpa / nepx::kPressureUnit;
+    // form pc in 1/GPa, then convert once (ensemble_control.cpp:84-95)
+    p.pc = c.bulk_gpa > 2000.0 ? 0.0 : 1.0 / (3.0 * c.tau_p * c.bulk_gpa);
+    p.pc *= nepx::kPressureUnit;
+  }
+  p.bdp_factor = c.Tdamp > 0.1 ? std::exp(-1.0 / c.Tdamp) : 0.0;
+  cudaStream_t s = md.stream;
+  // stochastic draws of every step, in the reference's consumption order
+  if (steps > md.noise_cap) {
+    cudaStreamSynchronize(s);
+    if (md.d_noise) cudaFree(md.d_noise);
+    if (m->h_noise) cudaFreeHost(m->h_noise);
+    md.d_noise = nullptr;
+    m->h_noise = nullptr;
+    if (!dalloc(md.d_noise, 3 * size_t(steps)) ||
+        cudaMallocHost(reinterpret_cast<void**>(&m->h_noise), sizeof(double) * 3 * steps) !=
+          cudaSuccess)
+      return md_cuda(m, "allocate noise buffers");
+    md.noise_cap = steps;
+  } else {
+    cudaEventSynchronize(m->noise_copied);   // previous upload has left the staging buffer
+  }
+  const bool stochastic_v = c.kind == nepx::kNvtBdp || c.kind == nepx::kNptScr;
+  for (int k = 0; k < steps; ++k) {
+    double* z = m->h_noise + 3 * k;
+    z[0] = z[1] = z[2] = 0.0;
+    if (stochastic_v) {
+      z[0] = md.rng.gasdev();
+      z[1] = md.rng.sumnoises(3 * N - 1);
+    }
+    if (c.kind == nepx::kNptScr) z[2] = md.rng.gasdev();
+  }
+  cudaMemcpyAsync(md.d_noise, m->h_noise, sizeof(double) * 3 * steps, cudaMemcpyHostToDevice, s);
+  cudaEventRecord(m->noise_copied, s);
+  const int rows = thermo_every > 0 ? steps / thermo_every : 0;
+  if (rows > md.rows_cap) {
+    cudaStreamSynchronize(s);
+    if (md.d_rows) cudaFree(md.d_rows);
+    md.d_rows = nullptr;
+    if (!dalloc(md.d_rows, size_t(rows) * nepx::kThermoCols)) return md_cuda(m, "allocate rows");
+    md.rows_cap = rows;
+  }
+  // the device box is authoritative while this md owns the engine; it is
+  // re-uploaded only after the handle served another caller
+  if (e.box_owner != &md) {
+    nepx::launch_set_box(e, md.box, s);
+    e.box_owner = &md;
+  }
+  nepx::md_init_scalars(md, p, c.T0, p.dt * c.Tdamp);
+  if (!md.forces_valid) {
+    nepx::launch_neighbor_update(e, N, md.d_pos, md.d_type, true, s);
+    nepx::launch_force(e, N, md.d_pos, md.d_type, md.d_pe, md.d_force, md.d_virial, false, s);
+    md.forces_valid = true;
+  }
+  e.force_rebuild = true;     // a later nepx_compute on this handle rebuilds
+  e.have_box = false;
+  int* d_status = status_buffer(m);
+  // capture one step as a graph (re-captured when the per-run constants change)
+  if (!md.graph || std::memcmp(&p, &md.graph_params, sizeof(p)) != 0) {
+    if (md.graph) cudaGraphExecDestroy(md.graph);
+    md.graph = nullptr;
+    cudaGraph_t g;
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+      return md_cuda(m, "begin capture");
+    nepx::md_enqueue_step(md, p, d_status);
+    if (cudaStreamEndCapture(s, &g) != cudaSuccess) return md_cuda(m, "end capture");
+    if (cudaGraphInstantiate(&md.graph, g, 0) != cudaSuccess) {
+      cudaGraphDestroy(g);
+      return md_cuda(m, "instantiate graph");
+    }
+    cudaGraphDestroy(g);
+    md.graph_params = p;
+  }
+  for (int k = 0; k < steps; ++k)
+    if (cudaGraphLaunch(md.graph, s) != cudaSuccess) return md_cuda(m, "graph launch");
+  // device-side status, box and neighbour flags land in pinned memory
+  cudaMemcpyAsync(&m->mirror->box, e.d_box, sizeof(nepx::Box), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(&m->mirror->status, d_status, sizeof(int), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(&m->mirror->nstate, e.d_nstate, sizeof(nepx::NeighborState),
+                  cudaMemcpyDeviceToHost, s);
+  if (h_thermo && rows > 0)
+    cudaMemcpyAsync(h_thermo, md.d_rows, sizeof(double) * rows * nepx::kThermoCols,
+                    cudaMemcpyDeviceToHost, s);
+  if (cudaPeekAtLastError() != cudaSuccess) return md_cuda(m, "enqueue run");
+  return NEPX_OK;
+}
+
+int md_finish(nepx_md* m)
+{
+  nepx::Md& md = m->md;
+  if (cudaStreamSynchronize(md.stream) != cudaSuccess) return md_cuda(m, "run");
+  md.box = m->mirror->box;
+  const int status = m->mirror->status;
+  const nepx::NeighborState& st = m->mirror->nstate;
+  if (status & 1) return md_fail(m, NEPX_ERR_NONFINITE, "invalid thermostat velocity factor");
+  if (status & 2) return md_fail(m, NEPX_ERR_NONFINITE, "invalid barostat box factor");
+  if (st.overflow) return md_fail(m, NEPX_ERR_OVERFLOW, "a neighbour row exceeded its capacity");
+  if (st.nonfinite) return md_fail(m, NEPX_ERR_NONFINITE, "non-finite energy or force");
+  return NEPX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int nepx_md_run(nepx_md_t* m, int steps, double dt_fs, int thermo_every, double* h_thermo)
+{
+  const int rc = md_enqueue_run(m, steps, dt_fs, thermo_every, h_thermo);
+  if (rc) return rc;
+  return md_finish(m);
+}
+
+int nepx_md_run_async(nepx_md_t* m, int steps, double dt_fs)
+{
+  return md_enqueue_run(m, steps, dt_fs, 0, nullptr);
+}
+
+int nepx_md_sync(nepx_md_t* m)
+{
+  if (!m) return NEPX_ERR_ARG;
+  return md_finish(m);
+}
+
+int nepx_md_get(nepx_md_t* m, double* h_pos, double* h_vel, double* h_force, double* h_pe,
+                double* h_virial, nepx_box* box)
+{
+  if (!m) return NEPX_ERR_ARG;
+  nepx::Md& md = m->md;
+  const size_t n = md.N;
+  cudaStreamSynchronize(md.stream);
+  bool ok = true;
+  if (h_pos) ok &= cudaMemcpy(h_pos, md.d_pos, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost) == cudaSuccess;
+  if (h_vel) {
+    ok &= cudaMemcpy(h_vel, md.d_vel, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost) == cudaSuccess;
+    for (size_t k = 0; k < 3 * n; ++k) h_vel[k] /= nepx::kTimeUnit;
+  }
+  if (h_force) ok &= cudaMemcpy(h_force, md.d_force, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost) == cudaSuccess;
+  if (h_pe) ok &= cudaMemcpy(h_pe, md.d_pe, sizeof(double) * n, cudaMemcpyDeviceToHost) == cudaSuccess;
+  if (h_virial) ok &= cudaMemcpy(h_virial, md.d_virial, sizeof(double) * 9 * n, cudaMemcpyDeviceToHost) == cudaSuccess;
+  if (box) {
+    std::memcpy(box->h, md.box.h, sizeof(double) * 9);
+    for (int d = 0; d < 3; ++d) box->pbc[d] = md.box.pbc[d];
+  }
+  return ok ? NEPX_OK : md_cuda(m, "copy state");
+}
+
+int nepx_md_device_state(nepx_md_t* m, double** d_pos, double** d_vel, double** d_force,
+                         int** d_type, void** stream)
+{
+  if (!m) return NEPX_ERR_ARG;
+  if (d_pos) *d_pos = m->md.d_pos;
+  if (d_vel) *d_vel = m->md.d_vel;
+  if (d_force) *d_force = m->md.d_force;
+  if (d_type) *d_type = m->md.d_type;
+  if (stream) *stream = m->md.stream;
+  return NEPX_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,77 @@
+// md.h -- device-resident molecular dynamics on one GPU.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "engine.h"
+#include "svr_rng.h"
+
+namespace nepx {
+
+enum EnsembleKind { kNVE = 0, kNvtBer = 1, kNvtNhc = 2, kNvtBdp = 3, kNptBer = 4, kNptScr = 5 };
+
+// run.in `ensemble` parameters (reference include/dmgmd/run_ir.hpp:12-117):
+// T0 -> T1 linear ramp, Tdamp coupling in steps; NPT: target pressure (GPa),
+// bulk modulus B (GPa) and pressure coupling tau_p (steps).
+struct EnsembleConfig {
+  int kind = kNVE;
+  double T0 = 0.0, T1 = 0.0, Tdamp = 100.0;
+  double p_gpa = 0.0, bulk_gpa = 0.0, tau_p = 1000.0;
+  uint32_t seed = 12345678u;   // reference default (ensemble_control.hpp:12-18)
+};
+
+constexpr int kChain = 4;      // Nose-Hoover chain length
+constexpr int kThermoCols = 20;  // thermo.out's 18 columns + velocity and box factors
+
+// Scalars the per-step kernels share, resident on the device.
+struct MdScalars {
+  long long step;      // step within the current run
+  double vfactor_pre;  // NHC scale applied before the first half kick
+  double vfactor;      // thermostat scale after the second half kick
+  double bfactor;      // isotropic box scale of this step
+  double thermo[8];    // T, PE, stresses xx yy zz xy xz yz (natural units, volume-normalised)
+  double nhc_pos[kChain], nhc_mom[kChain], nhc_mass[kChain];
+};
+
+// Per-run constants passed by value.
+struct StepParams {
+  int N;
+  int kind;
+  int steps;
+  int thermo_every;
+  double dt;           // natural time units
+  double T0, T1, Tdamp;
+  double p_target;     // eV/A^3
+  double pc;           // Berendsen pressure coupling, (eV/A^3)^-1
+  double bdp_factor;   // exp(-1/Tdamp) (0 when Tdamp <= 0.1)
+  double rc_v;         // rc + skin, for the NPT rebuild criterion
+  double skin;
+};
+
+struct Md {
+  Engine* engine = nullptr;
+  int N = 0;
+  int* d_type = nullptr;
+  double *d_mass = nullptr, *d_pos = nullptr, *d_vel = nullptr, *d_force = nullptr;
+  double *d_pe = nullptr, *d_virial = nullptr;
+  double* d_partials = nullptr;   // [blocks][8]
+  int partial_blocks = 0;
+  MdScalars* d_sc = nullptr;
+  double* d_noise = nullptr;      // [steps][3]
+  int noise_cap = 0;
+  double* d_rows = nullptr;       // [rows][kThermoCols]
+  int rows_cap = 0;
+  double* d_scale = nullptr;      // cumulative box scale since the last Verlet build
+  Box box{};
+  EnsembleConfig ens;
+  SvrRng rng{12345678u};
+  bool forces_valid = false;
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  StepParams graph_params{};
+  int graph_steps = 0;
+};
+
+}  // namespace nepx

@@ -43,10 +43,13 @@ __device__ __forceinline__ void cell_coords(const Box& b, const NeighborState& s
 }
 
 // Marks a rebuild when forced or when an atom moved more than skin/2
-// (reference neighbor.cu:446-533, without the host round trip).
+// (reference neighbor.cu:446-533, without the host round trip).  Under an
+// isotropic box scaling s since the build (x0 scaled along, so displacements
+// are co-moving) a pair distance also drifts by up to |1 - s| (rc + skin),
+// which shrinks the allowed displacement to (skin - |1 - s| (rc + skin)) / 2.
 __global__ void k_skin_check(int N, const Box* __restrict__ box, const double* __restrict__ pos,
-                             const double* __restrict__ x0, NeighborState* st, double half_skin_sq,
-                             int force)
+                             const double* __restrict__ x0, NeighborState* st, double skin,
+                             double rc_v, int force)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (force) {
@@ -54,6 +57,12 @@ __global__ void k_skin_check(int N, const Box* __restrict__ box, const double* _
     return;
   }
   if (i >= N) return;
+  const double half = 0.5 * (skin - fabs(1.0 - st->box_scale) * rc_v);
+  if (half <= 0.0) {
+    st->rebuild = 1;
+    return;
+  }
+  const double half_skin_sq = half * half;
   float dx = pos[i] - x0[i];
   float dy = pos[N + i] - x0[N + i];
   float dz = pos[2 * N + i] - x0[2 * N + i];
@@ -69,6 +78,7 @@ __global__ void k_cell_setup(const Box* __restrict__ box, NeighborState* st, int
   __shared__ int s_ncell;
   if (!st->rebuild) return;
   if (threadIdx.x == 0) {
+    st->box_scale = 1.0;
     const Box& b = *box;
     double vol = fabs(b.h[0] * (b.h[4] * b.h[8] - b.h[5] * b.h[7]) +
                       b.h[1] * (b.h[5] * b.h[6] - b.h[3] * b.h[8]) +
@@ -313,7 +323,7 @@ void launch_neighbor_update(Engine& e, int N, const double* pos, const int* type
   const float rc_v = e.model.rc_max + static_cast<float>(e.skin);
   const double rc_v_d = static_cast<double>(e.model.rc_max) + e.skin;
   k_skin_check<<<force ? 1 : grid, threads, 0, stream>>>(N, e.d_box, pos, nb.x0, e.d_nstate,
-                                                         e.skin * e.skin * 0.25, force ? 1 : 0);
+                                                         e.skin, rc_v_d, force ? 1 : 0);
   k_cell_setup<<<1, 1024, 0, stream>>>(e.d_box, e.d_nstate, nb.cell_count, rc_v_d, nb.cell_cap);
   k_cell_count<<<grid, threads, 0, stream>>>(N, e.d_box, pos, e.d_nstate, nb.cell_of,
                                              nb.cell_count);

@@ -788,8 +788,7 @@ void upload_invariant_tables()
 
 size_t descriptor_smem_bytes(const ModelParams& p) { return desc_layout(p).total_bytes; }
 
-void launch_force(Engine& e, int N, const double* pos, const int* type, double* pe,
-                  double* force, double* virial, bool accumulate, cudaStream_t stream)
+void launch_descriptor(Engine& e, int N, const double* pos, const int* type, cudaStream_t stream)
 {
   const ModelParams& p = e.params;
   NeighborBuffers& nb = e.nbr;
@@ -797,6 +796,13 @@ void launch_force(Engine& e, int N, const double* pos, const int* type, double* 
   k_descriptor_ann_f12<<<tiles, kThreads, e.smem_desc, stream>>>(
     p, N, e.d_box, pos, type, nb.nn_r, nb.nl_r, nb.mn_r, nb.nn_a, nb.nl_a, nb.mn_a,
     e.scratch.fp_rad, e.scratch.f12, e.scratch.pe_ann);
+}
+
+void launch_gather(Engine& e, int N, const double* pos, const int* type, double* pe,
+                   double* force, double* virial, bool accumulate, cudaStream_t stream)
+{
+  const ModelParams& p = e.params;
+  NeighborBuffers& nb = e.nbr;
   const int threads = 256;
   const size_t smem_g = static_cast<size_t>(p.T) * p.T * p.nR * p.kR * sizeof(float);
   const int blocks = static_cast<int>((static_cast<long long>(N) * kGroup + threads - 1) / threads);
@@ -804,6 +810,13 @@ void launch_force(Engine& e, int N, const double* pos, const int* type, double* 
     p, N, e.d_box, pos, type, nb.nn_r, nb.nl_r, nb.mn_r, nb.nn_a, nb.nl_a, nb.mn_a,
     e.scratch.fp_rad, e.scratch.f12, e.scratch.pe_ann, pe, force, virial, accumulate ? 1 : 0,
     e.d_nstate);
+}
+
+void launch_force(Engine& e, int N, const double* pos, const int* type, double* pe,
+                  double* force, double* virial, bool accumulate, cudaStream_t stream)
+{
+  launch_descriptor(e, N, pos, type, stream);
+  launch_gather(e, N, pos, type, pe, force, virial, accumulate, stream);
 }
 
 void set_descriptor_smem_limit(size_t bytes)

@@ -28,7 +28,14 @@ ERRORS = {1: "NEPX_ERR_ARG", 2: "NEPX_ERR_FILE", 3: "NEPX_ERR_UNSUPPORTED", 4: "
 
 # every symbol include/nepx.h declares (checked by tests/test_capi_symbols.py)
 EXPORTED = ["nepx_create", "nepx_destroy", "nepx_last_error", "nepx_info", "nepx_compute",
-            "nepx_notify_box_changed", "nepx_set_skin", "nepx_neighbors", "nepx_neighbor_stats"]
+            "nepx_notify_box_changed", "nepx_set_skin", "nepx_neighbors", "nepx_neighbor_stats",
+            "nepx_md_create", "nepx_md_destroy", "nepx_md_last_error", "nepx_md_set_ensemble",
+            "nepx_md_run", "nepx_md_get", "nepx_md_device_state", "nepx_profile",
+            "nepx_md_run_async", "nepx_md_sync"]
+
+ENSEMBLES = {"nve": 0, "nvt_ber": 1, "nvt_nhc": 2, "nvt_bdp": 3, "npt_ber": 4, "npt_scr": 5}
+THERMO_COLUMNS = ["T", "KE", "PE", "sxx", "syy", "szz", "syz", "sxz", "sxy", "ax", "ay", "az",
+                  "bx", "by", "bz", "cx", "cy", "cz", "velocity_factor", "box_factor"]
 
 
 class NepxError(RuntimeError):
@@ -68,8 +75,23 @@ def lib():
         L.nepx_set_skin.argtypes = [vp, ctypes.c_double]
         L.nepx_neighbors.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp, ctypes.c_int, vp]
         L.nepx_neighbor_stats.argtypes = [vp, ip, ip, ip, vp]
+        L.nepx_md_create.argtypes = [vp, ctypes.c_int, vp, vp, vp, vp, ctypes.POINTER(Box), vp,
+                                     ctypes.POINTER(vp)]
+        L.nepx_md_destroy.argtypes = [vp]
+        L.nepx_md_last_error.argtypes = [vp]
+        L.nepx_md_last_error.restype = ctypes.c_char_p
+        L.nepx_md_set_ensemble.argtypes = [vp, ctypes.c_int, dp, ctypes.c_uint]
+        L.nepx_md_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, dp]
+        L.nepx_md_get.argtypes = [vp, dp, dp, dp, dp, dp, ctypes.POINTER(Box)]
+        L.nepx_md_run_async.argtypes = [vp, ctypes.c_int, ctypes.c_double]
+        L.nepx_md_sync.argtypes = [vp]
+        L.nepx_profile.argtypes = [vp, ctypes.POINTER(Box), ctypes.c_int, vp, vp, vp, vp, vp,
+                                   ctypes.c_int, dp, vp]
+        L.nepx_md_device_state.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                           ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                           ctypes.POINTER(vp)]
         for name in EXPORTED:
-            if name != "nepx_last_error":
+            if name not in ("nepx_last_error", "nepx_md_last_error"):
                 getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib
@@ -168,5 +190,103 @@ class Potential:
                                               ctypes.byref(v), _stream_ptr(stream)))
         return r.value, a.value, v.value
 
+    def profile(self, types, h, pos, reps=20, pbc=(1, 1, 1), stream=None):
+        """Per-stage device ms: neighbour, descriptor, gather, total."""
+        import torch
+        n = types.numel()
+        pe = torch.empty(n, dtype=torch.float64, device=pos.device)
+        force = torch.empty(3, n, dtype=torch.float64, device=pos.device)
+        virial = torch.empty(9, n, dtype=torch.float64, device=pos.device)
+        ms = (ctypes.c_double * 4)()
+        box = make_box(h, pbc)
+        self._check(lib().nepx_profile(self._h, ctypes.byref(box), n, _ptr(types), _ptr(pos),
+                                       _ptr(pe), _ptr(force), _ptr(virial), int(reps), ms,
+                                       _stream_ptr(stream)))
+        return dict(zip(["neighbor", "descriptor", "gather", "total"], list(ms)))
+
     def notify_box_changed(self):
         self._check(lib().nepx_notify_box_changed(self._h))
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class MD:
+    """Device-resident MD of one system (nepx_md_* of include/nepx.h).
+
+    Host numpy inputs: types (n,), masses (n,) amu, positions (3, n) A,
+    velocities (3, n) A/fs, box h (9,) row-major with cell vectors as columns.
+    """
+
+    def __init__(self, potential, types, masses, pos, vel, h, pbc=(1, 1, 1)):
+        import numpy as np
+        self.pot = potential
+        self.n = len(types)
+        t = np.ascontiguousarray(types, dtype=np.int32)
+        m = np.ascontiguousarray(masses, dtype=np.float64)
+        x = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1)
+        v = np.ascontiguousarray(vel, dtype=np.float64).reshape(-1)
+        box = make_box(h, pbc)
+        self._h = ctypes.c_void_p()
+        rc = lib().nepx_md_create(potential._h, self.n, t.ctypes.data_as(ctypes.c_void_p),
+                                  m.ctypes.data_as(ctypes.c_void_p),
+                                  x.ctypes.data_as(ctypes.c_void_p),
+                                  v.ctypes.data_as(ctypes.c_void_p), ctypes.byref(box), None,
+                                  ctypes.byref(self._h))
+        if rc:
+            raise NepxError(rc, "nepx_md_create failed")
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().nepx_md_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc:
+            raise NepxError(rc, lib().nepx_md_last_error(self._h).decode())
+
+    def set_ensemble(self, kind, T0=0.0, T1=None, Tdamp=100.0, p_gpa=0.0, bulk_gpa=0.0,
+                     tau_p=1000.0, seed=12345678):
+        import numpy as np
+        T1 = T0 if T1 is None else T1
+        params = np.array([T0, T1, Tdamp, p_gpa, bulk_gpa, tau_p], dtype=np.float64)
+        self._check(lib().nepx_md_set_ensemble(self._h, ENSEMBLES[kind], _dp(params), seed))
+
+    def run(self, steps, dt_fs, thermo_every=0):
+        """Runs `steps` steps; returns the thermo rows (rows, 20) or None."""
+        import numpy as np
+        rows = steps // thermo_every if thermo_every else 0
+        out = np.zeros((max(rows, 1), len(THERMO_COLUMNS)))
+        self._check(lib().nepx_md_run(self._h, steps, dt_fs, thermo_every,
+                                      _dp(out) if rows else None))
+        return out[:rows] if rows else None
+
+    def run_async(self, steps, dt_fs):
+        self._check(lib().nepx_md_run_async(self._h, steps, dt_fs))
+
+    def sync(self):
+        self._check(lib().nepx_md_sync(self._h))
+
+    def device_state(self):
+        """(d_pos, d_vel, d_force, d_type, stream) raw pointers."""
+        ptrs = [ctypes.c_void_p() for _ in range(5)]
+        self._check(lib().nepx_md_device_state(self._h, *[ctypes.byref(p) for p in ptrs]))
+        return [p.value for p in ptrs]
+
+    def state(self):
+        import numpy as np
+        n = self.n
+        pos, vel, force = np.zeros(3 * n), np.zeros(3 * n), np.zeros(3 * n)
+        pe, vir = np.zeros(n), np.zeros(9 * n)
+        box = Box()
+        self._check(lib().nepx_md_get(self._h, _dp(pos), _dp(vel), _dp(force), _dp(pe),
+                                      _dp(vir), ctypes.byref(box)))
+        return {"pos": pos.reshape(3, n), "vel": vel.reshape(3, n), "force": force.reshape(3, n),
+                "pe": pe, "virial": vir.reshape(9, n), "h": np.array(box.h[:])}

@@ -109,6 +109,84 @@ int nepx_neighbors(nepx_t* handle, int which, int n, int* d_nn, int* d_nl, int m
 int nepx_neighbor_stats(nepx_t* handle, int* max_radial, int* max_angular, int* max_verlet,
                         void* stream);
 
+/*
+ * Per-stage device time of the force path, averaged over `reps` calls after
+ * one settling call: ms[0] neighbour update (skin check, conditional
+ * rebuild, typewise filter), ms[1] descriptor + ANN + angular partial
+ * forces, ms[2] force / virial gather, ms[3] the whole force call.
+ * Arguments as nepx_compute.  Replaces the wall-clock log_timing of the
+ * reference (src/mpi_runtime.cu:2048-2080) with CUDA events per kernel.
+ */
+int nepx_profile(nepx_t* handle, const nepx_box* box, int n, const int* d_type,
+                 const double* d_pos, double* d_pe, double* d_force, double* d_virial, int reps,
+                 double* ms, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Molecular dynamics on one GPU (velocity Verlet, FP64 integration).
+ * Replaces the single-rank loop run_segment / run_m1_replicated
+ * (src/runtime.cu:680-971) with its ensembles (src/ensemble_control.cpp).
+ * ---------------------------------------------------------------------- */
+
+typedef struct nepx_md nepx_md_t;
+
+/* ensemble kinds (run.in keywords) */
+#define NEPX_NVE 0
+#define NEPX_NVT_BER 1   /* Berendsen */
+#define NEPX_NVT_NHC 2   /* Nose-Hoover chain, length 4 */
+#define NEPX_NVT_BDP 3   /* Bussi-Donadio-Parrinello (stochastic velocity rescaling) */
+#define NEPX_NPT_BER 4   /* isotropic Berendsen barostat + Berendsen thermostat */
+#define NEPX_NPT_SCR 5   /* isotropic stochastic cell rescaling + BDP thermostat */
+
+/*
+ * A system of n atoms driven by `pot` (which must have capacity >= n).
+ * Host inputs: types, masses (amu), positions 3n SoA (A), velocities 3n SoA
+ * (A/fs, the model.xyz unit).  stream: cudaStream_t to run on (NULL = the
+ * engine creates a non-blocking stream).  Replaces the device-atom setup of
+ * run_m1_replicated (runtime.cu:855-905).
+ */
+int nepx_md_create(nepx_t* pot, int n, const int* h_type, const double* h_mass,
+                   const double* h_pos, const double* h_vel, const nepx_box* box, void* stream,
+                   nepx_md_t** out);
+int nepx_md_destroy(nepx_md_t* md);
+const char* nepx_md_last_error(const nepx_md_t* md);
+
+/*
+ * params (kind != NEPX_NVE): {T0, T1, Tdamp[, P_GPa, B_GPa, tau_p]} as the
+ * reference's `ensemble` command (run_parser.cpp:158-315); seed of the
+ * stochastic thermostat / barostat stream (reference default 12345678,
+ * env DMGMD_ENSEMBLE_SEED).  Replaces EnsembleController
+ * (src/ensemble_control.cpp:57-306).
+ */
+int nepx_md_set_ensemble(nepx_md_t* md, int kind, const double* params, unsigned seed);
+
+/*
+ * `steps` steps of dt_fs femtoseconds.  Every thermo_every steps (0 = never)
+ * one row of 20 doubles is written to h_thermo (rows = steps / thermo_every,
+ * may be NULL): the 18 thermo.out columns (T KE PE sxx syy szz syz sxz sxy
+ * ax ay az bx by bz cx cy cz; stresses in GPa) followed by that step's
+ * thermostat velocity factor and barostat box factor.  The target
+ * temperature ramps from T0 to T1 over the run, as in the reference.
+ * Synchronises the md stream before returning.
+ */
+int nepx_md_run(nepx_md_t* md, int steps, double dt_fs, int thermo_every, double* h_thermo);
+
+/* nepx_md_run without thermo rows and without waiting for the device:
+ * consecutive calls queue back to back on the md stream.  Device-side errors
+ * are reported by the next nepx_md_sync (or nepx_md_run).  Interleaving
+ * nepx_compute on the same potential handle requires nepx_md_sync first. */
+int nepx_md_run_async(nepx_md_t* md, int steps, double dt_fs);
+int nepx_md_sync(nepx_md_t* md);
+
+/* Copies the current state to host arrays (any may be NULL); velocities in
+ * A/fs; virial 9n in the compute order. */
+int nepx_md_get(nepx_md_t* md, double* h_pos, double* h_vel, double* h_force, double* h_pe,
+                double* h_virial, nepx_box* box);
+
+/* Device pointers of the state (positions, velocities in natural units,
+ * forces, types) and the stream the md runs on. */
+int nepx_md_device_state(nepx_md_t* md, double** d_pos, double** d_vel, double** d_force,
+                         int** d_type, void** stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -167,3 +167,64 @@ class RefCpuModel:
         f.argtypes = [ctypes.c_void_p, ctypes.c_int, _i32p, _f64p, _f64p, ctypes.c_int,
                       ctypes.c_int, ctypes.c_int, _f64p, _f64p, _f64p]
         return f(self._h, n, types, h, pos.reshape(-1), threads, begin, end, pe, force, virial)
+
+
+REF_GPU_SO = os.path.join(HERE, "_ref", "libnep_ref_gpu.so")
+_refgpu = None
+
+
+def ref_gpu_available():
+    return os.path.exists(REF_GPU_SO)
+
+
+def refgpu_lib():
+    global _refgpu
+    if _refgpu is None:
+        L = ctypes.CDLL(REF_GPU_SO)
+        vp = ctypes.c_void_p
+        L.refgpu_create.restype = vp
+        L.refgpu_create.argtypes = [ctypes.c_char_p, ctypes.c_int]
+        L.refgpu_destroy.argtypes = [vp]
+        L.refgpu_set_atoms.argtypes = [vp, vp, vp]
+        L.refgpu_compute.argtypes = [vp, _f64p, _i32p, vp, vp, vp]
+        L.refgpu_neighbors.argtypes = [vp, ctypes.c_int, _i32p, _i32p, ctypes.c_int]
+        for f in ("refgpu_set_atoms", "refgpu_compute", "refgpu_neighbors"):
+            getattr(L, f).restype = ctypes.c_int
+        _refgpu = L
+    return _refgpu
+
+
+class RefGpuModel:
+    """The reference's own FP32 GPU NEP (src/gpumd_compat compiled for sm_100a).
+
+    Device buffers are torch CUDA tensors; the reference copies them into its
+    own GPU_Vectors (set_atoms) and evaluates with its legacy kernel sequence.
+    """
+
+    def __init__(self, path, n):
+        self._h = refgpu_lib().refgpu_create(os.fsencode(path), int(n))
+        self.n = int(n)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            refgpu_lib().refgpu_destroy(self._h)
+            self._h = None
+
+    def set_atoms(self, d_type, d_pos):
+        if refgpu_lib().refgpu_set_atoms(self._h, ctypes.c_void_p(d_type.data_ptr()),
+                                         ctypes.c_void_p(d_pos.data_ptr())):
+            raise RuntimeError("reference set_atoms failed")
+
+    def compute(self, h, pbc=(1, 1, 1), out=None):
+        h = np.ascontiguousarray(np.asarray(h, dtype=np.float64).reshape(9))
+        pbc = np.ascontiguousarray(pbc, dtype=np.int32)
+        ptrs = [ctypes.c_void_p(t.data_ptr()) for t in out] if out else [None, None, None]
+        if refgpu_lib().refgpu_compute(self._h, h, pbc, *ptrs):
+            raise RuntimeError("reference compute failed")
+
+    def neighbors(self, which, mn):
+        nn = np.zeros(self.n, dtype=np.int32)
+        nl = np.zeros(self.n * mn, dtype=np.int32)
+        refgpu_lib().refgpu_neighbors(self._h, which, nn, nl, mn)
+        nl = nl.reshape(self.n, mn)
+        return [nl[i, :nn[i]].copy() for i in range(self.n)]

@@ -1,0 +1,138 @@
+"""GPU tests of the device-resident MD loop (nepx_md_* through the C ABI)."""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import workloads
+from conftest import ROOT, potential
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+K_B = 8.617343e-5
+MASS_C = 12.011
+
+
+def _nepx():
+    import nepx
+    return nepx
+
+
+def test_nve_follows_gpumd_golden_trajectory(goldens):
+    """6 NVE steps of 0.1 fs from the reference suite's single_large_nve case.
+
+    Positions at the suite's tolerance (rtol 2e-8, atol 2e-9 A); velocities at
+    5x the suite's (the FP32 force rounding differs from GPUMD's by ~5e-6 eV/A,
+    which alone moves v by ~2.5e-9 A/fs over 0.6 fs); forces, per-atom
+    energies and virials at the suite's force/energy/virial tolerances.
+    """
+    nepx = _nepx()
+    tr = goldens["trajectories"]["single_large_nve"]
+    model = tr["model"]
+    n = model["n"]
+    pot = nepx.Potential(potential(tr["potential"]), max_atoms=n)
+    md = nepx.MD(pot, model["type"], [MASS_C] * n, np.array(model["pos"]).T,
+                 np.array(model["vel"]).T, model["h"])
+    md.set_ensemble("nve")
+    rowmajor = [0, 3, 4, 6, 1, 5, 7, 8, 2]
+    for frame in tr["frames"]:
+        md.run(1, 0.1)
+        s = md.state()
+        pos = np.array(frame["pos"]).T
+        vel = np.array(frame["vel"]).T
+        assert np.all(np.abs(s["pos"] - pos) <= 2e-9 + 2e-8 * np.abs(pos)), frame["time_fs"]
+        assert np.all(np.abs(s["vel"] - vel) <= 5 * (2e-9 + 2e-7 * np.abs(vel))), frame["time_fs"]
+        f = np.array(frame["force"]).T
+        assert np.all(np.abs(s["force"] - f) <= 1e-6 + 1e-4 * np.abs(f) + 1e-5)
+        e = np.array(frame["energy_atom"])
+        assert np.all(np.abs(s["pe"] - e) <= 2e-5 + 1e-5 * np.abs(e))
+        w = np.array(frame["virial_rowmajor"]).T
+        assert np.all(np.abs(s["virial"][rowmajor] - w) <= 1e-5 + 1e-4 * np.abs(w))
+
+
+def _water_md(n_mol, T, seed, kind="nve", **ens):
+    nepx = _nepx()
+    t, h, p = workloads.water(n_mol=n_mol, seed=seed)
+    masses = np.where(t == 0, 15.999, 1.008)
+    v = workloads.maxwell_boltzmann(masses, T, seed=seed)
+    pot = nepx.Potential(potential("nep_water.txt"), max_atoms=len(t))
+    md = nepx.MD(pot, t, masses, p, v, h)
+    md.set_ensemble(kind, **ens)
+    return pot, md, t, h
+
+
+def test_nve_energy_conservation():
+    pot, md, t, h = _water_md(300, 300.0, 1)
+    rows = md.run(400, 0.5, thermo_every=10)
+    etot = rows[:, 1] + rows[:, 2]
+    n = len(t)
+    time_ns = np.arange(1, len(rows) + 1) * 10 * 0.5e-6
+    slope = np.polyfit(time_ns, etot / n, 1)[0]
+    assert abs(slope) < 5e-3, "drift %g eV/atom/ns" % slope
+    assert np.std(etot / n) < 2e-4
+
+
+def test_bdp_velocity_factor_bit_exact(tmp_path):
+    """Device resampling equals the reference formula on the same draws."""
+    lib = tmp_path / "libsvr.so"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off",
+                    os.path.join(ROOT, "tests", "cpp", "svr_harness.cpp"), "-o", str(lib)],
+                   check=True)
+    L = ctypes.CDLL(str(lib))
+    dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+    L.svr_step_draws.argtypes = [ctypes.c_uint32, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp]
+    L.resample.restype = ctypes.c_double
+    L.resample.argtypes = [ctypes.c_double] * 2 + [ctypes.c_int] + [ctypes.c_double] * 3
+    steps, seed = 60, 2024
+    pot, md, t, h = _water_md(200, 250.0, 2, kind="nvt_bdp", T0=300.0, T1=320.0, Tdamp=20.0,
+                              seed=seed)
+    rows = md.run(steps, 0.5, thermo_every=1)
+    n = len(t)
+    ndeg = 3 * n
+    draws = np.zeros(3 * steps)
+    L.svr_step_draws(seed, ndeg, steps, 0, draws)
+    factor = np.exp(-1.0 / 20.0)
+    for k in range(steps):
+        T = rows[k, 0]
+        Tt = 300.0 + (320.0 - 300.0) * (float(k) / float(steps))
+        old = T * ndeg * K_B * 0.5
+        sigma = ndeg * K_B * Tt * 0.5
+        new = L.resample(old, sigma, ndeg, factor, draws[3 * k], draws[3 * k + 1])
+        assert np.sqrt(new / old) == rows[k, 18], k
+
+
+@pytest.mark.parametrize("kind", ["nvt_ber", "nvt_nhc", "nvt_bdp"])
+def test_thermostats_reach_target(kind):
+    pot, md, t, h = _water_md(300, 200.0, 3, kind=kind, T0=350.0, T1=350.0, Tdamp=10.0)
+    rows = md.run(600, 0.5, thermo_every=5)
+    T_late = rows[-40:, 0].mean()
+    assert abs(T_late - 350.0) < 0.12 * 350.0, (kind, T_late)
+
+
+@pytest.mark.parametrize("kind", ["npt_ber", "npt_scr"])
+def test_npt_box_moves_and_lists_stay_complete(kind):
+    nepx = _nepx()
+    pot, md, t, h = _water_md(300, 300.0, 4, kind=kind, T0=300.0, Tdamp=20.0, p_gpa=0.5,
+                              bulk_gpa=2.0, tau_p=50.0)
+    rows = md.run(300, 0.5, thermo_every=10)
+    assert np.all(rows[:, 19] > 0)
+    assert abs(rows[-1, 9] - h[0]) > 1e-4          # the box moved
+    # Berendsen factor = 1 - pc (P_target - P_inst)
+    if kind == "npt_ber":
+        pc = 1.0 / (3.0 * 50.0 * 2.0)
+        p_inst = rows[:, 3:6].mean(axis=1)
+        np.testing.assert_allclose(rows[:, 19], 1.0 - pc * (0.5 - p_inst), rtol=0, atol=1e-12)
+    # the Verlet list kept across box rescalings must give the same forces as
+    # a freshly built one at the same positions and box
+    md.set_ensemble("nve")
+    md.run(1, 0.0)
+    s = md.state()
+    fresh = nepx.Potential(potential("nep_water.txt"), max_atoms=len(t))
+    tt = torch.as_tensor(t, device="cuda")
+    pp = torch.as_tensor(np.ascontiguousarray(s["pos"]), device="cuda")
+    pe, f, w = fresh.compute(tt, s["h"], pp, sync_check=True)
+    assert np.array_equal(f.cpu().numpy(), s["force"])
+    assert np.array_equal(pe.cpu().numpy(), s["pe"])
