@@ -6,7 +6,10 @@
 
 Default workload (the headline config): liquid water, 8000 molecules = 24,000
 atoms at 1.0 g/cm^3, synthetic two-type NEP4 (O/H, rc 6.0/4.0 A, n_max 4/4,
-basis 8/8, l_max 4 2 0, 50 hidden units, weights N(0, 0.1^2), seeded),
+basis 8/8, l_max 4 2 0, 50 hidden units, weights N(0, 0.1^2), seeded; a
+descriptor scale q_scaler = 0.02 keeps the random-weight landscape gentle so
+the liquid keeps water's density and neighbour counts through the run
+instead of clustering -- the cost per step is that of any NEP of this shape),
 Bussi NVT (nvt_bdp) at 300 K, dt 0.5 fs.  One "step" is one full MD step:
 neighbour update, NEP energy/force/virial, FP64 velocity Verlet, thermo
 reduction and thermostat.  Metric: atom-steps/s, whole job (sum over ranks).
@@ -54,18 +57,19 @@ SM_MAX_MHZ = 1965.0
 WORKLOADS = {
     # name: (builder, nep kwargs, ensemble kwargs, dt_fs)
     "water": dict(
-        nep=dict(version=4, symbols=("O", "H"), rc=(6.0, 4.0), mn=(150, 60), n_max=(4, 4),
-                 basis=(8, 8), l_max=(4, 2, 0), H=50, seed=2024, std=0.1),
+        nep=dict(version=4, symbols=("O", "H"), rc=(6.0, 4.0), mn=(250, 100), n_max=(4, 4),
+                 basis=(8, 8), l_max=(4, 2, 0), H=50, seed=2024, std=0.1, q_scaler=0.02),
         ens=dict(kind="nvt_bdp", T0=300.0, Tdamp=100.0), dt=0.5, T=300.0,
         desc="water_8000mol_24000atoms_nep4_O-H_rc6.0-4.0_H50_nvt_bdp_300K_dt0.5fs"),
     "carbon": dict(
         nep=dict(version=4, symbols=("C",), rc=(4.2, 3.7), mn=(100, 60), n_max=(4, 4),
-                 basis=(8, 8), l_max=(4, 2, 1), H=30, seed=2025, std=0.1),
+                 basis=(8, 8), l_max=(4, 2, 1), H=30, seed=2025, std=0.1, q_scaler=0.02),
         ens=dict(kind="nve"), dt=1.0, T=300.0,
         desc="diamond_8x8x8_4096atoms_nep4_C_rc4.2-3.7_H30_nve_dt1fs"),
     "copper": dict(
         nep=dict(version=4, symbols=("Cu",), zbl=(1.0, 2.0), rc=(5.0, 4.0), mn=(100, 60),
-                 n_max=(4, 4), basis=(8, 8), l_max=(4, 2, 1), H=40, seed=2026, std=0.1),
+                 n_max=(4, 4), basis=(8, 8), l_max=(4, 2, 1), H=40, seed=2026, std=0.1,
+                 q_scaler=0.02),
         ens=dict(kind="npt_ber", T0=300.0, Tdamp=100.0, p_gpa=0.0, bulk_gpa=140.0,
                  tau_p=1000.0), dt=1.0, T=300.0,
         desc="cu_fcc_63x63x63_1pct_vacancies_nepzbl_rc5.0-4.0_H40_npt_ber_dt1fs"),

@@ -20,6 +20,7 @@
 #include "../../include/nepx.h"
 #include "handle.h"
 #include "md.h"
+#include "nhc.h"
 
 struct MdMirror {
   nepx::Box box;
@@ -86,44 +87,6 @@ __global__ void k_ke_partials(int N, const double* __restrict__ mass,
   block_reduce8(v, partials);
 }
 
-// Nose-Hoover chain half step (Martyna-Tuckerman-Klein; Suzuki-Yoshida order
-// 7 x 4 RESPA substeps), the integrator of thermostat_nhc.cpp:47-116.
-__device__ double nhc_half_step(MdScalars& sc, double ek2, double kT, double dN, double dt_half)
-{
-  const double w[7] = {0.784513610477560,  0.235573213359357, -1.17767998417887,
-                       1.31518632068391,  -1.17767998417887,  0.235573213359357,
-                       0.784513610477560};
-  const int M = kChain;
-  double factor = 1.0;
-  for (int a = 0; a < 7; ++a) {
-    const double dt2 = dt_half * w[a] / 4;
-    const double dt4 = dt2 * 0.5;
-    const double dt8 = dt4 * 0.5;
-    for (int b = 0; b < 4; ++b) {
-      double G = sc.nhc_mom[M - 2] * sc.nhc_mom[M - 2] / sc.nhc_mass[M - 2] - kT;
-      sc.nhc_mom[M - 1] += dt4 * G;
-      for (int m = M - 2; m >= 0; --m) {
-        const double t = exp(-dt8 * sc.nhc_mom[m + 1] / sc.nhc_mass[m + 1]);
-        G = m == 0 ? ek2 - dN * kT
-                   : sc.nhc_mom[m - 1] * sc.nhc_mom[m - 1] / sc.nhc_mass[m - 1] - kT;
-        sc.nhc_mom[m] = t * (t * sc.nhc_mom[m] + dt4 * G);
-      }
-      for (int m = M - 1; m >= 0; --m) sc.nhc_pos[m] += dt2 * sc.nhc_mom[m] / sc.nhc_mass[m];
-      const double f = exp(-dt2 * sc.nhc_mom[0] / sc.nhc_mass[0]);
-      ek2 *= f * f;
-      factor *= f;
-      for (int m = 0; m < M - 1; ++m) {
-        const double t = exp(-dt8 * sc.nhc_mom[m + 1] / sc.nhc_mass[m + 1]);
-        G = m == 0 ? ek2 - dN * kT
-                   : sc.nhc_mom[m - 1] * sc.nhc_mom[m - 1] / sc.nhc_mass[m - 1] - kT;
-        sc.nhc_mom[m] = t * (t * sc.nhc_mom[m] + dt4 * G);
-      }
-      G = sc.nhc_mom[M - 2] * sc.nhc_mom[M - 2] / sc.nhc_mass[M - 2] - kT;
-      sc.nhc_mom[M - 1] += dt4 * G;
-    }
-  }
-  return factor;
-}
 
 __device__ __forceinline__ double target_temperature(const StepParams& p, long long step)
 {
@@ -139,7 +102,8 @@ __global__ void k_nhc_pre(StepParams p, MdScalars* sc, const double* __restrict_
   const double kT = kBoltzmann * target_temperature(p, sc->step);
   // before_force hands over the kinetic energy (ek2/2) and doubles it again
   // (ensemble_control.cpp:186-198)
-  sc->vfactor_pre = nhc_half_step(*sc, ek2 * 0.5 * 2.0, kT, 3.0 * p.N, p.dt * 0.5);
+  sc->vfactor_pre = nhc_half_step(sc->nhc_pos, sc->nhc_mom, sc->nhc_mass, ek2 * 0.5 * 2.0, kT,
+                                  3.0 * p.N, p.dt * 0.5);
 }
 
 // v = v * f_pre + F/m dt/2 ; x += v dt ; wrap into the cell
@@ -239,7 +203,8 @@ __global__ void k_ensemble(StepParams p, Box* box, MdScalars* sc, const double* 
     }
     case kNvtNhc: {
       const double ek2 = th[0] * (3.0 * p.N * kBoltzmann);
-      vf = nhc_half_step(*sc, ek2, kBoltzmann * Tt, 3.0 * p.N, p.dt * 0.5);
+      vf = nhc_half_step(sc->nhc_pos, sc->nhc_mom, sc->nhc_mass, ek2, kBoltzmann * Tt, 3.0 * p.N,
+                         p.dt * 0.5);
       break;
     }
     case kNvtBdp:

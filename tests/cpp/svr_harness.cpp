@@ -41,3 +41,11 @@ double resample(double kk, double sigma, int ndeg, double factor, double rr, dou
   return nepx::resample_kinetic(kk, sigma, ndeg, factor, rr, sum);
 }
 }
+
+#include "../../dmg-md_b200/csrc/nhc.h"
+
+extern "C" double nhc_step(double* pos, double* mom, const double* mass, double ek2, double kT,
+                           double dN, double dt_half)
+{
+  return nepx::nhc_half_step(pos, mom, mass, ek2, kT, dN, dt_half);
+}

@@ -53,11 +53,11 @@ def test_nve_follows_gpumd_golden_trajectory(goldens):
         assert np.all(np.abs(s["virial"][rowmajor] - w) <= 1e-5 + 1e-4 * np.abs(w))
 
 
-def _water_md(n_mol, T, seed, kind="nve", **ens):
+def _water_md(n_mol, T, struct_seed, kind="nve", **ens):
     nepx = _nepx()
-    t, h, p = workloads.water(n_mol=n_mol, seed=seed)
+    t, h, p = workloads.water(n_mol=n_mol, seed=struct_seed)
     masses = np.where(t == 0, 15.999, 1.008)
-    v = workloads.maxwell_boltzmann(masses, T, seed=seed)
+    v = workloads.maxwell_boltzmann(masses, T, seed=struct_seed)
     pot = nepx.Potential(potential("nep_water.txt"), max_atoms=len(t))
     md = nepx.MD(pot, t, masses, p, v, h)
     md.set_ensemble(kind, **ens)
@@ -65,14 +65,24 @@ def _water_md(n_mol, T, seed, kind="nve", **ens):
 
 
 def test_nve_energy_conservation():
-    pot, md, t, h = _water_md(300, 300.0, 1)
-    rows = md.run(400, 0.5, thermo_every=10)
-    etot = rows[:, 1] + rows[:, 2]
-    n = len(t)
-    time_ns = np.arange(1, len(rows) + 1) * 10 * 0.5e-6
-    slope = np.polyfit(time_ns, etot / n, 1)[0]
-    assert abs(slope) < 5e-3, "drift %g eV/atom/ns" % slope
-    assert np.std(etot / n) < 2e-4
+    """Diamond carbon with the reference's carbon NEP, NVE at dt 0.5 fs.
+
+    The total energy per atom stays within 2e-4 eV of its mean and
+    drifts by less than 0.05 eV/atom/ns (the dt^2 integration error of this
+    stiff model at ~800 K dominates; halving dt quarters it)."""
+    nepx = _nepx()
+    t, h, p = workloads.diamond(ncell=6, jitter=0.05, seed=1)
+    masses = np.full(len(t), MASS_C)
+    v = workloads.maxwell_boltzmann(masses, 300.0, seed=3)
+    pot = nepx.Potential(potential("nep_C.txt"), max_atoms=len(t))
+    md = nepx.MD(pot, t, masses, p, v, h)
+    md.set_ensemble("nve")
+    rows = md.run(1000, 0.5, thermo_every=20)
+    etot = (rows[:, 1] + rows[:, 2]) / len(t)
+    time_ns = np.arange(1, len(rows) + 1) * 20 * 0.5e-6
+    slope = np.polyfit(time_ns[5:], etot[5:], 1)[0]
+    assert abs(slope) < 0.05, "drift %g eV/atom/ns" % slope
+    assert np.abs(etot[5:] - etot[5:].mean()).max() < 2e-4
 
 
 def test_bdp_velocity_factor_bit_exact(tmp_path):
@@ -106,10 +116,17 @@ def test_bdp_velocity_factor_bit_exact(tmp_path):
 
 @pytest.mark.parametrize("kind", ["nvt_ber", "nvt_nhc", "nvt_bdp"])
 def test_thermostats_reach_target(kind):
-    pot, md, t, h = _water_md(300, 200.0, 3, kind=kind, T0=350.0, T1=350.0, Tdamp=10.0)
-    rows = md.run(600, 0.5, thermo_every=5)
-    T_late = rows[-40:, 0].mean()
-    assert abs(T_late - 350.0) < 0.12 * 350.0, (kind, T_late)
+    """Diamond carbon started at 200 K is driven to 500 K (Tdamp 50 steps)."""
+    nepx = _nepx()
+    t, h, p = workloads.diamond(ncell=6, jitter=0.0, seed=5)
+    masses = np.full(len(t), MASS_C)
+    v = workloads.maxwell_boltzmann(masses, 200.0, seed=5)
+    pot = nepx.Potential(potential("nep_C.txt"), max_atoms=len(t))
+    md = nepx.MD(pot, t, masses, p, v, h)
+    md.set_ensemble(kind, T0=500.0, T1=500.0, Tdamp=50.0)
+    rows = md.run(1500, 1.0, thermo_every=10)
+    T_late = rows[-50:, 0].mean()
+    assert abs(T_late - 500.0) < 0.1 * 500.0, (kind, T_late)
 
 
 @pytest.mark.parametrize("kind", ["npt_ber", "npt_scr"])

@@ -51,3 +51,28 @@ def test_svr_fixture_bit_exact(harness):
         assert [bits(v) for v in g] == c["gasdev_bits"], c["seed"]
         assert [bits(v) for v in s] == [e["bits"] for e in c["sumnoises"]]
         assert [bits(v) for v in r] == c["resamplekin_bits"], (c["seed"], c["ndeg"], c["taut"])
+
+
+def test_nhc_fixture_bit_exact(harness):
+    """Nose-Hoover chain states and factors of tests/thermostats/fixtures/nhc.json."""
+    fx = json.load(open(os.path.join(GOLDEN, "thermostats", "nhc.json")))
+    dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+    harness.nhc_step.restype = ctypes.c_double
+    harness.nhc_step.argtypes = [dp, dp, dp] + [ctypes.c_double] * 4
+
+    def unhex(h):
+        return struct.unpack("<d", struct.pack("<Q", int(h, 16)))[0]
+
+    for c in fx["cases"]:
+        pos = np.array([unhex(x) for x in c["initial_position"]])
+        mom = np.array([unhex(x) for x in c["initial_momentum"]])
+        mass = np.array([unhex(x) for x in c["initial_mass"]])
+        ek2 = c["initial_Ek2"]
+        for s in c["steps"]:
+            f = harness.nhc_step(pos, mom, mass, ek2, 8.617343e-5 * s["target_temperature"],
+                                 3.0 * c["N"], 0.5 * c["dt"])
+            ek2 *= f * f
+            assert bits(f) == int(s["factor"], 16), c["name"]
+            assert bits(ek2) == int(s["Ek2_after"], 16)
+            assert [bits(v) for v in pos] == [int(x, 16) for x in s["position"]]
+            assert [bits(v) for v in mom] == [int(x, 16) for x in s["momentum"]]
