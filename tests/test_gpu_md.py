@@ -123,9 +123,9 @@ def test_thermostats_reach_target(kind):
     v = workloads.maxwell_boltzmann(masses, 200.0, seed=5)
     pot = nepx.Potential(potential("nep_C.txt"), max_atoms=len(t))
     md = nepx.MD(pot, t, masses, p, v, h)
-    md.set_ensemble(kind, T0=500.0, T1=500.0, Tdamp=50.0)
-    rows = md.run(1500, 1.0, thermo_every=10)
-    T_late = rows[-50:, 0].mean()
+    md.set_ensemble(kind, T0=500.0, T1=500.0, Tdamp=20.0)
+    rows = md.run(4000, 1.0, thermo_every=10)
+    T_late = rows[-200:, 0].mean()   # a Nose-Hoover chain oscillates about the target
     assert abs(T_late - 500.0) < 0.1 * 500.0, (kind, T_late)
 
 
