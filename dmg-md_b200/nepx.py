@@ -31,7 +31,7 @@ EXPORTED = ["nepx_create", "nepx_destroy", "nepx_last_error", "nepx_info", "nepx
             "nepx_notify_box_changed", "nepx_set_skin", "nepx_neighbors", "nepx_neighbor_stats",
             "nepx_md_create", "nepx_md_destroy", "nepx_md_last_error", "nepx_md_set_ensemble",
             "nepx_md_run", "nepx_md_get", "nepx_md_device_state", "nepx_profile",
-            "nepx_md_run_async", "nepx_md_sync"]
+            "nepx_md_run_async", "nepx_md_sync", "nepx_compute_noalloc"]
 
 ENSEMBLES = {"nve": 0, "nvt_ber": 1, "nvt_nhc": 2, "nvt_bdp": 3, "npt_ber": 4, "npt_scr": 5}
 THERMO_COLUMNS = ["T", "KE", "PE", "sxx", "syy", "szz", "syz", "sxz", "sxy", "ax", "ay", "az",
@@ -83,6 +83,8 @@ def lib():
         L.nepx_md_set_ensemble.argtypes = [vp, ctypes.c_int, dp, ctypes.c_uint]
         L.nepx_md_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, dp]
         L.nepx_md_get.argtypes = [vp, dp, dp, dp, dp, dp, ctypes.POINTER(Box)]
+        L.nepx_compute_noalloc.argtypes = [vp, ctypes.POINTER(Box), ctypes.c_int, vp, vp, vp, vp,
+                                           vp, vp]
         L.nepx_md_run_async.argtypes = [vp, ctypes.c_int, ctypes.c_double]
         L.nepx_md_sync.argtypes = [vp]
         L.nepx_profile.argtypes = [vp, ctypes.POINTER(Box), ctypes.c_int, vp, vp, vp, vp, vp,

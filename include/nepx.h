@@ -85,6 +85,28 @@ int nepx_compute(nepx_t* handle, const nepx_box* box, int n, const int* d_type,
                  const double* d_pos, double* d_pe, double* d_force, double* d_virial,
                  unsigned flags, void* stream);
 
+/*
+ * nepx_compute for callers that cannot allocate device memory while they run:
+ * codes whose start-up hands all device memory to their own pool allocator,
+ * and real-time or safety-reviewed drivers that forbid allocator calls after
+ * initialisation.  This call allocates nothing (no cudaMalloc, cudaFree or
+ * allocating library routine): all per-call scratch comes from one 16 MiB
+ * static device array inside the library, held by every GPU that loads it
+ * until the process exits.  n is limited by what fits in those 16 MiB for
+ * the handle's neighbour capacities (about 5 KB per atom for MN_radial 250:
+ * some 2,500-3,000 atoms); larger n returns NEPX_ERR_CAPACITY.  The handle
+ * (nepx_create, max_atoms may be 1) supplies only the model parameters.
+ * The first call on a device resolves the array's device address; make it
+ * before any stream capture.  Calls share the array: neighbour rows are
+ * rebuilt and flags cleared on every call, and calls that overlap on the
+ * GPU race.  Synchronises `stream`.  Arguments and outputs as nepx_compute
+ * (outputs overwritten).
+ * This entry point has no counterpart in the reference.
+ */
+int nepx_compute_noalloc(nepx_t* handle, const nepx_box* box, int n, const int* d_type,
+                         const double* d_pos, double* d_pe, double* d_force, double* d_virial,
+                         void* stream);
+
 /* Forces a Verlet rebuild at the next compute.  Replaces
  * NEP::notify_box_changed (src/gpumd_compat/nep.cuh:170). */
 int nepx_notify_box_changed(nepx_t* handle);
