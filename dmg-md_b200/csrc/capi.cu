@@ -140,6 +140,7 @@ int nepx_compute(nepx_t* h, const nepx_box* box, int n, const int* d_type, const
   nepx::launch_set_box(e, b, s);
   e.box_owner = nullptr;
   nepx::launch_neighbor_update(e, n, d_pos, d_type, rebuild, s);
+  if (!e.tuned) nepx::engine_autotune(e, n, d_pos, d_type, s);
   nepx::launch_force(e, n, d_pos, d_type, d_pe, d_force, d_virial,
                      (flags & NEPX_ACCUMULATE) != 0, s);
   if (cudaPeekAtLastError() != cudaSuccess) return cuda_fail(h, "kernel launch");

@@ -88,6 +88,28 @@ __device__ __forceinline__ void displacement(const Box& b, const double* __restr
   mic_f32(b, dx, dy, dz);
 }
 
+// One atom as the neighbour sweeps read it: position and type in one
+// 32-byte record (one sector), repacked from the SoA inputs at every force
+// call.  The SoA layout would touch four cache lines per neighbour.
+struct __align__(32) Site {
+  double x, y, z;
+  long long type;
+};
+
+// Displacement to site j and j's type, same arithmetic as displacement().
+__device__ __forceinline__ void site_displacement(const Box& b, const Site* __restrict__ sites,
+                                                  double xi, double yi, double zi, int j,
+                                                  float& dx, float& dy, float& dz, int& tj)
+{
+  const double2 a = __ldg(reinterpret_cast<const double2*>(sites + j));
+  const double2 c = __ldg(reinterpret_cast<const double2*>(sites + j) + 1);
+  dx = a.x - xi;
+  dy = a.y - yi;
+  dz = c.x - zi;
+  tj = static_cast<int>(__double_as_longlong(c.y));
+  mic_f32(b, dx, dy, dz);
+}
+
 // Cutoff function fc = (1 + cos(pi d / rc)) / 2 and its d-derivative.
 __device__ __forceinline__ void cutoff_fc(float rc, float rcinv, float d, float& fc, float& fcp)
 {

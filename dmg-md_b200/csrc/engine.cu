@@ -1,6 +1,8 @@
 // engine.cu -- handle construction, device uploads and box handling.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "engine.h"
@@ -8,8 +10,6 @@
 namespace nepx {
 
 void upload_invariant_tables();
-size_t descriptor_smem_bytes(const ModelParams& p);
-void set_descriptor_smem_limit(size_t bytes);
 
 namespace {
 
@@ -157,9 +157,12 @@ std::string engine_create(Engine& e, const std::string& nep_path, int max_atoms)
   ok &= dalloc(nb.cell_atoms, N) == cudaSuccess;
   ok &= dalloc(nb.cell_of, N) == cudaSuccess;
   ok &= dalloc(nb.x0, 3 * static_cast<size_t>(N)) == cudaSuccess;
-  ok &= dalloc(e.scratch.fp_rad, static_cast<size_t>(N) * p.nR) == cudaSuccess;
+  ok &= dalloc(e.scratch.sites, N) == cudaSuccess;
+  ok &= dalloc(e.scratch.alpha, static_cast<size_t>(N) * p.T * basis_stride(p)) == cudaSuccess;
   ok &= dalloc(e.scratch.f12, static_cast<size_t>(N) * nb.mn_a) == cudaSuccess;
   ok &= dalloc(e.scratch.pe_ann, N) == cudaSuccess;
+  ok &= dalloc(e.scratch.acoef, static_cast<size_t>(N) * p.nA * kNumLM) == cudaSuccess;
+  ok &= dalloc(e.scratch.tune_out, 13 * static_cast<size_t>(N)) == cudaSuccess;
   ok &= dalloc(e.d_box, 1) == cudaSuccess;
   ok &= dalloc(e.d_nstate, 1) == cudaSuccess;
   if (!ok) return "cudaMalloc failed (per-atom buffers)";
@@ -168,11 +171,65 @@ std::string engine_create(Engine& e, const std::string& nep_path, int max_atoms)
   if (cudaMemcpy(e.d_nstate, &init, sizeof(init), cudaMemcpyHostToDevice) != cudaSuccess)
     return "cudaMemcpy failed (neighbour state)";
   if (cudaMemset(nb.nn_a, 0, sizeof(int) * N) != cudaSuccess) return "cudaMemset failed";
-  e.smem_desc = descriptor_smem_bytes(p);
-  if (e.smem_desc > 227 * 1024) return "descriptor kernel needs more shared memory than a CTA has";
-  set_descriptor_smem_limit(e.smem_desc);
+  if (fused_smem_bytes(p, 4) > 227 * 1024)
+    return "descriptor kernel needs more shared memory than a CTA has (not supported)";
+  set_fused_smem_limits(p);
   if (cudaGetLastError() != cudaSuccess) return "CUDA error during setup";
   return "";
+}
+
+void engine_autotune(Engine& e, int N, const double* pos, const int* type, cudaStream_t stream)
+{
+  // candidate lanes per center; each variant runs 3 times, the median counts
+  const int groups[2] = {4, 8};
+  float best_f = 1e30f, best_g = 1e30f;
+  int pick_f = e.group, pick_g = e.gather_group;
+  cudaEvent_t a, b, c;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  cudaEventCreate(&c);
+  int pick_a = e.f12_group;
+  for (int gf : groups) {
+    for (int gg : groups) {
+      e.group = gf;
+      e.f12_group = gg;   // angular-force grouping varies together with the gather's
+      e.gather_group = gg;
+      float tf[3], tg[3];
+      for (int r = 0; r < 3; ++r) {
+        cudaEventRecord(a, stream);
+        launch_descriptor(e, N, pos, type, stream);
+        cudaEventRecord(b, stream);
+        double* out = e.scratch.tune_out;   // 13 N doubles: pe, force, virial
+        launch_gather(e, N, pos, type, out, out + N, out + 4 * static_cast<size_t>(N), false,
+                      stream);
+        cudaEventRecord(c, stream);
+        cudaEventSynchronize(c);
+        cudaEventElapsedTime(&tf[r], a, b);
+        cudaEventElapsedTime(&tg[r], b, c);
+      }
+      std::sort(tf, tf + 3);
+      std::sort(tg, tg + 3);
+      if (tf[1] < best_f) {
+        best_f = tf[1];
+        pick_f = gf;
+        pick_a = gg;
+      }
+      if (tg[1] < best_g) {
+        best_g = tg[1];
+        pick_g = gg;
+      }
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaEventDestroy(c);
+  e.group = pick_f;
+  e.f12_group = pick_a;
+  e.gather_group = pick_g;
+  e.tuned = true;
+  if (std::getenv("NEPX_VERBOSE"))
+    std::fprintf(stderr, "nepx autotune (N=%d): fused G=%d, angular-force G=%d, gather G=%d\n", N,
+                 e.group, e.f12_group, e.gather_group);
 }
 
 void engine_destroy(Engine& e)
@@ -180,7 +237,8 @@ void engine_destroy(Engine& e)
   NeighborBuffers& nb = e.nbr;
   void* ptrs[] = {e.d_params, e.d_box, e.d_nstate, nb.nn_v, nb.nl_v, nb.nn_r, nb.nl_r,
                   nb.nn_a, nb.nl_a, nb.cell_count, nb.cell_start, nb.cell_atoms, nb.cell_of,
-                  nb.x0, e.scratch.fp_rad, e.scratch.f12, e.scratch.pe_ann, e.scratch.q};
+                  nb.x0, e.scratch.alpha, e.scratch.f12, e.scratch.pe_ann, e.scratch.q,
+                  e.scratch.tune_out, e.scratch.acoef, e.scratch.sites};
   for (void* q : ptrs)
     if (q) cudaFree(q);
 }

@@ -28,10 +28,13 @@ struct NeighborBuffers {
 };
 
 struct ForceScratch {
-  float* fp_rad = nullptr;   // [N][nR] dE/dq of the radial descriptors (scaled)
+  Site* sites = nullptr;     // [N] position + type records, packed by the skin check
+  float* alpha = nullptr;    // [N][T][kp] radial force coefficients sum_n dE/dq_n c(ti,t)[n][k]
   float4* f12 = nullptr;     // [N][mn_a] directed angular partial forces
+  float* acoef = nullptr;    // [N][nA][24] dE/ds[n][lm] of each center
   double* pe_ann = nullptr;  // [N] site energy of the ANN
   float* q = nullptr;        // [N][dim] descriptors (mixed-precision path)
+  double* tune_out = nullptr;  // [13 N] throw-away outputs of the autotuning calls
 };
 
 struct Engine {
@@ -53,9 +56,22 @@ struct Engine {
   bool force_rebuild = true;
   const void* box_owner = nullptr;   // md whose box the device copy holds (nullptr: none)
   int last_n = -1;
-  size_t smem_desc = 0;      // dynamic shared memory of the descriptor kernel
+  int group = 4;             // lanes per center in the fused kernel (autotuned)
+  int f12_group = 4;         // lanes per center in the angular-force kernel (autotuned)
+  int gather_group = 8;      // lanes per center in the gather (autotuned)
+  bool tuned = false;
   std::string error;
 };
+
+// Padded basis width of the kernel instance serving this model (row stride
+// of the shared-memory coefficient tables and of ForceScratch::alpha).
+int basis_stride(const ModelParams& p);
+size_t fused_smem_bytes(const ModelParams& p, int group);
+void set_fused_smem_limits(const ModelParams& p);
+
+// Times each kernel variant on the given system (a few calls each, stream
+// synchronised) and keeps the fastest.  Neighbour rows must be current.
+void engine_autotune(Engine& e, int N, const double* pos, const int* type, cudaStream_t stream);
 
 // Loads the potential, uploads it and sizes every buffer for max_atoms.
 std::string engine_create(Engine& e, const std::string& nep_path, int max_atoms);
@@ -70,7 +86,9 @@ bool large_box_ok(const Engine& e, const Box& b);
 // Writes the box to the device copy in stream order.
 void launch_set_box(Engine& e, const Box& b, cudaStream_t stream);
 
-// Skin check, conditional Verlet rebuild and typewise filter.
+// Site packing, skin check and conditional Verlet rebuild.  The force
+// launches read positions and types from the packed sites, so every force
+// launch follows a neighbour update at the same positions.
 void launch_neighbor_update(Engine& e, int N, const double* pos, const int* type, bool force,
                             cudaStream_t stream);
 

@@ -552,6 +552,7 @@ int md_enqueue_run(nepx_md* m, int steps, double dt_fs, int thermo_every, double
   nepx::md_init_scalars(md, p, c.T0, p.dt * c.Tdamp);
   if (!md.forces_valid) {
     nepx::launch_neighbor_update(e, N, md.d_pos, md.d_type, true, s);
+    if (!e.tuned) nepx::engine_autotune(e, N, md.d_pos, md.d_type, s);
     nepx::launch_force(e, N, md.d_pos, md.d_type, md.d_pe, md.d_force, md.d_virial, false, s);
     md.forces_valid = true;
   }

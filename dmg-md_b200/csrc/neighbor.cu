@@ -15,6 +15,7 @@
 // at least (rc + skin)/2 wide with a 5x5x5 stencil; each Verlet row is sorted
 // in shared memory, which makes every later sum over neighbours ordered and
 // bitwise reproducible.
+#include <algorithm>
 #include <climits>
 
 #include "engine.h"
@@ -42,30 +43,35 @@ __device__ __forceinline__ void cell_coords(const Box& b, const NeighborState& s
   cz = wrapped_cell(sz, st.nc[2], b.pbc[2]);
 }
 
-// Marks a rebuild when forced or when an atom moved more than skin/2
-// (reference neighbor.cu:446-533, without the host round trip).  Under an
-// isotropic box scaling s since the build (x0 scaled along, so displacements
-// are co-moving) a pair distance also drifts by up to |1 - s| (rc + skin),
-// which shrinks the allowed displacement to (skin - |1 - s| (rc + skin)) / 2.
+// Packs each atom into its Site record for the neighbour sweeps of this
+// step, and marks a rebuild when forced or when an atom moved more than
+// skin/2 (reference neighbor.cu:446-533, without the host round trip).  Under
+// an isotropic box scaling s since the build (x0 scaled along, so
+// displacements are co-moving) a pair distance also drifts by up to
+// |1 - s| (rc + skin), which shrinks the allowed displacement to
+// (skin - |1 - s| (rc + skin)) / 2.
 __global__ void k_skin_check(int N, const Box* __restrict__ box, const double* __restrict__ pos,
-                             const double* __restrict__ x0, NeighborState* st, double skin,
+                             const int* __restrict__ type, const double* __restrict__ x0,
+                             NeighborState* st, Site* __restrict__ sites, double skin,
                              double rc_v, int force)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const double xi = pos[i], yi = pos[N + i], zi = pos[2 * N + i];
+  sites[i] = Site{xi, yi, zi, static_cast<long long>(type[i])};
   if (force) {
     if (i == 0) st->rebuild = 1;
     return;
   }
-  if (i >= N) return;
   const double half = 0.5 * (skin - fabs(1.0 - st->box_scale) * rc_v);
   if (half <= 0.0) {
     st->rebuild = 1;
     return;
   }
   const double half_skin_sq = half * half;
-  float dx = pos[i] - x0[i];
-  float dy = pos[N + i] - x0[N + i];
-  float dz = pos[2 * N + i] - x0[2 * N + i];
+  float dx = xi - x0[i];
+  float dy = yi - x0[N + i];
+  float dz = zi - x0[2 * N + i];
   mic_f32(*box, dx, dy, dz);
   if ((dx * dx + dy * dy + dz * dz) > half_skin_sq) st->rebuild = 1;
 }
@@ -162,7 +168,7 @@ __global__ void k_cell_fill(int N, const NeighborState* __restrict__ st, const i
 // One warp per center: gathers every candidate of the 5x5x5 stencil with
 // float d^2 < (rc + skin)^2, sorts the row in shared memory (bitonic), and
 // writes it with the reference positions for the next skin check.
-__global__ void k_verlet_build(int N, const Box* __restrict__ box, const double* __restrict__ pos,
+__global__ void k_verlet_build(int N, const Box* __restrict__ box, const Site* __restrict__ sites,
                                NeighborState* st, const int* __restrict__ cell_count,
                                const int* __restrict__ cell_start, const int* __restrict__ cell_atoms,
                                const int* __restrict__ cell_of, int* nn_v, int* nl_v, int mn_v,
@@ -172,17 +178,14 @@ __global__ void k_verlet_build(int N, const Box* __restrict__ box, const double*
   if (!st->rebuild) return;
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  const int i = blockIdx.x * (blockDim.x >> 5) + warp;
-  if (i >= N) return;
+  const int wpb = blockDim.x >> 5;
   int* buf = s_rows + warp * (pow2 + 1);
   int* count = buf + pow2;
+  const Box b = *box;
+  for (int i = blockIdx.x * wpb + warp; i < N; i += gridDim.x * wpb) {
   if (lane == 0) *count = 0;
   __syncwarp();
-  const Box b = *box;
-  const double* x = pos;
-  const double* y = pos + N;
-  const double* z = pos + 2 * N;
-  const double xi = x[i], yi = y[i], zi = z[i];
+  const double xi = sites[i].x, yi = sites[i].y, zi = sites[i].z;
   const int nc0 = st->nc[0], nc1 = st->nc[1], nc2 = st->nc[2];
   const int ci = cell_of[i];
   const int cx = ci % nc0, cy = (ci / nc0) % nc1, cz = ci / (nc0 * nc1);
@@ -207,7 +210,8 @@ __global__ void k_verlet_build(int N, const Box* __restrict__ box, const double*
       const int j = cell_atoms[start + m];
       if (j == i) continue;
       float dx, dy, dz;
-      displacement(b, x, y, z, xi, yi, zi, j, dx, dy, dz);
+      int tj;
+      site_displacement(b, sites, xi, yi, zi, j, dx, dy, dz, tj);
       const float d2 = dx * dx + dy * dy + dz * dz;
       if (d2 < cutoff_square) {
         const int slot = atomicAdd(count, 1);
@@ -247,68 +251,7 @@ __global__ void k_verlet_build(int N, const Box* __restrict__ box, const double*
     x0[N + i] = yi;
     x0[2 * N + i] = zi;
   }
-}
-
-// One warp per center: typewise radial / angular rows from the Verlet row,
-// order preserved (reference nep.cu:503-561, same float predicate).
-__global__ void k_filter(int N, const Box* __restrict__ box, const double* __restrict__ pos,
-                         const int* __restrict__ type, const float* __restrict__ rc_r,
-                         const float* __restrict__ rc_a, NeighborState* st,
-                         const int* __restrict__ nn_v, const int* __restrict__ nl_v, int mn_v,
-                         int* nn_r, int* nl_r, int mn_r, int* nn_a, int* nl_a, int mn_a)
-{
-  const int lane = threadIdx.x & 31;
-  const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (blockIdx.x == 0 && threadIdx.x == 0) st->rebuild = 0;
-  if (i >= N) return;
-  const Box b = *box;
-  const double* x = pos;
-  const double* y = pos + N;
-  const double* z = pos + 2 * N;
-  const double xi = x[i], yi = y[i], zi = z[i];
-  const int t1 = type[i];
-  const float rr1 = rc_r[t1], ra1 = rc_a[t1];
-  const int nv = nn_v[i];
-  const int* vrow = nl_v + static_cast<size_t>(i) * mn_v;
-  int* rrow = nl_r + static_cast<size_t>(i) * mn_r;
-  int* arow = nl_a + static_cast<size_t>(i) * mn_a;
-  int cr = 0, ca = 0;
-  for (int base = 0; base < nv; base += 32) {
-    const int k = base + lane;
-    bool in_r = false, in_a = false;
-    int j = 0;
-    if (k < nv) {
-      j = vrow[k];
-      float x12, y12, z12;
-      displacement(b, x, y, z, xi, yi, zi, j, x12, y12, z12);
-      const float d12_square = x12 * x12 + y12 * y12 + z12 * z12;
-      const int t2 = type[j];
-      const float rc_radial = (rr1 + rc_r[t2]) * 0.5f;
-      const float rc_angular = (ra1 + rc_a[t2]) * 0.5f;
-      in_r = d12_square < rc_radial * rc_radial;
-      in_a = in_r && d12_square < rc_angular * rc_angular;
-    }
-    const unsigned mr = __ballot_sync(0xffffffffu, in_r);
-    const unsigned ma = __ballot_sync(0xffffffffu, in_a);
-    const unsigned below = (1u << lane) - 1u;
-    if (in_r) {
-      const int slot = cr + __popc(mr & below);
-      if (slot < mn_r) rrow[slot] = j;
-    }
-    if (in_a) {
-      const int slot = ca + __popc(ma & below);
-      if (slot < mn_a) arow[slot] = j;
-    }
-    cr += __popc(mr);
-    ca += __popc(ma);
-  }
-  if (lane == 0) {
-    nn_r[i] = min(cr, mn_r);
-    nn_a[i] = min(ca, mn_a);
-    if (cr > mn_r) atomicOr(&st->overflow, 2);
-    if (ca > mn_a) atomicOr(&st->overflow, 4);
-    atomicMax(&st->max_nn[1], cr);
-    atomicMax(&st->max_nn[2], ca);
+  __syncwarp();   // the row buffer is reused by this warp's next center
   }
 }
 
@@ -322,8 +265,8 @@ void launch_neighbor_update(Engine& e, int N, const double* pos, const int* type
   const int grid = (N + threads - 1) / threads;
   const float rc_v = e.model.rc_max + static_cast<float>(e.skin);
   const double rc_v_d = static_cast<double>(e.model.rc_max) + e.skin;
-  k_skin_check<<<force ? 1 : grid, threads, 0, stream>>>(N, e.d_box, pos, nb.x0, e.d_nstate,
-                                                         e.skin, rc_v_d, force ? 1 : 0);
+  k_skin_check<<<grid, threads, 0, stream>>>(N, e.d_box, pos, type, nb.x0, e.d_nstate,
+                                              e.scratch.sites, e.skin, rc_v_d, force ? 1 : 0);
   k_cell_setup<<<1, 1024, 0, stream>>>(e.d_box, e.d_nstate, nb.cell_count, rc_v_d, nb.cell_cap);
   k_cell_count<<<grid, threads, 0, stream>>>(N, e.d_box, pos, e.d_nstate, nb.cell_of,
                                              nb.cell_count);
@@ -331,16 +274,16 @@ void launch_neighbor_update(Engine& e, int N, const double* pos, const int* type
   k_cell_fill<<<grid, threads, 0, stream>>>(N, e.d_nstate, nb.cell_of, nb.cell_count,
                                             nb.cell_start, nb.cell_atoms);
   // cell counts were consumed as cursors; they now hold the per-cell totals again
+  // a grid of at most 16 CTAs per SM walks all centers, so the launch is
+  // cheap on the (common) steps whose skin check found nothing to rebuild
   const int warps = 4;
   const size_t smem = static_cast<size_t>(warps) * (nb.pow2_v + 1) * sizeof(int);
-  k_verlet_build<<<(N + warps - 1) / warps, warps * 32, smem, stream>>>(
-    N, e.d_box, pos, e.d_nstate, nb.cell_count, nb.cell_start, nb.cell_atoms, nb.cell_of,
+  const int vblocks = std::min((N + warps - 1) / warps, 148 * 16);
+  k_verlet_build<<<vblocks, warps * 32, smem, stream>>>(
+    N, e.d_box, e.scratch.sites, e.d_nstate, nb.cell_count, nb.cell_start, nb.cell_atoms, nb.cell_of,
     nb.nn_v, nb.nl_v, nb.mn_v, nb.pow2_v, static_cast<float>(rc_v_d * rc_v_d), nb.x0);
   (void)rc_v;
-  const int fw = 8;
-  k_filter<<<(N + fw - 1) / fw, fw * 32, 0, stream>>>(
-    N, e.d_box, pos, type, e.d_rc_r, e.d_rc_a, e.d_nstate, nb.nn_v, nb.nl_v, nb.mn_v, nb.nn_r,
-    nb.nl_r, nb.mn_r, nb.nn_a, nb.nl_a, nb.mn_a);
+  // the typewise radial / angular filter runs inside the fused force kernel
 }
 
 }  // namespace nepx

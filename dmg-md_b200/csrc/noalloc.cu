@@ -89,9 +89,11 @@ size_t bytes_needed(const nepx::Engine& e, int n)
   c.take<int>(N);               // cell_atoms
   c.take<int>(N);               // cell_of
   c.take<double>(3 * N);        // x0
-  c.take<float>(N * e.params.nR);
+  c.take<nepx::Site>(N);
+  c.take<float>(N * e.params.T * nepx::basis_stride(e.params));
   c.take<float4>(N * nb.mn_a);
   c.take<double>(N);
+  c.take<float>(N * e.params.nA * nepx::kNumLM);
   return c.used;
 }
 
@@ -143,10 +145,13 @@ extern "C" int nepx_compute_noalloc(nepx_t* h, const nepx_box* box, int n, const
   nb.cell_of = c.take<int>(N);
   nb.x0 = c.take<double>(3 * N);
   nb.cell_cap = static_cast<int>(cells);
-  view.scratch.fp_rad = c.take<float>(N * view.params.nR);
+  view.scratch.sites = c.take<nepx::Site>(N);
+  view.scratch.alpha = c.take<float>(N * view.params.T * nepx::basis_stride(view.params));
   view.scratch.f12 = c.take<float4>(N * nb.mn_a);
   view.scratch.pe_ann = c.take<double>(N);
+  view.scratch.acoef = c.take<float>(N * view.params.nA * nepx::kNumLM);
   view.capacity = n;
+  view.tuned = true;   // keeps the handle's kernel variants; no timing runs here
   auto s = static_cast<cudaStream_t>(stream);
   // the handle's pinned flag mirror may still receive a copy from an earlier
   // nepx_compute; let it land before this call reuses the mirror

@@ -142,14 +142,23 @@ def test_npt_box_moves_and_lists_stay_complete(kind):
         pc = 1.0 / (3.0 * 50.0 * 2.0)
         p_inst = rows[:, 3:6].mean(axis=1)
         np.testing.assert_allclose(rows[:, 19], 1.0 - pc * (0.5 - p_inst), rtol=0, atol=1e-12)
-    # the Verlet list kept across box rescalings must give the same forces as
-    # a freshly built one at the same positions and box
+    # the Verlet list kept across box rescalings must yield exactly the
+    # typewise rows a freshly built list yields at the same positions and box;
+    # forces then agree to rounding (the lane that sums a radial edge follows
+    # its slot in the Verlet row, which differs between the two lists)
     md.set_ensemble("nve")
     md.run(1, 0.0)
+    md.sync()
     s = md.state()
-    fresh = nepx.Potential(potential("nep_water.txt"), max_atoms=len(t))
+    kept = [pot.neighbors(w, len(t)) for w in (0, 1)]
     tt = torch.as_tensor(t, device="cuda")
     pp = torch.as_tensor(np.ascontiguousarray(s["pos"]), device="cuda")
-    pe, f, w = fresh.compute(tt, s["h"], pp, sync_check=True)
-    assert np.array_equal(f.cpu().numpy(), s["force"])
-    assert np.array_equal(pe.cpu().numpy(), s["pe"])
+    pot.notify_box_changed()
+    pe, f, w = pot.compute(tt, s["h"], pp, sync_check=True)
+    fresh = [pot.neighbors(w_, len(t)) for w_ in (0, 1)]
+    for a, b in zip(kept, fresh):
+        for i in range(len(t)):
+            assert np.array_equal(a[i], b[i]), i
+    f = f.cpu().numpy()
+    assert np.linalg.norm(f - s["force"]) / np.linalg.norm(f) < 1e-6
+    assert np.abs(pe.cpu().numpy() - s["pe"]).max() < 1e-5
