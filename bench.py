@@ -51,6 +51,9 @@ import numpy as np  # noqa: E402
 import workloads  # noqa: E402
 
 K_B = 8.617343e-5
+# DRAM bytes per force call of the descriptor stage from the committed ncu
+# captures (profiles/k_nep_fused_water24k.md): k_nep_fused + k_angular_f12
+TRAFFIC = {"water": 20.80e6 + 17.96e6}
 FP32_LANES = 148 * 128          # B200: SMs x FP32 lanes
 SM_MAX_MHZ = 1965.0
 
@@ -186,6 +189,41 @@ def cpu_reference_rate(nep_path, t, h, p, budget_s=8.0, max_reps=5):
                       "median of %d calls, %d threads" % (len(t), len(times), threads)}
 
 
+def gpu_reference_rate(nep_path, t, h, p, reps=50):
+    """The reference's own FP32 GPU NEP (its src/gpumd_compat kernels built for
+    sm_100a, oracle/_ref) on this GPU: force calls on static positions (the
+    Verlet list is built by the first call and kept), CUDA events on the
+    legacy default stream the reference launches on, L2 holding the inputs."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    try:
+        import torch
+    except ImportError:
+        return None
+    if not (oracle.ref_gpu_available() and torch.cuda.is_available()):
+        return None
+    n = len(t)
+    d_type = torch.as_tensor(np.asarray(t, dtype=np.int32), device="cuda")
+    d_pos = torch.as_tensor(np.ascontiguousarray(p, dtype=np.float64), device="cuda")
+    ref = oracle.RefGpuModel(nep_path, n)
+    ref.set_atoms(d_type, d_pos)
+    for _ in range(3):
+        ref.compute(h)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        ref.compute(h)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / reps
+    del ref
+    return {"value": n / (ms / 1e3), "unit": "atom-steps/s", "ms_per_call": ms,
+            "kind": "reference GPU FP32 NEP (its gpumd_compat kernels, sm_100a)",
+            "sample": "%d force calls on %d atoms after 3 warm-up calls, static positions"
+                      % (reps, n)}
+
+
 def run_reference_arm(args, rank):
     if rank != 0:
         return 0
@@ -194,6 +232,7 @@ def run_reference_arm(args, rank):
         path = workloads.write_nep(os.path.join(tmp, "nep.txt"), **spec["nep"])
         t, h, p = build_system(args.workload, seed=1)
         base = cpu_reference_rate(path, t, h, p, budget_s=max(4.0, 0.5 * args.steps))
+        ref_gpu = gpu_reference_rate(path, t, h, p)
     if base is None:
         print(json.dumps({"impl": "reference",
                           "unavailable": "reference NEP3_CPU library oracle/_ref not built"}))
@@ -205,7 +244,8 @@ def run_reference_arm(args, rank):
             "data": "synthetic", "config": {"workload": spec["desc"], "atoms": len(t)},
             "cpu_baseline": base,
             "e2e": {"value": base["value"], "unit": "atom-steps/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+                    "d2h_bytes_per_step": 0},
+            "reference_gpu": ref_gpu}
     print(json.dumps(line))
     return 0
 
@@ -324,9 +364,11 @@ def main():
     desc_flops = fpa * n
     achieved = desc_flops / (prof["descriptor"] * 1e-3) / 1e12
     peak = FP32_LANES * 2 * SM_MAX_MHZ * 1e6 / 1e12
-    roofline = {"bound": "fp32", "kernel": "k_descriptor_ann_f12",
+    roofline = {"bound": "fp32", "kernel": "k_nep_fused + k_angular_f12 (descriptor stage)",
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "traffic": None,
+                "traffic": TRAFFIC.get(args.workload),
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of both "
+                                  "kernels, one launch each (profiles/)",
                 "peak_source": "B200 FP32 FMA peak: 148 SMs x 128 lanes x 2 FLOP x 1965 MHz "
                                "(not in MEASURED_PEAKS.json, which holds HBM and bf16 only)",
                 "flops_per_atom": fpa, "mean_radial_neighbors": mean_r,
@@ -350,6 +392,10 @@ def main():
                            "l2": "flushed by a 512 MiB write before every %d-step chunk" % chunk,
                            "final_temperature_K": T_last},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "force_call": {"value": n / (prof["total"] * 1e-3), "unit": "atom-steps/s",
+                               "ms": prof["total"],
+                               "what": "nepx_compute on the final state, static positions "
+                                       "(neighbour update + descriptor + gather), L2 warm"},
                 "gpu_launches": launches, "clocks": clock_info}
         print(json.dumps(line))
     md.close()
