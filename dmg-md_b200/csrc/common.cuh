@@ -96,18 +96,35 @@ struct __align__(32) Site {
   long long type;
 };
 
-// Displacement to site j and j's type, same arithmetic as displacement().
-__device__ __forceinline__ void site_displacement(const Box& b, const Site* __restrict__ sites,
-                                                  double xi, double yi, double zi, int j,
-                                                  float& dx, float& dy, float& dz, int& tj)
+// A site record as two 16-byte loads: a = (x, y), c = (z, type bits).
+__device__ __forceinline__ void site_load(const Site* __restrict__ sites, int j, double2& a,
+                                          double2& c)
 {
-  const double2 a = __ldg(reinterpret_cast<const double2*>(sites + j));
-  const double2 c = __ldg(reinterpret_cast<const double2*>(sites + j) + 1);
+  a = __ldg(reinterpret_cast<const double2*>(sites + j));
+  c = __ldg(reinterpret_cast<const double2*>(sites + j) + 1);
+}
+
+// Displacement from (xi, yi, zi) to a loaded site and the site's type, same
+// arithmetic as displacement().
+__device__ __forceinline__ void site_delta(const Box& b, const double2& a, const double2& c,
+                                           double xi, double yi, double zi, float& dx, float& dy,
+                                           float& dz, int& tj)
+{
   dx = a.x - xi;
   dy = a.y - yi;
   dz = c.x - zi;
   tj = static_cast<int>(__double_as_longlong(c.y));
   mic_f32(b, dx, dy, dz);
+}
+
+// Displacement to site j and j's type.
+__device__ __forceinline__ void site_displacement(const Box& b, const Site* __restrict__ sites,
+                                                  double xi, double yi, double zi, int j,
+                                                  float& dx, float& dy, float& dz, int& tj)
+{
+  double2 a, c;
+  site_load(sites, j, a, c);
+  site_delta(b, a, c, xi, yi, zi, dx, dy, dz, tj);
 }
 
 // Cutoff function fc = (1 + cos(pi d / rc)) / 2 and its d-derivative.

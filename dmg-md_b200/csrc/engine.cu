@@ -105,7 +105,8 @@ std::string engine_create(Engine& e, const std::string& nep_path, int max_atoms)
     return "descriptor coefficient table too large for shared memory";
 
   upload_invariant_tables();
-  // one parameter allocation: c_pair | w0 | b0 | w1 | out_bias | q_scaler | zbl | rc_r | rc_a
+  // one parameter allocation: c_pair | w0 | b0 | w0t | w1 | out_bias | q_scaler | zbl | rc_r |
+  // rc_a
   std::vector<float> blob;
   auto append = [&blob](const std::vector<float>& v) {
     const size_t at = blob.size();
@@ -113,7 +114,16 @@ std::string engine_create(Engine& e, const std::string& nep_path, int max_atoms)
     while (blob.size() % 4) blob.push_back(0.0f);   // 16-byte aligned blocks
     return at;
   };
+  // w0 transposed for the ANN, rows zero-padded to H4 (float4 over hidden units)
+  p.H4 = (p.H + 3) & ~3;
+  std::vector<float> w0t(static_cast<size_t>(p.T) * p.dim * p.H4, 0.0f);
+  for (int t = 0; t < p.T; ++t)
+    for (int h = 0; h < p.H; ++h)
+      for (int d = 0; d < p.dim; ++d)
+        w0t[(static_cast<size_t>(t) * p.dim + d) * p.H4 + h] =
+          m.w0[(static_cast<size_t>(t) * p.H + h) * p.dim + d];
   const size_t o_c = append(m.c_pair), o_w0 = append(m.w0), o_b0 = append(m.b0);
+  const size_t o_w0t = append(w0t);
   const size_t o_w1 = append(m.w1), o_ob = append(m.out_bias), o_qs = append(m.q_scaler);
   const size_t o_z = append(m.zbl_para.empty() ? std::vector<float>(1, 0.0f) : m.zbl_para);
   const size_t o_rr = append(std::vector<float>(m.rc_radial, m.rc_radial + kMaxTypes));
@@ -124,6 +134,7 @@ std::string engine_create(Engine& e, const std::string& nep_path, int max_atoms)
     return "cudaMemcpy failed (parameters)";
   p.c_pair = e.d_params + o_c;
   p.w0 = e.d_params + o_w0;
+  p.w0t = e.d_params + o_w0t;
   p.b0 = e.d_params + o_b0;
   p.w1 = e.d_params + o_w1;
   p.out_bias = e.d_params + o_ob;

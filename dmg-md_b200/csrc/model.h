@@ -46,6 +46,8 @@ struct ModelParams {
   int Z[kMaxTypes];
   const float* c_pair;
   const float* w0;
+  const float* w0t;   // [T][dim][H4]: w0 transposed, rows zero-padded
+  int H4;
   const float* b0;
   const float* w1;
   const float* out_bias;

@@ -72,11 +72,15 @@ __host__ __device__ inline int round4(int x) { return (x + 3) & ~3; }
 struct FusedLayout {
   int kpr, kpa;        // basis sizes padded to float4
   int c_rad, c_ang;    // coefficient tables [T*T][n][kp]
+  int wt;              // transposed ANN weights [T][dim][H4], or -1: read from global
   int per_atom;        // floats of per-center scratch
-  int s, q, fp, gh;    // offsets inside one center's scratch
+  int s, a, q, fp, gh; // offsets inside one center's scratch
   int atoms_base;      // offset of the per-center scratch
   int total_bytes;
 };
+
+// Shared memory one CTA may use with the ANN weights staged (three CTAs per SM).
+constexpr int kFusedSmemBudget = 72 * 1024;
 
 // kp: row stride of the coefficient tables, the padded basis size of the
 // kernel instance (rows are zero-filled up to it, so float4 dot products of
@@ -90,9 +94,9 @@ __host__ __device__ inline FusedLayout fused_layout(const ModelParams& p, int at
   const int tt = p.T * p.T;
   L.c_rad = 0;
   L.c_ang = L.c_rad + tt * p.nR * L.kpr;
-  L.atoms_base = round4(L.c_ang + tt * p.nA * L.kpa);
   L.s = 0;
-  L.q = p.nA * kNumLM;
+  L.a = p.nA * kNumLM;
+  L.q = 2 * p.nA * kNumLM;
   L.fp = L.q + round4(p.dim);
   L.gh = L.fp + round4(p.dim);
   // per-center stride: 16-byte aligned (float4 reads of the a[n][lm] rows)
@@ -100,7 +104,16 @@ __host__ __device__ inline FusedLayout fused_layout(const ModelParams& p, int at
   // centers start on different banks
   L.per_atom = round4(L.gh + p.H);
   if ((L.per_atom / 4) % 2 == 0) L.per_atom += 4;
+  const int tables = round4(L.c_ang + tt * p.nA * L.kpa);
+  const int wsize = p.T * p.dim * p.H4;
+  L.wt = tables;
+  L.atoms_base = tables + wsize;
   L.total_bytes = 4 * (L.atoms_base + atoms_per_block * L.per_atom);
+  if (L.total_bytes > kFusedSmemBudget) {   // weights stay in global memory
+    L.wt = -1;
+    L.atoms_base = tables;
+    L.total_bytes = 4 * (L.atoms_base + atoms_per_block * L.per_atom);
+  }
   return L;
 }
 
@@ -169,8 +182,10 @@ __device__ __forceinline__ int reduce_scatter(float* v, int gl)
 }
 
 // NRM/KM/NAM: compile-time bounds of nR, basis size + 1, nA for this instance.
+// The small-shape instance is held to 168 registers (three CTAs per SM): the
+// kernel is latency bound and the extra warps outweigh a few spilled words.
 template <int G, int NRM, int KM, int NAM>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, (KM <= 9 ? 3 : 2))
 k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
             const Site* __restrict__ sites, NeighborState* st,
             const int* __restrict__ nn_v, const int* __restrict__ nl_v, int mn_v,
@@ -195,6 +210,11 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
     const int kk = k % Lay.kpa, row = k / Lay.kpa;
     sm[Lay.c_ang + k] = kk < kA ? __ldg(p.c_pair + p.num_c_radial + row * kA + kk) : 0.0f;
   }
+  if (Lay.wt >= 0) {
+    const float4* src = reinterpret_cast<const float4*>(p.w0t);
+    float4* dst = reinterpret_cast<float4*>(sm + Lay.wt);
+    for (int k = tid; k < T * dim * p.H4 / 4; k += kBlock) dst[k] = __ldg(src + k);
+  }
   if (blockIdx.x == 0 && tid == 0) st->rebuild = 0;   // the Verlet list is consumed
   __syncthreads();
 
@@ -205,6 +225,7 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
   const bool active = i < N;
   float* mine = sm + Lay.atoms_base + slot * Lay.per_atom;
   float* s_s = mine + Lay.s;
+  float* s_a = mine + Lay.a;
   float* s_q = mine + Lay.q;
   float* s_fp = mine + Lay.fp;
   float* s_gh = mine + Lay.gh;
@@ -225,14 +246,27 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
 #pragma unroll
   for (int n = 0; n < NRM; ++n) qr[n] = 0.0f;
   int cr = 0, ca = 0;
+  // software pipeline: the next candidate's index and site are in flight
+  // while the current one is filtered and evaluated
+  int j_next = 0;
+  double2 sa_next = make_double2(0.0, 0.0), sc_next = make_double2(0.0, 0.0);
+  if (gl < nv) {
+    j_next = vrow[gl];
+    site_load(sites, j_next, sa_next, sc_next);
+  }
   for (int base = 0; base < nv_max; base += G) {
     const int k = base + gl;
+    const int j = j_next;
+    const double2 sa = sa_next, sc = sc_next;
+    if (k + G < nv) {
+      j_next = vrow[k + G];
+      site_load(sites, j_next, sa_next, sc_next);
+    }
     bool in_r = false, in_a = false;
-    int j = 0, t2 = 0;
+    int t2 = 0;
     float x12 = 0.0f, y12 = 0.0f, z12 = 0.0f, d12_square = 0.0f, rc_radial = 1.0f;
     if (k < nv) {
-      j = vrow[k];
-      site_displacement(b, sites, xi, yi, zi, j, x12, y12, z12, t2);
+      site_delta(b, sa, sc, xi, yi, zi, x12, y12, z12, t2);
       d12_square = x12 * x12 + y12 * y12 + z12 * z12;
       rc_radial = (rr1 + p.rc_r[t2]) * 0.5f;
       const float rc_angular = (ra1 + p.rc_a[t2]) * 0.5f;
@@ -354,29 +388,72 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
     }
   }
   __syncwarp();
+  // scaled descriptors; hidden-unit derivatives zero-padded to H4 for the
+  // float4 dot products
   for (int d = gl; d < dim; d += G) s_q[d] *= __ldg(p.q_scaler + d);
+  for (int h = H + gl; h < p.H4; h += G) s_gh[h] = 0.0f;
+  const float* w0t = Lay.wt >= 0 ? sm + Lay.wt : p.w0t;
   __syncwarp();
   float e_part = 0.0f;
   if (active) {
-    for (int h = gl; h < H; h += G) {
-      const float* w0 = p.w0 + (static_cast<size_t>(t1) * H + h) * dim;
-      float zs = 0.0f;
-      for (int d = 0; d < dim; ++d) zs += __ldg(w0 + d) * s_q[d];
-      const float x1 = tanhf(zs - __ldg(p.b0 + t1 * H + h));
-      const float w1 = __ldg(p.w1 + t1 * H + h);
-      e_part += w1 * x1;
-      s_gh[h] = w1 * (1.0f - x1 * x1);
+    // hidden layer: each lane owns groups of four consecutive hidden units
+    // (float4 rows of the transposed w0, four independent FMA chains,
+    // sequential in d as in the reference)
+    const int hq = p.H4 / 4;
+    const float4* wt =
+      reinterpret_cast<const float4*>(w0t + static_cast<size_t>(t1) * dim * p.H4);
+    for (int h4 = gl; h4 < hq; h4 += G) {
+      float z0 = 0.0f, z1 = 0.0f, z2 = 0.0f, z3 = 0.0f;
+#pragma unroll 4
+      for (int d = 0; d < dim; ++d) {
+        const float q = s_q[d];
+        const float4 w = wt[d * hq + h4];
+        z0 = fmaf(w.x, q, z0);
+        z1 = fmaf(w.y, q, z1);
+        z2 = fmaf(w.z, q, z2);
+        z3 = fmaf(w.w, q, z3);
+      }
+      auto finish = [&](int h, float z) {
+        if (h < H) {
+          const float x1 = tanhf(z - __ldg(p.b0 + t1 * H + h));
+          const float w1 = __ldg(p.w1 + t1 * H + h);
+          e_part += w1 * x1;
+          s_gh[h] = w1 * (1.0f - x1 * x1);
+        }
+      };
+      finish(4 * h4, z0);
+      finish(4 * h4 + 1, z1);
+      finish(4 * h4 + 2, z2);
+      finish(4 * h4 + 3, z3);
     }
   }
   e_part = group_sum<G>(e_part);
   if (active && gl == 0) pe_ann[i] = static_cast<double>(e_part - __ldg(p.out_bias + t1));
   __syncwarp();
   if (active) {
-    for (int d = gl; d < dim; d += G) {
-      const float* w0 = p.w0 + static_cast<size_t>(t1) * H * dim + d;
-      float acc = 0.0f;
-      for (int h = 0; h < H; ++h) acc += s_gh[h] * __ldg(w0 + static_cast<size_t>(h) * dim);
-      s_fp[d] = acc * __ldg(p.q_scaler + d);
+    // dE/dq: two descriptor components per lane at once, float4 over h
+    const int hq = p.H4 / 4;
+    const float4* g4 = reinterpret_cast<const float4*>(s_gh);
+    const float4* wt =
+      reinterpret_cast<const float4*>(w0t + static_cast<size_t>(t1) * dim * p.H4);
+    for (int d0 = gl; d0 < dim; d0 += 2 * G) {
+      const int da = d0, db = min(d0 + G, dim - 1);   // db past dim: computed, dropped
+      float aa = 0.0f, ab = 0.0f;
+#pragma unroll 2
+      for (int h = 0; h < hq; ++h) {
+        const float4 g = g4[h];
+        const float4 wa = wt[da * hq + h], wb = wt[db * hq + h];
+        aa = fmaf(g.x, wa.x, aa);
+        ab = fmaf(g.x, wb.x, ab);
+        aa = fmaf(g.y, wa.y, aa);
+        ab = fmaf(g.y, wb.y, ab);
+        aa = fmaf(g.z, wa.z, aa);
+        ab = fmaf(g.z, wb.z, ab);
+        aa = fmaf(g.w, wa.w, aa);
+        ab = fmaf(g.w, wb.w, ab);
+      }
+      s_fp[da] = aa * __ldg(p.q_scaler + da);
+      if (d0 + G < dim) s_fp[d0 + G] = ab * __ldg(p.q_scaler + d0 + G);
     }
   }
   __syncwarp();
@@ -391,29 +468,20 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
       al[e] = acc;
     }
   }
-  // a[n][lm] = dE/ds[n][lm], in place of s[n][*] (one lane owns one n)
+  // a[n][lm] = dE/ds[n][lm] (one lane owns one n); the monomial terms read
+  // the moments at run-time indices, so both live in shared memory
   for (int n = gl; n < nA; n += G) {
-    float* sv = s_s + n * kNumLM;
+    const float* sv = s_s + n * kNumLM;
+    float* av = s_a + n * kNumLM;
     const float* fp = s_fp + nR;
-    float s[kNumLM], av[kNumLM];
-#pragma unroll
-    for (int lm = 0; lm < kNumLM; ++lm) {
-      s[lm] = sv[lm];
-      av[lm] = 0.0f;
-    }
     int col = 0;
-#pragma unroll
-    for (int Lq = 1; Lq <= 4; ++Lq) {
-      if (Lq > p.L_max) break;
+    for (int Lq = 1; Lq <= p.L_max; ++Lq, ++col) {
       const int st0 = Lq * Lq - 1;
       const float f = fp[col * nA + n];
-      av[st0] = 2.0f * f * c_C3B[st0] * s[st0];
-#pragma unroll
-      for (int k = 1; k < 2 * Lq + 1; ++k) av[st0 + k] = 4.0f * f * c_C3B[st0 + k] * s[st0 + k];
-      ++col;
+      av[st0] = 2.0f * f * c_C3B[st0] * sv[st0];
+      for (int k = 1; k < 2 * Lq + 1; ++k) av[st0 + k] = 4.0f * f * c_C3B[st0 + k] * sv[st0 + k];
     }
-#pragma unroll
-    for (int lm = 0; lm < kNumLM; ++lm) sv[lm] = av[lm];
+    for (int lm = (p.L_max + 1) * (p.L_max + 1) - 1; lm < kNumLM; ++lm) av[lm] = 0.0f;
     for (int w = 0; w < p.num_inv; ++w, ++col) {
       const int id = p.inv_id[w];
       const float f = fp[col * nA + n];
@@ -423,8 +491,8 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
         for (int a = 0; a < nf; ++a) {
           float t = f * mo.c;
           for (int r = 0; r < nf; ++r)
-            if (r != a) t *= s[mo.i[r] & 31];
-          sv[mo.i[a]] += t;
+            if (r != a) t *= sv[mo.i[r]];
+          av[mo.i[a]] += t;
         }
       }
     }
@@ -434,7 +502,7 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
   // ---- 4. hand a[n][lm] to the angular-force kernel -------------------------
   if (active) {
     float4* dst = reinterpret_cast<float4*>(acoef + static_cast<size_t>(i) * nA * kNumLM);
-    const float4* src = reinterpret_cast<const float4*>(s_s);
+    const float4* src = reinterpret_cast<const float4*>(s_a);
     for (int q = gl; q < nA * kNumLM / 4; q += G) dst[q] = src[q];
   }
 }
