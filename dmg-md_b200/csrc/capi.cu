@@ -23,6 +23,10 @@ int cuda_fail(nepx_handle* h, const char* what)
   return fail(h, NEPX_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(err));
 }
 
+const char* const kUnsupportedBox =
+  "box thinner than 2.5 (rc + 1) in one periodic direction and thicker than 10 rc in another "
+  "(unsupported, as in the reference)";
+
 // Device flags of the previous call; ready only when its copy has landed
 // (or immediately when `wait`).
 int check_state(nepx_handle* h, bool wait)
@@ -43,6 +47,7 @@ int check_state(nepx_handle* h, bool wait)
                   " neighbour row exceeded its capacity; raise MN_radial/MN_angular in nep.txt");
   }
   if (s.nonfinite) return fail(h, NEPX_ERR_NONFINITE, "non-finite energy or force");
+  if (s.box_error) return fail(h, NEPX_ERR_BOX, kUnsupportedBox);
   return NEPX_OK;
 }
 
@@ -131,9 +136,17 @@ int nepx_compute(nepx_t* h, const nepx_box* box, int n, const int* d_type, const
   nepx::Box b;
   std::string err = nepx::make_box(box->h, box->pbc, b);
   if (!err.empty()) return fail(h, NEPX_ERR_BOX, err);
-  if (!nepx::large_box_ok(e, b))
-    return fail(h, NEPX_ERR_BOX,
-                "box thinner than 2.5 (rc + skin) in a periodic direction (small-box path)");
+  // small boxes (and boxes too thin for the Verlet cell grid) take the
+  // explicit-row path, rebuilt at every call like the reference's small-box path
+  const int kind = nepx::box_kind(e, b);
+  if (kind < 0) return fail(h, NEPX_ERR_BOX, kUnsupportedBox);
+  const bool xr = kind == 1 || !nepx::large_box_ok(e, b);
+  if (xr) {
+    err = nepx::engine_enable_xr(e, 1);
+    if (!err.empty()) return fail(h, NEPX_ERR_CUDA, err);
+    e.xr.from_box = true;
+  }
+  e.use_xr = xr;
   const bool changed = !e.have_box || std::memcmp(&b, &e.last_box, sizeof(nepx::Box)) != 0;
   const bool rebuild = e.force_rebuild || changed || n != e.last_n;
   auto s = static_cast<cudaStream_t>(stream);
@@ -220,6 +233,11 @@ int nepx_neighbors(nepx_t* h, int which, int n, int* d_nn, int* d_nl, int mn, vo
   const int src_mn = which == 0 ? nb.mn_r : nb.mn_a;
   if (mn < src_mn) return fail(h, NEPX_ERR_ARG, "mn smaller than the row capacity");
   auto s = static_cast<cudaStream_t>(stream);
+  if (h->engine.use_xr) {
+    nepx::launch_explicit_row_indices(h->engine, which, n, d_nn, d_nl, mn, s);
+    if (cudaPeekAtLastError() != cudaSuccess) return cuda_fail(h, "copy neighbour rows");
+    return NEPX_OK;
+  }
   const int* nn = which == 0 ? nb.nn_r : nb.nn_a;
   const int* nl = which == 0 ? nb.nl_r : nb.nl_a;
   if (cudaMemcpyAsync(d_nn, nn, sizeof(int) * n, cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
@@ -246,6 +264,7 @@ int nepx_neighbor_stats(nepx_t* h, int* max_radial, int* max_angular, int* max_v
   cleared.max_nn[0] = cleared.max_nn[1] = cleared.max_nn[2] = 0;
   cleared.overflow = 0;
   cleared.nonfinite = 0;
+  cleared.box_error = 0;
   cudaMemcpy(h->engine.d_nstate, &cleared, sizeof(cleared), cudaMemcpyHostToDevice);
   if (st.overflow) return fail(h, NEPX_ERR_OVERFLOW, "a neighbour row exceeded its capacity");
   if (st.nonfinite) return fail(h, NEPX_ERR_NONFINITE, "non-finite energy or force");

@@ -31,6 +31,21 @@ struct Box {
   int ortho;
 };
 
+// One structure of an explicit-row evaluation (the small-box path, and every
+// structure of a batch): its box, the reference's expanded box for the image
+// arithmetic, and its slice [off, off + n) of the concatenated atom arrays.
+struct StructInfo {
+  Box box;
+  float eh[18];   // expanded box h (columns scaled by ncell) then its float inverse
+  int ncell[3];   // images per direction (1 where not periodic)
+  int small;      // 1: the reference's small-box image arithmetic; 0: minimum image
+  int off, n;
+};
+
+// Packed neighbour of an explicit row: index j (low 28 bits) and type (high 4).
+constexpr int kRowTypeShift = 28;
+constexpr int kRowIndexMask = (1 << kRowTypeShift) - 1;
+
 // Cell grid and rebuild bookkeeping of the Verlet list, device resident.
 struct NeighborState {
   int rebuild;         // 1: rebuild the Verlet list before the next filter
@@ -39,6 +54,7 @@ struct NeighborState {
   int ncell;
   int max_nn[3];       // largest Verlet / radial / angular row of the last build
   int nonfinite;       // a force or energy came out NaN/Inf
+  int box_error;       // the device box became unsupported (small in one direction, >10 rc in another)
   double box_scale;    // product of isotropic box factors since the last build (1 = none)
 };
 

@@ -249,7 +249,8 @@ void engine_destroy(Engine& e)
   void* ptrs[] = {e.d_params, e.d_box, e.d_nstate, nb.nn_v, nb.nl_v, nb.nn_r, nb.nl_r,
                   nb.nn_a, nb.nl_a, nb.cell_count, nb.cell_start, nb.cell_atoms, nb.cell_of,
                   nb.x0, e.scratch.alpha, e.scratch.f12, e.scratch.pe_ann, e.scratch.q,
-                  e.scratch.tune_out, e.scratch.acoef, e.scratch.sites};
+                  e.scratch.tune_out, e.scratch.acoef, e.scratch.sites, e.xr.er, e.xr.ea,
+                  e.xr.d_si, e.xr.d_soff};
   for (void* q : ptrs)
     if (q) cudaFree(q);
 }

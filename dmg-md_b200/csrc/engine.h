@@ -37,6 +37,18 @@ struct ForceScratch {
   double* tune_out = nullptr;  // [13 N] throw-away outputs of the autotuning calls
 };
 
+// Explicit-row state: the small-box path (one structure, rebuilt from the
+// device box at every call) and the batched path (many structures).
+struct ExplicitRows {
+  float4* er = nullptr;       // [N][mn_r] radial edges (r_ij, packed j | type << 28)
+  float4* ea = nullptr;       // [N][mn_a] angular edges
+  StructInfo* d_si = nullptr; // [max_struct] structures
+  int* d_soff = nullptr;      // [max_struct + 1] first atom of each structure, then the total
+  int max_struct = 0;
+  int n_struct = 0;
+  bool from_box = true;       // one structure whose StructInfo follows the device box
+};
+
 struct Engine {
   NepModel model;
   ModelParams params{};
@@ -50,6 +62,8 @@ struct Engine {
   NeighborState* d_nstate = nullptr;
   NeighborBuffers nbr;
   ForceScratch scratch;
+  ExplicitRows xr;
+  bool use_xr = false;       // neighbour rows with explicit displacements (small box, batch)
   // host-side bookkeeping
   Box last_box{};
   bool have_box = false;
@@ -91,6 +105,25 @@ void launch_set_box(Engine& e, const Box& b, cudaStream_t stream);
 // launch follows a neighbour update at the same positions.
 void launch_neighbor_update(Engine& e, int N, const double* pos, const int* type, bool force,
                             cudaStream_t stream);
+
+// Explicit rows: allocates them for the handle's capacity and max_struct
+// structures (once; later calls only check the size).
+std::string engine_enable_xr(Engine& e, int max_struct);
+
+// Small-box test of the reference with its cutoff (largest radial cutoff)
+// and skin 1 A; returns 0 large, 1 small, -1 small in one direction and
+// thicker than 10 rc in another (unsupported, as in the reference).
+int box_kind(const Engine& e, const Box& b);
+
+// Rebuilds the explicit rows (and the site records) from the positions: for
+// from_box mode first the single StructInfo from the device box.
+void launch_explicit_rows(Engine& e, int N, const double* pos, const int* type,
+                          cudaStream_t stream);
+
+// Neighbour indices of the explicit rows (which = 0 radial, 1 angular) into
+// caller arrays nn[n], nl[n][mn] (row-major), as for the Verlet-path rows.
+void launch_explicit_row_indices(const Engine& e, int which, int n, int* nn, int* nl, int mn,
+                                 cudaStream_t stream);
 
 // Descriptor + ANN + angular partial forces, then the force/virial gather.
 // accumulate = add into pe/force/virial instead of overwriting them.

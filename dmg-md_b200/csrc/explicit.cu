@@ -1,0 +1,283 @@
+// explicit.cu -- neighbour rows with explicit displacements: the small-box
+// path and the batched path.
+//
+// Reference small-box path (src/gpumd_compat/nep_small_box.cuh:56-120,
+// find_neighbor_list_small_box; nep.cu:1900-2000, compute_small_box): when a
+// periodic direction is thinner than 2.5 (rc + 1) every center scans every
+// atom of its system and every image of the expanded box, keeping the pairs
+// inside the typewise radial / angular cutoffs together with the float
+// displacement r12 of that image.  Rows follow (j ascending, then images
+// ia, ib, ic) and are rebuilt at every force call.
+//
+// Here one warp owns a center and its lanes take consecutive candidates j;
+// per 32-candidate chunk each lane counts its edges over all images, a warp
+// scan gives every lane its write offset and a second pass writes the edges,
+// so rows keep the reference's order.  The same kernel serves any number of
+// structures packed into one atom range (the batched path): a center finds
+// its structure by binary search over the structure offsets, and structures
+// that are not small use the large-box arithmetic (double difference rounded
+// to float, float minimum image, reference nep.cu:503-561) over all their
+// atoms, which yields the large-box path's typewise rows exactly.
+//
+// Row entry: float4 (x12, y12, z12, bits of j | type(j) << 28), row-major
+// [center][slot]; radial and angular rows are separate.
+#include <algorithm>
+#include <string>
+
+#include "engine.h"
+#include "xbox.h"
+
+namespace nepx {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+__global__ void k_pack_sites(int N, const double* __restrict__ pos, const int* __restrict__ type,
+                             Site* __restrict__ sites)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  sites[i] = Site{pos[i], pos[N + i], pos[2 * N + i], static_cast<long long>(type[i])};
+}
+
+// One structure spanning all N atoms, its StructInfo from the device box.
+__global__ void k_struct_from_box(const Box* __restrict__ box, double rc, int N, StructInfo* si,
+                                  int* soff, NeighborState* st)
+{
+  StructInfo s;
+  if (expanded_box(*box, rc, s)) st->box_error = 1;
+  s.off = 0;
+  s.n = N;
+  *si = s;
+  soff[0] = 0;
+  soff[1] = N;
+}
+
+// Minimum image in the expanded box (reference nep_small_box.cuh:39-54).
+__device__ __forceinline__ void mic_small_box(const StructInfo& s, float& x12, float& y12,
+                                              float& z12)
+{
+  const float* e = s.eh;
+  float sx12 = e[9] * x12 + e[10] * y12 + e[11] * z12;
+  float sy12 = e[12] * x12 + e[13] * y12 + e[14] * z12;
+  float sz12 = e[15] * x12 + e[16] * y12 + e[17] * z12;
+  if (s.box.pbc[0] == 1) sx12 -= nearbyintf(sx12);
+  if (s.box.pbc[1] == 1) sy12 -= nearbyintf(sy12);
+  if (s.box.pbc[2] == 1) sz12 -= nearbyintf(sz12);
+  x12 = e[0] * sx12 + e[1] * sy12 + e[2] * sz12;
+  y12 = e[3] * sx12 + e[4] * sy12 + e[5] * sz12;
+  z12 = e[6] * sx12 + e[7] * sy12 + e[8] * sz12;
+}
+
+__device__ __forceinline__ float4 row_entry(float x, float y, float z, int j, int t)
+{
+  return make_float4(x, y, z, __int_as_float(j | (t << kRowTypeShift)));
+}
+
+__global__ void __launch_bounds__(256)
+k_rows_explicit(const ModelParams p, int total, const StructInfo* __restrict__ si,
+                const int* __restrict__ soff, int S, const double* __restrict__ pos,
+                const int* __restrict__ type, int* __restrict__ nn_r, float4* __restrict__ er,
+                int mn_r, int* __restrict__ nn_a, float4* __restrict__ ea, int mn_a,
+                NeighborState* st)
+{
+  const int lane = threadIdx.x & 31;
+  const int wpb = blockDim.x >> 5;
+  const unsigned below = (1u << lane) - 1u;
+  for (int i = blockIdx.x * wpb + (threadIdx.x >> 5); i < total; i += gridDim.x * wpb) {
+    // structure of center i: the last s with soff[s] <= i
+    int lo = 0, hi = S - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (soff[mid] <= i) lo = mid; else hi = mid - 1;
+    }
+    const StructInfo& s = si[lo];
+    const int off = s.off, n = s.n;
+    const int t1 = type[i];
+    const float rr1 = p.rc_r[t1], ra1 = p.rc_a[t1];
+    float4* rrow = er + static_cast<size_t>(i) * mn_r;
+    float4* arow = ea + static_cast<size_t>(i) * mn_a;
+    int cr = 0, ca = 0;
+    if (!s.small) {
+      const double xi = pos[i], yi = pos[total + i], zi = pos[2 * total + i];
+      for (int base = 0; base < n; base += 32) {
+        const int j = off + base + lane;
+        bool in_r = false, in_a = false;
+        float x12 = 0.0f, y12 = 0.0f, z12 = 0.0f;
+        int t2 = 0;
+        if (base + lane < n && j != i) {
+          x12 = pos[j] - xi;
+          y12 = pos[total + j] - yi;
+          z12 = pos[2 * total + j] - zi;
+          mic_f32(s.box, x12, y12, z12);
+          const float d12_square = x12 * x12 + y12 * y12 + z12 * z12;
+          t2 = type[j];
+          const float rc_radial = (rr1 + p.rc_r[t2]) * 0.5f;
+          const float rc_angular = (ra1 + p.rc_a[t2]) * 0.5f;
+          in_r = d12_square < rc_radial * rc_radial;   // angular edges are radial ones
+          in_a = in_r && d12_square < rc_angular * rc_angular;
+        }
+        const unsigned mr = __ballot_sync(kFull, in_r), ma = __ballot_sync(kFull, in_a);
+        if (in_r) {
+          const int at = cr + __popc(mr & below);
+          if (at < mn_r) rrow[at] = row_entry(x12, y12, z12, j, t2);
+        }
+        if (in_a) {
+          const int at = ca + __popc(ma & below);
+          if (at < mn_a) arow[at] = row_entry(x12, y12, z12, j, t2);
+        }
+        cr += __popc(mr);
+        ca += __popc(ma);
+      }
+    } else {
+      // the small-box arithmetic: float center, double image position
+      const float x1 = pos[i], y1 = pos[total + i], z1 = pos[2 * total + i];
+      const float* fh = s.box.fh;
+      for (int base = 0; base < n; base += 32) {
+        const int j = off + base + lane;
+        const bool valid = base + lane < n;
+        const int t2 = valid ? type[j] : 0;
+        const float rc_radial = (rr1 + p.rc_r[t2]) * 0.5f;
+        const float rc_angular = (ra1 + p.rc_a[t2]) * 0.5f;
+        const double xj = valid ? pos[j] : 0.0, yj = valid ? pos[total + j] : 0.0,
+                     zj = valid ? pos[2 * total + j] : 0.0;
+        // pass 0 counts this lane's edges, pass 1 writes them at the scanned offsets
+        int wr = 0, wa = 0;
+        for (int pass = 0; pass < 2; ++pass) {
+          int kr = 0, ka = 0;
+          if (valid) {
+            for (int ia = 0; ia < s.ncell[0]; ++ia)
+              for (int ib = 0; ib < s.ncell[1]; ++ib)
+                for (int ic = 0; ic < s.ncell[2]; ++ic) {
+                  if (ia == 0 && ib == 0 && ic == 0 && j == i) continue;   // self
+                  const float d0 = fh[0] * ia + fh[1] * ib + fh[2] * ic;
+                  const float d1 = fh[3] * ia + fh[4] * ib + fh[5] * ic;
+                  const float d2 = fh[6] * ia + fh[7] * ib + fh[8] * ic;
+                  float x12 = xj + d0 - x1;
+                  float y12 = yj + d1 - y1;
+                  float z12 = zj + d2 - z1;
+                  mic_small_box(s, x12, y12, z12);
+                  const float d12_square = x12 * x12 + y12 * y12 + z12 * z12;
+                  if (d12_square < rc_radial * rc_radial) {
+                    if (pass == 1 && wr + kr < mn_r)
+                      rrow[wr + kr] = row_entry(x12, y12, z12, j, t2);
+                    ++kr;
+                  }
+                  if (d12_square < rc_angular * rc_angular) {
+                    if (pass == 1 && wa + ka < mn_a)
+                      arow[wa + ka] = row_entry(x12, y12, z12, j, t2);
+                    ++ka;
+                  }
+                }
+          }
+          if (pass == 0) {
+            // exclusive warp scan of the per-lane counts
+            int sr = kr, sa = ka;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+              const int ur = __shfl_up_sync(kFull, sr, o), ua = __shfl_up_sync(kFull, sa, o);
+              if (lane >= o) {
+                sr += ur;
+                sa += ua;
+              }
+            }
+            wr = cr + sr - kr;
+            wa = ca + sa - ka;
+            cr += __shfl_sync(kFull, sr, 31);
+            ca += __shfl_sync(kFull, sa, 31);
+          }
+        }
+      }
+    }
+    if (lane == 0) {
+      nn_r[i] = min(cr, mn_r);
+      nn_a[i] = min(ca, mn_a);
+      if (cr > mn_r) atomicOr(&st->overflow, 2);
+      if (ca > mn_a) atomicOr(&st->overflow, 4);
+      atomicMax(&st->max_nn[1], cr);
+      atomicMax(&st->max_nn[2], ca);
+    }
+  }
+}
+
+__global__ void k_row_indices(int n, const int* __restrict__ cnt, const float4* __restrict__ rows,
+                              int src_mn, int* nn, int* nl, int mn)
+{
+  const int i = blockIdx.x;
+  if (i >= n) return;
+  const int c = cnt[i];
+  if (threadIdx.x == 0) nn[i] = c;
+  for (int k = threadIdx.x; k < c; k += blockDim.x)
+    nl[static_cast<size_t>(i) * mn + k] =
+      __float_as_int(rows[static_cast<size_t>(i) * src_mn + k].w) & kRowIndexMask;
+}
+
+template <typename T>
+cudaError_t dalloc(T*& ptr, size_t count)
+{
+  return cudaMalloc(reinterpret_cast<void**>(&ptr), std::max<size_t>(count, 1) * sizeof(T));
+}
+
+}  // namespace
+
+int box_kind(const Engine& e, const Box& b)
+{
+  StructInfo s;
+  if (expanded_box(b, e.model.rc_radial_max, s)) return -1;
+  return s.small;
+}
+
+std::string engine_enable_xr(Engine& e, int max_struct)
+{
+  ExplicitRows& x = e.xr;
+  if (x.er && x.max_struct >= max_struct) return "";
+  const size_t N = e.capacity;
+  if (N > static_cast<size_t>(kRowIndexMask))
+    return "explicit neighbour rows address at most 2^28 atoms";
+  if (!x.er) {
+    bool ok = dalloc(x.er, N * e.nbr.mn_r) == cudaSuccess;
+    ok &= dalloc(x.ea, N * e.nbr.mn_a) == cudaSuccess;
+    if (!ok) return "cudaMalloc failed (explicit neighbour rows)";
+  }
+  if (x.max_struct < max_struct) {
+    if (x.d_si) cudaFree(x.d_si);
+    if (x.d_soff) cudaFree(x.d_soff);
+    x.d_si = nullptr;
+    x.d_soff = nullptr;
+    bool ok = dalloc(x.d_si, max_struct) == cudaSuccess;
+    ok &= dalloc(x.d_soff, max_struct + 1) == cudaSuccess;
+    if (!ok) return "cudaMalloc failed (structure table)";
+    x.max_struct = max_struct;
+  }
+  return "";
+}
+
+void launch_explicit_rows(Engine& e, int N, const double* pos, const int* type,
+                          cudaStream_t stream)
+{
+  ExplicitRows& x = e.xr;
+  const int threads = 256;
+  k_pack_sites<<<(N + threads - 1) / threads, threads, 0, stream>>>(N, pos, type,
+                                                                     e.scratch.sites);
+  if (x.from_box) {
+    k_struct_from_box<<<1, 1, 0, stream>>>(e.d_box, e.model.rc_radial_max, N, x.d_si, x.d_soff,
+                                           e.d_nstate);
+    x.n_struct = 1;
+  }
+  const int warps = threads / 32;
+  const int blocks = std::min((N + warps - 1) / warps, 148 * 8);
+  k_rows_explicit<<<blocks, threads, 0, stream>>>(e.params, N, x.d_si, x.d_soff, x.n_struct, pos,
+                                                  type, e.nbr.nn_r, x.er, e.nbr.mn_r, e.nbr.nn_a,
+                                                  x.ea, e.nbr.mn_a, e.d_nstate);
+}
+
+void launch_explicit_row_indices(const Engine& e, int which, int n, int* nn, int* nl, int mn,
+                                 cudaStream_t stream)
+{
+  const int src_mn = which == 0 ? e.nbr.mn_r : e.nbr.mn_a;
+  k_row_indices<<<n, 64, 0, stream>>>(n, which == 0 ? e.nbr.nn_r : e.nbr.nn_a,
+                                      which == 0 ? e.xr.er : e.xr.ea, src_mn, nn, nl, mn);
+}
+
+}  // namespace nepx

@@ -387,9 +387,21 @@ int nepx_md_create(nepx_t* pot, int n, const int* h_type, const double* h_mass,
   md.engine = &e;
   md.N = n;
   m->pot = pot;
-  if (!nepx::make_box(box->h, box->pbc, md.box).empty() || !nepx::large_box_ok(e, md.box)) {
+  if (!nepx::make_box(box->h, box->pbc, md.box).empty()) {
     delete m;
     return NEPX_ERR_BOX;
+  }
+  // small boxes run on explicit rows rebuilt every step (the reference's
+  // small-box path); the choice is made here for the whole trajectory
+  const int kind = nepx::box_kind(e, md.box);
+  if (kind < 0) {
+    delete m;
+    return NEPX_ERR_BOX;
+  }
+  md.xr = kind == 1 || !nepx::large_box_ok(e, md.box);
+  if (md.xr && !nepx::engine_enable_xr(e, 1).empty()) {
+    delete m;
+    return NEPX_ERR_CUDA;
   }
   if (stream) {
     md.stream = static_cast<cudaStream_t>(stream);
@@ -489,6 +501,8 @@ int md_enqueue_run(nepx_md* m, int steps, double dt_fs, int thermo_every, double
   nepx::Engine& e = *md.engine;
   const nepx::EnsembleConfig& c = md.ens;
   const int N = md.N;
+  e.use_xr = md.xr;
+  e.xr.from_box = true;
   nepx::StepParams p{};
   p.N = N;
   p.kind = c.kind;
@@ -600,6 +614,9 @@ int md_finish(nepx_md* m)
   if (status & 2) return md_fail(m, NEPX_ERR_NONFINITE, "invalid barostat box factor");
   if (st.overflow) return md_fail(m, NEPX_ERR_OVERFLOW, "a neighbour row exceeded its capacity");
   if (st.nonfinite) return md_fail(m, NEPX_ERR_NONFINITE, "non-finite energy or force");
+  if (st.box_error)
+    return md_fail(m, NEPX_ERR_BOX, "the box became small in one periodic direction and thicker "
+                                    "than 10 rc in another (unsupported, as in the reference)");
   return NEPX_OK;
 }
 

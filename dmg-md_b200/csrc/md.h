@@ -68,6 +68,7 @@ struct Md {
   EnsembleConfig ens;
   SvrRng rng{12345678u};
   bool forces_valid = false;
+  bool xr = false;                // explicit-row (small-box) force path
   cudaStream_t stream = nullptr;
   cudaGraphExec_t graph = nullptr;
   StepParams graph_params{};

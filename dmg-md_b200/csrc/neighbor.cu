@@ -260,6 +260,10 @@ __global__ void k_verlet_build(int N, const Box* __restrict__ box, const Site* _
 void launch_neighbor_update(Engine& e, int N, const double* pos, const int* type, bool force,
                             cudaStream_t stream)
 {
+  if (e.use_xr) {
+    launch_explicit_rows(e, N, pos, type, stream);
+    return;
+  }
   NeighborBuffers& nb = e.nbr;
   const int threads = 256;
   const int grid = (N + threads - 1) / threads;

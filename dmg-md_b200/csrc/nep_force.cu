@@ -184,13 +184,17 @@ __device__ __forceinline__ int reduce_scatter(float* v, int gl)
 // NRM/KM/NAM: compile-time bounds of nR, basis size + 1, nA for this instance.
 // The small-shape instance is held to 168 registers (three CTAs per SM): the
 // kernel is latency bound and the extra warps outweigh a few spilled words.
-template <int G, int NRM, int KM, int NAM>
+// XR: explicit rows (small-box and batched paths) -- the radial and angular
+// rows hold the displacement and packed neighbour of every edge (er, ea),
+// built beforehand; phase 1 then only accumulates the radial descriptors.
+template <int G, int NRM, int KM, int NAM, bool XR>
 __global__ void __launch_bounds__(kBlock, (KM <= 9 ? 3 : 2))
 k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
             const Site* __restrict__ sites, NeighborState* st,
             const int* __restrict__ nn_v, const int* __restrict__ nl_v, int mn_v,
             int* __restrict__ nn_r, int* __restrict__ nl_r, int mn_r, int* __restrict__ nn_a,
-            int* __restrict__ nl_a, int mn_a, float* __restrict__ alpha,
+            int* __restrict__ nl_a, int mn_a, const float4* __restrict__ er,
+            const float4* __restrict__ ea, float* __restrict__ alpha,
             float* __restrict__ acoef, double* __restrict__ pe_ann)
 {
   constexpr int APW = 32 / G;             // centers per warp
@@ -236,75 +240,95 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
   const unsigned below = (1u << gl) - 1u;
 
   // ---- 1. filter the Verlet row, radial descriptors -------------------------
-  const int nv = active ? nn_v[i] : 0;
-  const int nv_max = __reduce_max_sync(kFull, nv);
-  const int* vrow = nl_v + static_cast<size_t>(i) * mn_v;
-  int* rrow = nl_r + static_cast<size_t>(i) * mn_r;
-  int* arow = nl_a + static_cast<size_t>(i) * mn_a;
   const float rr1 = p.rc_r[t1], ra1 = p.rc_a[t1];
   float qr[NRM];
 #pragma unroll
   for (int n = 0; n < NRM; ++n) qr[n] = 0.0f;
+  // q_n += sum_k c(t1,t2)[n][k] f_k(d) for one radial edge
+  auto add_radial = [&](int t2, float d12_square, float rc_radial) {
+    const float d = sqrtf(d12_square);
+    const float rcinv = 1.0f / rc_radial;
+    float fc, fcp;
+    cutoff_fc(rc_radial, rcinv, d, fc, fcp);
+    float fn[KP];
+#pragma unroll
+    for (int kk = 0; kk < KP; ++kk) fn[kk] = 0.0f;
+    radial_basis<KM>(kR, rcinv, d, fc, fn);
+    const float* c = sm + Lay.c_rad + (t1 * T + t2) * nR * Lay.kpr;
+#pragma unroll
+    for (int n = 0; n < NRM; ++n)
+      if (n < nR) qr[n] += dot_basis<KM>(c + n * Lay.kpr, fn);
+  };
   int cr = 0, ca = 0;
-  // software pipeline: the next candidate's index and site are in flight
-  // while the current one is filtered and evaluated
-  int j_next = 0;
-  double2 sa_next = make_double2(0.0, 0.0), sc_next = make_double2(0.0, 0.0);
-  if (gl < nv) {
-    j_next = vrow[gl];
-    site_load(sites, j_next, sa_next, sc_next);
-  }
-  for (int base = 0; base < nv_max; base += G) {
-    const int k = base + gl;
-    const int j = j_next;
-    const double2 sa = sa_next, sc = sc_next;
-    if (k + G < nv) {
-      j_next = vrow[k + G];
+  if constexpr (XR) {
+    // explicit rows: counts clamped to capacity by the row builder
+    cr = active ? nn_r[i] : 0;
+    ca = active ? nn_a[i] : 0;
+    const int cr_max = __reduce_max_sync(kFull, cr);
+    const float4* erow = er + static_cast<size_t>(i) * mn_r;
+    for (int base = 0; base < cr_max; base += G) {
+      const int k = base + gl;
+      if (k < cr) {
+        const float4 e = erow[k];
+        const int t2 = static_cast<int>(static_cast<unsigned>(__float_as_int(e.w)) >> kRowTypeShift);
+        add_radial(t2, e.x * e.x + e.y * e.y + e.z * e.z, (rr1 + p.rc_r[t2]) * 0.5f);
+      }
+    }
+  } else {
+    const int nv = active ? nn_v[i] : 0;
+    const int nv_max = __reduce_max_sync(kFull, nv);
+    const int* vrow = nl_v + static_cast<size_t>(i) * mn_v;
+    int* rrow = nl_r + static_cast<size_t>(i) * mn_r;
+    int* arow = nl_a + static_cast<size_t>(i) * mn_a;
+    // software pipeline: the next candidate's index and site are in flight
+    // while the current one is filtered and evaluated
+    int j_next = 0;
+    double2 sa_next = make_double2(0.0, 0.0), sc_next = make_double2(0.0, 0.0);
+    if (gl < nv) {
+      j_next = vrow[gl];
       site_load(sites, j_next, sa_next, sc_next);
     }
-    bool in_r = false, in_a = false;
-    int t2 = 0;
-    float x12 = 0.0f, y12 = 0.0f, z12 = 0.0f, d12_square = 0.0f, rc_radial = 1.0f;
-    if (k < nv) {
-      site_delta(b, sa, sc, xi, yi, zi, x12, y12, z12, t2);
-      d12_square = x12 * x12 + y12 * y12 + z12 * z12;
-      rc_radial = (rr1 + p.rc_r[t2]) * 0.5f;
-      const float rc_angular = (ra1 + p.rc_a[t2]) * 0.5f;
-      in_r = d12_square < rc_radial * rc_radial;
-      in_a = in_r && d12_square < rc_angular * rc_angular;
+    for (int base = 0; base < nv_max; base += G) {
+      const int k = base + gl;
+      const int j = j_next;
+      const double2 sa = sa_next, sc = sc_next;
+      if (k + G < nv) {
+        j_next = vrow[k + G];
+        site_load(sites, j_next, sa_next, sc_next);
+      }
+      bool in_r = false, in_a = false;
+      int t2 = 0;
+      float x12 = 0.0f, y12 = 0.0f, z12 = 0.0f, d12_square = 0.0f, rc_radial = 1.0f;
+      if (k < nv) {
+        site_delta(b, sa, sc, xi, yi, zi, x12, y12, z12, t2);
+        d12_square = x12 * x12 + y12 * y12 + z12 * z12;
+        rc_radial = (rr1 + p.rc_r[t2]) * 0.5f;
+        const float rc_angular = (ra1 + p.rc_a[t2]) * 0.5f;
+        in_r = d12_square < rc_radial * rc_radial;
+        in_a = in_r && d12_square < rc_angular * rc_angular;
+      }
+      const unsigned mr = group_ballot<G>(in_r, group);
+      const unsigned ma = group_ballot<G>(in_a, group);
+      if (in_r) {
+        const int at = cr + __popc(mr & below);
+        if (at < mn_r) rrow[at] = j;
+        add_radial(t2, d12_square, rc_radial);
+      }
+      if (in_a) {
+        const int at = ca + __popc(ma & below);
+        if (at < mn_a) arow[at] = j;
+      }
+      cr += __popc(mr);
+      ca += __popc(ma);
     }
-    const unsigned mr = group_ballot<G>(in_r, group);
-    const unsigned ma = group_ballot<G>(in_a, group);
-    if (in_r) {
-      const int at = cr + __popc(mr & below);
-      if (at < mn_r) rrow[at] = j;
-      const float d = sqrtf(d12_square);
-      const float rcinv = 1.0f / rc_radial;
-      float fc, fcp;
-      cutoff_fc(rc_radial, rcinv, d, fc, fcp);
-      float fn[KP];
-#pragma unroll
-      for (int kk = 0; kk < KP; ++kk) fn[kk] = 0.0f;
-      radial_basis<KM>(kR, rcinv, d, fc, fn);
-      const float* c = sm + Lay.c_rad + (t1 * T + t2) * nR * Lay.kpr;
-#pragma unroll
-      for (int n = 0; n < NRM; ++n)
-        if (n < nR) qr[n] += dot_basis<KM>(c + n * Lay.kpr, fn);
+    if (active && gl == 0) {
+      nn_r[i] = min(cr, mn_r);
+      nn_a[i] = min(ca, mn_a);
+      if (cr > mn_r) atomicOr(&st->overflow, 2);
+      if (ca > mn_a) atomicOr(&st->overflow, 4);
+      atomicMax(&st->max_nn[1], cr);
+      atomicMax(&st->max_nn[2], ca);
     }
-    if (in_a) {
-      const int at = ca + __popc(ma & below);
-      if (at < mn_a) arow[at] = j;
-    }
-    cr += __popc(mr);
-    ca += __popc(ma);
-  }
-  if (active && gl == 0) {
-    nn_r[i] = min(cr, mn_r);
-    nn_a[i] = min(ca, mn_a);
-    if (cr > mn_r) atomicOr(&st->overflow, 2);
-    if (ca > mn_a) atomicOr(&st->overflow, 4);
-    atomicMax(&st->max_nn[1], cr);
-    atomicMax(&st->max_nn[2], ca);
   }
 #pragma unroll
   for (int n = 0; n < NRM; ++n) qr[n] = group_sum<G>(qr[n]);
@@ -317,6 +341,8 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
   // ---- 2. angular moments s[n][lm] -----------------------------------------
   const int na = min(ca, mn_a);
   const int na_max = __reduce_max_sync(kFull, na);
+  const int* arow = nl_a + static_cast<size_t>(i) * mn_a;
+  const float4* earow = ea + static_cast<size_t>(i) * mn_a;
   for (int nc = 0; nc < nA; nc += kChunkN) {
     float v[kChunkN * kNumLM];
 #pragma unroll
@@ -324,10 +350,17 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
     for (int base = 0; base < na_max; base += G) {
       const int k = base + gl;
       if (k < na) {
-        const int j = arow[k];
         int t2;
         float dx, dy, dz;
-        site_displacement(b, sites, xi, yi, zi, j, dx, dy, dz, t2);
+        if constexpr (XR) {
+          const float4 e = earow[k];
+          dx = e.x;
+          dy = e.y;
+          dz = e.z;
+          t2 = static_cast<int>(static_cast<unsigned>(__float_as_int(e.w)) >> kRowTypeShift);
+        } else {
+          site_displacement(b, sites, xi, yi, zi, arow[k], dx, dy, dz, t2);
+        }
         const float d = sqrtf(dx * dx + dy * dy + dz * dz);
         const float rc = (ra1 + p.rc_a[t2]) * 0.5f;
         const float rcinv = 1.0f / rc;
@@ -507,12 +540,113 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
   }
 }
 
-// One group of G lanes per center: directed angular partial forces
-//   f12(i,j) = (sum_lm B_lm Y_lm) r^ + (1/d)(I - r^r^T) sum_lm A_lm dY_lm/dr^,
+// Directed angular partial force of a center on one neighbour at
+// r = (dx, dy, dz) = r_j - r_i:
+//   f12 = (sum_lm B_lm Y_lm) r^ + (1/d)(I - r^r^T) sum_lm A_lm dY_lm/dr^,
 //   A_lm = sum_n a[n][lm] g_n(d), B_lm = sum_n a[n][lm] g'_n(d),
-// with a[n][lm] = dE_i/ds[n][lm] from k_nep_fused (reference
-// find_partial_force_angular, nep.cu:890-991, and the accumulate_f12 ladder,
-// nep_utilities.cuh:1240-1491, evaluated once per edge instead of per (edge, n)).
+// with a[n][lm] = dE/ds[n][lm] of the center (av, global) and c its angular
+// coefficient table for the pair (nA rows of the padded basis, shared memory).
+// Reference find_partial_force_angular (nep.cu:890-991) with the
+// accumulate_f12 ladder (nep_utilities.cuh:1240-1491) evaluated once per edge
+// instead of once per (edge, n).
+template <int KM, int NAM>
+__device__ __forceinline__ float3 angular_edge_force(const ModelParams& p, const float* c,
+                                                    const float* __restrict__ av, float rc,
+                                                    float dx, float dy, float dz)
+{
+  constexpr int KP = (KM + 3) & ~3;
+  const int nA = p.nA;
+  const float d = sqrtf(dx * dx + dy * dy + dz * dz);
+  const float dinv = 1.0f / d;
+  const float ux = dx * dinv, uy = dy * dinv, uz = dz * dinv;
+  const float rcinv = 1.0f / rc;
+  float fc, fcp;
+  cutoff_fc(rc, rcinv, d, fc, fcp);
+  float fn[KP], fnp[KP];
+#pragma unroll
+  for (int kk = 0; kk < KP; ++kk) {
+    fn[kk] = 0.0f;
+    fnp[kk] = 0.0f;
+  }
+  radial_basis_d<KM>(p.kA, rcinv, d, fc, fcp, fn, fnp);
+  float A[kNumLM], B[kNumLM];
+#pragma unroll
+  for (int lm = 0; lm < kNumLM; ++lm) {
+    A[lm] = 0.0f;
+    B[lm] = 0.0f;
+  }
+#pragma unroll
+  for (int n = 0; n < NAM; ++n) {
+    if (n < nA) {
+      const float g = dot_basis<KM>(c + n * KP, fn);
+      const float gp = dot_basis<KM>(c + n * KP, fnp);
+      const float* an = av + n * kNumLM;
+#pragma unroll
+      for (int q = 0; q < kNumLM / 4; ++q) {
+        const float4 a4 = __ldg(reinterpret_cast<const float4*>(an) + q);
+        A[4 * q] += a4.x * g;
+        A[4 * q + 1] += a4.y * g;
+        A[4 * q + 2] += a4.z * g;
+        A[4 * q + 3] += a4.w * g;
+        B[4 * q] += a4.x * gp;
+        B[4 * q + 1] += a4.y * gp;
+        B[4 * q + 2] += a4.z * gp;
+        B[4 * q + 3] += a4.w * gp;
+      }
+    }
+  }
+  // SB = sum B Y, V = sum A dY/du (u components independent)
+  float zp[5];
+  zp[0] = 1.0f;
+#pragma unroll
+  for (int q = 1; q < 5; ++q) zp[q] = zp[q - 1] * uz;
+  float SB = 0.0f, vx = 0.0f, vy = 0.0f, vz = 0.0f;
+  int idx = 0;
+#pragma unroll
+  for (int Lq = 1; Lq <= 4; ++Lq) {
+    if (Lq > p.L_max) break;
+    float re0 = 1.0f, im0 = 0.0f;   // (ux + i uy)^(m-1)
+#pragma unroll
+    for (int m = 0; m <= Lq; ++m) {
+      float dzf;
+      const float zf = zpoly(Lq, m, zp, &dzf);
+      if (m == 0) {
+        SB += B[idx] * zf;
+        vz += A[idx] * dzf;
+        ++idx;
+      } else {
+        const float re = ux * re0 - uy * im0;
+        const float im = ux * im0 + uy * re0;
+        const float Ar = A[idx], Ai = A[idx + 1];
+        SB += (B[idx] * re + B[idx + 1] * im) * zf;
+        const float mzf = m * zf;
+        vx += mzf * (Ar * re0 + Ai * im0);
+        vy += mzf * (Ai * re0 - Ar * im0);
+        vz += dzf * (Ar * re + Ai * im);
+        idx += 2;
+        re0 = re;
+        im0 = im;
+      }
+    }
+  }
+  const float uv = ux * vx + uy * vy + uz * vz;
+  return make_float3(SB * ux + (vx - uv * ux) * dinv, SB * uy + (vy - uv * uy) * dinv,
+                     SB * uz + (vz - uv * uz) * dinv);
+}
+
+// Angular coefficient tables [T*T][nA][KP] into shared memory (zero-padded rows).
+template <int KP>
+__device__ __forceinline__ void load_angular_tables(const ModelParams& p, float* sm)
+{
+  const int T = p.T, nA = p.nA, kA = p.kA;
+  for (int k = threadIdx.x; k < T * T * nA * KP; k += blockDim.x) {
+    const int kk = k % KP, row = k / KP;
+    sm[k] = kk < kA ? __ldg(p.c_pair + p.num_c_radial + row * kA + kk) : 0.0f;
+  }
+}
+
+// One group of G lanes per center: the directed angular partial force of
+// every edge of the center's angular row, f12[i][k] (float4, w unused).
 template <int G, int KM, int NAM>
 __global__ void __launch_bounds__(kBlock)
 k_angular_f12(const ModelParams p, int N, const Box* __restrict__ box,
@@ -522,13 +656,10 @@ k_angular_f12(const ModelParams p, int N, const Box* __restrict__ box,
 {
   constexpr int KP = (KM + 3) & ~3;
   extern __shared__ float sm[];
-  const int tid = threadIdx.x;
-  const int T = p.T, nA = p.nA, kA = p.kA;
-  for (int k = tid; k < T * T * nA * KP; k += kBlock) {
-    const int kk = k % KP, row = k / KP;
-    sm[k] = kk < kA ? __ldg(p.c_pair + p.num_c_radial + row * kA + kk) : 0.0f;
-  }
+  load_angular_tables<KP>(p, sm);
   __syncthreads();
+  const int tid = threadIdx.x;
+  const int T = p.T, nA = p.nA;
   const int gl = tid % G;
   const int i = blockIdx.x * (kBlock / G) + tid / G;
   if (i >= N) return;
@@ -541,89 +672,13 @@ k_angular_f12(const ModelParams p, int N, const Box* __restrict__ box,
   const int* arow = nl_a + static_cast<size_t>(i) * mn_a;
   const float* ai = acoef + static_cast<size_t>(i) * nA * kNumLM;
   for (int k = gl; k < na; k += G) {
-    const int j = arow[k];
     int t2;
     float dx, dy, dz;
-    site_displacement(b, sites, xi, yi, zi, j, dx, dy, dz, t2);
-    const float d = sqrtf(dx * dx + dy * dy + dz * dz);
-    const float dinv = 1.0f / d;
-    const float ux = dx * dinv, uy = dy * dinv, uz = dz * dinv;
+    site_displacement(b, sites, xi, yi, zi, arow[k], dx, dy, dz, t2);
     const float rc = (ra1 + p.rc_a[t2]) * 0.5f;
-    const float rcinv = 1.0f / rc;
-    float fc, fcp;
-    cutoff_fc(rc, rcinv, d, fc, fcp);
-    float fn[KP], fnp[KP];
-#pragma unroll
-    for (int kk = 0; kk < KP; ++kk) {
-      fn[kk] = 0.0f;
-      fnp[kk] = 0.0f;
-    }
-    radial_basis_d<KM>(kA, rcinv, d, fc, fcp, fn, fnp);
-    const float* c = sm + (t1 * T + t2) * nA * KP;
-    float A[kNumLM], B[kNumLM];
-#pragma unroll
-    for (int lm = 0; lm < kNumLM; ++lm) {
-      A[lm] = 0.0f;
-      B[lm] = 0.0f;
-    }
-#pragma unroll
-    for (int n = 0; n < NAM; ++n) {
-      if (n < nA) {
-        const float g = dot_basis<KM>(c + n * KP, fn);
-        const float gp = dot_basis<KM>(c + n * KP, fnp);
-        const float* av = ai + n * kNumLM;
-#pragma unroll
-        for (int q = 0; q < kNumLM / 4; ++q) {
-          const float4 a4 = __ldg(reinterpret_cast<const float4*>(av) + q);
-          A[4 * q] += a4.x * g;
-          A[4 * q + 1] += a4.y * g;
-          A[4 * q + 2] += a4.z * g;
-          A[4 * q + 3] += a4.w * g;
-          B[4 * q] += a4.x * gp;
-          B[4 * q + 1] += a4.y * gp;
-          B[4 * q + 2] += a4.z * gp;
-          B[4 * q + 3] += a4.w * gp;
-        }
-      }
-    }
-    // SB = sum B Y, V = sum A dY/du (u components independent)
-    float zp[5];
-    zp[0] = 1.0f;
-#pragma unroll
-    for (int q = 1; q < 5; ++q) zp[q] = zp[q - 1] * uz;
-    float SB = 0.0f, vx = 0.0f, vy = 0.0f, vz = 0.0f;
-    int idx = 0;
-#pragma unroll
-    for (int Lq = 1; Lq <= 4; ++Lq) {
-      if (Lq > p.L_max) break;
-      float re0 = 1.0f, im0 = 0.0f;   // (ux + i uy)^(m-1)
-#pragma unroll
-      for (int m = 0; m <= Lq; ++m) {
-        float dzf;
-        const float zf = zpoly(Lq, m, zp, &dzf);
-        if (m == 0) {
-          SB += B[idx] * zf;
-          vz += A[idx] * dzf;
-          ++idx;
-        } else {
-          const float re = ux * re0 - uy * im0;
-          const float im = ux * im0 + uy * re0;
-          const float Ar = A[idx], Ai = A[idx + 1];
-          SB += (B[idx] * re + B[idx + 1] * im) * zf;
-          const float mzf = m * zf;
-          vx += mzf * (Ar * re0 + Ai * im0);
-          vy += mzf * (Ai * re0 - Ar * im0);
-          vz += dzf * (Ar * re + Ai * im);
-          idx += 2;
-          re0 = re;
-          im0 = im;
-        }
-      }
-    }
-    const float uv = ux * vx + uy * vy + uz * vz;
-    f12[static_cast<size_t>(i) * mn_a + k] =
-      make_float4(SB * ux + (vx - uv * ux) * dinv, SB * uy + (vy - uv * uy) * dinv,
-                  SB * uz + (vz - uv * uz) * dinv, 0.0f);
+    const float3 f = angular_edge_force<KM, NAM>(p, sm + (t1 * T + t2) * nA * KP, ai, rc, dx,
+                                                 dy, dz);
+    f12[static_cast<size_t>(i) * mn_a + k] = make_float4(f.x, f.y, f.z, 0.0f);
   }
 }
 
@@ -631,16 +686,27 @@ k_angular_f12(const ModelParams p, int N, const Box* __restrict__ box,
 // gather
 // ---------------------------------------------------------------------------
 
-template <int G, int KM>
+// XR: explicit rows.  The rows then may hold one neighbour several times
+// (periodic images), so the reverse partial force f12(j,i) is not looked up
+// but evaluated here from j's moment derivatives at -r: the angular force
+// work doubles and the f12 buffer and its kernel drop out.
+template <int G, int KM, int NAM, bool XR>
 __global__ void __launch_bounds__(256)
 k_gather(const ModelParams p, int N, const Box* __restrict__ box,
          const Site* __restrict__ sites, const int* __restrict__ nn_r, const int* __restrict__ nl_r,
          int mn_r, const int* __restrict__ nn_a, const int* __restrict__ nl_a, int mn_a,
-         const float* __restrict__ alpha, const float4* __restrict__ f12,
-         const double* __restrict__ pe_ann, double* __restrict__ pe, double* __restrict__ force,
-         double* __restrict__ virial, int accumulate, NeighborState* st)
+         const float4* __restrict__ er, const float4* __restrict__ ea,
+         const float* __restrict__ acoef, const float* __restrict__ alpha,
+         const float4* __restrict__ f12, const double* __restrict__ pe_ann,
+         double* __restrict__ pe, double* __restrict__ force, double* __restrict__ virial,
+         int accumulate, NeighborState* st)
 {
   constexpr int KP = (KM + 3) & ~3;
+  extern __shared__ float sm[];
+  if constexpr (XR) {
+    load_angular_tables<KP>(p, sm);
+    __syncthreads();
+  }
   const int gl = threadIdx.x % G;
   const int i = (blockIdx.x * blockDim.x + threadIdx.x) / G;
   const bool active = i < N;
@@ -659,10 +725,20 @@ k_gather(const ModelParams p, int N, const Box* __restrict__ box,
     const int nr = nn_r[i];
     const int* rrow = nl_r + static_cast<size_t>(i) * mn_r;
     for (int k = gl; k < nr; k += G) {
-      const int j = rrow[k];
-      int t2;
+      int j, t2;
       float dx, dy, dz;
-      site_displacement(b, sites, xi, yi, zi, j, dx, dy, dz, t2);
+      if constexpr (XR) {
+        const float4 e = er[static_cast<size_t>(i) * mn_r + k];
+        const unsigned bits = static_cast<unsigned>(__float_as_int(e.w));
+        j = static_cast<int>(bits & kRowIndexMask);
+        t2 = static_cast<int>(bits >> kRowTypeShift);
+        dx = e.x;
+        dy = e.y;
+        dz = e.z;
+      } else {
+        j = rrow[k];
+        site_displacement(b, sites, xi, yi, zi, j, dx, dy, dz, t2);
+      }
       const float d = sqrtf(dx * dx + dy * dy + dz * dz);
       const float dinv = 1.0f / d;
       const float rc = (rr1 + p.rc_r[t2]) * 0.5f;
@@ -700,24 +776,45 @@ k_gather(const ModelParams p, int N, const Box* __restrict__ box,
     const int zi_ = p.Z[t1];
     const float pow_zi = p.zbl ? powf(static_cast<float>(zi_), 0.23f) : 0.0f;
     for (int k = gl; k < na; k += G) {
-      const int j = arow[k];
       int t2;
       float dx, dy, dz;
-      site_displacement(b, sites, xi, yi, zi, j, dx, dy, dz, t2);
-      const float4 a12 = f12[static_cast<size_t>(i) * mn_a + k];
-      // reverse slot: i inside j's ascending row
-      const int* jrow = nl_a + static_cast<size_t>(j) * mn_a;
-      const int nj = nn_a[j];
-      int lo = 0, hi = nj - 1;
-      while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (__ldg(jrow + mid) < i) lo = mid + 1; else hi = mid;
-      }
-      float4 a21 = f12[static_cast<size_t>(j) * mn_a + lo];
-      if (nj == 0 || __ldg(jrow + lo) != i) {
-        // only a truncated (overflowed) row can lose the reverse edge
-        a21 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        atomicOr(&st->overflow, 4);
+      float4 a12, a21;
+      if constexpr (XR) {
+        const float4 e = ea[static_cast<size_t>(i) * mn_a + k];
+        const unsigned bits = static_cast<unsigned>(__float_as_int(e.w));
+        const int j = static_cast<int>(bits & kRowIndexMask);
+        t2 = static_cast<int>(bits >> kRowTypeShift);
+        dx = e.x;
+        dy = e.y;
+        dz = e.z;
+        const float rc = (p.rc_a[t1] + p.rc_a[t2]) * 0.5f;
+        const int nA = p.nA;
+        const float3 fij = angular_edge_force<KM, NAM>(
+          p, sm + (t1 * T + t2) * nA * KP, acoef + static_cast<size_t>(i) * nA * kNumLM, rc, dx,
+          dy, dz);
+        const float3 fji = angular_edge_force<KM, NAM>(
+          p, sm + (t2 * T + t1) * nA * KP, acoef + static_cast<size_t>(j) * nA * kNumLM, rc, -dx,
+          -dy, -dz);
+        a12 = make_float4(fij.x, fij.y, fij.z, 0.0f);
+        a21 = make_float4(fji.x, fji.y, fji.z, 0.0f);
+      } else {
+        const int j = arow[k];
+        site_displacement(b, sites, xi, yi, zi, j, dx, dy, dz, t2);
+        a12 = f12[static_cast<size_t>(i) * mn_a + k];
+        // reverse slot: i inside j's ascending row
+        const int* jrow = nl_a + static_cast<size_t>(j) * mn_a;
+        const int nj = nn_a[j];
+        int lo = 0, hi = nj - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi) >> 1;
+          if (__ldg(jrow + mid) < i) lo = mid + 1; else hi = mid;
+        }
+        a21 = f12[static_cast<size_t>(j) * mn_a + lo];
+        if (nj == 0 || __ldg(jrow + lo) != i) {
+          // only a truncated (overflowed) row can lose the reverse edge
+          a21 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+          atomicOr(&st->overflow, 4);
+        }
       }
       F[0] += a12.x - a21.x;
       F[1] += a12.y - a21.y;
@@ -800,20 +897,21 @@ bool small_shape(const ModelParams& p)
   return p.nR <= kSmallN && p.nA <= kSmallN && p.kR <= kSmallK && p.kA <= kSmallK;
 }
 
-template <int G, int NRM, int KM, int NAM>
-void launch_fused_t(Engine& e, int N, const double* pos, const int* type, cudaStream_t s)
+template <int G, int NRM, int KM, int NAM, bool XR>
+void launch_fused_t(Engine& e, int N, cudaStream_t s)
 {
   NeighborBuffers& nb = e.nbr;
   constexpr int APB = kBlock / G;
   const int blocks = (N + APB - 1) / APB;
   const size_t smem = fused_layout(e.params, APB, (KM + 3) & ~3).total_bytes;
-  k_nep_fused<G, NRM, KM, NAM><<<blocks, kBlock, smem, s>>>(
+  k_nep_fused<G, NRM, KM, NAM, XR><<<blocks, kBlock, smem, s>>>(
     e.params, N, e.d_box, e.scratch.sites, e.d_nstate, nb.nn_v, nb.nl_v, nb.mn_v, nb.nn_r, nb.nl_r,
-    nb.mn_r, nb.nn_a, nb.nl_a, nb.mn_a, e.scratch.alpha, e.scratch.acoef, e.scratch.pe_ann);
+    nb.mn_r, nb.nn_a, nb.nl_a, nb.mn_a, e.xr.er, e.xr.ea, e.scratch.alpha, e.scratch.acoef,
+    e.scratch.pe_ann);
 }
 
 template <int G, int KM, int NAM>
-void launch_f12_t(Engine& e, int N, const double* pos, const int* type, cudaStream_t s)
+void launch_f12_t(Engine& e, int N, cudaStream_t s)
 {
   NeighborBuffers& nb = e.nbr;
   constexpr int APB = kBlock / G;
@@ -828,21 +926,40 @@ void launch_f12_t(Engine& e, int N, const double* pos, const int* type, cudaStre
 template <int G, int NRM, int KM, int NAM>
 void set_fused_smem_t(size_t bytes)
 {
-  cudaFuncSetAttribute(k_nep_fused<G, NRM, KM, NAM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       static_cast<int>(bytes));
+  cudaFuncSetAttribute(k_nep_fused<G, NRM, KM, NAM, false>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+  cudaFuncSetAttribute(k_nep_fused<G, NRM, KM, NAM, true>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
 }
 
-template <int G, int KM>
-void launch_gather_t(Engine& e, int N, const double* pos, const int* type, double* pe,
-                     double* force, double* virial, bool accumulate, cudaStream_t s)
+template <int G, int KM, int NAM, bool XR>
+void launch_gather_t(Engine& e, int N, double* pe, double* force, double* virial,
+                     bool accumulate, cudaStream_t s)
 {
   NeighborBuffers& nb = e.nbr;
   const int threads = 256;
   const int blocks = static_cast<int>((static_cast<long long>(N) * G + threads - 1) / threads);
-  k_gather<G, KM><<<blocks, threads, 0, s>>>(
+  const size_t smem =
+    XR ? sizeof(float) * e.params.T * e.params.T * e.params.nA * ((KM + 3) & ~3) : 0;
+  k_gather<G, KM, NAM, XR><<<blocks, threads, smem, s>>>(
     e.params, N, e.d_box, e.scratch.sites, nb.nn_r, nb.nl_r, nb.mn_r, nb.nn_a, nb.nl_a, nb.mn_a,
-    e.scratch.alpha, e.scratch.f12, e.scratch.pe_ann, pe, force, virial, accumulate ? 1 : 0,
-    e.d_nstate);
+    e.xr.er, e.xr.ea, e.scratch.acoef, e.scratch.alpha, e.scratch.f12, e.scratch.pe_ann, pe,
+    force, virial, accumulate ? 1 : 0, e.d_nstate);
+}
+
+template <int G, int NRM, int KM, int NAM>
+void launch_fused_g(Engine& e, int N, cudaStream_t s)
+{
+  if (e.use_xr) launch_fused_t<G, NRM, KM, NAM, true>(e, N, s);
+  else launch_fused_t<G, NRM, KM, NAM, false>(e, N, s);
+}
+
+template <int G, int KM, int NAM>
+void launch_gather_g(Engine& e, int N, double* pe, double* force, double* virial,
+                     bool accumulate, cudaStream_t s)
+{
+  if (e.use_xr) launch_gather_t<G, KM, NAM, true>(e, N, pe, force, virial, accumulate, s);
+  else launch_gather_t<G, KM, NAM, false>(e, N, pe, force, virial, accumulate, s);
 }
 
 }  // namespace
@@ -870,35 +987,36 @@ void set_fused_smem_limits(const ModelParams& p)
   }
 }
 
-void launch_descriptor(Engine& e, int N, const double* pos, const int* type, cudaStream_t stream)
+void launch_descriptor(Engine& e, int N, const double*, const int*, cudaStream_t stream)
 {
   const bool small = small_shape(e.params);
   if (e.group == 8) {
-    if (small) launch_fused_t<8, kSmallN, kSmallK, kSmallN>(e, N, pos, type, stream);
-    else launch_fused_t<8, kMaxN, kMaxBasis, kMaxN>(e, N, pos, type, stream);
+    if (small) launch_fused_g<8, kSmallN, kSmallK, kSmallN>(e, N, stream);
+    else launch_fused_g<8, kMaxN, kMaxBasis, kMaxN>(e, N, stream);
   } else {
-    if (small) launch_fused_t<4, kSmallN, kSmallK, kSmallN>(e, N, pos, type, stream);
-    else launch_fused_t<4, kMaxN, kMaxBasis, kMaxN>(e, N, pos, type, stream);
+    if (small) launch_fused_g<4, kSmallN, kSmallK, kSmallN>(e, N, stream);
+    else launch_fused_g<4, kMaxN, kMaxBasis, kMaxN>(e, N, stream);
   }
+  if (e.use_xr) return;   // the explicit-row gather evaluates the angular forces itself
   if (e.f12_group == 8) {
-    if (small) launch_f12_t<8, kSmallK, kSmallN>(e, N, pos, type, stream);
-    else launch_f12_t<8, kMaxBasis, kMaxN>(e, N, pos, type, stream);
+    if (small) launch_f12_t<8, kSmallK, kSmallN>(e, N, stream);
+    else launch_f12_t<8, kMaxBasis, kMaxN>(e, N, stream);
   } else {
-    if (small) launch_f12_t<4, kSmallK, kSmallN>(e, N, pos, type, stream);
-    else launch_f12_t<4, kMaxBasis, kMaxN>(e, N, pos, type, stream);
+    if (small) launch_f12_t<4, kSmallK, kSmallN>(e, N, stream);
+    else launch_f12_t<4, kMaxBasis, kMaxN>(e, N, stream);
   }
 }
 
-void launch_gather(Engine& e, int N, const double* pos, const int* type, double* pe,
-                   double* force, double* virial, bool accumulate, cudaStream_t stream)
+void launch_gather(Engine& e, int N, const double*, const int*, double* pe, double* force,
+                   double* virial, bool accumulate, cudaStream_t stream)
 {
   const bool small = small_shape(e.params);
   if (e.gather_group == 4) {
-    if (small) launch_gather_t<4, kSmallK>(e, N, pos, type, pe, force, virial, accumulate, stream);
-    else launch_gather_t<4, kMaxBasis>(e, N, pos, type, pe, force, virial, accumulate, stream);
+    if (small) launch_gather_g<4, kSmallK, kSmallN>(e, N, pe, force, virial, accumulate, stream);
+    else launch_gather_g<4, kMaxBasis, kMaxN>(e, N, pe, force, virial, accumulate, stream);
   } else {
-    if (small) launch_gather_t<8, kSmallK>(e, N, pos, type, pe, force, virial, accumulate, stream);
-    else launch_gather_t<8, kMaxBasis>(e, N, pos, type, pe, force, virial, accumulate, stream);
+    if (small) launch_gather_g<8, kSmallK, kSmallN>(e, N, pe, force, virial, accumulate, stream);
+    else launch_gather_g<8, kMaxBasis, kMaxN>(e, N, pe, force, virial, accumulate, stream);
   }
 }
 

@@ -188,7 +188,9 @@ def refgpu_lib():
         L.refgpu_set_atoms.argtypes = [vp, vp, vp]
         L.refgpu_compute.argtypes = [vp, _f64p, _i32p, vp, vp, vp]
         L.refgpu_neighbors.argtypes = [vp, ctypes.c_int, _i32p, _i32p, ctypes.c_int]
-        for f in ("refgpu_set_atoms", "refgpu_compute", "refgpu_neighbors"):
+        L.refgpu_neighbors_small.argtypes = [vp, ctypes.c_int, _i32p, _i32p, ctypes.c_int]
+        for f in ("refgpu_set_atoms", "refgpu_compute", "refgpu_neighbors",
+                  "refgpu_neighbors_small"):
             getattr(L, f).restype = ctypes.c_int
         _refgpu = L
     return _refgpu
@@ -222,9 +224,11 @@ class RefGpuModel:
         if refgpu_lib().refgpu_compute(self._h, h, pbc, *ptrs):
             raise RuntimeError("reference compute failed")
 
-    def neighbors(self, which, mn):
+    def neighbors(self, which, mn, small=False):
         nn = np.zeros(self.n, dtype=np.int32)
         nl = np.zeros(self.n * mn, dtype=np.int32)
-        refgpu_lib().refgpu_neighbors(self._h, which, nn, nl, mn)
+        fn = refgpu_lib().refgpu_neighbors_small if small else refgpu_lib().refgpu_neighbors
+        if fn(self._h, which, nn, nl, mn):
+            raise RuntimeError("reference neighbour rows unavailable")
         nl = nl.reshape(self.n, mn)
         return [nl[i, :nn[i]].copy() for i in range(self.n)]

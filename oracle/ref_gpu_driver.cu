@@ -102,3 +102,26 @@ extern "C" int refgpu_neighbors(void* p, int which, int* nn, int* nl, int mn)
   }
   return 0;
 }
+
+// Typewise rows of the last small-box compute (which = 0 radial, 1 angular):
+// the neighbour index of every (atom, image) edge in the reference's order,
+// copied row-major like refgpu_neighbors (small_box_data, nep.cu:2080-2095).
+extern "C" int refgpu_neighbors_small(void* p, int which, int* nn, int* nl, int mn)
+{
+  auto* r = static_cast<RefGpu*>(p);
+  const int n = r->n;
+  auto& sb = r->nep->small_box_data;
+  auto& NN = which == 0 ? sb.NN_radial : sb.NN_angular;
+  auto& NL = which == 0 ? sb.NL_radial : sb.NL_angular;
+  if (NN.size() != static_cast<size_t>(n)) return 1;
+  std::vector<int> hnn(n), hnl(NL.size());
+  NN.copy_to_host(hnn.data(), n);
+  NL.copy_to_host(hnl.data(), NL.size());
+  const size_t cap = NL.size() / n;
+  for (int i = 0; i < n; ++i) {
+    nn[i] = hnn[i];
+    for (int k = 0; k < hnn[i] && k < mn && static_cast<size_t>(k) < cap; ++k)
+      nl[static_cast<size_t>(i) * mn + k] = hnl[static_cast<size_t>(k) * n + i];
+  }
+  return 0;
+}
