@@ -1,0 +1,748 @@
+// serve.cu -- many independent structures on one GPU: nepx_compute_batch and
+// the continuous-batching server (include/nepx.h).
+//
+// Both run the explicit-row force path (explicit.cu) over structures packed
+// back to back in one atom range; each structure's rows, descriptors and
+// forces depend on its own atoms only, so a structure gets the same result
+// alone and in any mix.
+//
+// Server design.  A worker thread owns the potential handle and an arena of
+// max_atoms atoms (SoA arrays, double-buffered).  Each step it
+//   1. admits queued requests in arrival order while they fit the arena,
+//   2. rebuilds the arena: survivors move to their new offsets and the new
+//      requests' inputs arrive in one host-to-device copy of a pinned block,
+//      scattered by one kernel (k_arena_build); the structure table
+//      (StructInfo, offsets, per-structure step flags) is one more copy,
+//   3. runs the NVE first half step for the MD segments, the explicit rows,
+//      the descriptor/ANN kernel and the gather over every resident atom,
+//      then the second half step,
+//   4. gathers the outputs of the requests that finish with this step into
+//      one block (k_pack_out) and copies it back in one transfer.
+// A single-point request finishes with its first step; an MD segment of k
+// steps after 1 + k steps (the first evaluates the initial forces).  The
+// velocity-Verlet arithmetic is that of the nepx_md NVE path (md.cu), with
+// positions wrapped into each structure's own box.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <new>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/nepx.h"
+#include "handle.h"
+#include "xbox.h"
+
+namespace nepx {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kOutFields = 19;   // pe, force 3, virial 9, pos 3, vel 3
+
+__device__ __forceinline__ int find_struct(const int* __restrict__ soff, int S, int i)
+{
+  int lo = 0, hi = S - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (soff[mid] <= i) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// New arena from the old one and the incoming block.  src[s].x >= 0: the
+// structure's old offset; else src[s].y is its offset in the incoming block
+// (SoA doubles pos 3, vel 3, mass with stride t_in, then t_in ints of type).
+__global__ void k_arena_build(int T, int S, const int* __restrict__ soff,
+                              const int2* __restrict__ src, int t_old,
+                              const int* __restrict__ o_type, const double* __restrict__ o_pos,
+                              const double* __restrict__ o_vel, const double* __restrict__ o_mass,
+                              const double* __restrict__ o_force, int t_in,
+                              const double* __restrict__ in_d, const int* __restrict__ in_type,
+                              int* n_type, int* n_sid, double* n_pos, double* n_vel,
+                              double* n_mass, double* n_force)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= T) return;
+  const int s = find_struct(soff, S, i);
+  const int local = i - soff[s];
+  const int2 sr = src[s];
+  n_sid[i] = s;
+  if (sr.x >= 0) {
+    const int j = sr.x + local;
+    n_type[i] = o_type[j];
+    n_mass[i] = o_mass[j];
+    for (int d = 0; d < 3; ++d) {
+      n_pos[d * T + i] = o_pos[d * t_old + j];
+      n_vel[d * T + i] = o_vel[d * t_old + j];
+      n_force[d * T + i] = o_force[d * t_old + j];
+    }
+  } else {
+    const int j = sr.y + local;
+    n_type[i] = in_type[j];
+    n_mass[i] = in_d[6 * t_in + j];
+    for (int d = 0; d < 3; ++d) {
+      n_pos[d * T + i] = in_d[d * t_in + j];
+      n_vel[d * T + i] = in_d[(3 + d) * t_in + j];
+      n_force[d * T + i] = 0.0;
+    }
+  }
+}
+
+// First half kick and drift of the atoms whose structure steps (flag bit 0),
+// wrapped into the structure's box: the arithmetic of md.cu k_vv1 (NVE).
+__global__ void k_vv1_batch(int T, const int* __restrict__ sid, const int* __restrict__ sflag,
+                            const double* __restrict__ sdt, const StructInfo* __restrict__ si,
+                            const double* __restrict__ mass, const double* __restrict__ force,
+                            double* pos, double* vel)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= T) return;
+  const int s = sid[i];
+  if (!(sflag[s] & 1)) return;
+  const double dt = sdt[s];
+  const double half = dt * 0.5;
+  const double im = 1.0 / mass[i];
+  double r[3];
+  for (int d = 0; d < 3; ++d) {
+    const double v = vel[d * T + i] * 1.0 + force[d * T + i] * im * half;
+    vel[d * T + i] = v;
+    r[d] = pos[d * T + i] + v * dt;
+  }
+  const Box& b = si[s].box;
+  double f[3];
+  for (int d = 0; d < 3; ++d) {
+    f[d] = b.hinv[3 * d] * r[0] + b.hinv[3 * d + 1] * r[1] + b.hinv[3 * d + 2] * r[2];
+    if (b.pbc[d] == 1) {
+      if (f[d] < 0.0) f[d] += 1.0;
+      else if (f[d] > 1.0) f[d] -= 1.0;
+    }
+  }
+  for (int d = 0; d < 3; ++d)
+    pos[d * T + i] = b.h[3 * d] * f[0] + b.h[3 * d + 1] * f[1] + b.h[3 * d + 2] * f[2];
+}
+
+// Second half kick (md.cu k_vv2_thermo without the thermo sums).
+__global__ void k_vv2_batch(int T, const int* __restrict__ sid, const int* __restrict__ sflag,
+                            const double* __restrict__ sdt, const double* __restrict__ mass,
+                            const double* __restrict__ force, double* vel)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= T) return;
+  const int s = sid[i];
+  if (!(sflag[s] & 1)) return;
+  const double half = sdt[s] * 0.5;
+  const double im = 1.0 / mass[i];
+  for (int d = 0; d < 3; ++d) vel[d * T + i] = vel[d * T + i] + force[d * T + i] * im * half;
+}
+
+// Outputs of the finishing structures into one block, SoA with stride t_out:
+// pe, force 3, virial 9, pos 3, vel 3.  fin[k] = (arena offset, out offset).
+__global__ void k_pack_out(int t_out, int nfin, const int* __restrict__ fin_out_off,
+                           const int* __restrict__ fin_arena_off, int T,
+                           const double* __restrict__ pe, const double* __restrict__ force,
+                           const double* __restrict__ virial, const double* __restrict__ pos,
+                           const double* __restrict__ vel, double* out)
+{
+  const int o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= t_out) return;
+  const int k = find_struct(fin_out_off, nfin, o);
+  const int a = fin_arena_off[k] + (o - fin_out_off[k]);
+  out[o] = pe[a];
+  for (int d = 0; d < 3; ++d) out[(1 + d) * t_out + o] = force[d * T + a];
+  for (int d = 0; d < 9; ++d) out[(4 + d) * t_out + o] = virial[d * T + a];
+  for (int d = 0; d < 3; ++d) out[(13 + d) * t_out + o] = pos[d * T + a];
+  for (int d = 0; d < 3; ++d) out[(16 + d) * t_out + o] = vel[d * T + a];
+}
+
+std::string struct_info(const Engine& e, const nepx_box& box, int off, int n, StructInfo& si)
+{
+  Box b;
+  const std::string err = make_box(box.h, box.pbc, b);
+  if (!err.empty()) return err;
+  if (expanded_box(b, e.model.rc_radial_max, si))
+    return "box thinner than 2.5 (rc + 1) in one periodic direction and thicker than 10 rc "
+           "in another (unsupported, as in the reference)";
+  si.off = off;
+  si.n = n;
+  return "";
+}
+
+template <typename T>
+bool dalloc(T*& p, size_t n)
+{
+  return cudaMalloc(reinterpret_cast<void**>(&p), std::max<size_t>(n, 1) * sizeof(T)) ==
+         cudaSuccess;
+}
+
+template <typename T>
+bool halloc(T*& p, size_t n)
+{
+  return cudaMallocHost(reinterpret_cast<void**>(&p), std::max<size_t>(n, 1) * sizeof(T)) ==
+         cudaSuccess;
+}
+
+int grid(int n) { return (n + kThreads - 1) / kThreads; }
+
+}  // namespace
+
+// Explicit rows + force over structures already described in e.xr (d_si,
+// d_soff, n_struct uploaded).  Shared by the batch call and the server.
+void launch_batch_force(Engine& e, int T, const double* pos, const int* type, double* pe,
+                        double* force, double* virial, bool accumulate, cudaStream_t s)
+{
+  e.use_xr = true;
+  e.xr.from_box = false;
+  launch_explicit_rows(e, T, pos, type, s);
+  if (!e.tuned) engine_autotune(e, T, pos, type, s);
+  launch_force(e, T, pos, type, pe, force, virial, accumulate, s);
+  // the Verlet-path state of the handle no longer matches its last box
+  e.force_rebuild = true;
+  e.have_box = false;
+  e.box_owner = nullptr;
+}
+
+}  // namespace nepx
+
+// ---------------------------------------------------------------------------
+// the server
+// ---------------------------------------------------------------------------
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Pending {
+  long long ticket = 0;
+  int n = 0, md_steps = 0;
+  double dt = 0.0;          // fs
+  nepx_box box{};
+  std::vector<int> type;
+  std::vector<double> pos, vel, mass;   // vel in natural units
+  nepx_result* out = nullptr;
+  double t_submit = 0.0;
+};
+
+struct Resident {
+  long long ticket = 0;
+  int n = 0, md_steps = 0, steps_done = 0;
+  bool fresh = true;        // initial forces not evaluated yet
+  double dt = 0.0;          // fs
+  nepx::StructInfo si{};
+  int off = 0;              // offset in the current arena
+  nepx_result* out = nullptr;
+  double t_submit = 0.0, t_admit = 0.0;
+};
+
+// Device arrays of one arena buffer.
+struct Arena {
+  int* type = nullptr;
+  int* sid = nullptr;
+  double *pos = nullptr, *vel = nullptr, *mass = nullptr, *force = nullptr;
+};
+
+}  // namespace
+
+struct nepx_server {
+  nepx_t* h = nullptr;
+  int max_atoms = 0, max_struct = 0;
+  cudaStream_t stream = nullptr;
+  Arena arena[2];
+  int cur = 0;
+  double *d_pe = nullptr, *d_virial = nullptr, *d_out = nullptr, *d_in = nullptr;
+  int* d_ctl = nullptr;       // per-structure src (int2), flags, finishing lists
+  double* d_sdt = nullptr;
+  double *h_in = nullptr, *h_out = nullptr, *h_sdt = nullptr;
+  int* h_ctl = nullptr;
+  nepx::StructInfo* h_si = nullptr;
+  int* h_soff = nullptr;
+  std::thread worker;
+  std::mutex mu;
+  std::condition_variable cv, done_cv;
+  std::deque<Pending> queue;
+  std::unordered_map<long long, int> status;   // -1 pending, else the request's code
+  long long next_ticket = 1;
+  bool stopping = false;
+  std::string error;
+  Clock::time_point t0;
+  // statistics
+  double done = 0, steps = 0, atom_steps = 0, busy = 0, resident_atoms = 0, resident_structs = 0;
+
+  double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
+  void run();
+};
+
+namespace {
+
+void free_server(nepx_server* S)
+{
+  for (auto& a : S->arena) {
+    void* ptrs[] = {a.type, a.sid, a.pos, a.vel, a.mass, a.force};
+    for (void* p : ptrs)
+      if (p) cudaFree(p);
+  }
+  void* dptrs[] = {S->d_pe, S->d_virial, S->d_out, S->d_in, S->d_ctl, S->d_sdt};
+  for (void* p : dptrs)
+    if (p) cudaFree(p);
+  void* hptrs[] = {S->h_in, S->h_out, S->h_sdt, S->h_ctl, S->h_si, S->h_soff};
+  for (void* p : hptrs)
+    if (p) cudaFreeHost(p);
+  if (S->stream) cudaStreamDestroy(S->stream);
+}
+
+}  // namespace
+
+void nepx_server::run()
+{
+  using namespace nepx;
+  Engine& e = h->engine;
+  cudaStream_t s = stream;
+  std::vector<Resident> res;   // arena order
+  int T = 0;                   // atoms in the current arena
+  const int MS = max_struct;
+  // control block layout (ints): src int2[MS] | flags[MS] | fin_out_off[MS+1] | fin_arena_off[MS]
+  int* c_src = h_ctl;
+  int* c_flag = h_ctl + 2 * MS;
+  int* c_fout = c_flag + MS;
+  int* c_farena = c_fout + MS + 1;
+  const size_t ctl_ints = 2 * MS + MS + (MS + 1) + MS;
+  for (;;) {
+    // ---- 1. admission --------------------------------------------------------
+    std::vector<Pending> adm;
+    {
+      std::unique_lock<std::mutex> lk(mu);
+      cv.wait(lk, [&] { return !queue.empty() || !res.empty() || stopping; });
+      if (queue.empty() && res.empty()) break;   // stopping with nothing left
+      int atoms = T;
+      int nst = static_cast<int>(res.size());
+      while (!queue.empty()) {
+        Pending& p = queue.front();
+        if (atoms + p.n > max_atoms || nst + 1 > MS) break;
+        atoms += p.n;
+        ++nst;
+        adm.push_back(std::move(p));
+        queue.pop_front();
+      }
+    }
+    const double t_tick = now();
+    // ---- 2. new arena layout: survivors in order, then the admitted ------------
+    const int S_old = static_cast<int>(res.size());
+    int t_in = 0;
+    for (const Pending& p : adm) t_in += p.n;
+    std::vector<int> in_off(adm.size());
+    {
+      int o = 0;
+      for (size_t k = 0; k < adm.size(); ++k) {
+        in_off[k] = o;
+        o += adm[k].n;
+      }
+    }
+    int Tn = 0;
+    for (int k = 0; k < S_old; ++k) {
+      c_src[2 * k] = res[k].off;
+      c_src[2 * k + 1] = 0;
+      res[k].off = Tn;
+      Tn += res[k].n;
+    }
+    for (size_t k = 0; k < adm.size(); ++k) {
+      Pending& p = adm[k];
+      Resident r;
+      r.ticket = p.ticket;
+      r.n = p.n;
+      r.md_steps = p.md_steps;
+      r.dt = p.dt;
+      r.out = p.out;
+      r.t_submit = p.t_submit;
+      r.t_admit = t_tick;
+      r.off = Tn;
+      struct_info(e, p.box, 0, p.n, r.si);   // validated at submit
+      const int idx = static_cast<int>(res.size());
+      c_src[2 * idx] = -1;
+      c_src[2 * idx + 1] = in_off[k];
+      // incoming block: pos 3, vel 3, mass (doubles, stride t_in), then types
+      for (int d = 0; d < 3; ++d) {
+        std::memcpy(h_in + static_cast<size_t>(d) * t_in + in_off[k], p.pos.data() + d * p.n,
+                    sizeof(double) * p.n);
+        if (!p.vel.empty())
+          std::memcpy(h_in + static_cast<size_t>(3 + d) * t_in + in_off[k],
+                      p.vel.data() + d * p.n, sizeof(double) * p.n);
+        else
+          std::memset(h_in + static_cast<size_t>(3 + d) * t_in + in_off[k], 0,
+                      sizeof(double) * p.n);
+      }
+      for (int a = 0; a < p.n; ++a)
+        h_in[static_cast<size_t>(6) * t_in + in_off[k] + a] = p.mass.empty() ? 1.0 : p.mass[a];
+      std::memcpy(reinterpret_cast<int*>(h_in + static_cast<size_t>(7) * t_in) + in_off[k],
+                  p.type.data(), sizeof(int) * p.n);
+      Tn += p.n;
+      res.push_back(r);
+    }
+    const int S = static_cast<int>(res.size());
+    // structure table, offsets and step flags
+    int nfin = 0, t_out = 0;
+    std::vector<int> fin_idx;
+    for (int k = 0; k < S; ++k) {
+      Resident& r = res[k];
+      r.si.off = r.off;
+      r.si.n = r.n;
+      h_si[k] = r.si;
+      h_soff[k] = r.off;
+      c_flag[k] = r.fresh ? 0 : 1;
+      h_sdt[k] = r.dt / kTimeUnit;
+      const bool finishes = r.fresh ? r.md_steps == 0 : r.steps_done + 1 == r.md_steps;
+      if (finishes) {
+        c_fout[nfin] = t_out;
+        c_farena[nfin] = r.off;
+        fin_idx.push_back(k);
+        ++nfin;
+        t_out += r.n;
+      }
+    }
+    h_soff[S] = Tn;
+    c_fout[nfin] = t_out;
+    // ---- uploads and the arena rebuild ------------------------------------------
+    Arena& A = arena[cur];
+    Arena& B = arena[1 - cur];
+    if (t_in > 0)
+      cudaMemcpyAsync(d_in, h_in, (sizeof(double) * 7 + sizeof(int)) * t_in,
+                      cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_ctl, h_ctl, sizeof(int) * ctl_ints, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(d_sdt, h_sdt, sizeof(double) * S, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(e.xr.d_si, h_si, sizeof(StructInfo) * S, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(e.xr.d_soff, h_soff, sizeof(int) * (S + 1), cudaMemcpyHostToDevice, s);
+    e.xr.n_struct = S;
+    const int* d_src = d_ctl;
+    const int* d_flag = d_ctl + 2 * MS;
+    const int* d_fout = d_flag + MS;
+    const int* d_farena = d_fout + MS + 1;
+    k_arena_build<<<grid(Tn), kThreads, 0, s>>>(
+      Tn, S, e.xr.d_soff, reinterpret_cast<const int2*>(d_src), T, A.type, A.pos, A.vel, A.mass,
+      A.force, t_in, d_in, reinterpret_cast<const int*>(d_in + static_cast<size_t>(7) * t_in),
+      B.type, B.sid, B.pos, B.vel, B.mass, B.force);
+    cur = 1 - cur;
+    Arena& R = arena[cur];
+    T = Tn;
+    // ---- 3. the step ---------------------------------------------------------------
+    k_vv1_batch<<<grid(T), kThreads, 0, s>>>(T, R.sid, d_flag, d_sdt, e.xr.d_si, R.mass, R.force,
+                                            R.pos, R.vel);
+    launch_batch_force(e, T, R.pos, R.type, d_pe, R.force, d_virial, false, s);
+    k_vv2_batch<<<grid(T), kThreads, 0, s>>>(T, R.sid, d_flag, d_sdt, R.mass, R.force, R.vel);
+    // ---- 4. outputs of the finishing requests ----------------------------------
+    if (nfin > 0) {
+      k_pack_out<<<grid(t_out), kThreads, 0, s>>>(t_out, nfin, d_fout, d_farena, T, d_pe,
+                                                   R.force, d_virial, R.pos, R.vel, d_out);
+      cudaMemcpyAsync(h_out, d_out, sizeof(double) * kOutFields * t_out, cudaMemcpyDeviceToHost,
+                      s);
+    }
+    cudaMemcpyAsync(h->h_state, e.d_nstate, sizeof(NeighborState), cudaMemcpyDeviceToHost, s);
+    const cudaError_t cerr = cudaStreamSynchronize(s);
+    int code = NEPX_OK;
+    std::string msg;
+    if (cerr != cudaSuccess) {
+      code = NEPX_ERR_CUDA;
+      msg = std::string("server step: ") + cudaGetErrorString(cerr);
+    } else {
+      const NeighborState& st = *h->h_state;
+      if (st.overflow) {
+        code = NEPX_ERR_OVERFLOW;
+        msg = "a neighbour row exceeded its capacity; raise MN_radial/MN_angular in nep.txt";
+      } else if (st.nonfinite) {
+        code = NEPX_ERR_NONFINITE;
+        msg = "non-finite energy or force";
+      }
+      if (code) {
+        NeighborState cleared = st;
+        cleared.overflow = 0;
+        cleared.nonfinite = 0;
+        cudaMemcpy(e.d_nstate, &cleared, sizeof(cleared), cudaMemcpyHostToDevice);
+      }
+    }
+    const double t_end = now();
+    // ---- deliver, retire, advance ------------------------------------------------------
+    for (int k = 0; k < nfin; ++k) {
+      Resident& r = res[fin_idx[k]];
+      nepx_result* o = r.out;
+      const int n = r.n;
+      const size_t base = c_fout[k];
+      auto take = [&](double* dst, int field0, int nf, double scale) {
+        if (!dst) return;
+        for (int f = 0; f < nf; ++f)
+          for (int a = 0; a < n; ++a)
+            dst[static_cast<size_t>(f) * n + a] =
+              h_out[static_cast<size_t>(field0 + f) * t_out + base + a] * scale;
+      };
+      take(o->pe, 0, 1, 1.0);
+      take(o->force, 1, 3, 1.0);
+      take(o->virial, 4, 9, 1.0);
+      take(o->pos, 13, 3, 1.0);
+      take(o->vel, 16, 3, 1.0 / kTimeUnit);
+      o->t_submit = r.t_submit;
+      o->t_admit = r.t_admit;
+      o->t_done = t_end;
+    }
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      for (int k = 0; k < nfin; ++k) status[res[fin_idx[k]].ticket] = code;
+      if (code) error = msg;
+      done += nfin;
+      steps += 1;
+      atom_steps += T;
+      busy += t_end - t_tick;
+      resident_atoms += T;
+      resident_structs += S;
+    }
+    if (nfin) done_cv.notify_all();
+    std::vector<Resident> keep;
+    keep.reserve(res.size());
+    for (int k = 0; k < S; ++k) {
+      Resident& r = res[k];
+      const bool fin = r.fresh ? r.md_steps == 0 : r.steps_done + 1 == r.md_steps;
+      if (!r.fresh) ++r.steps_done;
+      r.fresh = false;
+      if (!fin) keep.push_back(r);
+    }
+    // survivors keep their offsets in arena[cur] (the next layout reads them there)
+    res.swap(keep);
+    if (res.empty()) T = 0;
+  }
+}
+
+extern "C" {
+
+int nepx_compute_batch(nepx_t* h, const nepx_struct_desc* descs, int nstruct, const int* d_type,
+                       const double* d_pos, double* d_pe, double* d_force, double* d_virial,
+                       unsigned flags, void* stream)
+{
+  if (!h) return NEPX_ERR_ARG;
+  if (!descs || nstruct < 1 || !d_type || !d_pos || !d_pe || !d_force || !d_virial) {
+    h->error = "null pointer or nstruct < 1";
+    return NEPX_ERR_ARG;
+  }
+  nepx::Engine& e = h->engine;
+  std::vector<nepx::StructInfo> si(nstruct);
+  std::vector<int> soff(nstruct + 1);
+  long long T = 0;
+  for (int k = 0; k < nstruct; ++k) {
+    if (descs[k].n < 1) {
+      h->error = "structure " + std::to_string(k) + " has no atoms";
+      return NEPX_ERR_ARG;
+    }
+    const std::string err = nepx::struct_info(e, descs[k].box, static_cast<int>(T), descs[k].n,
+                                              si[k]);
+    if (!err.empty()) {
+      h->error = "structure " + std::to_string(k) + ": " + err;
+      return NEPX_ERR_BOX;
+    }
+    soff[k] = static_cast<int>(T);
+    T += descs[k].n;
+  }
+  soff[nstruct] = static_cast<int>(T);
+  if (T > e.capacity) {
+    h->error = std::to_string(T) + " atoms exceed the capacity " + std::to_string(e.capacity) +
+               " of this handle";
+    return NEPX_ERR_CAPACITY;
+  }
+  const std::string err = nepx::engine_enable_xr(e, nstruct);
+  if (!err.empty()) {
+    h->error = err;
+    return NEPX_ERR_CUDA;
+  }
+  auto s = static_cast<cudaStream_t>(stream);
+  // a copy of the flags of an earlier call may still be landing in h_state
+  if (h->state_pending) cudaEventSynchronize(h->state_ready);
+  h->state_pending = false;
+  // pageable sources: the copies complete before the calls return
+  cudaMemcpyAsync(e.xr.d_si, si.data(), sizeof(nepx::StructInfo) * nstruct,
+                  cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(e.xr.d_soff, soff.data(), sizeof(int) * (nstruct + 1), cudaMemcpyHostToDevice,
+                  s);
+  e.xr.n_struct = nstruct;
+  nepx::launch_batch_force(e, static_cast<int>(T), d_pos, d_type, d_pe, d_force, d_virial,
+                           (flags & NEPX_ACCUMULATE) != 0, s);
+  if (cudaPeekAtLastError() != cudaSuccess) {
+    h->error = std::string("kernel launch: ") + cudaGetErrorString(cudaGetLastError());
+    return NEPX_ERR_CUDA;
+  }
+  cudaMemcpyAsync(h->h_state, e.d_nstate, sizeof(nepx::NeighborState), cudaMemcpyDeviceToHost, s);
+  cudaEventRecord(h->state_ready, s);
+  h->state_pending = true;
+  if (flags & NEPX_SYNC_CHECK) {
+    if (cudaEventSynchronize(h->state_ready) != cudaSuccess) {
+      h->error = "stream sync failed";
+      return NEPX_ERR_CUDA;
+    }
+    h->state_pending = false;
+    const nepx::NeighborState& st = *h->h_state;
+    if (st.overflow) {
+      h->error = "a neighbour row exceeded its capacity; raise MN_radial/MN_angular in nep.txt";
+      return NEPX_ERR_OVERFLOW;
+    }
+    if (st.nonfinite) {
+      h->error = "non-finite energy or force";
+      return NEPX_ERR_NONFINITE;
+    }
+  }
+  return NEPX_OK;
+}
+
+int nepx_server_create(nepx_t* h, int max_atoms, int max_struct, nepx_server_t** out)
+{
+  if (!h || !out || max_atoms < 1 || max_struct < 1) return NEPX_ERR_ARG;
+  *out = nullptr;
+  nepx::Engine& e = h->engine;
+  if (max_atoms > e.capacity) {
+    h->error = "server arena larger than the handle's max_atoms";
+    return NEPX_ERR_CAPACITY;
+  }
+  if (!nepx::engine_enable_xr(e, max_struct).empty()) return NEPX_ERR_CUDA;
+  auto* S = new (std::nothrow) nepx_server();
+  if (!S) return NEPX_ERR_ARG;
+  S->h = h;
+  S->max_atoms = max_atoms;
+  S->max_struct = max_struct;
+  S->t0 = Clock::now();
+  const size_t N = max_atoms, MS = max_struct;
+  bool ok = cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking) == cudaSuccess;
+  for (auto& a : S->arena)
+    ok = ok && nepx::dalloc(a.type, N) && nepx::dalloc(a.sid, N) &&
+         nepx::dalloc(a.pos, 3 * N) && nepx::dalloc(a.vel, 3 * N) && nepx::dalloc(a.mass, N) &&
+         nepx::dalloc(a.force, 3 * N);
+  ok = ok && nepx::dalloc(S->d_pe, N) && nepx::dalloc(S->d_virial, 9 * N) &&
+       nepx::dalloc(S->d_out, size_t(nepx::kOutFields) * N) && nepx::dalloc(S->d_in, 8 * N) &&
+       nepx::dalloc(S->d_ctl, 5 * MS + 1) && nepx::dalloc(S->d_sdt, MS);
+  ok = ok && nepx::halloc(S->h_in, 8 * N) && nepx::halloc(S->h_out, nepx::kOutFields * N) &&
+       nepx::halloc(S->h_sdt, MS) && nepx::halloc(S->h_ctl, 5 * MS + 1) &&
+       nepx::halloc(S->h_si, MS) && nepx::halloc(S->h_soff, MS + 1);
+  if (ok) ok = cudaMemsetAsync(S->arena[0].force, 0, sizeof(double) * 3 * N, S->stream) ==
+               cudaSuccess;
+  if (!ok) {
+    free_server(S);
+    delete S;
+    h->error = "server allocation failed";
+    return NEPX_ERR_CUDA;
+  }
+  S->worker = std::thread([S] { S->run(); });
+  *out = S;
+  return NEPX_OK;
+}
+
+int nepx_server_destroy(nepx_server_t* S)
+{
+  if (!S) return NEPX_ERR_ARG;
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->stopping = true;
+  }
+  S->cv.notify_all();
+  if (S->worker.joinable()) S->worker.join();
+  free_server(S);
+  delete S;
+  return NEPX_OK;
+}
+
+const char* nepx_server_last_error(const nepx_server_t* S)
+{
+  return S ? S->error.c_str() : "null server";
+}
+
+int nepx_server_submit(nepx_server_t* S, const nepx_request* req, nepx_result* out,
+                       long long* ticket)
+{
+  if (!S || !req || !out || !ticket || req->n < 1 || !req->type || !req->pos)
+    return NEPX_ERR_ARG;
+  if (req->md_steps < 0 || (req->md_steps > 0 && (!req->mass || !req->vel || !(req->dt_fs > 0))))
+    return NEPX_ERR_ARG;
+  const nepx::Engine& e = S->h->engine;
+  if (req->n > S->max_atoms) {
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->error = "request of " + std::to_string(req->n) + " atoms is larger than the arena";
+    return NEPX_ERR_CAPACITY;
+  }
+  nepx::StructInfo si;
+  const std::string err = nepx::struct_info(e, req->box, 0, req->n, si);
+  if (!err.empty()) {
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->error = err;
+    return NEPX_ERR_BOX;
+  }
+  for (int a = 0; a < req->n; ++a)
+    if (req->type[a] < 0 || req->type[a] >= e.model.num_types) return NEPX_ERR_ARG;
+  Pending p;
+  p.n = req->n;
+  p.md_steps = req->md_steps;
+  p.dt = req->dt_fs;
+  p.box = req->box;
+  p.type.assign(req->type, req->type + req->n);
+  p.pos.assign(req->pos, req->pos + 3 * static_cast<size_t>(req->n));
+  if (req->md_steps > 0) {
+    p.mass.assign(req->mass, req->mass + req->n);
+    p.vel.resize(3 * static_cast<size_t>(req->n));
+    for (size_t k = 0; k < p.vel.size(); ++k) p.vel[k] = req->vel[k] * nepx::kTimeUnit;
+  }
+  p.out = out;
+  p.t_submit = S->now();
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    p.ticket = S->next_ticket++;
+    *ticket = p.ticket;
+    S->status[p.ticket] = -1;
+    S->queue.push_back(std::move(p));
+  }
+  S->cv.notify_one();
+  return NEPX_OK;
+}
+
+int nepx_server_poll(nepx_server_t* S, long long ticket, int* done, int* status)
+{
+  if (!S || !done) return NEPX_ERR_ARG;
+  std::lock_guard<std::mutex> lk(S->mu);
+  auto it = S->status.find(ticket);
+  if (it == S->status.end()) return NEPX_ERR_ARG;
+  *done = it->second >= 0;
+  if (status) *status = it->second;
+  return NEPX_OK;
+}
+
+int nepx_server_wait(nepx_server_t* S, long long ticket, int* status)
+{
+  if (!S) return NEPX_ERR_ARG;
+  std::unique_lock<std::mutex> lk(S->mu);
+  auto it = S->status.find(ticket);
+  if (it == S->status.end()) return NEPX_ERR_ARG;
+  S->done_cv.wait(lk, [&] { return S->status[ticket] >= 0; });
+  if (status) *status = S->status[ticket];
+  return NEPX_OK;
+}
+
+int nepx_server_drain(nepx_server_t* S)
+{
+  if (!S) return NEPX_ERR_ARG;
+  std::unique_lock<std::mutex> lk(S->mu);
+  S->done_cv.wait(lk, [&] {
+    for (const auto& kv : S->status)
+      if (kv.second < 0) return false;
+    return true;
+  });
+  return NEPX_OK;
+}
+
+int nepx_server_stats(nepx_server_t* S, double* stats)
+{
+  if (!S || !stats) return NEPX_ERR_ARG;
+  std::lock_guard<std::mutex> lk(S->mu);
+  stats[0] = S->done;
+  stats[1] = S->steps;
+  stats[2] = S->atom_steps;
+  stats[3] = S->busy;
+  stats[4] = S->steps > 0 ? S->resident_atoms / S->steps : 0.0;
+  stats[5] = S->steps > 0 ? S->resident_structs / S->steps : 0.0;
+  stats[6] = static_cast<double>(S->queue.size());
+  stats[7] = S->now();
+  return NEPX_OK;
+}
+
+}  // extern "C"

@@ -31,7 +31,10 @@ EXPORTED = ["nepx_create", "nepx_destroy", "nepx_last_error", "nepx_info", "nepx
             "nepx_notify_box_changed", "nepx_set_skin", "nepx_neighbors", "nepx_neighbor_stats",
             "nepx_md_create", "nepx_md_destroy", "nepx_md_last_error", "nepx_md_set_ensemble",
             "nepx_md_run", "nepx_md_get", "nepx_md_device_state", "nepx_profile",
-            "nepx_md_run_async", "nepx_md_sync", "nepx_compute_noalloc"]
+            "nepx_md_run_async", "nepx_md_sync", "nepx_compute_noalloc", "nepx_compute_batch",
+            "nepx_server_create", "nepx_server_destroy", "nepx_server_last_error",
+            "nepx_server_submit", "nepx_server_poll", "nepx_server_wait", "nepx_server_drain",
+            "nepx_server_stats"]
 
 ENSEMBLES = {"nve": 0, "nvt_ber": 1, "nvt_nhc": 2, "nvt_bdp": 3, "npt_ber": 4, "npt_scr": 5}
 THERMO_COLUMNS = ["T", "KE", "PE", "sxx", "syy", "szz", "syz", "sxz", "sxy", "ax", "ay", "az",
@@ -46,6 +49,22 @@ class NepxError(RuntimeError):
 
 class Box(ctypes.Structure):
     _fields_ = [("h", ctypes.c_double * 9), ("pbc", ctypes.c_int * 3)]
+
+
+class StructDesc(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("box", Box)]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("box", Box), ("type", ctypes.c_void_p),
+                ("pos", ctypes.c_void_p), ("md_steps", ctypes.c_int), ("dt_fs", ctypes.c_double),
+                ("mass", ctypes.c_void_p), ("vel", ctypes.c_void_p)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("pe", ctypes.c_void_p), ("force", ctypes.c_void_p), ("virial", ctypes.c_void_p),
+                ("pos", ctypes.c_void_p), ("vel", ctypes.c_void_p), ("t_submit", ctypes.c_double),
+                ("t_admit", ctypes.c_double), ("t_done", ctypes.c_double)]
 
 
 _lib = None
@@ -92,8 +111,20 @@ def lib():
         L.nepx_md_device_state.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(vp),
                                            ctypes.POINTER(vp), ctypes.POINTER(vp),
                                            ctypes.POINTER(vp)]
+        L.nepx_compute_batch.argtypes = [vp, ctypes.POINTER(StructDesc), ctypes.c_int, vp, vp, vp,
+                                         vp, vp, ctypes.c_uint, vp]
+        L.nepx_server_create.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
+        L.nepx_server_destroy.argtypes = [vp]
+        L.nepx_server_last_error.argtypes = [vp]
+        L.nepx_server_last_error.restype = ctypes.c_char_p
+        L.nepx_server_submit.argtypes = [vp, ctypes.POINTER(Request), ctypes.POINTER(Result),
+                                         ctypes.POINTER(ctypes.c_longlong)]
+        L.nepx_server_poll.argtypes = [vp, ctypes.c_longlong, ip, ip]
+        L.nepx_server_wait.argtypes = [vp, ctypes.c_longlong, ip]
+        L.nepx_server_drain.argtypes = [vp]
+        L.nepx_server_stats.argtypes = [vp, dp]
         for name in EXPORTED:
-            if name not in ("nepx_last_error", "nepx_md_last_error"):
+            if name not in ("nepx_last_error", "nepx_md_last_error", "nepx_server_last_error"):
                 getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib
@@ -171,6 +202,33 @@ class Potential:
         self._check(lib().nepx_compute(self._h, ctypes.byref(box), n, _ptr(types), _ptr(pos),
                                        _ptr(pe), _ptr(force), _ptr(virial), flags,
                                        _stream_ptr(stream)))
+        return pe, force, virial
+
+    def compute_batch(self, structs, types, pos, out=None, accumulate=False, sync_check=False,
+                      stream=None):
+        """Independent structures in one call.
+
+        structs: list of (n, h, pbc); types (T,) int32 and pos (3, T) float64
+        CUDA tensors with the structures back to back.  Returns pe (T,),
+        force (3, T), virial (9, T)."""
+        import torch
+        T = types.numel()
+        descs = (StructDesc * len(structs))()
+        for k, (n, h, pbc) in enumerate(structs):
+            descs[k].n = int(n)
+            descs[k].box = make_box(h, pbc)
+        if out is None:
+            pe = torch.empty(T, dtype=torch.float64, device=pos.device)
+            force = torch.empty(3, T, dtype=torch.float64, device=pos.device)
+            virial = torch.empty(9, T, dtype=torch.float64, device=pos.device)
+        else:
+            pe, force, virial = out
+        assert types.dtype == torch.int32 and pos.dtype == torch.float64
+        assert types.is_contiguous() and pos.is_contiguous()
+        flags = (NEPX_ACCUMULATE if accumulate else 0) | (NEPX_SYNC_CHECK if sync_check else 0)
+        self._check(lib().nepx_compute_batch(self._h, descs, len(structs), _ptr(types), _ptr(pos),
+                                             _ptr(pe), _ptr(force), _ptr(virial), flags,
+                                             _stream_ptr(stream)))
         return pe, force, virial
 
     def neighbors(self, which, n, stream=None):
@@ -292,3 +350,101 @@ class MD:
                                       _dp(vir), ctypes.byref(box)))
         return {"pos": pos.reshape(3, n), "vel": vel.reshape(3, n), "force": force.reshape(3, n),
                 "pe": pe, "virial": vir.reshape(9, n), "h": np.array(box.h[:])}
+
+
+class Server:
+    """Continuous-batching server over one potential (nepx_server_* of include/nepx.h).
+
+    submit() copies a request (host numpy arrays) and returns a ticket; the
+    results land in numpy arrays owned by this object once wait()/poll()
+    report the ticket done."""
+
+    def __init__(self, potential, max_atoms, max_struct):
+        self.pot = potential
+        self._h = ctypes.c_void_p()
+        rc = lib().nepx_server_create(potential._h, int(max_atoms), int(max_struct),
+                                      ctypes.byref(self._h))
+        if rc:
+            raise NepxError(rc, lib().nepx_last_error(potential._h).decode())
+        self._out = {}
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().nepx_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc:
+            raise NepxError(rc, lib().nepx_server_last_error(self._h).decode())
+
+    def submit(self, types, pos, h, pbc=(1, 1, 1), md_steps=0, dt_fs=0.0, masses=None, vel=None,
+               want_virial=True, want_state=False):
+        import numpy as np
+        n = len(types)
+        keep = {"type": np.ascontiguousarray(types, dtype=np.int32),
+                "pos_in": np.ascontiguousarray(pos, dtype=np.float64).reshape(-1)}
+        req = Request()
+        req.n = n
+        req.box = make_box(h, pbc)
+        req.type = keep["type"].ctypes.data
+        req.pos = keep["pos_in"].ctypes.data
+        req.md_steps = int(md_steps)
+        req.dt_fs = float(dt_fs)
+        if md_steps:
+            keep["mass"] = np.ascontiguousarray(masses, dtype=np.float64)
+            keep["vel_in"] = np.ascontiguousarray(vel, dtype=np.float64).reshape(-1)
+            req.mass = keep["mass"].ctypes.data
+            req.vel = keep["vel_in"].ctypes.data
+        res = Result()
+        keep["pe"] = np.zeros(n)
+        keep["force"] = np.zeros((3, n))
+        res.pe = keep["pe"].ctypes.data
+        res.force = keep["force"].ctypes.data
+        if want_virial:
+            keep["virial"] = np.zeros((9, n))
+            res.virial = keep["virial"].ctypes.data
+        if want_state:
+            keep["pos"] = np.zeros((3, n))
+            keep["vel"] = np.zeros((3, n))
+            res.pos = keep["pos"].ctypes.data
+            res.vel = keep["vel"].ctypes.data
+        keep["result"] = res
+        ticket = ctypes.c_longlong()
+        self._check(lib().nepx_server_submit(self._h, ctypes.byref(req), ctypes.byref(res),
+                                             ctypes.byref(ticket)))
+        self._out[ticket.value] = keep
+        return ticket.value
+
+    def poll(self, ticket):
+        done, status = ctypes.c_int(), ctypes.c_int()
+        self._check(lib().nepx_server_poll(self._h, ticket, ctypes.byref(done),
+                                           ctypes.byref(status)))
+        return bool(done.value)
+
+    def wait(self, ticket):
+        """Blocks until the ticket is done; returns its results (dict of numpy arrays)."""
+        status = ctypes.c_int()
+        self._check(lib().nepx_server_wait(self._h, ticket, ctypes.byref(status)))
+        if status.value:
+            raise NepxError(status.value, lib().nepx_server_last_error(self._h).decode())
+        keep = self._out.pop(ticket)
+        r = keep["result"]
+        out = {k: keep[k] for k in ("pe", "force", "virial", "pos", "vel") if k in keep}
+        out.update(t_submit=r.t_submit, t_admit=r.t_admit, t_done=r.t_done)
+        return out
+
+    def drain(self):
+        self._check(lib().nepx_server_drain(self._h))
+
+    def stats(self):
+        s = (ctypes.c_double * 8)()
+        self._check(lib().nepx_server_stats(self._h, s))
+        keys = ["done", "steps", "atom_steps", "busy_s", "mean_atoms", "mean_structs", "queued",
+                "uptime_s"]
+        return dict(zip(keys, list(s)))

@@ -209,6 +209,80 @@ int nepx_md_get(nepx_md_t* md, double* h_pos, double* h_vel, double* h_force, do
 int nepx_md_device_state(nepx_md_t* md, double** d_pos, double** d_vel, double** d_force,
                          int** d_type, void** stream);
 
+/* ---- many independent structures --------------------------------------- */
+
+/* One structure of a batch: n atoms, consecutive in the batch arrays. */
+typedef struct nepx_struct_desc {
+  int n;
+  nepx_box box;
+} nepx_struct_desc;
+
+/*
+ * Energy, force and virial of nstruct independent structures in one launch
+ * sequence.  The batch arrays hold the structures' atoms back to back, T =
+ * sum of descs[s].n atoms: d_type[T], d_pos[3][T] (SoA, stride T), outputs
+ * d_pe[T], d_force[3][T], d_virial[9][T] (order as nepx_compute).  Each
+ * structure is evaluated as nepx_compute would evaluate it alone, on
+ * explicit neighbour rows (any box the reference accepts, small or large),
+ * and its results do not depend on the other structures of the batch.  T
+ * must not exceed the handle's max_atoms.  No counterpart in the reference
+ * (it evaluates one system per process); the per-structure contract is
+ * Potential::compute (potential.cuh:82-88).
+ */
+int nepx_compute_batch(nepx_t* handle, const nepx_struct_desc* descs, int nstruct,
+                       const int* d_type, const double* d_pos, double* d_pe, double* d_force,
+                       double* d_virial, unsigned flags, void* stream);
+
+/*
+ * Serving loop: a worker thread owns the potential handle and a device
+ * arena of max_atoms atoms and max_struct structure slots.  Requests are
+ * admitted while they fit the arena (continuous batching: new requests join
+ * between steps while others are mid-segment); every step evaluates all
+ * resident structures in one launch sequence, runs the NVE velocity-Verlet
+ * half steps of the MD segments, and retires finished requests (results
+ * copied to the caller's host buffers).  The handle must not be used by the
+ * caller while the server exists.  No counterpart in the reference.
+ */
+typedef struct nepx_server nepx_server_t;
+
+typedef struct nepx_request {
+  int n;                  /* atoms */
+  nepx_box box;
+  const int* type;        /* host [n] */
+  const double* pos;      /* host [3][n] */
+  int md_steps;           /* 0: single point; > 0: NVE steps after the first force call */
+  double dt_fs;           /* MD time step */
+  const double* mass;     /* host [n] amu (MD only) */
+  const double* vel;      /* host [3][n] A/fs (MD only) */
+} nepx_request;
+
+typedef struct nepx_result {
+  double* pe;             /* [n] per-atom energy of the final state (eV) */
+  double* force;          /* [3][n] */
+  double* virial;         /* [9][n] or NULL */
+  double* pos;            /* [3][n] final positions (MD) or NULL */
+  double* vel;            /* [3][n] final velocities A/fs (MD) or NULL */
+  double t_submit, t_admit, t_done;   /* seconds on the server's steady clock */
+} nepx_result;
+
+int nepx_server_create(nepx_t* handle, int max_atoms, int max_struct, nepx_server_t** out);
+/* Stops the worker after the queued requests are done, then frees the arena. */
+int nepx_server_destroy(nepx_server_t* server);
+const char* nepx_server_last_error(const nepx_server_t* server);
+/* Copies the request's inputs and queues it; *ticket identifies it.  `out`
+ * must stay valid until the request is done. */
+int nepx_server_submit(nepx_server_t* server, const nepx_request* req, nepx_result* out,
+                       long long* ticket);
+/* *done = 1 once the results are in `out` (status: the request's own code). */
+int nepx_server_poll(nepx_server_t* server, long long ticket, int* done, int* status);
+int nepx_server_wait(nepx_server_t* server, long long ticket, int* status);
+/* Blocks until every submitted request is done. */
+int nepx_server_drain(nepx_server_t* server);
+/* stats[8]: requests done, steps run, atom-steps, busy seconds (GPU steps),
+ * mean resident atoms per step, mean resident structures per step, current
+ * queue length, seconds since creation. */
+int nepx_server_stats(nepx_server_t* server, double* stats);
+
 #ifdef __cplusplus
 }
 #endif
