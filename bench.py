@@ -80,6 +80,116 @@ WORKLOADS = {
 
 MASSES = {"O": 15.999, "H": 1.008, "C": 12.011, "Cu": 63.546}
 
+# serving stream: one shared synthetic four-type NEP5 (C, H, O, Cu)
+SERVING_NEP = dict(version=5, symbols=("C", "H", "O", "Cu"), rc=(5.0, 4.0), mn=(160, 80),
+                   n_max=(4, 4), basis=(8, 8), l_max=(4, 2, 1), H=64, seed=2027, std=0.1,
+                   q_scaler=0.02)
+
+
+def _percentile_ms(xs, q):
+    return float(np.percentile(np.asarray(xs) * 1e3, q)) if len(xs) else None
+
+
+def run_serving(args):
+    """Served structures/s and p50/p99 latency of the continuous-batching
+    server on a stream of independent structures (log-uniform 16..8192
+    atoms; diamond C, FCC Cu, random-packed C/H/O/Cu; a fifth of the
+    requests are 100-step NVE segments at dt 1 fs), next to the same
+    requests evaluated one at a time through the plain single-system path
+    (nepx_compute / nepx_md per request, host buffers in and out)."""
+    import torch
+    import nepx
+    count = args.requests
+    stream = workloads.serving_stream(count, seed=11)
+    tmp = tempfile.mkdtemp()
+    path = workloads.write_nep(os.path.join(tmp, "nep.txt"), **SERVING_NEP)
+    arena, slots = args.arena, 2048
+    pot = nepx.Potential(path, max_atoms=arena)
+    work = [len(r["type"]) * (1 + r["md_steps"]) for r in stream]
+    total_atom_steps = float(sum(work))
+
+    def submit(srv, r):
+        return srv.submit(r["type"], r["pos"], r["h"], md_steps=r["md_steps"], dt_fs=1.0,
+                          masses=r["mass"], vel=r["vel"], want_virial=False)
+
+    # warm-up: autotune and first-touch of the arena
+    srv = nepx.Server(pot, max_atoms=arena, max_struct=slots)
+    for r in stream[:8]:
+        srv.wait(submit(srv, dict(r, md_steps=0, mass=None, vel=None)))
+    srv.close()
+    # 1. saturation: every request queued at t = 0
+    srv = nepx.Server(pot, max_atoms=arena, max_struct=slots)
+    t0 = time.perf_counter()
+    tickets = [submit(srv, r) for r in stream]
+    srv.drain()
+    wall = time.perf_counter() - t0
+    sat = [srv.wait(tk) for tk in tickets]
+    st = srv.stats()
+    srv.close()
+    rate_sat = count / wall
+    # 2. Poisson arrivals at 60% of the saturation rate: latency
+    rate = 0.6 * rate_sat
+    rng = np.random.default_rng(5)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, count))
+    srv = nepx.Server(pot, max_atoms=arena, max_struct=slots)
+    t0 = time.perf_counter()
+    tickets = []
+    for r, ta in zip(stream, arrivals):
+        dt_wait = ta - (time.perf_counter() - t0)
+        if dt_wait > 0:
+            time.sleep(dt_wait)
+        tickets.append(submit(srv, r))
+    srv.drain()
+    wall_p = time.perf_counter() - t0
+    res = [srv.wait(tk) for tk in tickets]
+    srv.close()
+    lat = [x["t_done"] - x["t_submit"] for x in res]
+    lat_sp = [x for x, r in zip(lat, stream) if r["md_steps"] == 0]
+    lat_md = [x for x, r in zip(lat, stream) if r["md_steps"] > 0]
+    # 3. the plain path on a sample: one request at a time, host buffers in and out
+    plain_pot = nepx.Potential(path, max_atoms=8192)
+    sample = stream[:args.plain_sample]
+    t0 = time.perf_counter()
+    for r in sample:
+        tt = torch.as_tensor(r["type"], device="cuda")
+        pp = torch.as_tensor(np.ascontiguousarray(r["pos"]), device="cuda")
+        if r["md_steps"] == 0:
+            pe, f, _ = plain_pot.compute(tt, r["h"], pp)
+            pe.cpu(), f.cpu()
+        else:
+            md = nepx.MD(plain_pot, r["type"], r["mass"], r["pos"], r["vel"], r["h"])
+            md.set_ensemble("nve")
+            md.run(r["md_steps"], 1.0)
+            md.state()
+            md.close()
+    torch.cuda.synchronize()
+    plain_wall = time.perf_counter() - t0
+    plain_work = float(sum(work[:len(sample)]))
+    plain_rate = plain_work / plain_wall
+    served_rate = total_atom_steps / wall
+    n_atoms = [len(r["type"]) for r in stream]
+    return {
+        "metric": "served structures/s", "value": rate_sat, "unit": "structures/s",
+        "n_gpus": 1, "higher_is_better": True, "dtype": "fp32 (descriptors, ANN, forces) + "
+        "fp64 (integration)", "data": "synthetic (seeded structures and NEP5 weights)",
+        "config": {"workload": "serving_stream_%d_structs_16-8192_atoms_nep5_4type_rc5.0-4.0"
+                               "_H64_20pct_nve100" % count,
+                   "arena_atoms": arena, "slots": slots, "mean_atoms": float(np.mean(n_atoms)),
+                   "md_fraction": float(np.mean([r["md_steps"] > 0 for r in stream]))},
+        "atom_steps_per_s": served_rate,
+        "saturation": {"wall_s": wall, "steps": st["steps"], "mean_resident_atoms":
+                       st["mean_atoms"], "mean_resident_structs": st["mean_structs"]},
+        "latency_ms": {"arrival_rate_per_s": rate, "wall_s": wall_p,
+                       "p50": _percentile_ms(lat, 50), "p99": _percentile_ms(lat, 99),
+                       "single_point_p50": _percentile_ms(lat_sp, 50),
+                       "single_point_p99": _percentile_ms(lat_sp, 99),
+                       "nve100_p50": _percentile_ms(lat_md, 50),
+                       "nve100_p99": _percentile_ms(lat_md, 99)},
+        "plain_fp32_one_at_a_time": {"atom_steps_per_s": plain_rate, "requests": len(sample),
+                                     "wall_s": plain_wall},
+        "batched_over_plain": served_rate / plain_rate,
+    }
+
 
 def build_system(name, seed):
     if name == "water":
@@ -227,6 +337,10 @@ def gpu_reference_rate(nep_path, t, h, p, reps=50):
 def run_reference_arm(args, rank):
     if rank != 0:
         return 0
+    if args.workload == "serving":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference evaluates one "
+                          "system per process: it has no batched or served path"}))
+        return 0
     spec = WORKLOADS[args.workload]
     with tempfile.TemporaryDirectory() as tmp:
         path = workloads.write_nep(os.path.join(tmp, "nep.txt"), **spec["nep"])
@@ -256,7 +370,10 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="water", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="water", choices=sorted(WORKLOADS) + ["serving"])
+    ap.add_argument("--requests", type=int, default=20000)
+    ap.add_argument("--arena", type=int, default=262144)
+    ap.add_argument("--plain-sample", type=int, default=200)
     ap.add_argument("--chunk", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -267,6 +384,10 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference_arm(args, rank)
+    if args.workload == "serving":
+        if rank == 0:
+            print(json.dumps(run_serving(args)))
+        return 0
 
     import torch
     torch.cuda.set_device(local)

@@ -143,3 +143,53 @@ def maxwell_boltzmann(masses, T, seed=0):
     ek = 0.5 * (masses * (v * v).sum(axis=0)).sum()
     v *= math.sqrt(1.5 * len(masses) * K_B * T / ek)
     return v / 10.18051
+
+
+DIAMOND_BASE = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0],
+                         [.25, .25, .25], [.25, .75, .75], [.75, .25, .75], [.75, .75, .25]])
+FCC_BASE = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0]])
+
+
+def crystal(base, a, dims, jitter=0.0, seed=0):
+    """Orthorhombic supercell dims = (nx, ny, nz) of a cubic cell with `base` sites."""
+    dims = np.asarray(dims)
+    g = np.stack(np.meshgrid(*[np.arange(d) for d in dims], indexing="ij"), -1).reshape(-1, 3)
+    frac = (g[:, None, :] + base[None, :, :]).reshape(-1, 3)
+    L = a * dims
+    rng = np.random.default_rng(seed)
+    pos = frac * a + rng.normal(0.0, jitter, frac.shape)
+    h = np.diag(L.astype(np.float64)).reshape(-1)
+    return np.zeros(len(pos), dtype=np.int32), h, np.ascontiguousarray((pos % L).T)
+
+
+def _near_cubic_dims(n_atoms, per_cell):
+    a = max(1, int(round((n_atoms / per_cell) ** (1.0 / 3.0))))
+    c = max(1, int(round(n_atoms / (per_cell * a * a))))
+    return (a, a, c)
+
+
+def serving_stream(count, seed=0, md_fraction=0.2, md_steps=100, lo=16, hi=8192):
+    """Independent structures of log-uniform size lo..hi atoms: jittered
+    (sigma 0.1 A) diamond C and FCC Cu supercells and random-packed C/H/O/Cu
+    at 0.08 atoms/A^3 (types 0..3 = C, H, O, Cu).  A fraction md_fraction of
+    the requests are NVE segments of md_steps steps at 300 K.  Returns a list
+    of dicts (type, h, pos, md_steps, mass, vel)."""
+    rng = np.random.default_rng(seed)
+    masses = np.array([12.011, 1.008, 15.999, 63.546])
+    out = []
+    for k in range(count):
+        n = int(round(math.exp(rng.uniform(math.log(lo), math.log(hi)))))
+        kind = rng.integers(0, 3)
+        if kind == 0:
+            t, h, p = crystal(DIAMOND_BASE, 3.567, _near_cubic_dims(n, 8), 0.1, seed + k)
+        elif kind == 1:
+            t, h, p = crystal(FCC_BASE, 3.615, _near_cubic_dims(n, 4), 0.1, seed + k)
+            t = np.full(len(t), 3, dtype=np.int32)
+        else:
+            t, h, p = random_packed(n, 4, density=0.08, seed=seed + k)
+        req = {"type": t, "h": h, "pos": p, "md_steps": 0, "mass": None, "vel": None}
+        if rng.random() < md_fraction:
+            m = masses[t]
+            req.update(md_steps=md_steps, mass=m, vel=maxwell_boltzmann(m, 300.0, seed + k))
+        out.append(req)
+    return out
