@@ -48,6 +48,8 @@ int check_state(nepx_handle* h, bool wait)
   }
   if (s.nonfinite) return fail(h, NEPX_ERR_NONFINITE, "non-finite energy or force");
   if (s.box_error) return fail(h, NEPX_ERR_BOX, kUnsupportedBox);
+  if (s.ann_error)
+    return fail(h, NEPX_ERR_CUDA, "a tensor-core ANN tile timed out waiting for its MMAs");
   return NEPX_OK;
 }
 
@@ -244,6 +246,16 @@ int nepx_neighbors(nepx_t* h, int which, int n, int* d_nn, int* d_nl, int mn, vo
       cudaMemcpy2DAsync(d_nl, sizeof(int) * mn, nl, sizeof(int) * src_mn, sizeof(int) * src_mn, n,
                         cudaMemcpyDeviceToDevice, s) != cudaSuccess)
     return cuda_fail(h, "copy neighbour rows");
+  return NEPX_OK;
+}
+
+int nepx_set_precision(nepx_t* h, int mode)
+{
+  if (!h) return NEPX_ERR_ARG;
+  if (mode != NEPX_PRECISION_FP32 && mode != NEPX_PRECISION_MIXED)
+    return fail(h, NEPX_ERR_ARG, "unknown precision mode");
+  const std::string err = nepx::engine_set_precision(h->engine, mode);
+  if (!err.empty()) return fail(h, NEPX_ERR_UNSUPPORTED, err);
   return NEPX_OK;
 }
 

@@ -55,6 +55,7 @@ struct NeighborState {
   int max_nn[3];       // largest Verlet / radial / angular row of the last build
   int nonfinite;       // a force or energy came out NaN/Inf
   int box_error;       // the device box became unsupported (small in one direction, >10 rc in another)
+  int ann_error;       // a tensor-core ANN tile gave up waiting for its MMAs
   double box_scale;    // product of isotropic box factors since the last build (1 = none)
 };
 

@@ -85,6 +85,7 @@ std::string engine_create(Engine& e, const std::string& nep_path, int max_atoms)
   p.nlm = (m.L_max + 1) * (m.L_max + 1) - 1;
   p.num_L = m.num_L;
   p.dim = m.dim;
+  p.dimK = (m.dim + 7) & ~7;
   p.H = m.H;
   p.num_inv = 0;
   for (int v = 0; v < kMaxInv; ++v)
@@ -243,13 +244,36 @@ void engine_autotune(Engine& e, int N, const double* pos, const int* type, cudaS
                  e.group, e.f12_group, e.gather_group);
 }
 
+std::string engine_set_precision(Engine& e, int mode)
+{
+  if (mode != 0 && mode != 1) return "precision mode must be 0 (FP32) or 1 (mixed)";
+  if (mode == 1) {
+    std::string why;
+    if (!ann_tc_supported(e.params, why)) return why;
+    ForceScratch& sc = e.scratch;
+    const size_t N = e.capacity;
+    if (!sc.q) {
+      bool ok = dalloc(sc.q, N * e.params.dimK) == cudaSuccess;
+      ok &= dalloc(sc.fp, N * e.params.dimK) == cudaSuccess;
+      ok &= dalloc(sc.order, N) == cudaSuccess;
+      ok &= dalloc(sc.type_counts, 2 * kMaxTypes) == cudaSuccess;
+      if (!ok) return "cudaMalloc failed (mixed-precision buffers)";
+    }
+    ann_tc_prepare(e.params);
+  }
+  if (e.precision != mode) e.tuned = false;
+  e.precision = mode;
+  return "";
+}
+
 void engine_destroy(Engine& e)
 {
   NeighborBuffers& nb = e.nbr;
   void* ptrs[] = {e.d_params, e.d_box, e.d_nstate, nb.nn_v, nb.nl_v, nb.nn_r, nb.nl_r,
                   nb.nn_a, nb.nl_a, nb.cell_count, nb.cell_start, nb.cell_atoms, nb.cell_of,
                   nb.x0, e.scratch.alpha, e.scratch.f12, e.scratch.pe_ann, e.scratch.q,
-                  e.scratch.tune_out, e.scratch.acoef, e.scratch.sites, e.xr.er, e.xr.ea,
+                  e.scratch.tune_out, e.scratch.acoef, e.scratch.sites, e.scratch.fp,
+                  e.scratch.order, e.scratch.type_counts, e.xr.er, e.xr.ea,
                   e.xr.d_si, e.xr.d_soff};
   for (void* q : ptrs)
     if (q) cudaFree(q);

@@ -33,7 +33,10 @@ struct ForceScratch {
   float4* f12 = nullptr;     // [N][mn_a] directed angular partial forces
   float* acoef = nullptr;    // [N][nA][24] dE/ds[n][lm] of each center
   double* pe_ann = nullptr;  // [N] site energy of the ANN
-  float* q = nullptr;        // [N][dim] descriptors (mixed-precision path)
+  float* q = nullptr;        // [N][dimK] scaled descriptors (mixed-precision path)
+  float* fp = nullptr;       // [N][dimK] dE/dq (mixed-precision path)
+  int* order = nullptr;      // [N] centers sorted by type (mixed-precision path)
+  int* type_counts = nullptr;  // [2 kMaxTypes] type histogram and starts
   double* tune_out = nullptr;  // [13 N] throw-away outputs of the autotuning calls
 };
 
@@ -64,6 +67,7 @@ struct Engine {
   ForceScratch scratch;
   ExplicitRows xr;
   bool use_xr = false;       // neighbour rows with explicit displacements (small box, batch)
+  int precision = 0;         // 0: FP32 SIMT ANN; 1: mixed (ANN on the tensor cores, ann_tc.cu)
   // host-side bookkeeping
   Box last_box{};
   bool have_box = false;
@@ -124,6 +128,14 @@ void launch_explicit_rows(Engine& e, int N, const double* pos, const int* type,
 // caller arrays nn[n], nl[n][mn] (row-major), as for the Verlet-path rows.
 void launch_explicit_row_indices(const Engine& e, int which, int n, int* nn, int* nl, int mn,
                                  cudaStream_t stream);
+
+// Mixed-precision path: the tensor-core ANN (ann_tc.cu).
+bool ann_tc_supported(const ModelParams& p, std::string& why);
+size_t ann_tc_smem_bytes(const ModelParams& p);
+void ann_tc_prepare(const ModelParams& p);
+void launch_ann_tc(Engine& e, int N, cudaStream_t stream);
+// Switches the ANN precision (0 FP32, 1 mixed); allocates the mixed buffers.
+std::string engine_set_precision(Engine& e, int mode);
 
 // Descriptor + ANN + angular partial forces, then the force/virial gather.
 // accumulate = add into pe/force/virial instead of overwriting them.

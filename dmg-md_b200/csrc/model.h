@@ -39,6 +39,7 @@ std::string load_nep(const std::string& path, NepModel& m);
 // Kernel-side view (passed by value; pointers are device pointers).
 struct ModelParams {
   int version, T, nR, nA, kR, kA, L_max, nlm, num_L, dim, H;
+  int dimK;           // dim rounded up to 8: row stride of the descriptor and dE/dq buffers
   int num_inv, inv_id[kMaxInv];
   float rc_r[kMaxTypes], rc_a[kMaxTypes];
   int zbl, zbl_flexible, typewise_zbl;

@@ -66,7 +66,7 @@ __constant__ int c_inv_start[kMaxInv + 1];
 
 #include "zbl.cuh"
 
-__host__ __device__ inline int round4(int x) { return (x + 3) & ~3; }
+__host__ __device__ constexpr int round4(int x) { return (x + 3) & ~3; }
 
 // Shared-memory layout of k_nep_fused (in floats).
 struct FusedLayout {
@@ -181,6 +181,59 @@ __device__ __forceinline__ int reduce_scatter(float* v, int gl)
   return base;
 }
 
+// Radial force coefficients of one center, alpha[t][k] = sum_n Fp[n] c(t1,t)[n][k]
+// (the group's lanes split the T * kpr entries); c_rad: shared-memory table.
+template <int G>
+__device__ __forceinline__ void center_alpha(const ModelParams& p, int t1, const float* s_fp,
+                                             const float* c_rad, int kpr, int gl, float* al)
+{
+  const int T = p.T, nR = p.nR;
+  for (int e = gl; e < T * kpr; e += G) {
+    const int t = e / kpr, kk = e % kpr;
+    const float* c = c_rad + (t1 * T + t) * nR * kpr + kk;
+    float acc = 0.0f;
+    for (int n = 0; n < nR; ++n) acc += s_fp[n] * c[n * kpr];
+    al[e] = acc;
+  }
+}
+
+// Moment derivatives of one center, a[n][lm] = dE/ds[n][lm] (one lane owns
+// one n); the monomial terms read the moments at run-time indices, so both
+// live in shared memory.
+template <int G>
+__device__ __forceinline__ void center_acoef(const ModelParams& p, const float* s_s, float* s_a,
+                                             const float* s_fp, int gl)
+{
+  const int nR = p.nR, nA = p.nA;
+  for (int n = gl; n < nA; n += G) {
+    const float* sv = s_s + n * kNumLM;
+    float* av = s_a + n * kNumLM;
+    const float* fp = s_fp + nR;
+    int col = 0;
+    for (int Lq = 1; Lq <= p.L_max; ++Lq, ++col) {
+      const int st0 = Lq * Lq - 1;
+      const float f = fp[col * nA + n];
+      av[st0] = 2.0f * f * c_C3B[st0] * sv[st0];
+      for (int k = 1; k < 2 * Lq + 1; ++k) av[st0 + k] = 4.0f * f * c_C3B[st0 + k] * sv[st0 + k];
+    }
+    for (int lm = (p.L_max + 1) * (p.L_max + 1) - 1; lm < kNumLM; ++lm) av[lm] = 0.0f;
+    for (int w = 0; w < p.num_inv; ++w, ++col) {
+      const int id = p.inv_id[w];
+      const float f = fp[col * nA + n];
+      for (int m = c_inv_start[id]; m < c_inv_start[id + 1]; ++m) {
+        const Monomial mo = c_mono[m];
+        const int nf = mo.i[3] >= 0 ? 4 : 3;
+        for (int a = 0; a < nf; ++a) {
+          float t = f * mo.c;
+          for (int r = 0; r < nf; ++r)
+            if (r != a) t *= sv[mo.i[r]];
+          av[mo.i[a]] += t;
+        }
+      }
+    }
+  }
+}
+
 // NRM/KM/NAM: compile-time bounds of nR, basis size + 1, nA for this instance.
 // The small-shape instance is held to 168 registers (three CTAs per SM): the
 // kernel is latency bound and the extra warps outweigh a few spilled words.
@@ -195,7 +248,7 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
             int* __restrict__ nn_r, int* __restrict__ nl_r, int mn_r, int* __restrict__ nn_a,
             int* __restrict__ nl_a, int mn_a, const float4* __restrict__ er,
             const float4* __restrict__ ea, float* __restrict__ alpha,
-            float* __restrict__ acoef, double* __restrict__ pe_ann)
+            float* __restrict__ acoef, double* __restrict__ pe_ann, float* __restrict__ qout)
 {
   constexpr int APW = 32 / G;             // centers per warp
   constexpr int APB = kBlock / G;         // centers per block
@@ -427,6 +480,18 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
   for (int h = H + gl; h < p.H4; h += G) s_gh[h] = 0.0f;
   const float* w0t = Lay.wt >= 0 ? sm + Lay.wt : p.w0t;
   __syncwarp();
+  if (qout) {
+    // mixed-precision path: the ANN runs on the tensor cores (ann_tc.cu); hand
+    // over the scaled descriptors (zero-padded to dimK) and the moments
+    if (active) {
+      float* qrow = qout + static_cast<size_t>(i) * p.dimK;
+      for (int d = gl; d < p.dimK; d += G) qrow[d] = d < dim ? s_q[d] : 0.0f;
+      float4* dst = reinterpret_cast<float4*>(acoef + static_cast<size_t>(i) * nA * kNumLM);
+      const float4* src = reinterpret_cast<const float4*>(s_s);
+      for (int q = gl; q < nA * kNumLM / 4; q += G) dst[q] = src[q];
+    }
+    return;
+  }
   float e_part = 0.0f;
   if (active) {
     // hidden layer: each lane owns groups of four consecutive hidden units
@@ -490,46 +555,9 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
     }
   }
   __syncwarp();
-  // radial force coefficients alpha[t][k] = sum_n Fp[n] c(t1, t)[n][k]
-  if (active) {
-    float* al = alpha + static_cast<size_t>(i) * T * Lay.kpr;
-    for (int e = gl; e < T * Lay.kpr; e += G) {
-      const int t = e / Lay.kpr, kk = e % Lay.kpr;
-      const float* c = sm + Lay.c_rad + (t1 * T + t) * nR * Lay.kpr + kk;
-      float acc = 0.0f;
-      for (int n = 0; n < nR; ++n) acc += s_fp[n] * c[n * Lay.kpr];
-      al[e] = acc;
-    }
-  }
-  // a[n][lm] = dE/ds[n][lm] (one lane owns one n); the monomial terms read
-  // the moments at run-time indices, so both live in shared memory
-  for (int n = gl; n < nA; n += G) {
-    const float* sv = s_s + n * kNumLM;
-    float* av = s_a + n * kNumLM;
-    const float* fp = s_fp + nR;
-    int col = 0;
-    for (int Lq = 1; Lq <= p.L_max; ++Lq, ++col) {
-      const int st0 = Lq * Lq - 1;
-      const float f = fp[col * nA + n];
-      av[st0] = 2.0f * f * c_C3B[st0] * sv[st0];
-      for (int k = 1; k < 2 * Lq + 1; ++k) av[st0 + k] = 4.0f * f * c_C3B[st0 + k] * sv[st0 + k];
-    }
-    for (int lm = (p.L_max + 1) * (p.L_max + 1) - 1; lm < kNumLM; ++lm) av[lm] = 0.0f;
-    for (int w = 0; w < p.num_inv; ++w, ++col) {
-      const int id = p.inv_id[w];
-      const float f = fp[col * nA + n];
-      for (int m = c_inv_start[id]; m < c_inv_start[id + 1]; ++m) {
-        const Monomial mo = c_mono[m];
-        const int nf = mo.i[3] >= 0 ? 4 : 3;
-        for (int a = 0; a < nf; ++a) {
-          float t = f * mo.c;
-          for (int r = 0; r < nf; ++r)
-            if (r != a) t *= sv[mo.i[r]];
-          av[mo.i[a]] += t;
-        }
-      }
-    }
-  }
+  if (active) center_alpha<G>(p, t1, s_fp, sm + Lay.c_rad, Lay.kpr, gl,
+                              alpha + static_cast<size_t>(i) * T * Lay.kpr);
+  center_acoef<G>(p, s_s, s_a, s_fp, gl);
   __syncwarp();
 
   // ---- 4. hand a[n][lm] to the angular-force kernel -------------------------
@@ -538,6 +566,46 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
     const float4* src = reinterpret_cast<const float4*>(s_a);
     for (int q = gl; q < nA * kNumLM / 4; q += G) dst[q] = src[q];
   }
+}
+
+// Mixed-precision path: moment derivatives and radial force coefficients of
+// every center from its moments (left in acoef by k_nep_fused) and dE/dq of
+// the tensor-core ANN (fp, ann_tc.cu) -- the tail of k_nep_fused.
+template <int G, int KP>
+__global__ void __launch_bounds__(kBlock)
+k_acoef(const ModelParams p, int N, const Site* __restrict__ sites, const float* __restrict__ fp,
+        float* __restrict__ acoef, float* __restrict__ alpha)
+{
+  extern __shared__ float sm[];
+  const int T = p.T, nR = p.nR, kR = p.kR, nA = p.nA;
+  const int tab = round4(T * T * nR * KP);
+  for (int k = threadIdx.x; k < T * T * nR * KP; k += kBlock) {
+    const int kk = k % KP, row = k / KP;
+    sm[k] = kk < kR ? __ldg(p.c_pair + row * kR + kk) : 0.0f;
+  }
+  __syncthreads();
+  constexpr int APB = kBlock / G;
+  const int per = round4(2 * nA * kNumLM + p.dimK);
+  const int gl = threadIdx.x % G, slot = threadIdx.x / G;
+  const int i = blockIdx.x * APB + slot;
+  const bool active = i < N;
+  float* s_s = sm + tab + slot * per;
+  float* s_a = s_s + nA * kNumLM;
+  float* s_fp = s_a + nA * kNumLM;
+  float4* arow = reinterpret_cast<float4*>(acoef + static_cast<size_t>(i) * nA * kNumLM);
+  if (active) {
+    for (int q = gl; q < nA * kNumLM / 4; q += G) reinterpret_cast<float4*>(s_s)[q] = arow[q];
+    for (int d = gl; d < p.dimK; d += G) s_fp[d] = fp[static_cast<size_t>(i) * p.dimK + d];
+  }
+  __syncwarp();
+  if (active) {
+    const int t1 = static_cast<int>(sites[i].type);
+    center_alpha<G>(p, t1, s_fp, sm, KP, gl, alpha + static_cast<size_t>(i) * T * KP);
+    center_acoef<G>(p, s_s, s_a, s_fp, gl);
+  }
+  __syncwarp();
+  if (active)
+    for (int q = gl; q < nA * kNumLM / 4; q += G) arow[q] = reinterpret_cast<const float4*>(s_a)[q];
 }
 
 // Directed angular partial force of a center on one neighbour at
@@ -907,7 +975,24 @@ void launch_fused_t(Engine& e, int N, cudaStream_t s)
   k_nep_fused<G, NRM, KM, NAM, XR><<<blocks, kBlock, smem, s>>>(
     e.params, N, e.d_box, e.scratch.sites, e.d_nstate, nb.nn_v, nb.nl_v, nb.mn_v, nb.nn_r, nb.nl_r,
     nb.mn_r, nb.nn_a, nb.nl_a, nb.mn_a, e.xr.er, e.xr.ea, e.scratch.alpha, e.scratch.acoef,
-    e.scratch.pe_ann);
+    e.scratch.pe_ann, e.precision == 1 ? e.scratch.q : nullptr);
+}
+
+template <int KP>
+size_t acoef_smem_bytes(const ModelParams& p)
+{
+  return sizeof(float) * (round4(p.T * p.T * p.nR * KP) +
+                          (kBlock / 4) * round4(2 * p.nA * kNumLM + p.dimK));
+}
+
+template <int KP>
+void launch_acoef_t(Engine& e, int N, cudaStream_t s)
+{
+  constexpr int G = 4, APB = kBlock / G;
+  const ModelParams& p = e.params;
+  const size_t smem = acoef_smem_bytes<KP>(p);
+  k_acoef<G, KP><<<(N + APB - 1) / APB, kBlock, smem, s>>>(p, N, e.scratch.sites, e.scratch.fp,
+                                                           e.scratch.acoef, e.scratch.alpha);
 }
 
 template <int G, int KM, int NAM>
@@ -977,6 +1062,10 @@ size_t fused_smem_bytes(const ModelParams& p, int group)
 
 void set_fused_smem_limits(const ModelParams& p)
 {
+  cudaFuncSetAttribute(k_acoef<4, round4(kSmallK)>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(acoef_smem_bytes<round4(kSmallK)>(p)));
+  cudaFuncSetAttribute(k_acoef<4, round4(kMaxBasis)>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(acoef_smem_bytes<round4(kMaxBasis)>(p)));
   const size_t b4 = fused_smem_bytes(p, 4), b8 = fused_smem_bytes(p, 8);
   if (small_shape(p)) {
     set_fused_smem_t<4, kSmallN, kSmallK, kSmallN>(b4);
@@ -996,6 +1085,12 @@ void launch_descriptor(Engine& e, int N, const double*, const int*, cudaStream_t
   } else {
     if (small) launch_fused_g<4, kSmallN, kSmallK, kSmallN>(e, N, stream);
     else launch_fused_g<4, kMaxN, kMaxBasis, kMaxN>(e, N, stream);
+  }
+  if (e.precision == 1) {
+    // mixed precision: the ANN on the tensor cores, then the fused kernel's tail
+    launch_ann_tc(e, N, stream);
+    if (small) launch_acoef_t<round4(kSmallK)>(e, N, stream);
+    else launch_acoef_t<round4(kMaxBasis)>(e, N, stream);
   }
   if (e.use_xr) return;   // the explicit-row gather evaluates the angular forces itself
   if (e.f12_group == 8) {

@@ -152,6 +152,8 @@ extern "C" int nepx_compute_noalloc(nepx_t* h, const nepx_box* box, int n, const
   view.scratch.acoef = c.take<float>(N * view.params.nA * nepx::kNumLM);
   view.capacity = n;
   view.tuned = true;   // keeps the handle's kernel variants; no timing runs here
+  view.precision = 0;  // the mixed path's buffers are not part of the static scratch
+  view.use_xr = false;
   auto s = static_cast<cudaStream_t>(stream);
   // the handle's pinned flag mirror may still receive a copy from an earlier
   // nepx_compute; let it land before this call reuses the mirror

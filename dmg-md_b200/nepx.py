@@ -34,7 +34,7 @@ EXPORTED = ["nepx_create", "nepx_destroy", "nepx_last_error", "nepx_info", "nepx
             "nepx_md_run_async", "nepx_md_sync", "nepx_compute_noalloc", "nepx_compute_batch",
             "nepx_server_create", "nepx_server_destroy", "nepx_server_last_error",
             "nepx_server_submit", "nepx_server_poll", "nepx_server_wait", "nepx_server_drain",
-            "nepx_server_stats"]
+            "nepx_server_stats", "nepx_set_precision"]
 
 ENSEMBLES = {"nve": 0, "nvt_ber": 1, "nvt_nhc": 2, "nvt_bdp": 3, "npt_ber": 4, "npt_scr": 5}
 THERMO_COLUMNS = ["T", "KE", "PE", "sxx", "syy", "szz", "syz", "sxz", "sxy", "ax", "ay", "az",
@@ -111,6 +111,7 @@ def lib():
         L.nepx_md_device_state.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(vp),
                                            ctypes.POINTER(vp), ctypes.POINTER(vp),
                                            ctypes.POINTER(vp)]
+        L.nepx_set_precision.argtypes = [vp, ctypes.c_int]
         L.nepx_compute_batch.argtypes = [vp, ctypes.POINTER(StructDesc), ctypes.c_int, vp, vp, vp,
                                          vp, vp, ctypes.c_uint, vp]
         L.nepx_server_create.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
@@ -203,6 +204,10 @@ class Potential:
                                        _ptr(pe), _ptr(force), _ptr(virial), flags,
                                        _stream_ptr(stream)))
         return pe, force, virial
+
+    def set_precision(self, mode):
+        """"fp32" (default) or "mixed" (the ANN on the tensor cores)."""
+        self._check(lib().nepx_set_precision(self._h, {"fp32": 0, "mixed": 1}[mode]))
 
     def compute_batch(self, structs, types, pos, out=None, accumulate=False, sync_check=False,
                       stream=None):

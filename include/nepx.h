@@ -28,6 +28,10 @@ extern "C" {
 #define NEPX_ERR_NONFINITE 7    /* an energy or force came out NaN/Inf */
 #define NEPX_ERR_BOX 8          /* box too thin for the large-box path, or singular */
 
+/* ANN precision (nepx_set_precision) */
+#define NEPX_PRECISION_FP32 0   /* FP32 SIMT ANN: the reference's arithmetic */
+#define NEPX_PRECISION_MIXED 1  /* ANN on the tensor cores, 3xTF32 with FP32 accumulation */
+
 /* compute flags */
 #define NEPX_ACCUMULATE 1u      /* add into pe/force/virial (the reference's += contract) */
 #define NEPX_SYNC_CHECK 2u      /* synchronise the stream and report device-side errors */
@@ -208,6 +212,16 @@ int nepx_md_get(nepx_md_t* md, double* h_pos, double* h_vel, double* h_force, do
  * forces, types) and the stream the md runs on. */
 int nepx_md_device_state(nepx_md_t* md, double** d_pos, double** d_vel, double** d_force,
                          int** d_type, void** stream);
+
+/*
+ * Chooses how the per-atom ANN runs for every later call on this handle
+ * (compute, batch, MD, server): NEPX_PRECISION_FP32 (default) or
+ * NEPX_PRECISION_MIXED, the two ANN contractions as tcgen05 tensor-core
+ * GEMMs over tiles of 128 type-sorted atoms (descriptors and forces stay
+ * FP32).  NEPX_ERR_UNSUPPORTED when the model's ANN does not fit the tiles.
+ * No counterpart in the reference (its ANN is FP32 only).
+ */
+int nepx_set_precision(nepx_t* handle, int mode);
 
 /* ---- many independent structures --------------------------------------- */
 
