@@ -25,7 +25,15 @@ roofline -- the dominant kernel (fused descriptor/ANN/angular-force kernel),
           runs, see flops_per_atom) over its CUDA-event time, against the FP32
           FMA peak of B200 (148 SMs x 128 lanes x 2 FLOP x max SM clock).
 cpu_baseline -- the reference's own FP64 CPU NEP evaluator (NEP3_CPU,
-          oracle/_ref) over the full system on all host cores, force call.
+          oracle/_ref) over the full system on all host cores, force call,
+          on the final MD state; the same FP64 values give err_vs_fp64 (force
+          RMSE and energy error of the FP32 and mixed paths).
+mixed_precision -- the same MD with the ANN on the tcgen05 tensor cores.
+nve_drift -- NVE energy drift (eV/atom/ns) of 4096-atom diamond carbon,
+          1000 steps of 1 fs, both precisions.
+serving -- a bounded sample of the serving workload (--workload serving
+          runs the full stream): served structures/s, p50/p99 latency,
+          batched mixed-precision engine over the plain FP32 path.
 
 --impl reference times that same reference CPU evaluator alone (rank 0).
 Multi-GPU: one independent replica per GPU (the reference's one-rank path
@@ -105,6 +113,7 @@ def run_serving(args):
     path = workloads.write_nep(os.path.join(tmp, "nep.txt"), **SERVING_NEP)
     arena, slots = args.arena, 2048
     pot = nepx.Potential(path, max_atoms=arena)
+    pot.set_precision(args.precision)
     work = [len(r["type"]) * (1 + r["md_steps"]) for r in stream]
     total_atom_steps = float(sum(work))
 
@@ -148,7 +157,9 @@ def run_serving(args):
     lat_md = [x for x, r in zip(lat, stream) if r["md_steps"] > 0]
     # 3. the plain path on a sample: one request at a time, host buffers in and out
     plain_pot = nepx.Potential(path, max_atoms=8192)
-    sample = stream[:args.plain_sample]
+    step = max(1, count // max(1, args.plain_sample))
+    picked = list(range(0, count, step))[:args.plain_sample]   # spread over the stream
+    sample = [stream[k] for k in picked]
     t0 = time.perf_counter()
     for r in sample:
         tt = torch.as_tensor(r["type"], device="cuda")
@@ -164,14 +175,16 @@ def run_serving(args):
             md.close()
     torch.cuda.synchronize()
     plain_wall = time.perf_counter() - t0
-    plain_work = float(sum(work[:len(sample)]))
+    plain_work = float(sum(work[k] for k in picked))
     plain_rate = plain_work / plain_wall
     served_rate = total_atom_steps / wall
     n_atoms = [len(r["type"]) for r in stream]
     return {
         "metric": "served structures/s", "value": rate_sat, "unit": "structures/s",
-        "n_gpus": 1, "higher_is_better": True, "dtype": "fp32 (descriptors, ANN, forces) + "
-        "fp64 (integration)", "data": "synthetic (seeded structures and NEP5 weights)",
+        "n_gpus": 1, "higher_is_better": True,
+        "dtype": "fp32 descriptors and forces, %s ANN, fp64 integration" %
+                 ("tcgen05 3xTF32" if args.precision == "mixed" else "fp32"),
+        "data": "synthetic (seeded structures and NEP5 weights)",
         "config": {"workload": "serving_stream_%d_structs_16-8192_atoms_nep5_4type_rc5.0-4.0"
                                "_H64_20pct_nve100" % count,
                    "arena_atoms": arena, "slots": slots, "mean_atoms": float(np.mean(n_atoms)),
@@ -278,8 +291,9 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_reference_rate(nep_path, t, h, p, budget_s=8.0, max_reps=5):
-    """The reference's NEP3_CPU over all atoms on all host cores: atom-steps/s."""
+def cpu_reference_rate(nep_path, t, h, p, budget_s=8.0, max_reps=5, want_result=False):
+    """The reference's NEP3_CPU over all atoms on all host cores: atom-steps/s
+    (and, with want_result, its FP64 energies and forces of the last call)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     if not oracle.ref_cpu_available():
@@ -289,14 +303,54 @@ def cpu_reference_rate(nep_path, t, h, p, budget_s=8.0, max_reps=5):
     ref.compute(t, h, p, threads=threads)           # warm (thread pool, pages)
     times = []
     t_end = time.perf_counter() + budget_s
+    result = None
     while len(times) < max_reps and time.perf_counter() < t_end:
         t0 = time.perf_counter()
-        ref.compute(t, h, p, threads=threads)
+        result = ref.compute(t, h, p, threads=threads)
         times.append(time.perf_counter() - t0)
     sec = statistics.median(times)
-    return {"value": len(t) / sec, "unit": "atom-steps/s", "cores": threads, "kind": "reference",
+    line = {"value": len(t) / sec, "unit": "atom-steps/s", "cores": threads, "kind": "reference",
             "sample": "NEP3_CPU (reference FP64 CPU evaluator) force call on all %d atoms, "
                       "median of %d calls, %d threads" % (len(t), len(times), threads)}
+    return (line, result) if want_result else line
+
+
+def errors_vs(ref, pe, f):
+    """Force RMSE / max and energy errors per atom of (pe, f) against ref."""
+    pe0, f0 = ref[0], ref[1]
+    n = len(pe0)
+    return {"force_rmse_eV_per_A": float(np.sqrt(np.mean((f - f0) ** 2))),
+            "force_max_abs_eV_per_A": float(np.abs(f - f0).max()),
+            "force_rel_2norm": float(np.linalg.norm(f - f0) / np.linalg.norm(f0)),
+            "energy_mae_eV_per_atom": float(np.abs(pe - pe0).mean()),
+            "energy_total_eV_per_atom": float(abs(pe.sum() - pe0.sum()) / n)}
+
+
+def nve_drift(precision, steps=1000):
+    """NVE energy drift of the diamond-carbon workload (8x8x8 cells, 4096
+    atoms, synthetic NEP4, 300 K, dt 1 fs): least-squares slope of the total
+    energy per atom against time, the reference's definition
+    (tests/long_nve/long_nve_common.py nve_metrics), in eV/atom/ns."""
+    import nepx
+    spec = WORKLOADS["carbon"]
+    tmp = tempfile.mkdtemp()
+    path = workloads.write_nep(os.path.join(tmp, "nep.txt"), **spec["nep"])
+    t, h, p = build_system("carbon", seed=3)
+    masses = np.full(len(t), MASSES["C"])
+    v = workloads.maxwell_boltzmann(masses, 300.0, seed=4)
+    pot = nepx.Potential(path, max_atoms=len(t))
+    pot.set_precision(precision)
+    md = nepx.MD(pot, t, masses, p, v, h)
+    md.set_ensemble("nve")
+    md.run(1, 1.0)
+    rows = md.run(steps, 1.0, thermo_every=10)
+    e = (rows[:, 1] + rows[:, 2]) / len(t)
+    time_ns = np.arange(1, len(e) + 1) * 10 * 1.0e-6
+    slope = float(np.polyfit(time_ns, e, 1)[0])
+    md.close()
+    pot.close()
+    return {"drift_eV_per_atom_per_ns": slope, "max_excursion_eV_per_atom":
+            float(np.abs(e - e[0]).max()), "steps": steps, "dt_fs": 1.0, "atoms": len(t)}
 
 
 def gpu_reference_rate(nep_path, t, h, p, reps=50):
@@ -376,6 +430,11 @@ def main():
     ap.add_argument("--plain-sample", type=int, default=200)
     ap.add_argument("--chunk", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the NVE-drift and serving-sample measurements")
+    ap.add_argument("--serving-sample", type=int, default=600)
+    ap.add_argument("--precision", default="mixed", choices=["fp32", "mixed"],
+                    help="ANN precision of the serving workload")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -470,11 +529,46 @@ def main():
            "d2h_bytes_per_step": 20 * 8 + 4 + 232 + 56,   # thermo row, status, box, flags
            "api": "nepx_md_run(steps=1, thermo_every=1) per step"}
 
-    # per-kernel profile of the force path on the final state
+    # the same MD with the ANN on the tensor cores (mixed precision), from the
+    # same initial state
     st = md.state()
+    md.close()
+    pot.set_precision("mixed")
+    md = nepx.MD(pot, t, masses, p, v, h)
+    md.set_ensemble(kind, seed=12345678 + rank, **ens)
+    md.run(args.warmup, dt)
+    d_pos, d_vel, d_force, d_type, stream_ptr = md.device_state()
+    stream = torch.cuda.ExternalStream(stream_ptr)
+    ev_m = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            for _ in chunks]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    for c, steps in enumerate(chunks):
+        with torch.cuda.stream(stream):
+            flush.fill_((c + 7) & 0xFF)
+        ev_m[c][0].record(stream)
+        md.run_async(steps, dt)
+        ev_m[c][1].record(stream)
+    md.sync()
+    torch.cuda.synchronize()
+    dev_ms_m = sum(a.elapsed_time(b) for a, b in ev_m)
+    if dist:
+        tt = torch.tensor([dev_ms_m], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        dev_ms_m = float(tt.item())
+    value_mixed = atoms_total * K / (dev_ms_m / 1e3)
+    launches += K * (kernels_per_step + 5) + len(chunks)   # + type sort, tcgen05 ANN, k_acoef
+
+    # per-kernel profile of the force path on the final state of the FP32
+    # run, both precisions
     tt_ = torch.as_tensor(np.asarray(t, dtype=np.int32), device="cuda")
     pp_ = torch.as_tensor(np.ascontiguousarray(st["pos"]), device="cuda")
+    prof_mixed = pot.profile(tt_, st["h"], pp_, reps=50)
+    out_mixed = [x.cpu().numpy() for x in pot.compute(tt_, st["h"], pp_, sync_check=True)]
+    pot.set_precision("fp32")
     prof = pot.profile(tt_, st["h"], pp_, reps=50)
+    out_fp32 = [x.cpu().numpy() for x in pot.compute(tt_, st["h"], pp_, sync_check=True)]
     nr, na, nv = pot.neighbor_stats()
     # mean neighbour counts of the final state
     rr = pot.neighbors(0, n)
@@ -495,12 +589,36 @@ def main():
                 "flops_per_atom": fpa, "mean_radial_neighbors": mean_r,
                 "mean_angular_neighbors": mean_a,
                 "stage_ms": prof}
+    mixed = {"value": value_mixed, "unit": "atom-steps/s", "ms_per_step": dev_ms_m / K,
+             "over_fp32": value_mixed / value,
+             "what": "the same MD with the ANN contractions on tcgen05 (3xTF32, FP32 "
+                     "accumulation in TMEM); descriptors and forces FP32",
+             "stage_ms": prof_mixed}
+    drift = None
+    if rank == 0 and not args.no_extras:
+        drift = {"fp32": nve_drift("fp32"), "mixed": nve_drift("mixed")}
+    serving = None
+    if rank == 0 and not args.no_extras and args.serving_sample > 0:
+        sargs = argparse.Namespace(requests=args.serving_sample, arena=args.arena,
+                                   plain_sample=max(20, args.serving_sample // 10),
+                                   precision="mixed")
+        sv = run_serving(sargs)
+        serving = {k: sv[k] for k in ("value", "unit", "atom_steps_per_s", "latency_ms",
+                                      "plain_fp32_one_at_a_time", "batched_over_plain",
+                                      "config")}
 
     line = None
     if rank == 0:
         cpu = None
+        err = None
         if world == 1 and not args.no_cpu_baseline:
-            cpu = cpu_reference_rate(path, t, h, p)
+            # the reference FP64 CPU evaluator on the final state: the timed
+            # CPU baseline, and the FP64 values the GPU results are checked against
+            cpu, ref64 = cpu_reference_rate(path, t, st["h"], st["pos"], want_result=True)
+            if ref64 is not None:
+                err = {"against": "NEP3_CPU (reference, FP64) on the final MD state",
+                       "fp32": errors_vs(ref64, out_fp32[0], out_fp32[1]),
+                       "mixed": errors_vs(ref64, out_mixed[0], out_mixed[1])}
         T_last = float(rows[-1, 0]) if rows is not None else None
         line = {"metric": "atom-steps/s", "value": value, "unit": "atom-steps/s",
                 "n_gpus": world, "steps": K, "warmup": args.warmup,
@@ -517,6 +635,8 @@ def main():
                                "ms": prof["total"],
                                "what": "nepx_compute on the final state, static positions "
                                        "(neighbour update + descriptor + gather), L2 warm"},
+                "mixed_precision": mixed, "err_vs_fp64": err, "nve_drift": drift,
+                "serving": serving,
                 "gpu_launches": launches, "clocks": clock_info}
         print(json.dumps(line))
     md.close()

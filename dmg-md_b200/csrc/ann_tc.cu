@@ -173,15 +173,18 @@ __host__ __device__ inline AnnTcLayout ann_tc_layout(const ModelParams& p, int H
 
 constexpr int kSmemLimit = 227 * 1024;
 
-// Largest hidden-unit chunk (64, else 32, else 16) whose tiles fit one SM.
+// Hidden-unit chunk: the largest (64, 32, 16) whose tiles let two CTAs share
+// an SM, else the largest that fits one.
 __host__ __device__ inline int ann_tc_chunk(const ModelParams& p)
 {
+  for (int hc = 64; hc >= 16; hc /= 2)
+    if (ann_tc_layout(p, hc).total <= kSmemLimit / 2 - 1024) return hc;
   for (int hc = 64; hc >= 16; hc /= 2)
     if (ann_tc_layout(p, hc).total <= kSmemLimit) return hc;
   return 0;
 }
 
-__global__ void __launch_bounds__(kRows, 1)
+__global__ void __launch_bounds__(kRows, 2)
 k_ann_tc(const ModelParams p, int N, int HC, const int* __restrict__ order,
          const Site* __restrict__ sites, const float* __restrict__ qbuf,
          double* __restrict__ pe_ann, float* __restrict__ fpbuf, int* err)
@@ -208,16 +211,33 @@ k_ann_tc(const ModelParams p, int N, int HC, const int* __restrict__ order,
   const int idx = first + tid;
   const int c = idx < N ? order[idx] : -1;
   const int tc = c >= 0 ? static_cast<int>(sites[c].type) : -1;
-  const int t_lo = static_cast<int>(sites[order[first]].type);
-  const int t_hi = static_cast<int>(sites[order[min(first + kRows, N) - 1]].type);
+  // type range of the tile (a reduction, so any row order is handled)
+  __shared__ int s_trange[2];
+  if (tid == 0) {
+    s_trange[0] = kMaxTypes;
+    s_trange[1] = -1;
+  }
+  __syncthreads();
+  if (tc >= 0) {
+    atomicMin(&s_trange[0], tc);
+    atomicMax(&s_trange[1], tc);
+  }
+  __syncthreads();
+  const int t_lo = s_trange[0], t_hi = s_trange[1];
 
   // this row of the descriptor tile (zero rows past N)
-  for (int k = 0; k < dimK; ++k) {
-    const float x = c >= 0 ? qbuf[static_cast<size_t>(c) * p.dimK + k] : 0.0f;
-    float hi, lo;
-    split_tf32(x, hi, lo);
-    put(Qh, core_off(tid, k, dimK), hi);
-    put(Ql, core_off(tid, k, dimK), lo);
+  const float4* qrow = reinterpret_cast<const float4*>(qbuf + static_cast<size_t>(c < 0 ? 0 : c) *
+                                                                p.dimK);
+  for (int k4 = 0; k4 < dimK / 4; ++k4) {
+    const float4 x4 = c >= 0 ? __ldg(qrow + k4) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const float xs[4] = {x4.x, x4.y, x4.z, x4.w};
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      float hi, lo;
+      split_tf32(xs[u], hi, lo);
+      put(Qh, core_off(tid, 4 * k4 + u, dimK), hi);
+      put(Ql, core_off(tid, 4 * k4 + u, dimK), lo);
+    }
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -363,16 +383,33 @@ k_ann_tc(const ModelParams p, int N, int HC, const int* __restrict__ order,
                  : "memory");
 }
 
-// Centers sorted by type: a histogram, one scan, a scatter (order within a
-// type is arbitrary; every center's result is independent of it).
-__global__ void k_type_hist(int N, const Site* __restrict__ sites, int* counts)
+// Centers sorted by type: a histogram, one scan, a scatter, with one atomic
+// per warp and type (order within a type is arbitrary; every center's result
+// is independent of it).  Unless `always`, the sort runs only when the Verlet
+// list is rebuilt: the types of a system do not change between rebuilds, and
+// k_ann_tc takes each tile's type range from its rows, so a stale order costs
+// speed, never correctness.
+__global__ void k_type_clear(int* counts, const NeighborState* st)
 {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < N) atomicAdd(counts + sites[i].type, 1);
+  if (st->rebuild && threadIdx.x < 2 * kMaxTypes) counts[threadIdx.x] = 0;
 }
 
-__global__ void k_type_scan(int T, int* counts)
+__global__ void k_type_hist(int N, const Site* __restrict__ sites, int T, int* counts,
+                            const NeighborState* st, int always)
 {
+  if (!always && !st->rebuild) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = i < N ? static_cast<int>(sites[i].type) : -1;
+  const int lane = threadIdx.x & 31;
+  for (int u = 0; u < T; ++u) {
+    const unsigned m = __ballot_sync(0xffffffffu, t == u);
+    if (m && lane == __ffs(m) - 1) atomicAdd(counts + u, __popc(m));
+  }
+}
+
+__global__ void k_type_scan(int T, int* counts, const NeighborState* st, int always)
+{
+  if (!always && !st->rebuild) return;
   // counts[0..T) -> exclusive starts in counts[T..2T), cursors reset to them
   int acc = 0;
   for (int t = 0; t < T; ++t) {
@@ -383,10 +420,23 @@ __global__ void k_type_scan(int T, int* counts)
   }
 }
 
-__global__ void k_type_scatter(int N, const Site* __restrict__ sites, int* cursor, int* order)
+__global__ void k_type_scatter(int N, const Site* __restrict__ sites, int T, int* cursor,
+                               int* order, const NeighborState* st, int always)
 {
+  if (!always && !st->rebuild) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < N) order[atomicAdd(cursor + sites[i].type, 1)] = i;
+  const int t = i < N ? static_cast<int>(sites[i].type) : -1;
+  const int lane = threadIdx.x & 31;
+  const unsigned below = (1u << lane) - 1u;
+  for (int u = 0; u < T; ++u) {
+    const unsigned m = __ballot_sync(0xffffffffu, t == u);
+    if (!m) continue;
+    const int leader = __ffs(m) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(cursor + u, __popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (t == u) order[base + __popc(m & below)] = i;
+  }
 }
 
 }  // namespace
@@ -413,15 +463,23 @@ void ann_tc_prepare(const ModelParams& p)
                        static_cast<int>(ann_tc_smem_bytes(p)));
 }
 
-void launch_ann_tc(Engine& e, int N, cudaStream_t s)
+void launch_type_order(Engine& e, int N, bool always, cudaStream_t s)
 {
   const ModelParams& p = e.params;
   ForceScratch& sc = e.scratch;
   const int threads = 256, grid = (N + threads - 1) / threads;
-  cudaMemsetAsync(sc.type_counts, 0, sizeof(int) * 2 * kMaxTypes, s);
-  k_type_hist<<<grid, threads, 0, s>>>(N, sc.sites, sc.type_counts);
-  k_type_scan<<<1, 1, 0, s>>>(p.T, sc.type_counts);
-  k_type_scatter<<<grid, threads, 0, s>>>(N, sc.sites, sc.type_counts, sc.order);
+  if (always) cudaMemsetAsync(sc.type_counts, 0, sizeof(int) * 2 * kMaxTypes, s);
+  else k_type_clear<<<1, 32, 0, s>>>(sc.type_counts, e.d_nstate);
+  k_type_hist<<<grid, threads, 0, s>>>(N, sc.sites, p.T, sc.type_counts, e.d_nstate, always);
+  k_type_scan<<<1, 1, 0, s>>>(p.T, sc.type_counts, e.d_nstate, always);
+  k_type_scatter<<<grid, threads, 0, s>>>(N, sc.sites, p.T, sc.type_counts, sc.order, e.d_nstate,
+                                          always);
+}
+
+void launch_ann_tc(Engine& e, int N, cudaStream_t s)
+{
+  const ModelParams& p = e.params;
+  ForceScratch& sc = e.scratch;
   const int tiles = (N + kRows - 1) / kRows;
   k_ann_tc<<<tiles, kRows, ann_tc_smem_bytes(p), s>>>(p, N, ann_tc_chunk(p), sc.order, sc.sites,
                                                        sc.q, sc.pe_ann, sc.fp,

@@ -263,6 +263,7 @@ std::string engine_set_precision(Engine& e, int mode)
   }
   if (e.precision != mode) e.tuned = false;
   e.precision = mode;
+  e.order_valid = false;
   return "";
 }
 

@@ -68,6 +68,7 @@ struct Engine {
   ExplicitRows xr;
   bool use_xr = false;       // neighbour rows with explicit displacements (small box, batch)
   int precision = 0;         // 0: FP32 SIMT ANN; 1: mixed (ANN on the tensor cores, ann_tc.cu)
+  bool order_valid = false;  // scratch.order holds this system's type order
   // host-side bookkeeping
   Box last_box{};
   bool have_box = false;
@@ -134,6 +135,9 @@ bool ann_tc_supported(const ModelParams& p, std::string& why);
 size_t ann_tc_smem_bytes(const ModelParams& p);
 void ann_tc_prepare(const ModelParams& p);
 void launch_ann_tc(Engine& e, int N, cudaStream_t stream);
+// Centers sorted by type for the tensor-core tiles; unless `always`, only
+// when the Verlet list is about to be consumed after a rebuild.
+void launch_type_order(Engine& e, int N, bool always, cudaStream_t stream);
 // Switches the ANN precision (0 FP32, 1 mixed); allocates the mixed buffers.
 std::string engine_set_precision(Engine& e, int mode);
 

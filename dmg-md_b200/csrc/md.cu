@@ -574,7 +574,8 @@ int md_enqueue_run(nepx_md* m, int steps, double dt_fs, int thermo_every, double
   e.have_box = false;
   int* d_status = status_buffer(m);
   // capture one step as a graph (re-captured when the per-run constants change)
-  if (!md.graph || std::memcmp(&p, &md.graph_params, sizeof(p)) != 0) {
+  if (!md.graph || std::memcmp(&p, &md.graph_params, sizeof(p)) != 0 ||
+      md.graph_precision != e.precision) {
     if (md.graph) cudaGraphExecDestroy(md.graph);
     md.graph = nullptr;
     cudaGraph_t g;
@@ -588,6 +589,7 @@ int md_enqueue_run(nepx_md* m, int steps, double dt_fs, int thermo_every, double
     }
     cudaGraphDestroy(g);
     md.graph_params = p;
+    md.graph_precision = e.precision;
   }
   for (int k = 0; k < steps; ++k)
     if (cudaGraphLaunch(md.graph, s) != cudaSuccess) return md_cuda(m, "graph launch");

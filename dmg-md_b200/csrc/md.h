@@ -72,6 +72,7 @@ struct Md {
   cudaStream_t stream = nullptr;
   cudaGraphExec_t graph = nullptr;
   StepParams graph_params{};
+  int graph_precision = -1;       // ANN precision the graph's kernels were captured with
   int graph_steps = 0;
 };
 

@@ -1079,6 +1079,11 @@ void set_fused_smem_limits(const ModelParams& p)
 void launch_descriptor(Engine& e, int N, const double*, const int*, cudaStream_t stream)
 {
   const bool small = small_shape(e.params);
+  // the type order is taken while the rebuild flag is still up (k_nep_fused clears it)
+  if (e.precision == 1) {
+    launch_type_order(e, N, e.use_xr || !e.order_valid, stream);
+    e.order_valid = true;
+  }
   if (e.group == 8) {
     if (small) launch_fused_g<8, kSmallN, kSmallK, kSmallN>(e, N, stream);
     else launch_fused_g<8, kMaxN, kMaxBasis, kMaxN>(e, N, stream);
