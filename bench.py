@@ -30,7 +30,7 @@ cpu_baseline -- the reference's own FP64 CPU NEP evaluator (NEP3_CPU,
           RMSE and energy error of the FP32 and mixed paths).
 mixed_precision -- the same MD with the ANN on the tcgen05 tensor cores.
 nve_drift -- NVE energy drift (eV/atom/ns) of 4096-atom diamond carbon,
-          1000 steps of 1 fs, both precisions.
+          20,000 steps of 1 fs, both precisions.
 serving -- a bounded sample of the serving workload (--workload serving
           runs the full stream): served structures/s, p50/p99 latency,
           batched mixed-precision engine over the plain FP32 path.
@@ -326,9 +326,9 @@ def errors_vs(ref, pe, f):
             "energy_total_eV_per_atom": float(abs(pe.sum() - pe0.sum()) / n)}
 
 
-def nve_drift(precision, steps=1000):
+def nve_drift(precision, steps=20000, every=100):
     """NVE energy drift of the diamond-carbon workload (8x8x8 cells, 4096
-    atoms, synthetic NEP4, 300 K, dt 1 fs): least-squares slope of the total
+    atoms, synthetic NEP4, 300 K, dt 1 fs, 20 ps): least-squares slope of the total
     energy per atom against time, the reference's definition
     (tests/long_nve/long_nve_common.py nve_metrics), in eV/atom/ns."""
     import nepx
@@ -343,9 +343,9 @@ def nve_drift(precision, steps=1000):
     md = nepx.MD(pot, t, masses, p, v, h)
     md.set_ensemble("nve")
     md.run(1, 1.0)
-    rows = md.run(steps, 1.0, thermo_every=10)
+    rows = md.run(steps, 1.0, thermo_every=every)
     e = (rows[:, 1] + rows[:, 2]) / len(t)
-    time_ns = np.arange(1, len(e) + 1) * 10 * 1.0e-6
+    time_ns = np.arange(1, len(e) + 1) * every * 1.0e-6
     slope = float(np.polyfit(time_ns, e, 1)[0])
     md.close()
     pot.close()

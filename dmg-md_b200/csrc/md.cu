@@ -193,7 +193,8 @@ __global__ void k_ensemble(StepParams p, Box* box, MdScalars* sc, const double* 
   for (int q = 0; q < 8; ++q) sc->thermo[q] = th[q];
   const double Tt = target_temperature(p, step);
   double vf = 1.0, bf = 1.0;
-  const double* nz = noise + 3 * step;
+  const long long local = step - sc->step0;   // step within this call
+  const double* nz = noise + 3 * local;
   switch (p.kind) {
     case kNvtBer:
     case kNptBer: {
@@ -248,8 +249,8 @@ __global__ void k_ensemble(StepParams p, Box* box, MdScalars* sc, const double* 
   }
   sc->vfactor = vf;
   sc->bfactor = bf;
-  if (p.thermo_every > 0 && (step + 1) % p.thermo_every == 0) {
-    const long long row = (step + 1) / p.thermo_every - 1;
+  if (p.thermo_every > 0 && (local + 1) % p.thermo_every == 0) {
+    const long long row = (local + 1) / p.thermo_every - 1;
     if (row < rows_cap) {
       double* r = rows + row * kThermoCols;
       r[0] = th[0];
@@ -291,6 +292,7 @@ __global__ void k_scale(int N, double* vel, double* pos, double* x0,
 __global__ void k_init_scalars(MdScalars* sc, StepParams p, double T0, double tau)
 {
   sc->step = 0;
+  sc->step0 = 0;
   sc->vfactor_pre = 1.0;
   sc->vfactor = 1.0;
   sc->bfactor = 1.0;
@@ -326,6 +328,12 @@ void md_enqueue_step(Md& md, const StepParams& p, int* d_status)
                               md.rows_cap, e.d_nstate, d_status);
   k_scale<<<blocks, kThreads, 0, s>>>(N, md.d_vel, md.d_pos, e.nbr.x0, md.d_sc);
 }
+
+// A call that continues a segment: thermostat state and segment step carry
+// over; per-call buffers (draws, thermo rows) restart at this step.
+__global__ void k_mark_call(MdScalars* sc) { sc->step0 = sc->step; }
+
+void md_continue_scalars(Md& md) { k_mark_call<<<1, 1, 0, md.stream>>>(md.d_sc); }
 
 void md_init_scalars(Md& md, const StepParams& p, double T0, double tau)
 {
@@ -494,9 +502,11 @@ int nepx_md_set_ensemble(nepx_md_t* m, int kind, const double* params, unsigned 
 namespace {
 
 // Enqueues `steps` steps on the md stream; nothing waits for the device.
-int md_enqueue_run(nepx_md* m, int steps, double dt_fs, int thermo_every, double* h_thermo)
+int md_enqueue_run(nepx_md* m, int steps, double dt_fs, int thermo_every, double* h_thermo,
+                   int first_step, int segment_steps)
 {
   if (!m || steps < 1 || !(dt_fs >= 0.0) || thermo_every < 0) return NEPX_ERR_ARG;
+  if (first_step < 0 || segment_steps < first_step + steps) return NEPX_ERR_ARG;
   nepx::Md& md = m->md;
   nepx::Engine& e = *md.engine;
   const nepx::EnsembleConfig& c = md.ens;
@@ -506,7 +516,7 @@ int md_enqueue_run(nepx_md* m, int steps, double dt_fs, int thermo_every, double
   nepx::StepParams p{};
   p.N = N;
   p.kind = c.kind;
-  p.steps = steps;
+  p.steps = segment_steps;
   p.thermo_every = thermo_every;
   p.dt = dt_fs / nepx::kTimeUnit;
   p.T0 = c.T0;
@@ -563,7 +573,8 @@ int md_enqueue_run(nepx_md* m, int steps, double dt_fs, int thermo_every, double
     nepx::launch_set_box(e, md.box, s);
     e.box_owner = &md;
   }
-  nepx::md_init_scalars(md, p, c.T0, p.dt * c.Tdamp);
+  if (first_step == 0) nepx::md_init_scalars(md, p, c.T0, p.dt * c.Tdamp);
+  else nepx::md_continue_scalars(md);
   if (!md.forces_valid) {
     nepx::launch_neighbor_update(e, N, md.d_pos, md.d_type, true, s);
     if (!e.tuned) nepx::engine_autotune(e, N, md.d_pos, md.d_type, s);
@@ -628,14 +639,23 @@ extern "C" {
 
 int nepx_md_run(nepx_md_t* m, int steps, double dt_fs, int thermo_every, double* h_thermo)
 {
-  const int rc = md_enqueue_run(m, steps, dt_fs, thermo_every, h_thermo);
+  const int rc = md_enqueue_run(m, steps, dt_fs, thermo_every, h_thermo, 0, steps);
+  if (rc) return rc;
+  return md_finish(m);
+}
+
+int nepx_md_run_segment(nepx_md_t* m, int steps, double dt_fs, int thermo_every,
+                        double* h_thermo, int first_step, int segment_steps)
+{
+  const int rc = md_enqueue_run(m, steps, dt_fs, thermo_every, h_thermo, first_step,
+                                segment_steps);
   if (rc) return rc;
   return md_finish(m);
 }
 
 int nepx_md_run_async(nepx_md_t* m, int steps, double dt_fs)
 {
-  return md_enqueue_run(m, steps, dt_fs, 0, nullptr);
+  return md_enqueue_run(m, steps, dt_fs, 0, nullptr, 0, steps);
 }
 
 int nepx_md_sync(nepx_md_t* m)

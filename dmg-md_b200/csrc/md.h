@@ -27,7 +27,8 @@ constexpr int kThermoCols = 20;  // thermo.out's 18 columns + velocity and box f
 
 // Scalars the per-step kernels share, resident on the device.
 struct MdScalars {
-  long long step;      // step within the current run
+  long long step;      // step within the current segment
+  long long step0;     // segment step at which the current call started
   double vfactor_pre;  // NHC scale applied before the first half kick
   double vfactor;      // thermostat scale after the second half kick
   double bfactor;      // isotropic box scale of this step
@@ -39,7 +40,7 @@ struct MdScalars {
 struct StepParams {
   int N;
   int kind;
-  int steps;
+  int steps;           // segment length (the denominator of the temperature ramp)
   int thermo_every;
   double dt;           // natural time units
   double T0, T1, Tdamp;

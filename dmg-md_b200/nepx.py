@@ -34,7 +34,7 @@ EXPORTED = ["nepx_create", "nepx_destroy", "nepx_last_error", "nepx_info", "nepx
             "nepx_md_run_async", "nepx_md_sync", "nepx_compute_noalloc", "nepx_compute_batch",
             "nepx_server_create", "nepx_server_destroy", "nepx_server_last_error",
             "nepx_server_submit", "nepx_server_poll", "nepx_server_wait", "nepx_server_drain",
-            "nepx_server_stats", "nepx_set_precision"]
+            "nepx_server_stats", "nepx_set_precision", "nepx_md_run_segment"]
 
 ENSEMBLES = {"nve": 0, "nvt_ber": 1, "nvt_nhc": 2, "nvt_bdp": 3, "npt_ber": 4, "npt_scr": 5}
 THERMO_COLUMNS = ["T", "KE", "PE", "sxx", "syy", "szz", "syz", "sxz", "sxy", "ax", "ay", "az",
@@ -112,6 +112,8 @@ def lib():
                                            ctypes.POINTER(vp), ctypes.POINTER(vp),
                                            ctypes.POINTER(vp)]
         L.nepx_set_precision.argtypes = [vp, ctypes.c_int]
+        L.nepx_md_run_segment.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, dp,
+                                          ctypes.c_int, ctypes.c_int]
         L.nepx_compute_batch.argtypes = [vp, ctypes.POINTER(StructDesc), ctypes.c_int, vp, vp, vp,
                                          vp, vp, ctypes.c_uint, vp]
         L.nepx_server_create.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]
@@ -331,6 +333,16 @@ class MD:
         out = np.zeros((max(rows, 1), len(THERMO_COLUMNS)))
         self._check(lib().nepx_md_run(self._h, steps, dt_fs, thermo_every,
                                       _dp(out) if rows else None))
+        return out[:rows] if rows else None
+
+    def run_segment(self, steps, dt_fs, first_step, segment_steps, thermo_every=0):
+        """Steps [first_step, first_step + steps) of a segment of segment_steps."""
+        import numpy as np
+        rows = steps // thermo_every if thermo_every else 0
+        out = np.zeros((max(rows, 1), len(THERMO_COLUMNS)))
+        self._check(lib().nepx_md_run_segment(self._h, steps, dt_fs, thermo_every,
+                                              _dp(out) if rows else None, first_step,
+                                              segment_steps))
         return out[:rows] if rows else None
 
     def run_async(self, steps, dt_fs):

@@ -201,6 +201,16 @@ int nepx_md_run(nepx_md_t* md, int steps, double dt_fs, int thermo_every, double
  * are reported by the next nepx_md_sync (or nepx_md_run).  Interleaving
  * nepx_compute on the same potential handle requires nepx_md_sync first. */
 int nepx_md_run_async(nepx_md_t* md, int steps, double dt_fs);
+
+/* Part of one segment: steps [first_step, first_step + steps) of a segment of
+ * segment_steps steps (the reference's `run segment_steps`).  first_step = 0
+ * starts the segment (thermostat state initialised, temperature ramp from
+ * T0); later calls continue it (thermostat state kept, ramp continued), so a
+ * driver can stop between steps for output without changing the trajectory.
+ * Thermo rows count from this call's first step.  nepx_md_run(md, n, ...)
+ * equals nepx_md_run_segment(md, n, ..., 0, n). */
+int nepx_md_run_segment(nepx_md_t* md, int steps, double dt_fs, int thermo_every,
+                        double* h_thermo, int first_step, int segment_steps);
 int nepx_md_sync(nepx_md_t* md);
 
 /* Copies the current state to host arrays (any may be NULL); velocities in

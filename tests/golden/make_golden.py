@@ -136,6 +136,26 @@ def main():
         "thermo_out": open(os.path.join(base, "goldens", "single_large_nve", "main",
                                         "thermo.out")).read(),
     }
+    # whole programs: run.in / model.xyz of every stage and the golden output
+    # files, for the end-to-end driver tests (nepx-md)
+    manifest = json.load(open(os.path.join(base, "manifest.json")))
+    out["programs"] = {}
+    for case, spec in manifest["cases"].items():
+        pot = os.path.basename(spec["potential"])
+        stages = []
+        for st in spec["stages"]:
+            rec = {"name": st["name"],
+                   "run_in": open(os.path.join(base, st["run"])).read(),
+                   "model_xyz": open(os.path.join(base, st["model"])).read() if st.get("model")
+                   else None,
+                   "model_from_stage": st.get("model_from_stage"),
+                   "outputs": {}}
+            for name, o in st["outputs"].items():
+                if o["kind"] in ("xyz", "thermo", "restart"):
+                    rec["outputs"][name] = open(os.path.join(base, "goldens", case, st["name"],
+                                                             name)).read()
+            stages.append(rec)
+        out["programs"][case] = {"potential": pot, "stages": stages}
     with open(os.path.join(HERE, "baseline_goldens.json"), "w") as f:
         json.dump(out, f, indent=1)
     os.makedirs(os.path.join(HERE, "thermostats"), exist_ok=True)
