@@ -170,6 +170,7 @@ std::string engine_create(Engine& e, const std::string& nep_path, int max_atoms)
   ok &= dalloc(nb.cell_of, N) == cudaSuccess;
   ok &= dalloc(nb.x0, 3 * static_cast<size_t>(N)) == cudaSuccess;
   ok &= dalloc(e.scratch.sites, N) == cudaSuccess;
+  ok &= dalloc(e.scratch.qrad, static_cast<size_t>(N) * p.nR) == cudaSuccess;
   ok &= dalloc(e.scratch.alpha, static_cast<size_t>(N) * p.T * basis_stride(p)) == cudaSuccess;
   ok &= dalloc(e.scratch.f12, static_cast<size_t>(N) * nb.mn_a) == cudaSuccess;
   ok &= dalloc(e.scratch.pe_ann, N) == cudaSuccess;
@@ -201,6 +202,27 @@ void engine_autotune(Engine& e, int N, const double* pos, const int* type, cudaS
   cudaEventCreate(&b);
   cudaEventCreate(&c);
   int pick_a = e.f12_group;
+  if (!e.use_xr) {
+    float best = 1e30f;
+    int pick = e.filter_group;
+    for (int g : groups) {
+      e.filter_group = g;
+      float t[3];
+      for (int r = 0; r < 3; ++r) {
+        cudaEventRecord(a, stream);
+        launch_filter(e, N, stream);
+        cudaEventRecord(b, stream);
+        cudaEventSynchronize(b);
+        cudaEventElapsedTime(&t[r], a, b);
+      }
+      std::sort(t, t + 3);
+      if (t[1] < best) {
+        best = t[1];
+        pick = g;
+      }
+    }
+    e.filter_group = pick;
+  }
   for (int gf : groups) {
     for (int gg : groups) {
       e.group = gf;
@@ -240,8 +262,9 @@ void engine_autotune(Engine& e, int N, const double* pos, const int* type, cudaS
   e.gather_group = pick_g;
   e.tuned = true;
   if (std::getenv("NEPX_VERBOSE"))
-    std::fprintf(stderr, "nepx autotune (N=%d): fused G=%d, angular-force G=%d, gather G=%d\n", N,
-                 e.group, e.f12_group, e.gather_group);
+    std::fprintf(stderr,
+                 "nepx autotune (N=%d): filter G=%d, fused G=%d, angular-force G=%d, gather G=%d\n",
+                 N, e.filter_group, e.group, e.f12_group, e.gather_group);
 }
 
 std::string engine_set_precision(Engine& e, int mode)
@@ -273,7 +296,8 @@ void engine_destroy(Engine& e)
   void* ptrs[] = {e.d_params, e.d_box, e.d_nstate, nb.nn_v, nb.nl_v, nb.nn_r, nb.nl_r,
                   nb.nn_a, nb.nl_a, nb.cell_count, nb.cell_start, nb.cell_atoms, nb.cell_of,
                   nb.x0, e.scratch.alpha, e.scratch.f12, e.scratch.pe_ann, e.scratch.q,
-                  e.scratch.tune_out, e.scratch.acoef, e.scratch.sites, e.scratch.fp,
+                  e.scratch.tune_out, e.scratch.acoef, e.scratch.sites, e.scratch.qrad,
+                  e.scratch.fp,
                   e.scratch.order, e.scratch.type_counts, e.xr.er, e.xr.ea,
                   e.xr.d_si, e.xr.d_soff};
   for (void* q : ptrs)

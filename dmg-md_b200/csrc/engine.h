@@ -29,6 +29,7 @@ struct NeighborBuffers {
 
 struct ForceScratch {
   Site* sites = nullptr;     // [N] position + type records, packed by the skin check
+  float* qrad = nullptr;     // [N][nR] radial descriptors from the typewise filter
   float* alpha = nullptr;    // [N][T][kp] radial force coefficients sum_n dE/dq_n c(ti,t)[n][k]
   float4* f12 = nullptr;     // [N][mn_a] directed angular partial forces
   float* acoef = nullptr;    // [N][nA][24] dE/ds[n][lm] of each center
@@ -76,6 +77,7 @@ struct Engine {
   const void* box_owner = nullptr;   // md whose box the device copy holds (nullptr: none)
   int last_n = -1;
   int group = 4;             // lanes per center in the fused kernel (autotuned)
+  int filter_group = 8;      // lanes per center in the typewise filter (autotuned)
   int f12_group = 4;         // lanes per center in the angular-force kernel (autotuned)
   int gather_group = 8;      // lanes per center in the gather (autotuned)
   bool tuned = false;
@@ -146,6 +148,8 @@ std::string engine_set_precision(Engine& e, int mode);
 void launch_force(Engine& e, int N, const double* pos, const int* type, double* pe,
                   double* force, double* virial, bool accumulate, cudaStream_t stream);
 void launch_descriptor(Engine& e, int N, const double* pos, const int* type, cudaStream_t stream);
+// The typewise filter + radial descriptors alone (large-box path).
+void launch_filter(Engine& e, int N, cudaStream_t stream);
 void launch_gather(Engine& e, int N, const double* pos, const int* type, double* pe,
                    double* force, double* virial, bool accumulate, cudaStream_t stream);
 

@@ -222,19 +222,22 @@ __global__ void k_verlet_build(int N, const Box* __restrict__ box, const Site* _
   __syncwarp();
   const int total = *count;
   const int used = min(total, pow2);
-  for (int k = used + lane; k < pow2; k += 32) buf[k] = INT_MAX;
+  // bitonic sort of the smallest power of two that holds the row (padding
+  // INT_MAX), one compare-exchange pair per lane and pass
+  int p2 = 1;
+  while (p2 < used) p2 <<= 1;
+  for (int k = used + lane; k < p2; k += 32) buf[k] = INT_MAX;
   __syncwarp();
-  for (int k = 2; k <= pow2; k <<= 1) {
+  for (int k = 2; k <= p2; k <<= 1) {
     for (int j = k >> 1; j > 0; j >>= 1) {
-      for (int t = lane; t < pow2; t += 32) {
-        const int p = t ^ j;
-        if (p > t) {
-          const int a = buf[t], c = buf[p];
-          const bool up = (t & k) == 0;
-          if ((a > c) == up) {
-            buf[t] = c;
-            buf[p] = a;
-          }
+      for (int q = lane; q < (p2 >> 1); q += 32) {
+        const int t = ((q & ~(j - 1)) << 1) | (q & (j - 1));   // lower index of the pair
+        const int u = t | j;
+        const int a = buf[t], c = buf[u];
+        const bool up = (t & k) == 0;
+        if ((a > c) == up) {
+          buf[t] = c;
+          buf[u] = a;
         }
       }
       __syncwarp();

@@ -234,6 +234,119 @@ __device__ __forceinline__ void center_acoef(const ModelParams& p, const float* 
   }
 }
 
+// Typewise filter and radial descriptors (large-box path): one group of G
+// lanes per center sweeps its sorted Verlet row with the next candidate's
+// site in flight, applies the reference's FP32 predicate bit for bit (double
+// difference rounded to float, float minimum image, the same x*x + y*y + z*z
+// expression; nep.cu:503-561) and writes the radial and angular rows in
+// order (group ballot + popcount), summing
+// q_n = sum_j sum_k c(ti,tj)[n][k] f_k(d_ij) on the way.  Kept apart from
+// k_nep_fused so this latency-bound sweep runs at the occupancy of its own
+// register count.
+template <int G, int NRM, int KM>
+__global__ void __launch_bounds__(kBlock)
+k_filter_radial(const ModelParams p, int N, const Box* __restrict__ box,
+                const Site* __restrict__ sites, NeighborState* st,
+                const int* __restrict__ nn_v, const int* __restrict__ nl_v, int mn_v,
+                int* __restrict__ nn_r, int* __restrict__ nl_r, int mn_r,
+                int* __restrict__ nn_a, int* __restrict__ nl_a, int mn_a,
+                float* __restrict__ qrad)
+{
+  constexpr int APW = 32 / G, APB = kBlock / G;
+  constexpr int KP = (KM + 3) & ~3;
+  extern __shared__ float sm[];   // radial coefficient table [T*T][nR][KP]
+  const int tid = threadIdx.x;
+  const int T = p.T, nR = p.nR, kR = p.kR;
+  for (int k = tid; k < T * T * nR * KP; k += kBlock) {
+    const int kk = k % KP, row = k / KP;
+    sm[k] = kk < kR ? __ldg(p.c_pair + row * kR + kk) : 0.0f;
+  }
+  if (blockIdx.x == 0 && tid == 0) st->rebuild = 0;   // the Verlet list is consumed
+  __syncthreads();
+  const int lane = tid & 31, warp = tid >> 5;
+  const int group = lane / G, gl = lane % G;
+  const int i = blockIdx.x * APB + warp * APW + group;
+  const bool active = i < N;
+  const Box b = *box;
+  const Site me = active ? sites[i] : Site{0.0, 0.0, 0.0, 0};
+  const double xi = me.x, yi = me.y, zi = me.z;
+  const int t1 = static_cast<int>(me.type);
+  const unsigned below = (1u << gl) - 1u;
+  const float rr1 = p.rc_r[t1], ra1 = p.rc_a[t1];
+  float qr[NRM];
+#pragma unroll
+  for (int n = 0; n < NRM; ++n) qr[n] = 0.0f;
+  const int nv = active ? nn_v[i] : 0;
+  const int nv_max = __reduce_max_sync(kFull, nv);
+  const int* vrow = nl_v + static_cast<size_t>(i) * mn_v;
+  int* rrow = nl_r + static_cast<size_t>(i) * mn_r;
+  int* arow = nl_a + static_cast<size_t>(i) * mn_a;
+  int cr = 0, ca = 0;
+  int j_next = 0;
+  double2 sa_next = make_double2(0.0, 0.0), sc_next = make_double2(0.0, 0.0);
+  if (gl < nv) {
+    j_next = vrow[gl];
+    site_load(sites, j_next, sa_next, sc_next);
+  }
+  for (int base = 0; base < nv_max; base += G) {
+    const int k = base + gl;
+    const int j = j_next;
+    const double2 sa = sa_next, sc = sc_next;
+    if (k + G < nv) {
+      j_next = vrow[k + G];
+      site_load(sites, j_next, sa_next, sc_next);
+    }
+    bool in_r = false, in_a = false;
+    int t2 = 0;
+    float x12 = 0.0f, y12 = 0.0f, z12 = 0.0f, d12_square = 0.0f, rc_radial = 1.0f;
+    if (k < nv) {
+      site_delta(b, sa, sc, xi, yi, zi, x12, y12, z12, t2);
+      d12_square = x12 * x12 + y12 * y12 + z12 * z12;
+      rc_radial = (rr1 + p.rc_r[t2]) * 0.5f;
+      const float rc_angular = (ra1 + p.rc_a[t2]) * 0.5f;
+      in_r = d12_square < rc_radial * rc_radial;
+      in_a = in_r && d12_square < rc_angular * rc_angular;
+    }
+    const unsigned mr = group_ballot<G>(in_r, group);
+    const unsigned ma = group_ballot<G>(in_a, group);
+    if (in_r) {
+      const int at = cr + __popc(mr & below);
+      if (at < mn_r) rrow[at] = j;
+      const float d = sqrtf(d12_square);
+      const float rcinv = 1.0f / rc_radial;
+      float fc, fcp;
+      cutoff_fc(rc_radial, rcinv, d, fc, fcp);
+      float fn[KP];
+#pragma unroll
+      for (int kk = 0; kk < KP; ++kk) fn[kk] = 0.0f;
+      radial_basis<KM>(kR, rcinv, d, fc, fn);
+      const float* c = sm + (t1 * T + t2) * nR * KP;
+#pragma unroll
+      for (int n = 0; n < NRM; ++n)
+        if (n < nR) qr[n] += dot_basis<KM>(c + n * KP, fn);
+    }
+    if (in_a) {
+      const int at = ca + __popc(ma & below);
+      if (at < mn_a) arow[at] = j;
+    }
+    cr += __popc(mr);
+    ca += __popc(ma);
+  }
+#pragma unroll
+  for (int n = 0; n < NRM; ++n) qr[n] = group_sum<G>(qr[n]);
+  if (active && gl == 0) {
+    nn_r[i] = min(cr, mn_r);
+    nn_a[i] = min(ca, mn_a);
+    if (cr > mn_r) atomicOr(&st->overflow, 2);
+    if (ca > mn_a) atomicOr(&st->overflow, 4);
+    atomicMax(&st->max_nn[1], cr);
+    atomicMax(&st->max_nn[2], ca);
+#pragma unroll
+    for (int n = 0; n < NRM; ++n)
+      if (n < nR) qrad[static_cast<size_t>(i) * nR + n] = qr[n];
+  }
+}
+
 // NRM/KM/NAM: compile-time bounds of nR, basis size + 1, nA for this instance.
 // The small-shape instance is held to 168 registers (three CTAs per SM): the
 // kernel is latency bound and the extra warps outweigh a few spilled words.
@@ -247,8 +360,9 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
             const int* __restrict__ nn_v, const int* __restrict__ nl_v, int mn_v,
             int* __restrict__ nn_r, int* __restrict__ nl_r, int mn_r, int* __restrict__ nn_a,
             int* __restrict__ nl_a, int mn_a, const float4* __restrict__ er,
-            const float4* __restrict__ ea, float* __restrict__ alpha,
-            float* __restrict__ acoef, double* __restrict__ pe_ann, float* __restrict__ qout)
+            const float4* __restrict__ ea, const float* __restrict__ qrad,
+            float* __restrict__ alpha, float* __restrict__ acoef, double* __restrict__ pe_ann,
+            float* __restrict__ qout)
 {
   constexpr int APW = 32 / G;             // centers per warp
   constexpr int APB = kBlock / G;         // centers per block
@@ -290,7 +404,6 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
   const Site me = active ? sites[i] : Site{0.0, 0.0, 0.0, 0};
   const double xi = me.x, yi = me.y, zi = me.z;
   const int t1 = static_cast<int>(me.type);
-  const unsigned below = (1u << gl) - 1u;
 
   // ---- 1. filter the Verlet row, radial descriptors -------------------------
   const float rr1 = p.rc_r[t1], ra1 = p.rc_a[t1];
@@ -328,60 +441,14 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
       }
     }
   } else {
-    const int nv = active ? nn_v[i] : 0;
-    const int nv_max = __reduce_max_sync(kFull, nv);
-    const int* vrow = nl_v + static_cast<size_t>(i) * mn_v;
-    int* rrow = nl_r + static_cast<size_t>(i) * mn_r;
-    int* arow = nl_a + static_cast<size_t>(i) * mn_a;
-    // software pipeline: the next candidate's index and site are in flight
-    // while the current one is filtered and evaluated
-    int j_next = 0;
-    double2 sa_next = make_double2(0.0, 0.0), sc_next = make_double2(0.0, 0.0);
-    if (gl < nv) {
-      j_next = vrow[gl];
-      site_load(sites, j_next, sa_next, sc_next);
-    }
-    for (int base = 0; base < nv_max; base += G) {
-      const int k = base + gl;
-      const int j = j_next;
-      const double2 sa = sa_next, sc = sc_next;
-      if (k + G < nv) {
-        j_next = vrow[k + G];
-        site_load(sites, j_next, sa_next, sc_next);
-      }
-      bool in_r = false, in_a = false;
-      int t2 = 0;
-      float x12 = 0.0f, y12 = 0.0f, z12 = 0.0f, d12_square = 0.0f, rc_radial = 1.0f;
-      if (k < nv) {
-        site_delta(b, sa, sc, xi, yi, zi, x12, y12, z12, t2);
-        d12_square = x12 * x12 + y12 * y12 + z12 * z12;
-        rc_radial = (rr1 + p.rc_r[t2]) * 0.5f;
-        const float rc_angular = (ra1 + p.rc_a[t2]) * 0.5f;
-        in_r = d12_square < rc_radial * rc_radial;
-        in_a = in_r && d12_square < rc_angular * rc_angular;
-      }
-      const unsigned mr = group_ballot<G>(in_r, group);
-      const unsigned ma = group_ballot<G>(in_a, group);
-      if (in_r) {
-        const int at = cr + __popc(mr & below);
-        if (at < mn_r) rrow[at] = j;
-        add_radial(t2, d12_square, rc_radial);
-      }
-      if (in_a) {
-        const int at = ca + __popc(ma & below);
-        if (at < mn_a) arow[at] = j;
-      }
-      cr += __popc(mr);
-      ca += __popc(ma);
-    }
-    if (active && gl == 0) {
-      nn_r[i] = min(cr, mn_r);
-      nn_a[i] = min(ca, mn_a);
-      if (cr > mn_r) atomicOr(&st->overflow, 2);
-      if (ca > mn_a) atomicOr(&st->overflow, 4);
-      atomicMax(&st->max_nn[1], cr);
-      atomicMax(&st->max_nn[2], ca);
-    }
+    // the typewise rows, their counts and the radial descriptors come from
+    // k_filter_radial (lane 0 of the group holds q, the group sum spreads it)
+    cr = active ? nn_r[i] : 0;
+    ca = active ? nn_a[i] : 0;
+    if (active && gl == 0)
+#pragma unroll
+      for (int n = 0; n < NRM; ++n)
+        if (n < nR) qr[n] = qrad[static_cast<size_t>(i) * nR + n];
   }
 #pragma unroll
   for (int n = 0; n < NRM; ++n) qr[n] = group_sum<G>(qr[n]);
@@ -974,8 +1041,19 @@ void launch_fused_t(Engine& e, int N, cudaStream_t s)
   const size_t smem = fused_layout(e.params, APB, (KM + 3) & ~3).total_bytes;
   k_nep_fused<G, NRM, KM, NAM, XR><<<blocks, kBlock, smem, s>>>(
     e.params, N, e.d_box, e.scratch.sites, e.d_nstate, nb.nn_v, nb.nl_v, nb.mn_v, nb.nn_r, nb.nl_r,
-    nb.mn_r, nb.nn_a, nb.nl_a, nb.mn_a, e.xr.er, e.xr.ea, e.scratch.alpha, e.scratch.acoef,
-    e.scratch.pe_ann, e.precision == 1 ? e.scratch.q : nullptr);
+    nb.mn_r, nb.nn_a, nb.nl_a, nb.mn_a, e.xr.er, e.xr.ea, e.scratch.qrad, e.scratch.alpha,
+    e.scratch.acoef, e.scratch.pe_ann, e.precision == 1 ? e.scratch.q : nullptr);
+}
+
+template <int G, int NRM, int KM>
+void launch_filter_t(Engine& e, int N, cudaStream_t s)
+{
+  NeighborBuffers& nb = e.nbr;
+  constexpr int APB = kBlock / G;
+  const size_t smem = sizeof(float) * e.params.T * e.params.T * e.params.nR * ((KM + 3) & ~3);
+  k_filter_radial<G, NRM, KM><<<(N + APB - 1) / APB, kBlock, smem, s>>>(
+    e.params, N, e.d_box, e.scratch.sites, e.d_nstate, nb.nn_v, nb.nl_v, nb.mn_v, nb.nn_r,
+    nb.nl_r, nb.mn_r, nb.nn_a, nb.nl_a, nb.mn_a, e.scratch.qrad);
 }
 
 template <int KP>
@@ -1076,6 +1154,18 @@ void set_fused_smem_limits(const ModelParams& p)
   }
 }
 
+void launch_filter(Engine& e, int N, cudaStream_t s)
+{
+  const bool small = small_shape(e.params);
+  if (e.filter_group == 8) {
+    if (small) launch_filter_t<8, kSmallN, kSmallK>(e, N, s);
+    else launch_filter_t<8, kMaxN, kMaxBasis>(e, N, s);
+  } else {
+    if (small) launch_filter_t<4, kSmallN, kSmallK>(e, N, s);
+    else launch_filter_t<4, kMaxN, kMaxBasis>(e, N, s);
+  }
+}
+
 void launch_descriptor(Engine& e, int N, const double*, const int*, cudaStream_t stream)
 {
   const bool small = small_shape(e.params);
@@ -1084,6 +1174,7 @@ void launch_descriptor(Engine& e, int N, const double*, const int*, cudaStream_t
     launch_type_order(e, N, e.use_xr || !e.order_valid, stream);
     e.order_valid = true;
   }
+  if (!e.use_xr) launch_filter(e, N, stream);
   if (e.group == 8) {
     if (small) launch_fused_g<8, kSmallN, kSmallK, kSmallN>(e, N, stream);
     else launch_fused_g<8, kMaxN, kMaxBasis, kMaxN>(e, N, stream);

@@ -90,6 +90,7 @@ size_t bytes_needed(const nepx::Engine& e, int n)
   c.take<int>(N);               // cell_of
   c.take<double>(3 * N);        // x0
   c.take<nepx::Site>(N);
+  c.take<float>(N * e.params.nR);
   c.take<float>(N * e.params.T * nepx::basis_stride(e.params));
   c.take<float4>(N * nb.mn_a);
   c.take<double>(N);
@@ -146,6 +147,7 @@ extern "C" int nepx_compute_noalloc(nepx_t* h, const nepx_box* box, int n, const
   nb.x0 = c.take<double>(3 * N);
   nb.cell_cap = static_cast<int>(cells);
   view.scratch.sites = c.take<nepx::Site>(N);
+  view.scratch.qrad = c.take<float>(N * view.params.nR);
   view.scratch.alpha = c.take<float>(N * view.params.T * nepx::basis_stride(view.params));
   view.scratch.f12 = c.take<float4>(N * nb.mn_a);
   view.scratch.pe_ann = c.take<double>(N);
