@@ -40,6 +40,8 @@ struct StructInfo {
   int ncell[3];   // images per direction (1 where not periodic)
   int small;      // 1: the reference's small-box image arithmetic; 0: minimum image
   int off, n;
+  int nc[3];      // cell grid of a large structure's candidate search (nc[0] = 0: scan all atoms)
+  int cell_base;  // first cell of this structure in the batch's cell arrays
 };
 
 // Packed neighbour of an explicit row: index j (low 28 bits) and type (high 4).

@@ -51,6 +51,13 @@ struct ExplicitRows {
   int max_struct = 0;
   int n_struct = 0;
   bool from_box = true;       // one structure whose StructInfo follows the device box
+  // cell lists of the large structures of a batch (candidate search)
+  int* cell_count = nullptr;
+  int* cell_start = nullptr;
+  int* cell_atoms = nullptr;  // [N]
+  int* cell_of = nullptr;     // [N], -1: the atom's structure scans all its atoms
+  int cell_cap = 0;
+  int n_cells = 0;            // cells in use (set with the structure table)
 };
 
 struct Engine {
@@ -116,6 +123,11 @@ void launch_neighbor_update(Engine& e, int N, const double* pos, const int* type
 // Explicit rows: allocates them for the handle's capacity and max_struct
 // structures (once; later calls only check the size).
 std::string engine_enable_xr(Engine& e, int max_struct);
+
+// Cell grids of the large structures of a batch: each gets cells at least
+// rc thick (at most cell_cap in total, else it scans all its atoms); returns
+// the number of cells.  Structures are described by si[0..n).
+int assign_cells(const Engine& e, StructInfo* si, int n);
 
 // Small-box test of the reference with its cutoff (largest radial cutoff)
 // and skin 1 A; returns 0 large, 1 small, -1 small in one direction and

@@ -14,14 +14,18 @@
 // scan gives every lane its write offset and a second pass writes the edges,
 // so rows keep the reference's order.  The same kernel serves any number of
 // structures packed into one atom range (the batched path): a center finds
-// its structure by binary search over the structure offsets, and structures
+// its structure by binary search over the structure offsets.  Structures
 // that are not small use the large-box arithmetic (double difference rounded
-// to float, float minimum image, reference nep.cu:503-561) over all their
-// atoms, which yields the large-box path's typewise rows exactly.
+// to float, float minimum image, reference nep.cu:503-561); their candidates
+// come from a cell grid of their own (cells at least rc thick, 3x3x3 stencil,
+// one counting sort over the whole batch), and each row is sorted in shared
+// memory, which yields the large-box path's typewise rows exactly.
 //
 // Row entry: float4 (x12, y12, z12, bits of j | type(j) << 28), row-major
 // [center][slot]; radial and angular rows are separate.
 #include <algorithm>
+#include <climits>
+#include <cmath>
 #include <string>
 
 #include "engine.h"
@@ -80,8 +84,11 @@ k_rows_explicit(const ModelParams p, int total, const StructInfo* __restrict__ s
                 const int* __restrict__ soff, int S, const double* __restrict__ pos,
                 const int* __restrict__ type, int* __restrict__ nn_r, float4* __restrict__ er,
                 int mn_r, int* __restrict__ nn_a, float4* __restrict__ ea, int mn_a,
+                const int* __restrict__ cell_count, const int* __restrict__ cell_start,
+                const int* __restrict__ cell_atoms, const int* __restrict__ cell_of, int p2r,
                 NeighborState* st)
 {
+  extern __shared__ int s_rows[];   // per warp: p2r row slots + a counter
   const int lane = threadIdx.x & 31;
   const int wpb = blockDim.x >> 5;
   const unsigned below = (1u << lane) - 1u;
@@ -101,35 +108,95 @@ k_rows_explicit(const ModelParams p, int total, const StructInfo* __restrict__ s
     int cr = 0, ca = 0;
     if (!s.small) {
       const double xi = pos[i], yi = pos[total + i], zi = pos[2 * total + i];
-      for (int base = 0; base < n; base += 32) {
-        const int j = off + base + lane;
-        bool in_r = false, in_a = false;
-        float x12 = 0.0f, y12 = 0.0f, z12 = 0.0f;
-        int t2 = 0;
-        if (base + lane < n && j != i) {
-          x12 = pos[j] - xi;
-          y12 = pos[total + j] - yi;
-          z12 = pos[2 * total + j] - zi;
+      int* buf = s_rows + (threadIdx.x >> 5) * (p2r + 1);
+      int* count = buf + p2r;
+      if (lane == 0) *count = 0;
+      __syncwarp();
+      auto consider = [&](int j) {
+        float x12 = pos[j] - xi, y12 = pos[total + j] - yi, z12 = pos[2 * total + j] - zi;
+        mic_f32(s.box, x12, y12, z12);
+        const float d12_square = x12 * x12 + y12 * y12 + z12 * z12;
+        const float rc_radial = (rr1 + p.rc_r[type[j]]) * 0.5f;
+        if (d12_square < rc_radial * rc_radial) {
+          const int slot = atomicAdd(count, 1);
+          if (slot < p2r) buf[slot] = j;
+        }
+      };
+      if (s.nc[0] > 0) {
+        // the 3x3x3 cells around the center's (every cell once where the grid is narrower)
+        const int nc0 = s.nc[0], nc1 = s.nc[1], nc2 = s.nc[2];
+        const int lc = cell_of[i] - s.cell_base;
+        const int cx = lc % nc0, cy = (lc / nc0) % nc1, cz = lc / (nc0 * nc1);
+        const int sp0 = (s.box.pbc[0] && nc0 >= 3) ? 3 : nc0;
+        const int sp1 = (s.box.pbc[1] && nc1 >= 3) ? 3 : nc1;
+        const int sp2 = (s.box.pbc[2] && nc2 >= 3) ? 3 : nc2;
+        for (int q = 0; q < sp0 * sp1 * sp2; ++q) {
+          const int q0 = q % sp0, q1 = (q / sp0) % sp1, q2 = q / (sp0 * sp1);
+          int gx = sp0 == 3 ? cx + q0 - 1 : q0;
+          int gy = sp1 == 3 ? cy + q1 - 1 : q1;
+          int gz = sp2 == 3 ? cz + q2 - 1 : q2;
+          if (gx < 0) gx += nc0; else if (gx >= nc0) gx -= nc0;
+          if (gy < 0) gy += nc1; else if (gy >= nc1) gy -= nc1;
+          if (gz < 0) gz += nc2; else if (gz >= nc2) gz -= nc2;
+          const int c = s.cell_base + (gz * nc1 + gy) * nc0 + gx;
+          const int start = cell_start[c], cnt = cell_count[c];
+          for (int m = lane; m < cnt; m += 32) {
+            const int j = cell_atoms[start + m];
+            if (j != i) consider(j);
+          }
+        }
+      } else {
+        for (int base = 0; base < n; base += 32) {
+          const int j = off + base + lane;
+          if (base + lane < n && j != i) consider(j);
+        }
+      }
+      __syncwarp();
+      const int found = *count;
+      const int used = min(found, p2r);
+      int p2 = 1;
+      while (p2 < used) p2 <<= 1;
+      for (int k = used + lane; k < p2; k += 32) buf[k] = INT_MAX;
+      __syncwarp();
+      for (int k = 2; k <= p2; k <<= 1) {   // bitonic sort, one pair per lane and pass
+        for (int jj = k >> 1; jj > 0; jj >>= 1) {
+          for (int q = lane; q < (p2 >> 1); q += 32) {
+            const int t = ((q & ~(jj - 1)) << 1) | (q & (jj - 1));
+            const int u = t | jj;
+            const int a = buf[t], c = buf[u];
+            if ((a > c) == ((t & k) == 0)) {
+              buf[t] = c;
+              buf[u] = a;
+            }
+          }
+          __syncwarp();
+        }
+      }
+      // ascending radial row; the angular row is its subset inside the angular cutoff
+      for (int k0 = 0; k0 < used; k0 += 32) {
+        const int k = k0 + lane;
+        bool in_a = false;
+        float4 entry = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (k < used) {
+          const int j = buf[k];
+          float x12 = pos[j] - xi, y12 = pos[total + j] - yi, z12 = pos[2 * total + j] - zi;
           mic_f32(s.box, x12, y12, z12);
           const float d12_square = x12 * x12 + y12 * y12 + z12 * z12;
-          t2 = type[j];
-          const float rc_radial = (rr1 + p.rc_r[t2]) * 0.5f;
+          const int t2 = type[j];
           const float rc_angular = (ra1 + p.rc_a[t2]) * 0.5f;
-          in_r = d12_square < rc_radial * rc_radial;   // angular edges are radial ones
-          in_a = in_r && d12_square < rc_angular * rc_angular;
+          in_a = d12_square < rc_angular * rc_angular;
+          entry = row_entry(x12, y12, z12, j, t2);
+          if (k < mn_r) rrow[k] = entry;
         }
-        const unsigned mr = __ballot_sync(kFull, in_r), ma = __ballot_sync(kFull, in_a);
-        if (in_r) {
-          const int at = cr + __popc(mr & below);
-          if (at < mn_r) rrow[at] = row_entry(x12, y12, z12, j, t2);
-        }
+        const unsigned ma = __ballot_sync(kFull, in_a);
         if (in_a) {
           const int at = ca + __popc(ma & below);
-          if (at < mn_a) arow[at] = row_entry(x12, y12, z12, j, t2);
+          if (at < mn_a) arow[at] = entry;
         }
-        cr += __popc(mr);
         ca += __popc(ma);
       }
+      cr = found;
+      __syncwarp();   // the buffer is reused by this warp's next center
     } else {
       // the small-box arithmetic: float center, double image position
       const float x1 = pos[i], y1 = pos[total + i], z1 = pos[2 * total + i];
@@ -201,6 +268,72 @@ k_rows_explicit(const ModelParams p, int total, const StructInfo* __restrict__ s
   }
 }
 
+// Cell of every atom of a large structure (fractional coordinates, wrapped
+// where periodic, one cell where not), counted per cell.
+__global__ void k_xcell_assign(int total, const StructInfo* __restrict__ si,
+                               const int* __restrict__ soff, int S, const double* __restrict__ pos,
+                               int* cell_count, int* cell_of)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  int lo = 0, hi = S - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (soff[mid] <= i) lo = mid; else hi = mid - 1;
+  }
+  const StructInfo& s = si[lo];
+  if (s.small || s.nc[0] == 0) {
+    cell_of[i] = -1;
+    return;
+  }
+  const double r[3] = {pos[i], pos[total + i], pos[2 * total + i]};
+  int c[3];
+  for (int d = 0; d < 3; ++d) {
+    double f = s.box.hinv[3 * d] * r[0] + s.box.hinv[3 * d + 1] * r[1] + s.box.hinv[3 * d + 2] * r[2];
+    f -= floor(f);
+    int k = static_cast<int>(f * s.nc[d]);
+    c[d] = k < 0 ? 0 : (k >= s.nc[d] ? s.nc[d] - 1 : k);
+  }
+  const int cell = s.cell_base + (c[2] * s.nc[1] + c[1]) * s.nc[0] + c[0];
+  cell_of[i] = cell;
+  atomicAdd(cell_count + cell, 1);
+}
+
+// Exclusive scan of the cell counts (one block); counts reset as fill cursors.
+__global__ void k_xcell_scan(int ncells, int* cell_count, int* cell_start)
+{
+  __shared__ int part[1024];
+  const int per = (ncells + blockDim.x - 1) / blockDim.x;
+  const int lo = threadIdx.x * per, hi = min(ncells, lo + per);
+  int sum = 0;
+  for (int c = lo; c < hi; ++c) sum += cell_count[c];
+  part[threadIdx.x] = sum;
+  __syncthreads();
+  for (int o = 1; o < blockDim.x; o <<= 1) {
+    const int v = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  int run = part[threadIdx.x] - sum;
+  for (int c = lo; c < hi; ++c) {
+    const int k = cell_count[c];
+    cell_start[c] = run;
+    run += k;
+    cell_count[c] = 0;
+  }
+}
+
+__global__ void k_xcell_fill(int total, const int* __restrict__ cell_of, int* cell_count,
+                             const int* __restrict__ cell_start, int* cell_atoms)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  const int c = cell_of[i];
+  if (c < 0) return;
+  cell_atoms[cell_start[c] + atomicAdd(cell_count + c, 1)] = i;
+}
+
 __global__ void k_row_indices(int n, const int* __restrict__ cnt, const float4* __restrict__ rows,
                               int src_mn, int* nn, int* nl, int mn)
 {
@@ -221,6 +354,30 @@ cudaError_t dalloc(T*& ptr, size_t count)
 
 }  // namespace
 
+int assign_cells(const Engine& e, StructInfo* si, int n)
+{
+  const double rc = e.model.rc_radial_max;
+  int used = 0;
+  for (int k = 0; k < n; ++k) {
+    StructInfo& s = si[k];
+    s.nc[0] = s.nc[1] = s.nc[2] = 0;
+    s.cell_base = 0;
+    if (s.small) continue;
+    int nc[3], cells = 1;
+    for (int d = 0; d < 3; ++d) {
+      const double* r = s.box.hinv + 3 * d;
+      const double thick = 1.0 / std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+      nc[d] = s.box.pbc[d] ? std::max(1, static_cast<int>(thick / rc)) : 1;
+      cells *= nc[d];
+    }
+    if (cells < 27 || used + cells > e.xr.cell_cap) continue;   // scan all atoms instead
+    for (int d = 0; d < 3; ++d) s.nc[d] = nc[d];
+    s.cell_base = used;
+    used += cells;
+  }
+  return used;
+}
+
 int box_kind(const Engine& e, const Box& b)
 {
   StructInfo s;
@@ -236,8 +393,13 @@ std::string engine_enable_xr(Engine& e, int max_struct)
   if (N > static_cast<size_t>(kRowIndexMask))
     return "explicit neighbour rows address at most 2^28 atoms";
   if (!x.er) {
+    x.cell_cap = static_cast<int>(std::max<size_t>(N, 4096));
     bool ok = dalloc(x.er, N * e.nbr.mn_r) == cudaSuccess;
     ok &= dalloc(x.ea, N * e.nbr.mn_a) == cudaSuccess;
+    ok &= dalloc(x.cell_count, x.cell_cap) == cudaSuccess;
+    ok &= dalloc(x.cell_start, x.cell_cap) == cudaSuccess;
+    ok &= dalloc(x.cell_atoms, N) == cudaSuccess;
+    ok &= dalloc(x.cell_of, N) == cudaSuccess;
     if (!ok) return "cudaMalloc failed (explicit neighbour rows)";
   }
   if (x.max_struct < max_struct) {
@@ -265,11 +427,23 @@ void launch_explicit_rows(Engine& e, int N, const double* pos, const int* type,
                                            e.d_nstate);
     x.n_struct = 1;
   }
+  if (!x.from_box && x.n_cells > 0) {
+    cudaMemsetAsync(x.cell_count, 0, sizeof(int) * x.n_cells, stream);
+    k_xcell_assign<<<(N + threads - 1) / threads, threads, 0, stream>>>(
+      N, x.d_si, x.d_soff, x.n_struct, pos, x.cell_count, x.cell_of);
+    k_xcell_scan<<<1, 1024, 0, stream>>>(x.n_cells, x.cell_count, x.cell_start);
+    k_xcell_fill<<<(N + threads - 1) / threads, threads, 0, stream>>>(
+      N, x.cell_of, x.cell_count, x.cell_start, x.cell_atoms);
+  }
+  int p2r = 1;
+  while (p2r < e.nbr.mn_r) p2r <<= 1;
   const int warps = threads / 32;
   const int blocks = std::min((N + warps - 1) / warps, 148 * 8);
-  k_rows_explicit<<<blocks, threads, 0, stream>>>(e.params, N, x.d_si, x.d_soff, x.n_struct, pos,
-                                                  type, e.nbr.nn_r, x.er, e.nbr.mn_r, e.nbr.nn_a,
-                                                  x.ea, e.nbr.mn_a, e.d_nstate);
+  const size_t smem = sizeof(int) * warps * (p2r + 1);
+  k_rows_explicit<<<blocks, threads, smem, stream>>>(
+    e.params, N, x.d_si, x.d_soff, x.n_struct, pos, type, e.nbr.nn_r, x.er, e.nbr.mn_r,
+    e.nbr.nn_a, x.ea, e.nbr.mn_a, x.cell_count, x.cell_start, x.cell_atoms, x.cell_of, p2r,
+    e.d_nstate);
 }
 
 void launch_explicit_row_indices(const Engine& e, int which, int n, int* nn, int* nl, int mn,

@@ -404,6 +404,7 @@ void nepx_server::run()
     }
     h_soff[S] = Tn;
     c_fout[nfin] = t_out;
+    e.xr.n_cells = assign_cells(e, h_si, S);
     // ---- uploads and the arena rebuild ------------------------------------------
     Arena& A = arena[cur];
     Arena& B = arena[1 - cur];
@@ -555,6 +556,7 @@ int nepx_compute_batch(nepx_t* h, const nepx_struct_desc* descs, int nstruct, co
   // a copy of the flags of an earlier call may still be landing in h_state
   if (h->state_pending) cudaEventSynchronize(h->state_ready);
   h->state_pending = false;
+  e.xr.n_cells = nepx::assign_cells(e, si.data(), nstruct);
   // pageable sources: the copies complete before the calls return
   cudaMemcpyAsync(e.xr.d_si, si.data(), sizeof(nepx::StructInfo) * nstruct,
                   cudaMemcpyHostToDevice, s);

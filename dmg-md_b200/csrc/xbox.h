@@ -59,6 +59,8 @@ __host__ __device__ inline int expanded_box(const Box& b, double rc, StructInfo&
                            vol / xbox_area(va, vb)};
   si.box = b;
   si.small = 0;
+  si.nc[0] = si.nc[1] = si.nc[2] = 0;
+  si.cell_base = 0;
   for (int d = 0; d < 3; ++d) {
     si.ncell[d] = b.pbc[d] ? static_cast<int>(ceil(2.0 * rc / thick[d])) : 1;
     if (b.pbc[d] && thick[d] <= 2.5 * (rc + 1.0)) si.small = 1;
