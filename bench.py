@@ -86,6 +86,10 @@ WORKLOADS = {
         desc="cu_fcc_63x63x63_1pct_vacancies_nepzbl_rc5.0-4.0_H40_npt_ber_dt1fs"),
 }
 
+WORKLOADS["carbon8m"] = dict(
+    WORKLOADS["carbon"], steps=200,
+    desc="diamond_100x100x100_8000000atoms_10pct_displaced_nep4_C_rc4.2-3.7_H30_nve_dt1fs")
+
 MASSES = {"O": 15.999, "H": 1.008, "C": 12.011, "Cu": 63.546}
 
 # serving stream: one shared synthetic four-type NEP5 (C, H, O, Cu)
@@ -209,6 +213,14 @@ def build_system(name, seed):
         t, h, p = workloads.water(n_mol=8000, seed=seed)
     elif name == "carbon":
         t, h, p = workloads.diamond(a=3.567, ncell=8, jitter=0.05, seed=seed)
+    elif name == "carbon8m":
+        # 8,000,000 atoms (100^3 cubic cells of 8); a random 10% of the atoms
+        # displaced by N(0, 0.3 A) (amorphous regions)
+        t, h, p = workloads.diamond(a=3.567, ncell=100, jitter=0.05, seed=seed)
+        rng = np.random.default_rng(seed + 100)
+        pick = rng.random(len(t)) < 0.10
+        L = h[0]
+        p[:, pick] = (p[:, pick] + rng.normal(0.0, 0.3, (3, int(pick.sum())))) % L
     else:
         t, h, p = workloads.fcc(a=3.615, ncell=63, vacancy=0.01, seed=seed)
     return t, h, p
