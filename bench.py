@@ -60,8 +60,9 @@ import workloads  # noqa: E402
 
 K_B = 8.617343e-5
 # DRAM bytes per force call of the descriptor stage from the committed ncu
-# captures (profiles/k_nep_fused_water24k.md): k_nep_fused + k_angular_f12
-TRAFFIC = {"water": 20.80e6 + 17.96e6}
+# captures (profiles/descriptor_kernels_water24k.md): k_filter_radial +
+# k_nep_fused + k_angular_f12
+TRAFFIC = {"water": 18.72e6 + 6.93e6 + 17.97e6}
 FP32_LANES = 148 * 128          # B200: SMs x FP32 lanes
 SM_MAX_MHZ = 1965.0
 
@@ -591,11 +592,12 @@ def main():
     desc_flops = fpa * n
     achieved = desc_flops / (prof["descriptor"] * 1e-3) / 1e12
     peak = FP32_LANES * 2 * SM_MAX_MHZ * 1e6 / 1e12
-    roofline = {"bound": "fp32", "kernel": "k_nep_fused + k_angular_f12 (descriptor stage)",
+    roofline = {"bound": "fp32",
+                "kernel": "k_filter_radial + k_nep_fused + k_angular_f12 (descriptor stage)",
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                 "traffic": TRAFFIC.get(args.workload),
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of both "
-                                  "kernels, one launch each (profiles/)",
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the "
+                                  "three kernels, one launch each (profiles/)",
                 "peak_source": "B200 FP32 FMA peak: 148 SMs x 128 lanes x 2 FLOP x 1965 MHz "
                                "(not in MEASURED_PEAKS.json, which holds HBM and bf16 only)",
                 "flops_per_atom": fpa, "mean_radial_neighbors": mean_r,
