@@ -13,6 +13,7 @@ constexpr int kMaxTypes = 16;
 constexpr int kMaxBasis = 17;   // basis_size + 1
 constexpr int kMaxN = 13;       // n_max + 1
 constexpr int kNumLM = 24;      // (L_max + 1)^2 - 1 at L_max = 4
+constexpr int kNumLMHigh = 80;  // (L_max + 1)^2 - 1 at L_max = 8, the largest the format has
 constexpr int kMaxDim = 128;
 constexpr int kMaxInv = 6;      // q_222, q_1111, q_112, q_123, q_233, q_134
 constexpr double kBoltzmann = 8.617343e-5;           // eV/K, GPUMD natural units
@@ -207,9 +208,10 @@ __device__ __forceinline__ void radial_basis_d(int kmax, float rcinv, float d, f
 }
 
 // Real solid harmonics of degree L = 1..4 at the unit vector (x, y, z):
-// Y = P_L^m(z) * Re/Im (x + i y)^m with the z-polynomials below, in the
-// component order of the reference's blm moments (L^2 - 1 + {0, 2m-1, 2m}).
-// ZP[L][m] holds the coefficients of z^0..z^4.
+// Y = Z_Lm(z) * Re/Im (x + i y)^m with the z-polynomials below, in the
+// component order of the reference's blm moments (L^2 - 1 + {0, 2m-1, 2m});
+// zp[k] = z^k.  Degrees 5..8 read their coefficients from a table
+// (harmonic_tables.h).
 __device__ __forceinline__ float zpoly(int L, int m, const float* zp, float* dzf)
 {
   // coefficients of the reference's Z_COEFFICIENT_L tables (nep_utilities.cuh:89-117)
@@ -233,35 +235,6 @@ __device__ __forceinline__ float zpoly(int L, int m, const float* zp, float* dzf
   }
   *dzf = df;
   return f;
-}
-
-// Harmonics Y[0..nlm) at unit vector u.
-__device__ __forceinline__ void harmonics(int L_max, float ux, float uy, float uz, float* Y)
-{
-  float zp[5];
-  zp[0] = 1.0f;
-#pragma unroll
-  for (int k = 1; k < 5; ++k) zp[k] = zp[k - 1] * uz;
-  int idx = 0;
-#pragma unroll
-  for (int L = 1; L <= 4; ++L) {
-    if (L > L_max) break;
-    float re = ux, im = uy;
-#pragma unroll
-    for (int m = 0; m <= L; ++m) {
-      float dzf;
-      const float zf = zpoly(L, m, zp, &dzf);
-      if (m == 0) {
-        Y[idx++] = zf;
-      } else {
-        Y[idx++] = zf * re;
-        Y[idx++] = zf * im;
-        const float r2 = ux * re - uy * im;
-        im = ux * im + uy * re;
-        re = r2;
-      }
-    }
-  }
 }
 
 }  // namespace nepx

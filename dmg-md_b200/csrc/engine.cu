@@ -82,7 +82,7 @@ std::string engine_create(Engine& e, const std::string& nep_path, int max_atoms)
   p.kR = m.basis_radial + 1;
   p.kA = m.basis_angular + 1;
   p.L_max = m.L_max;
-  p.nlm = (m.L_max + 1) * (m.L_max + 1) - 1;
+  p.nlm = m.L_max > 4 ? kNumLMHigh : kNumLM;   // moment stride per n
   p.num_L = m.num_L;
   p.dim = m.dim;
   p.dimK = (m.dim + 7) & ~7;
@@ -174,7 +174,7 @@ std::string engine_create(Engine& e, const std::string& nep_path, int max_atoms)
   ok &= dalloc(e.scratch.alpha, static_cast<size_t>(N) * p.T * basis_stride(p)) == cudaSuccess;
   ok &= dalloc(e.scratch.f12, static_cast<size_t>(N) * nb.mn_a) == cudaSuccess;
   ok &= dalloc(e.scratch.pe_ann, N) == cudaSuccess;
-  ok &= dalloc(e.scratch.acoef, static_cast<size_t>(N) * p.nA * kNumLM) == cudaSuccess;
+  ok &= dalloc(e.scratch.acoef, static_cast<size_t>(N) * p.nA * p.nlm) == cudaSuccess;
   ok &= dalloc(e.scratch.tune_out, 13 * static_cast<size_t>(N)) == cudaSuccess;
   ok &= dalloc(e.d_box, 1) == cudaSuccess;
   ok &= dalloc(e.d_nstate, 1) == cudaSuccess;
@@ -184,7 +184,7 @@ std::string engine_create(Engine& e, const std::string& nep_path, int max_atoms)
   if (cudaMemcpy(e.d_nstate, &init, sizeof(init), cudaMemcpyHostToDevice) != cudaSuccess)
     return "cudaMemcpy failed (neighbour state)";
   if (cudaMemset(nb.nn_a, 0, sizeof(int) * N) != cudaSuccess) return "cudaMemset failed";
-  if (fused_smem_bytes(p, 4) > 227 * 1024)
+  if (fused_smem_bytes(p) > 227 * 1024)
     return "descriptor kernel needs more shared memory than a CTA has (not supported)";
   set_fused_smem_limits(p);
   if (cudaGetLastError() != cudaSuccess) return "CUDA error during setup";

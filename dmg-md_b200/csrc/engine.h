@@ -94,7 +94,7 @@ struct Engine {
 // Padded basis width of the kernel instance serving this model (row stride
 // of the shared-memory coefficient tables and of ForceScratch::alpha).
 int basis_stride(const ModelParams& p);
-size_t fused_smem_bytes(const ModelParams& p, int group);
+size_t fused_smem_bytes(const ModelParams& p);
 void set_fused_smem_limits(const ModelParams& p);
 
 // Times each kernel variant on the given system (a few calls each, stream

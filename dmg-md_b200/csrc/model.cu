@@ -144,7 +144,7 @@ std::string load_nep(const std::string& path, NepModel& m)
   if (!next_tokens(in, tok) || tok.size() < 4 || tok.size() > 8)
     return "l_max line should be l_max L has_q_222 has_q_1111 [has_q_112 ...]";
   if (!to_int(tok[1], m.L_max) || m.L_max < 0) return "bad l_max";
-  if (m.L_max > 4) return "l_max above 4 is not supported by this engine";
+  if (m.L_max > 8) return "l_max above 8 is not supported (the harmonics stop at degree 8)";
   m.num_L = m.L_max;
   for (int k = 0; k < kMaxInv; ++k) {
     int f = 0;

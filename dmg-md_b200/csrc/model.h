@@ -38,7 +38,8 @@ std::string load_nep(const std::string& path, NepModel& m);
 
 // Kernel-side view (passed by value; pointers are device pointers).
 struct ModelParams {
-  int version, T, nR, nA, kR, kA, L_max, nlm, num_L, dim, H;
+  int version, T, nR, nA, kR, kA, L_max, num_L, dim, H;
+  int nlm;            // moment components stored per n: 24 (l_max <= 4) or 80 (l_max 5..8)
   int dimK;           // dim rounded up to 8: row stride of the descriptor and dE/dq buffers
   int num_inv, inv_id[kMaxInv];
   float rc_r[kMaxTypes], rc_a[kMaxTypes];

@@ -35,6 +35,7 @@
 #include <cstdio>
 
 #include "engine.h"
+#include "harmonic_tables.h"
 
 namespace nepx {
 
@@ -44,14 +45,62 @@ constexpr int kBlock = 128;      // threads per CTA
 constexpr int kChunkN = 5;       // radial functions per angular-moment sweep
 constexpr unsigned kFull = 0xffffffffu;
 
-// three-body invariant weights (reference nep_utilities.cuh:52-75, L <= 4)
-__constant__ float c_C3B[kNumLM] = {
-  0.238732414637843f, 0.119366207318922f, 0.119366207318922f, 0.099471839432435f,
-  0.596831036594608f, 0.596831036594608f, 0.149207759148652f, 0.149207759148652f,
-  0.139260575205408f, 0.104445431404056f, 0.104445431404056f, 1.044454314040563f,
-  1.044454314040563f, 0.174075719006761f, 0.174075719006761f, 0.011190581936149f,
-  0.223811638722978f, 0.223811638722978f, 0.111905819361489f, 0.111905819361489f,
-  1.566681471060845f, 1.566681471060845f, 0.195835183882606f, 0.195835183882606f};
+// Weights of the three-body invariants q_L and coefficients of the
+// z-polynomials of the harmonics, degrees 1..8 (harmonic_tables.h; the
+// reference's C3B and Z_COEFFICIENT_L tables, nep_utilities.cuh:51-187).
+__constant__ float c_C3B[kNumLMHigh];
+__constant__ float c_Zc[kHarmonicLMax + 1][kHarmonicLMax + 1][kHarmonicLMax + 1];
+
+template <int LMAX>
+__host__ __device__ constexpr int num_lm() { return (LMAX + 1) * (LMAX + 1) - 1; }
+
+// Z_Lm(z) and dZ_Lm/dz with zp[k] = z^k; degrees above 4 from c_Zc.
+__device__ __forceinline__ float zpoly_any(int L, int m, const float* zp, float* dzf)
+{
+  if (L <= 4) return zpoly(L, m, zp, dzf);
+  float f = 0.0f, df = 0.0f;
+#pragma unroll
+  for (int k = 0; k <= kHarmonicLMax; ++k) {
+    if (k <= L - m && ((L - m - k) & 1) == 0) {
+      const float c = c_Zc[L][m][k];
+      f += c * zp[k];
+      if (k > 0) df += c * static_cast<float>(k) * zp[k - 1];
+    }
+  }
+  *dzf = df;
+  return f;
+}
+
+// Harmonics Y[0 .. (L_max + 1)^2 - 1) at the unit vector u, degrees up to
+// LMAX (the instance's bound) and L_max (the model's).
+template <int LMAX>
+__device__ __forceinline__ void harmonics(int L_max, float ux, float uy, float uz, float* Y)
+{
+  float zp[LMAX + 1];
+  zp[0] = 1.0f;
+#pragma unroll
+  for (int k = 1; k <= LMAX; ++k) zp[k] = zp[k - 1] * uz;
+  int idx = 0;
+#pragma unroll
+  for (int L = 1; L <= LMAX; ++L) {
+    if (L > L_max) break;
+    float re = ux, im = uy;
+#pragma unroll
+    for (int m = 0; m <= L; ++m) {
+      float dzf;
+      const float zf = zpoly_any(L, m, zp, &dzf);
+      if (m == 0) {
+        Y[idx++] = zf;
+      } else {
+        Y[idx++] = zf * re;
+        Y[idx++] = zf * im;
+        const float r2 = ux * re - uy * im;
+        im = ux * im + uy * re;
+        re = r2;
+      }
+    }
+  }
+}
 
 // Many-body invariants as monomials c * s[i0] s[i1] s[i2] (s[i3]) of the raw
 // moments, transcribed from the polynomials of find_q
@@ -95,8 +144,8 @@ __host__ __device__ inline FusedLayout fused_layout(const ModelParams& p, int at
   L.c_rad = 0;
   L.c_ang = L.c_rad + tt * p.nR * L.kpr;
   L.s = 0;
-  L.a = p.nA * kNumLM;
-  L.q = 2 * p.nA * kNumLM;
+  L.a = p.nA * p.nlm;
+  L.q = 2 * p.nA * p.nlm;
   L.fp = L.q + round4(p.dim);
   L.gh = L.fp + round4(p.dim);
   // per-center stride: 16-byte aligned (float4 reads of the a[n][lm] rows)
@@ -200,14 +249,14 @@ __device__ __forceinline__ void center_alpha(const ModelParams& p, int t1, const
 // Moment derivatives of one center, a[n][lm] = dE/ds[n][lm] (one lane owns
 // one n); the monomial terms read the moments at run-time indices, so both
 // live in shared memory.
-template <int G>
+template <int G, int NLM>
 __device__ __forceinline__ void center_acoef(const ModelParams& p, const float* s_s, float* s_a,
                                              const float* s_fp, int gl)
 {
   const int nR = p.nR, nA = p.nA;
   for (int n = gl; n < nA; n += G) {
-    const float* sv = s_s + n * kNumLM;
-    float* av = s_a + n * kNumLM;
+    const float* sv = s_s + n * NLM;
+    float* av = s_a + n * NLM;
     const float* fp = s_fp + nR;
     int col = 0;
     for (int Lq = 1; Lq <= p.L_max; ++Lq, ++col) {
@@ -216,7 +265,7 @@ __device__ __forceinline__ void center_acoef(const ModelParams& p, const float* 
       av[st0] = 2.0f * f * c_C3B[st0] * sv[st0];
       for (int k = 1; k < 2 * Lq + 1; ++k) av[st0 + k] = 4.0f * f * c_C3B[st0 + k] * sv[st0 + k];
     }
-    for (int lm = (p.L_max + 1) * (p.L_max + 1) - 1; lm < kNumLM; ++lm) av[lm] = 0.0f;
+    for (int lm = (p.L_max + 1) * (p.L_max + 1) - 1; lm < NLM; ++lm) av[lm] = 0.0f;
     for (int w = 0; w < p.num_inv; ++w, ++col) {
       const int id = p.inv_id[w];
       const float f = fp[col * nA + n];
@@ -353,7 +402,9 @@ k_filter_radial(const ModelParams p, int N, const Box* __restrict__ box,
 // XR: explicit rows (small-box and batched paths) -- the radial and angular
 // rows hold the displacement and packed neighbour of every edge (er, ea),
 // built beforehand; phase 1 then only accumulates the radial descriptors.
-template <int G, int NRM, int KM, int NAM, bool XR>
+// LMAX: 4 (moments of 24 components per n, five n per sweep) or 8 (80
+// components, one n per sweep).
+template <int G, int NRM, int KM, int NAM, bool XR, int LMAX>
 __global__ void __launch_bounds__(kBlock, (KM <= 9 ? 3 : 2))
 k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
             const Site* __restrict__ sites, NeighborState* st,
@@ -367,6 +418,8 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
   constexpr int APW = 32 / G;             // centers per warp
   constexpr int APB = kBlock / G;         // centers per block
   constexpr int KP = (KM + 3) & ~3;
+  constexpr int NLM = num_lm<LMAX>();
+  constexpr int CN = LMAX <= 4 ? kChunkN : 1;   // radial functions per moment sweep
   extern __shared__ float sm[];
   const FusedLayout Lay = fused_layout(p, APB, KP);
   const int tid = threadIdx.x;
@@ -463,10 +516,10 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
   const int na_max = __reduce_max_sync(kFull, na);
   const int* arow = nl_a + static_cast<size_t>(i) * mn_a;
   const float4* earow = ea + static_cast<size_t>(i) * mn_a;
-  for (int nc = 0; nc < nA; nc += kChunkN) {
-    float v[kChunkN * kNumLM];
+  for (int nc = 0; nc < nA; nc += CN) {
+    float v[CN * NLM];
 #pragma unroll
-    for (int q = 0; q < kChunkN * kNumLM; ++q) v[q] = 0.0f;
+    for (int q = 0; q < CN * NLM; ++q) v[q] = 0.0f;
     for (int base = 0; base < na_max; base += G) {
       const int k = base + gl;
       if (k < na) {
@@ -491,33 +544,33 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
         for (int kk = 0; kk < KP; ++kk) fn[kk] = 0.0f;
         radial_basis<KM>(kA, rcinv, d, fc, fn);
         const float* c = sm + Lay.c_ang + ((t1 * T + t2) * nA + nc) * Lay.kpa;
-        float g[kChunkN];
+        float g[CN];
 #pragma unroll
-        for (int n = 0; n < kChunkN; ++n)
+        for (int n = 0; n < CN; ++n)
           g[n] = (nc + n < nA) ? dot_basis<KM>(c + n * Lay.kpa, fn) : 0.0f;
         const float dinv = 1.0f / d;
-        float Y[kNumLM];
+        float Y[NLM];
 #pragma unroll
-        for (int lm = 0; lm < kNumLM; ++lm) Y[lm] = 0.0f;
-        harmonics(p.L_max, dx * dinv, dy * dinv, dz * dinv, Y);
+        for (int lm = 0; lm < NLM; ++lm) Y[lm] = 0.0f;
+        harmonics<LMAX>(p.L_max, dx * dinv, dy * dinv, dz * dinv, Y);
 #pragma unroll
-        for (int n = 0; n < kChunkN; ++n)
+        for (int n = 0; n < CN; ++n)
 #pragma unroll
-          for (int lm = 0; lm < kNumLM; ++lm) v[n * kNumLM + lm] += g[n] * Y[lm];
+          for (int lm = 0; lm < NLM; ++lm) v[n * NLM + lm] += g[n] * Y[lm];
       }
     }
-    const int at = reduce_scatter<G, kChunkN * kNumLM>(v, gl);
-    constexpr int share = kChunkN * kNumLM / G;
-    const int lim = (nA - nc < kChunkN ? nA - nc : kChunkN) * kNumLM;
+    const int at = reduce_scatter<G, CN * NLM>(v, gl);
+    constexpr int share = CN * NLM / G;
+    const int lim = (nA - nc < CN ? nA - nc : CN) * NLM;
 #pragma unroll
     for (int q = 0; q < share; ++q)
-      if (at + q < lim) s_s[nc * kNumLM + at + q] = v[q];
+      if (at + q < lim) s_s[nc * NLM + at + q] = v[q];
   }
   __syncwarp();
 
   // ---- 3. invariants, ANN, derivatives ---------------------------------------
   for (int n = gl; n < nA; n += G) {
-    const float* s = s_s + n * kNumLM;
+    const float* s = s_s + n * NLM;
     float* q = s_q + nR;
     int col = 0;
     for (int Lq = 1; Lq <= p.L_max; ++Lq, ++col) {
@@ -553,9 +606,9 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
     if (active) {
       float* qrow = qout + static_cast<size_t>(i) * p.dimK;
       for (int d = gl; d < p.dimK; d += G) qrow[d] = d < dim ? s_q[d] : 0.0f;
-      float4* dst = reinterpret_cast<float4*>(acoef + static_cast<size_t>(i) * nA * kNumLM);
+      float4* dst = reinterpret_cast<float4*>(acoef + static_cast<size_t>(i) * nA * NLM);
       const float4* src = reinterpret_cast<const float4*>(s_s);
-      for (int q = gl; q < nA * kNumLM / 4; q += G) dst[q] = src[q];
+      for (int q = gl; q < nA * NLM / 4; q += G) dst[q] = src[q];
     }
     return;
   }
@@ -624,21 +677,21 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
   __syncwarp();
   if (active) center_alpha<G>(p, t1, s_fp, sm + Lay.c_rad, Lay.kpr, gl,
                               alpha + static_cast<size_t>(i) * T * Lay.kpr);
-  center_acoef<G>(p, s_s, s_a, s_fp, gl);
+  center_acoef<G, NLM>(p, s_s, s_a, s_fp, gl);
   __syncwarp();
 
   // ---- 4. hand a[n][lm] to the angular-force kernel -------------------------
   if (active) {
-    float4* dst = reinterpret_cast<float4*>(acoef + static_cast<size_t>(i) * nA * kNumLM);
+    float4* dst = reinterpret_cast<float4*>(acoef + static_cast<size_t>(i) * nA * NLM);
     const float4* src = reinterpret_cast<const float4*>(s_a);
-    for (int q = gl; q < nA * kNumLM / 4; q += G) dst[q] = src[q];
+    for (int q = gl; q < nA * NLM / 4; q += G) dst[q] = src[q];
   }
 }
 
 // Mixed-precision path: moment derivatives and radial force coefficients of
 // every center from its moments (left in acoef by k_nep_fused) and dE/dq of
 // the tensor-core ANN (fp, ann_tc.cu) -- the tail of k_nep_fused.
-template <int G, int KP>
+template <int G, int KP, int LMAX>
 __global__ void __launch_bounds__(kBlock)
 k_acoef(const ModelParams p, int N, const Site* __restrict__ sites, const float* __restrict__ fp,
         float* __restrict__ acoef, float* __restrict__ alpha)
@@ -652,27 +705,28 @@ k_acoef(const ModelParams p, int N, const Site* __restrict__ sites, const float*
   }
   __syncthreads();
   constexpr int APB = kBlock / G;
-  const int per = round4(2 * nA * kNumLM + p.dimK);
+  constexpr int NLM = num_lm<LMAX>();
+  const int per = round4(2 * nA * NLM + p.dimK);
   const int gl = threadIdx.x % G, slot = threadIdx.x / G;
   const int i = blockIdx.x * APB + slot;
   const bool active = i < N;
   float* s_s = sm + tab + slot * per;
-  float* s_a = s_s + nA * kNumLM;
-  float* s_fp = s_a + nA * kNumLM;
-  float4* arow = reinterpret_cast<float4*>(acoef + static_cast<size_t>(i) * nA * kNumLM);
+  float* s_a = s_s + nA * NLM;
+  float* s_fp = s_a + nA * NLM;
+  float4* arow = reinterpret_cast<float4*>(acoef + static_cast<size_t>(i) * nA * NLM);
   if (active) {
-    for (int q = gl; q < nA * kNumLM / 4; q += G) reinterpret_cast<float4*>(s_s)[q] = arow[q];
+    for (int q = gl; q < nA * NLM / 4; q += G) reinterpret_cast<float4*>(s_s)[q] = arow[q];
     for (int d = gl; d < p.dimK; d += G) s_fp[d] = fp[static_cast<size_t>(i) * p.dimK + d];
   }
   __syncwarp();
   if (active) {
     const int t1 = static_cast<int>(sites[i].type);
     center_alpha<G>(p, t1, s_fp, sm, KP, gl, alpha + static_cast<size_t>(i) * T * KP);
-    center_acoef<G>(p, s_s, s_a, s_fp, gl);
+    center_acoef<G, NLM>(p, s_s, s_a, s_fp, gl);
   }
   __syncwarp();
   if (active)
-    for (int q = gl; q < nA * kNumLM / 4; q += G) arow[q] = reinterpret_cast<const float4*>(s_a)[q];
+    for (int q = gl; q < nA * NLM / 4; q += G) arow[q] = reinterpret_cast<const float4*>(s_a)[q];
 }
 
 // Directed angular partial force of a center on one neighbour at
@@ -684,12 +738,13 @@ k_acoef(const ModelParams p, int N, const Site* __restrict__ sites, const float*
 // Reference find_partial_force_angular (nep.cu:890-991) with the
 // accumulate_f12 ladder (nep_utilities.cuh:1240-1491) evaluated once per edge
 // instead of once per (edge, n).
-template <int KM, int NAM>
+template <int KM, int NAM, int LMAX>
 __device__ __forceinline__ float3 angular_edge_force(const ModelParams& p, const float* c,
                                                     const float* __restrict__ av, float rc,
                                                     float dx, float dy, float dz)
 {
   constexpr int KP = (KM + 3) & ~3;
+  constexpr int NLM = num_lm<LMAX>();
   const int nA = p.nA;
   const float d = sqrtf(dx * dx + dy * dy + dz * dz);
   const float dinv = 1.0f / d;
@@ -704,9 +759,9 @@ __device__ __forceinline__ float3 angular_edge_force(const ModelParams& p, const
     fnp[kk] = 0.0f;
   }
   radial_basis_d<KM>(p.kA, rcinv, d, fc, fcp, fn, fnp);
-  float A[kNumLM], B[kNumLM];
+  float A[NLM], B[NLM];
 #pragma unroll
-  for (int lm = 0; lm < kNumLM; ++lm) {
+  for (int lm = 0; lm < NLM; ++lm) {
     A[lm] = 0.0f;
     B[lm] = 0.0f;
   }
@@ -715,9 +770,9 @@ __device__ __forceinline__ float3 angular_edge_force(const ModelParams& p, const
     if (n < nA) {
       const float g = dot_basis<KM>(c + n * KP, fn);
       const float gp = dot_basis<KM>(c + n * KP, fnp);
-      const float* an = av + n * kNumLM;
+      const float* an = av + n * NLM;
 #pragma unroll
-      for (int q = 0; q < kNumLM / 4; ++q) {
+      for (int q = 0; q < NLM / 4; ++q) {
         const float4 a4 = __ldg(reinterpret_cast<const float4*>(an) + q);
         A[4 * q] += a4.x * g;
         A[4 * q + 1] += a4.y * g;
@@ -731,20 +786,20 @@ __device__ __forceinline__ float3 angular_edge_force(const ModelParams& p, const
     }
   }
   // SB = sum B Y, V = sum A dY/du (u components independent)
-  float zp[5];
+  float zp[LMAX + 1];
   zp[0] = 1.0f;
 #pragma unroll
-  for (int q = 1; q < 5; ++q) zp[q] = zp[q - 1] * uz;
+  for (int q = 1; q <= LMAX; ++q) zp[q] = zp[q - 1] * uz;
   float SB = 0.0f, vx = 0.0f, vy = 0.0f, vz = 0.0f;
   int idx = 0;
 #pragma unroll
-  for (int Lq = 1; Lq <= 4; ++Lq) {
+  for (int Lq = 1; Lq <= LMAX; ++Lq) {
     if (Lq > p.L_max) break;
     float re0 = 1.0f, im0 = 0.0f;   // (ux + i uy)^(m-1)
 #pragma unroll
     for (int m = 0; m <= Lq; ++m) {
       float dzf;
-      const float zf = zpoly(Lq, m, zp, &dzf);
+      const float zf = zpoly_any(Lq, m, zp, &dzf);
       if (m == 0) {
         SB += B[idx] * zf;
         vz += A[idx] * dzf;
@@ -782,7 +837,7 @@ __device__ __forceinline__ void load_angular_tables(const ModelParams& p, float*
 
 // One group of G lanes per center: the directed angular partial force of
 // every edge of the center's angular row, f12[i][k] (float4, w unused).
-template <int G, int KM, int NAM>
+template <int G, int KM, int NAM, int LMAX>
 __global__ void __launch_bounds__(kBlock)
 k_angular_f12(const ModelParams p, int N, const Box* __restrict__ box,
               const Site* __restrict__ sites,
@@ -805,14 +860,14 @@ k_angular_f12(const ModelParams p, int N, const Box* __restrict__ box,
   const float ra1 = p.rc_a[t1];
   const int na = nn_a[i];
   const int* arow = nl_a + static_cast<size_t>(i) * mn_a;
-  const float* ai = acoef + static_cast<size_t>(i) * nA * kNumLM;
+  const float* ai = acoef + static_cast<size_t>(i) * nA * num_lm<LMAX>();
   for (int k = gl; k < na; k += G) {
     int t2;
     float dx, dy, dz;
     site_displacement(b, sites, xi, yi, zi, arow[k], dx, dy, dz, t2);
     const float rc = (ra1 + p.rc_a[t2]) * 0.5f;
-    const float3 f = angular_edge_force<KM, NAM>(p, sm + (t1 * T + t2) * nA * KP, ai, rc, dx,
-                                                 dy, dz);
+    const float3 f = angular_edge_force<KM, NAM, LMAX>(p, sm + (t1 * T + t2) * nA * KP, ai, rc,
+                                                       dx, dy, dz);
     f12[static_cast<size_t>(i) * mn_a + k] = make_float4(f.x, f.y, f.z, 0.0f);
   }
 }
@@ -825,7 +880,7 @@ k_angular_f12(const ModelParams p, int N, const Box* __restrict__ box,
 // (periodic images), so the reverse partial force f12(j,i) is not looked up
 // but evaluated here from j's moment derivatives at -r: the angular force
 // work doubles and the f12 buffer and its kernel drop out.
-template <int G, int KM, int NAM, bool XR>
+template <int G, int KM, int NAM, bool XR, int LMAX>
 __global__ void __launch_bounds__(256)
 k_gather(const ModelParams p, int N, const Box* __restrict__ box,
          const Site* __restrict__ sites, const int* __restrict__ nn_r, const int* __restrict__ nl_r,
@@ -924,11 +979,12 @@ k_gather(const ModelParams p, int N, const Box* __restrict__ box,
         dz = e.z;
         const float rc = (p.rc_a[t1] + p.rc_a[t2]) * 0.5f;
         const int nA = p.nA;
-        const float3 fij = angular_edge_force<KM, NAM>(
-          p, sm + (t1 * T + t2) * nA * KP, acoef + static_cast<size_t>(i) * nA * kNumLM, rc, dx,
+        constexpr int NLM = num_lm<LMAX>();
+        const float3 fij = angular_edge_force<KM, NAM, LMAX>(
+          p, sm + (t1 * T + t2) * nA * KP, acoef + static_cast<size_t>(i) * nA * NLM, rc, dx,
           dy, dz);
-        const float3 fji = angular_edge_force<KM, NAM>(
-          p, sm + (t2 * T + t1) * nA * KP, acoef + static_cast<size_t>(j) * nA * kNumLM, rc, -dx,
+        const float3 fji = angular_edge_force<KM, NAM, LMAX>(
+          p, sm + (t2 * T + t1) * nA * KP, acoef + static_cast<size_t>(j) * nA * NLM, rc, -dx,
           -dy, -dz);
         a12 = make_float4(fij.x, fij.y, fij.z, 0.0f);
         a21 = make_float4(fji.x, fji.y, fji.z, 0.0f);
@@ -1026,20 +1082,29 @@ k_gather(const ModelParams p, int N, const Box* __restrict__ box,
 
 // shape classes: small (n_max <= 4, basis_size <= 8) and general
 constexpr int kSmallN = 5, kSmallK = 9;
+// Models with l_max 5..8 run one general-shape instance of each kernel (LMAX
+// 8): their moments take 80 floats per n, so the descriptor and a-coefficient
+// kernels take 16 centers per CTA (groups of 8 lanes), the force kernels 4.
+constexpr int kHighFusedGroup = 8, kHighGroup = 4;
 
+bool high_degree(const ModelParams& p) { return p.L_max > 4; }
+
+// every kernel of a model uses one basis stride, so high-degree models take
+// the general shape throughout
 bool small_shape(const ModelParams& p)
 {
-  return p.nR <= kSmallN && p.nA <= kSmallN && p.kR <= kSmallK && p.kA <= kSmallK;
+  return !high_degree(p) && p.nR <= kSmallN && p.nA <= kSmallN && p.kR <= kSmallK &&
+         p.kA <= kSmallK;
 }
 
-template <int G, int NRM, int KM, int NAM, bool XR>
+template <int G, int NRM, int KM, int NAM, bool XR, int LMAX>
 void launch_fused_t(Engine& e, int N, cudaStream_t s)
 {
   NeighborBuffers& nb = e.nbr;
   constexpr int APB = kBlock / G;
   const int blocks = (N + APB - 1) / APB;
   const size_t smem = fused_layout(e.params, APB, (KM + 3) & ~3).total_bytes;
-  k_nep_fused<G, NRM, KM, NAM, XR><<<blocks, kBlock, smem, s>>>(
+  k_nep_fused<G, NRM, KM, NAM, XR, LMAX><<<blocks, kBlock, smem, s>>>(
     e.params, N, e.d_box, e.scratch.sites, e.d_nstate, nb.nn_v, nb.nl_v, nb.mn_v, nb.nn_r, nb.nl_r,
     nb.mn_r, nb.nn_a, nb.nl_a, nb.mn_a, e.xr.er, e.xr.ea, e.scratch.qrad, e.scratch.alpha,
     e.scratch.acoef, e.scratch.pe_ann, e.precision == 1 ? e.scratch.q : nullptr);
@@ -1056,24 +1121,24 @@ void launch_filter_t(Engine& e, int N, cudaStream_t s)
     nb.nl_r, nb.mn_r, nb.nn_a, nb.nl_a, nb.mn_a, e.scratch.qrad);
 }
 
-template <int KP>
+template <int G, int KP, int LMAX>
 size_t acoef_smem_bytes(const ModelParams& p)
 {
   return sizeof(float) * (round4(p.T * p.T * p.nR * KP) +
-                          (kBlock / 4) * round4(2 * p.nA * kNumLM + p.dimK));
+                          (kBlock / G) * round4(2 * p.nA * num_lm<LMAX>() + p.dimK));
 }
 
-template <int KP>
+template <int G, int KP, int LMAX>
 void launch_acoef_t(Engine& e, int N, cudaStream_t s)
 {
-  constexpr int G = 4, APB = kBlock / G;
+  constexpr int APB = kBlock / G;
   const ModelParams& p = e.params;
-  const size_t smem = acoef_smem_bytes<KP>(p);
-  k_acoef<G, KP><<<(N + APB - 1) / APB, kBlock, smem, s>>>(p, N, e.scratch.sites, e.scratch.fp,
-                                                           e.scratch.acoef, e.scratch.alpha);
+  const size_t smem = acoef_smem_bytes<G, KP, LMAX>(p);
+  k_acoef<G, KP, LMAX><<<(N + APB - 1) / APB, kBlock, smem, s>>>(
+    p, N, e.scratch.sites, e.scratch.fp, e.scratch.acoef, e.scratch.alpha);
 }
 
-template <int G, int KM, int NAM>
+template <int G, int KM, int NAM, int LMAX>
 void launch_f12_t(Engine& e, int N, cudaStream_t s)
 {
   NeighborBuffers& nb = e.nbr;
@@ -1081,21 +1146,21 @@ void launch_f12_t(Engine& e, int N, cudaStream_t s)
   const int blocks = (N + APB - 1) / APB;
   const size_t smem =
     sizeof(float) * e.params.T * e.params.T * e.params.nA * ((KM + 3) & ~3);
-  k_angular_f12<G, KM, NAM><<<blocks, kBlock, smem, s>>>(
+  k_angular_f12<G, KM, NAM, LMAX><<<blocks, kBlock, smem, s>>>(
     e.params, N, e.d_box, e.scratch.sites, nb.nn_a, nb.nl_a, nb.mn_a, e.scratch.acoef,
     e.scratch.f12);
 }
 
-template <int G, int NRM, int KM, int NAM>
+template <int G, int NRM, int KM, int NAM, int LMAX>
 void set_fused_smem_t(size_t bytes)
 {
-  cudaFuncSetAttribute(k_nep_fused<G, NRM, KM, NAM, false>,
+  cudaFuncSetAttribute(k_nep_fused<G, NRM, KM, NAM, false, LMAX>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
-  cudaFuncSetAttribute(k_nep_fused<G, NRM, KM, NAM, true>,
+  cudaFuncSetAttribute(k_nep_fused<G, NRM, KM, NAM, true, LMAX>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
 }
 
-template <int G, int KM, int NAM, bool XR>
+template <int G, int KM, int NAM, bool XR, int LMAX>
 void launch_gather_t(Engine& e, int N, double* pe, double* force, double* virial,
                      bool accumulate, cudaStream_t s)
 {
@@ -1104,53 +1169,63 @@ void launch_gather_t(Engine& e, int N, double* pe, double* force, double* virial
   const int blocks = static_cast<int>((static_cast<long long>(N) * G + threads - 1) / threads);
   const size_t smem =
     XR ? sizeof(float) * e.params.T * e.params.T * e.params.nA * ((KM + 3) & ~3) : 0;
-  k_gather<G, KM, NAM, XR><<<blocks, threads, smem, s>>>(
+  k_gather<G, KM, NAM, XR, LMAX><<<blocks, threads, smem, s>>>(
     e.params, N, e.d_box, e.scratch.sites, nb.nn_r, nb.nl_r, nb.mn_r, nb.nn_a, nb.nl_a, nb.mn_a,
     e.xr.er, e.xr.ea, e.scratch.acoef, e.scratch.alpha, e.scratch.f12, e.scratch.pe_ann, pe,
     force, virial, accumulate ? 1 : 0, e.d_nstate);
 }
 
-template <int G, int NRM, int KM, int NAM>
+template <int G, int NRM, int KM, int NAM, int LMAX>
 void launch_fused_g(Engine& e, int N, cudaStream_t s)
 {
-  if (e.use_xr) launch_fused_t<G, NRM, KM, NAM, true>(e, N, s);
-  else launch_fused_t<G, NRM, KM, NAM, false>(e, N, s);
+  if (e.use_xr) launch_fused_t<G, NRM, KM, NAM, true, LMAX>(e, N, s);
+  else launch_fused_t<G, NRM, KM, NAM, false, LMAX>(e, N, s);
 }
 
-template <int G, int KM, int NAM>
+template <int G, int KM, int NAM, int LMAX>
 void launch_gather_g(Engine& e, int N, double* pe, double* force, double* virial,
                      bool accumulate, cudaStream_t s)
 {
-  if (e.use_xr) launch_gather_t<G, KM, NAM, true>(e, N, pe, force, virial, accumulate, s);
-  else launch_gather_t<G, KM, NAM, false>(e, N, pe, force, virial, accumulate, s);
+  if (e.use_xr) launch_gather_t<G, KM, NAM, true, LMAX>(e, N, pe, force, virial, accumulate, s);
+  else launch_gather_t<G, KM, NAM, false, LMAX>(e, N, pe, force, virial, accumulate, s);
 }
 
 }  // namespace
 
 #include "invariants_upload.inc"
 
-// Largest dynamic shared memory any variant needs for this model.
 // Padded basis width (row stride of the coefficient tables and of alpha).
 int basis_stride(const ModelParams& p) { return small_shape(p) ? round4(kSmallK) : round4(kMaxBasis); }
 
-size_t fused_smem_bytes(const ModelParams& p, int group)
+// Largest dynamic shared memory a descriptor-kernel variant this model runs needs.
+size_t fused_smem_bytes(const ModelParams& p)
 {
-  return fused_layout(p, kBlock / group, basis_stride(p)).total_bytes;
+  if (high_degree(p)) return fused_layout(p, kBlock / kHighFusedGroup, basis_stride(p)).total_bytes;
+  return fused_layout(p, kBlock / 4, basis_stride(p)).total_bytes;
 }
 
 void set_fused_smem_limits(const ModelParams& p)
 {
-  cudaFuncSetAttribute(k_acoef<4, round4(kSmallK)>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       static_cast<int>(acoef_smem_bytes<round4(kSmallK)>(p)));
-  cudaFuncSetAttribute(k_acoef<4, round4(kMaxBasis)>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       static_cast<int>(acoef_smem_bytes<round4(kMaxBasis)>(p)));
-  const size_t b4 = fused_smem_bytes(p, 4), b8 = fused_smem_bytes(p, 8);
+  constexpr int KS = round4(kSmallK), KG = round4(kMaxBasis);
+  if (high_degree(p)) {
+    cudaFuncSetAttribute(k_acoef<kHighFusedGroup, KG, 8>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(acoef_smem_bytes<kHighFusedGroup, KG, 8>(p)));
+    set_fused_smem_t<kHighFusedGroup, kMaxN, kMaxBasis, kMaxN, 8>(fused_smem_bytes(p));
+    return;
+  }
+  cudaFuncSetAttribute(k_acoef<4, KS, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(acoef_smem_bytes<4, KS, 4>(p)));
+  cudaFuncSetAttribute(k_acoef<4, KG, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(acoef_smem_bytes<4, KG, 4>(p)));
+  const size_t b4 = fused_layout(p, kBlock / 4, basis_stride(p)).total_bytes;
+  const size_t b8 = fused_layout(p, kBlock / 8, basis_stride(p)).total_bytes;
   if (small_shape(p)) {
-    set_fused_smem_t<4, kSmallN, kSmallK, kSmallN>(b4);
-    set_fused_smem_t<8, kSmallN, kSmallK, kSmallN>(b8);
+    set_fused_smem_t<4, kSmallN, kSmallK, kSmallN, 4>(b4);
+    set_fused_smem_t<8, kSmallN, kSmallK, kSmallN, 4>(b8);
   } else {
-    set_fused_smem_t<4, kMaxN, kMaxBasis, kMaxN>(b4);
-    set_fused_smem_t<8, kMaxN, kMaxBasis, kMaxN>(b8);
+    set_fused_smem_t<4, kMaxN, kMaxBasis, kMaxN, 4>(b4);
+    set_fused_smem_t<8, kMaxN, kMaxBasis, kMaxN, 4>(b8);
   }
 }
 
@@ -1169,32 +1244,36 @@ void launch_filter(Engine& e, int N, cudaStream_t s)
 void launch_descriptor(Engine& e, int N, const double*, const int*, cudaStream_t stream)
 {
   const bool small = small_shape(e.params);
+  const bool high = high_degree(e.params);
   // the type order is taken while the rebuild flag is still up (k_nep_fused clears it)
   if (e.precision == 1) {
     launch_type_order(e, N, e.use_xr || !e.order_valid, stream);
     e.order_valid = true;
   }
   if (!e.use_xr) launch_filter(e, N, stream);
-  if (e.group == 8) {
-    if (small) launch_fused_g<8, kSmallN, kSmallK, kSmallN>(e, N, stream);
-    else launch_fused_g<8, kMaxN, kMaxBasis, kMaxN>(e, N, stream);
+  if (high) launch_fused_g<kHighFusedGroup, kMaxN, kMaxBasis, kMaxN, 8>(e, N, stream);
+  else if (e.group == 8) {
+    if (small) launch_fused_g<8, kSmallN, kSmallK, kSmallN, 4>(e, N, stream);
+    else launch_fused_g<8, kMaxN, kMaxBasis, kMaxN, 4>(e, N, stream);
   } else {
-    if (small) launch_fused_g<4, kSmallN, kSmallK, kSmallN>(e, N, stream);
-    else launch_fused_g<4, kMaxN, kMaxBasis, kMaxN>(e, N, stream);
+    if (small) launch_fused_g<4, kSmallN, kSmallK, kSmallN, 4>(e, N, stream);
+    else launch_fused_g<4, kMaxN, kMaxBasis, kMaxN, 4>(e, N, stream);
   }
   if (e.precision == 1) {
     // mixed precision: the ANN on the tensor cores, then the fused kernel's tail
     launch_ann_tc(e, N, stream);
-    if (small) launch_acoef_t<round4(kSmallK)>(e, N, stream);
-    else launch_acoef_t<round4(kMaxBasis)>(e, N, stream);
+    if (high) launch_acoef_t<kHighFusedGroup, round4(kMaxBasis), 8>(e, N, stream);
+    else if (small) launch_acoef_t<4, round4(kSmallK), 4>(e, N, stream);
+    else launch_acoef_t<4, round4(kMaxBasis), 4>(e, N, stream);
   }
   if (e.use_xr) return;   // the explicit-row gather evaluates the angular forces itself
-  if (e.f12_group == 8) {
-    if (small) launch_f12_t<8, kSmallK, kSmallN>(e, N, stream);
-    else launch_f12_t<8, kMaxBasis, kMaxN>(e, N, stream);
+  if (high) launch_f12_t<kHighGroup, kMaxBasis, kMaxN, 8>(e, N, stream);
+  else if (e.f12_group == 8) {
+    if (small) launch_f12_t<8, kSmallK, kSmallN, 4>(e, N, stream);
+    else launch_f12_t<8, kMaxBasis, kMaxN, 4>(e, N, stream);
   } else {
-    if (small) launch_f12_t<4, kSmallK, kSmallN>(e, N, stream);
-    else launch_f12_t<4, kMaxBasis, kMaxN>(e, N, stream);
+    if (small) launch_f12_t<4, kSmallK, kSmallN, 4>(e, N, stream);
+    else launch_f12_t<4, kMaxBasis, kMaxN, 4>(e, N, stream);
   }
 }
 
@@ -1202,12 +1281,14 @@ void launch_gather(Engine& e, int N, const double*, const int*, double* pe, doub
                    double* virial, bool accumulate, cudaStream_t stream)
 {
   const bool small = small_shape(e.params);
-  if (e.gather_group == 4) {
-    if (small) launch_gather_g<4, kSmallK, kSmallN>(e, N, pe, force, virial, accumulate, stream);
-    else launch_gather_g<4, kMaxBasis, kMaxN>(e, N, pe, force, virial, accumulate, stream);
+  if (high_degree(e.params))
+    launch_gather_g<kHighGroup, kMaxBasis, kMaxN, 8>(e, N, pe, force, virial, accumulate, stream);
+  else if (e.gather_group == 4) {
+    if (small) launch_gather_g<4, kSmallK, kSmallN, 4>(e, N, pe, force, virial, accumulate, stream);
+    else launch_gather_g<4, kMaxBasis, kMaxN, 4>(e, N, pe, force, virial, accumulate, stream);
   } else {
-    if (small) launch_gather_g<8, kSmallK, kSmallN>(e, N, pe, force, virial, accumulate, stream);
-    else launch_gather_g<8, kMaxBasis, kMaxN>(e, N, pe, force, virial, accumulate, stream);
+    if (small) launch_gather_g<8, kSmallK, kSmallN, 4>(e, N, pe, force, virial, accumulate, stream);
+    else launch_gather_g<8, kMaxBasis, kMaxN, 4>(e, N, pe, force, virial, accumulate, stream);
   }
 }
 

@@ -94,7 +94,7 @@ size_t bytes_needed(const nepx::Engine& e, int n)
   c.take<float>(N * e.params.T * nepx::basis_stride(e.params));
   c.take<float4>(N * nb.mn_a);
   c.take<double>(N);
-  c.take<float>(N * e.params.nA * nepx::kNumLM);
+  c.take<float>(N * e.params.nA * e.params.nlm);
   return c.used;
 }
 
@@ -151,7 +151,7 @@ extern "C" int nepx_compute_noalloc(nepx_t* h, const nepx_box* box, int n, const
   view.scratch.alpha = c.take<float>(N * view.params.T * nepx::basis_stride(view.params));
   view.scratch.f12 = c.take<float4>(N * nb.mn_a);
   view.scratch.pe_ann = c.take<double>(N);
-  view.scratch.acoef = c.take<float>(N * view.params.nA * nepx::kNumLM);
+  view.scratch.acoef = c.take<float>(N * view.params.nA * view.params.nlm);
   view.capacity = n;
   view.tuned = true;   // keeps the handle's kernel variants; no timing runs here
   view.precision = 0;  // the mixed path's buffers are not part of the static scratch

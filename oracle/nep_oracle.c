@@ -25,8 +25,9 @@
 
 #define MAXT 16
 #define MAXN 17        /* basis_size + 1 */
-#define NUM_ABC 24     /* (L_max+1)^2 - 1 for L_max = 4 */
-#define MAX_DIM 160
+#define LMAXH 8        /* largest l_max of the format */
+#define NUM_ABC 80     /* (L_max+1)^2 - 1 for L_max = 8 */
+#define MAX_DIM 256
 #define MAX_INV 6
 #define K_C_SP 14.399645
 #define PI_D 3.14159265358979323846
@@ -56,24 +57,80 @@ static const double kCovalentRadius[94] = {
 /*
  * Real solid-harmonic building blocks.  For degree L and order m the
  * z-polynomial is sum_k kZ[L][m][k] z^k (z = cos theta); the full harmonic is
- * that polynomial times Re/Im (x + i y)^m.  Tables follow the coefficients of
- * nep_utilities.cuh:89-152 for L = 1..4.
+ * that polynomial times Re/Im (x + i y)^m.  kZ[L][m] is the primitive integer
+ * polynomial (content divided out, positive leading coefficient) of
+ * d^m P_L / dz^m, and kC3B the weight that makes
+ *   q_L = kC3B[L0] s_L0^2 + 2 sum_{m>0} kC3B[Lm] (s_Lm,re^2 + s_Lm,im^2)
+ * the rotation invariant sum_m |moment of the normalised Y_Lm|^2 (the
+ * reference's Z_COEFFICIENT_L and C3B tables, nep_utilities.cuh:51-187).
+ * Both come from Rodrigues' formula P_L = d^L/dz^L (z^2 - 1)^L / (2^L L!).
  */
-static const double kZ[5][5][5] = {
-  {{0}},
-  {{0, 1}, {1, 0}},
-  {{-1, 0, 3}, {0, 1, 0}, {1, 0, 0}},
-  {{0, -3, 0, 5}, {-1, 0, 5, 0}, {0, 1, 0, 0}, {1, 0, 0, 0}},
-  {{3, 0, -30, 0, 35}, {0, -3, 0, 7, 0}, {-1, 0, 7, 0, 0}, {0, 1, 0, 0, 0}, {1, 0, 0, 0, 0}}};
+static double kZ[LMAXH + 1][LMAXH + 1][LMAXH + 1];
+static double kC3B[NUM_ABC];
+static int g_harm_ready = 0;
 
-/* normalisation weights of the three-body invariants (nep_utilities.cuh:52, L<=4) */
-static const double kC3B[NUM_ABC] = {
-  0.238732414637843, 0.119366207318922, 0.119366207318922, 0.099471839432435,
-  0.596831036594608, 0.596831036594608, 0.149207759148652, 0.149207759148652,
-  0.139260575205408, 0.104445431404056, 0.104445431404056, 1.044454314040563,
-  1.044454314040563, 0.174075719006761, 0.174075719006761, 0.011190581936149,
-  0.223811638722978, 0.223811638722978, 0.111905819361489, 0.111905819361489,
-  1.566681471060845, 1.566681471060845, 0.195835183882606, 0.195835183882606};
+static long long gcd_ll(long long a, long long b)
+{
+  if (a < 0) a = -a;
+  if (b < 0) b = -b;
+  while (b) {
+    long long t = a % b;
+    a = b;
+    b = t;
+  }
+  return a;
+}
+
+static void build_harmonics(void)
+{
+  if (g_harm_ready) return;
+  memset(kZ, 0, sizeof(kZ));
+  for (int L = 1; L <= LMAXH; ++L) {
+    /* (z^2 - 1)^L, coefficients of z^0 .. z^2L */
+    long long w[2 * LMAXH + 1];
+    memset(w, 0, sizeof(w));
+    long long binom = 1;
+    for (int k = 0; k <= L; ++k) {
+      w[2 * k] = ((L - k) % 2 ? -1 : 1) * binom;
+      binom = binom * (L - k) / (k + 1);
+    }
+    double lfact = 1.0;
+    for (int r = 2; r <= L; ++r) lfact *= r;
+    for (int m = 0; m <= L; ++m) {
+      /* R = d^(L+m)/dz^(L+m) (z^2 - 1)^L, degree L - m */
+      long long R[LMAXH + 1];
+      long long g = 0;
+      for (int k = 0; k <= L - m; ++k) {
+        long long f = 1;
+        for (int r = k + 1; r <= k + L + m; ++r) f *= r;
+        R[k] = w[k + L + m] * f;
+        g = gcd_ll(g, R[k]);
+      }
+      if (R[L - m] < 0) g = -g;
+      for (int k = 0; k <= L - m; ++k) kZ[L][m][k] = (double)(R[k] / g);
+      double kappa = (double)g / (ldexp(1.0, L) * lfact);
+      double ratio = 1.0;
+      for (int r = L - m + 1; r <= L + m; ++r) ratio /= r;
+      double c = (2.0 * L + 1.0) / (4.0 * 3.14159265358979323846) * ratio * kappa * kappa;
+      int st = L * L - 1;
+      if (m == 0) {
+        kC3B[st] = c;
+      } else {
+        kC3B[st + 2 * m - 1] = c;
+        kC3B[st + 2 * m] = c;
+      }
+    }
+  }
+  g_harm_ready = 1;
+}
+
+void nepo_harmonic_tables(double* z, double* c3b)
+{
+  build_harmonics();
+  if (z) memcpy(z, kZ, sizeof(kZ));
+  if (c3b) memcpy(c3b, kC3B, sizeof(kC3B));
+}
+
 static const double kC4B[5] = {-0.007499480826664, -0.134990654879954, 0.067495327439977,
                                0.404971964639861, -0.809943929279723};
 static const double kC5B[3] = {0.026596810706114, 0.053193621412227, 0.026596810706114};
@@ -313,6 +370,7 @@ static int next_line(reader_t* r)
 nepo_model* nepo_load(const char* path, char* err, int errlen)
 {
   build_invariants();
+  build_harmonics();
   reader_t r;
   memset(&r, 0, sizeof(r));
   nepo_model* m = (nepo_model*)calloc(1, sizeof(nepo_model));
@@ -378,7 +436,7 @@ nepo_model* nepo_load(const char* path, char* err, int errlen)
   if (m->basis_r + 1 > MAXN || m->basis_a + 1 > MAXN) FAIL("basis too large");
   if (!next_line(&r) || r.ntok < 4) FAIL("l_max line");
   m->L_max = atoi(r.tok[1]);
-  if (m->L_max < 0 || m->L_max > 4) FAIL("oracle supports l_max <= 4");
+  if (m->L_max < 0 || m->L_max > LMAXH) FAIL("oracle supports l_max <= 8");
   m->num_L = m->L_max;
   for (int k = 0; k < MAX_INV; ++k) {
     m->has_inv[k] = (2 + k < r.ntok) ? atoi(r.tok[2 + k]) : 0;
@@ -633,7 +691,7 @@ static void harmonics(int L_max, const double* u, double d, double* Y, double (*
   double dzv[3] = {-u[0] * u[2] * dinv, -u[1] * u[2] * dinv, (1.0 - u[2] * u[2]) * dinv};
   int idx = 0;
   for (int L = 1; L <= L_max; ++L) {
-    double zp[6];
+    double zp[LMAXH + 1];
     zp[0] = 1.0;
     for (int k = 1; k <= L; ++k) zp[k] = zp[k - 1] * u[2];
     double re = 1.0, im = 0.0; /* (x + i y)^(m-1) */

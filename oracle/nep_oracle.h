@@ -46,6 +46,13 @@ void nepo_free(nepo_model* m);
 void nepo_info(const nepo_model* m, int* info, double* rc);
 
 /*
+ * The harmonic tables of degrees 1..8: z[9][9][9] the z-polynomial
+ * coefficients [L][m][power], c3b[80] the weights of the q_L invariants.
+ * Either pointer may be NULL.
+ */
+void nepo_harmonic_tables(double* z, double* c3b);
+
+/*
  * Per-atom energy, force and virial.
  *   h[9]    box matrix, row-major with the cell vectors a, b, c as columns
  *           (the reference's Box::cpu_h[0..8] layout)

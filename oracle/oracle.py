@@ -49,7 +49,16 @@ def lib():
                                           _f64p, _f64p]
         _lib.nepo_neighbors_f32.argtypes = [ctypes.c_void_p, ctypes.c_int, _i32p, _f64p, _i32p,
                                             _f64p, ctypes.c_int, ctypes.c_int, _i32p, _i32p]
+        _lib.nepo_harmonic_tables.argtypes = [_f64p, _f64p]
     return _lib
+
+
+def harmonic_tables():
+    """(z[9, 9, 9], c3b[80]): z-polynomial coefficients [L][m][power] and q_L weights."""
+    z = np.zeros((9, 9, 9))
+    c3b = np.zeros(80)
+    lib().nepo_harmonic_tables(z, c3b)
+    return z, c3b
 
 
 def _prep(types, h, pbc, pos):
