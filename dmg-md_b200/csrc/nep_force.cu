@@ -179,6 +179,23 @@ __device__ __forceinline__ float dot_basis(const float* __restrict__ c, const fl
   return acc;
 }
 
+// Shared memory of k_filter_radial: the coefficient table, then per-lane
+// type bins of the basis sums when T * kp <= kFilterBinMax floats.
+constexpr int kFilterBinMax = 48;
+__host__ __device__ inline int filter_table_floats(const ModelParams& p, int kp)
+{
+  return round4(p.T * p.T * p.nR * kp);
+}
+__host__ __device__ inline int filter_bin_float4(const ModelParams& p, int kp)
+{
+  const int q = p.T * kp / 4;
+  return q | 1;
+}
+__host__ __device__ inline bool filter_bins(const ModelParams& p, int kp)
+{
+  return p.T * kp <= kFilterBinMax;
+}
+
 // group ballot: the bits of the G lanes of this lane's group
 template <int G>
 __device__ __forceinline__ unsigned group_ballot(bool pred, int group)
@@ -289,10 +306,13 @@ __device__ __forceinline__ void center_acoef(const ModelParams& p, const float* 
 // difference rounded to float, float minimum image, the same x*x + y*y + z*z
 // expression; nep.cu:503-561) and writes the radial and angular rows in
 // order (group ballot + popcount), summing
-// q_n = sum_j sum_k c(ti,tj)[n][k] f_k(d_ij) on the way.  Kept apart from
-// k_nep_fused so this latency-bound sweep runs at the occupancy of its own
-// register count.
-template <int G, int NRM, int KM>
+// q_n = sum_j sum_k c(ti,tj)[n][k] f_k(d_ij) on the way.  BIN: each lane
+// sums its edges' basis values per neighbour type, B[tj][k] += f_k(d_ij), in
+// its own shared-memory bins and contracts them with c once at the end
+// (q_n = sum_t sum_k c(ti,t)[n][k] B[t][k]): a few float4 updates per edge
+// instead of the nR x kR contraction.  Kept apart from k_nep_fused so this
+// latency-bound sweep runs at the occupancy of its own register count.
+template <int G, int NRM, int KM, bool BIN>
 __global__ void __launch_bounds__(kBlock)
 k_filter_radial(const ModelParams p, int N, const Box* __restrict__ box,
                 const Site* __restrict__ sites, NeighborState* st,
@@ -303,13 +323,18 @@ k_filter_radial(const ModelParams p, int N, const Box* __restrict__ box,
 {
   constexpr int APW = 32 / G, APB = kBlock / G;
   constexpr int KP = (KM + 3) & ~3;
-  extern __shared__ float sm[];   // radial coefficient table [T*T][nR][KP]
+  extern __shared__ float sm[];   // radial coefficient table [T*T][nR][KP], then the bins
   const int tid = threadIdx.x;
   const int T = p.T, nR = p.nR, kR = p.kR;
   for (int k = tid; k < T * T * nR * KP; k += kBlock) {
     const int kk = k % KP, row = k / KP;
     sm[k] = kk < kR ? __ldg(p.c_pair + row * kR + kk) : 0.0f;
   }
+  // this lane's bins [T][KP] (an odd number of float4 per lane: no bank conflicts)
+  float4* bin = reinterpret_cast<float4*>(sm + filter_table_floats(p, KP)) +
+                tid * filter_bin_float4(p, KP);
+  if constexpr (BIN)
+    for (int q = 0; q < T * KP / 4; ++q) bin[q] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   if (blockIdx.x == 0 && tid == 0) st->rebuild = 0;   // the Verlet list is consumed
   __syncthreads();
   const int lane = tid & 31, warp = tid >> 5;
@@ -369,10 +394,23 @@ k_filter_radial(const ModelParams p, int N, const Box* __restrict__ box,
 #pragma unroll
       for (int kk = 0; kk < KP; ++kk) fn[kk] = 0.0f;
       radial_basis<KM>(kR, rcinv, d, fc, fn);
-      const float* c = sm + (t1 * T + t2) * nR * KP;
+      if constexpr (BIN) {
+        float4* bt = bin + t2 * (KP / 4);
 #pragma unroll
-      for (int n = 0; n < NRM; ++n)
-        if (n < nR) qr[n] += dot_basis<KM>(c + n * KP, fn);
+        for (int q = 0; q < KP / 4; ++q) {
+          float4 v = bt[q];
+          v.x += fn[4 * q];
+          v.y += fn[4 * q + 1];
+          v.z += fn[4 * q + 2];
+          v.w += fn[4 * q + 3];
+          bt[q] = v;
+        }
+      } else {
+        const float* c = sm + (t1 * T + t2) * nR * KP;
+#pragma unroll
+        for (int n = 0; n < NRM; ++n)
+          if (n < nR) qr[n] += dot_basis<KM>(c + n * KP, fn);
+      }
     }
     if (in_a) {
       const int at = ca + __popc(ma & below);
@@ -380,6 +418,15 @@ k_filter_radial(const ModelParams p, int N, const Box* __restrict__ box,
     }
     cr += __popc(mr);
     ca += __popc(ma);
+  }
+  if constexpr (BIN) {
+    const float* bf = reinterpret_cast<const float*>(bin);
+    for (int t = 0; t < T; ++t) {
+      const float* c = sm + (t1 * T + t) * nR * KP;
+#pragma unroll
+      for (int n = 0; n < NRM; ++n)
+        if (n < nR) qr[n] += dot_basis<KM>(c + n * KP, bf + t * KP);
+    }
   }
 #pragma unroll
   for (int n = 0; n < NRM; ++n) qr[n] = group_sum<G>(qr[n]);
@@ -1114,11 +1161,21 @@ template <int G, int NRM, int KM>
 void launch_filter_t(Engine& e, int N, cudaStream_t s)
 {
   NeighborBuffers& nb = e.nbr;
-  constexpr int APB = kBlock / G;
-  const size_t smem = sizeof(float) * e.params.T * e.params.T * e.params.nR * ((KM + 3) & ~3);
-  k_filter_radial<G, NRM, KM><<<(N + APB - 1) / APB, kBlock, smem, s>>>(
-    e.params, N, e.d_box, e.scratch.sites, e.d_nstate, nb.nn_v, nb.nl_v, nb.mn_v, nb.nn_r,
-    nb.nl_r, nb.mn_r, nb.nn_a, nb.nl_a, nb.mn_a, e.scratch.qrad);
+  constexpr int APB = kBlock / G, KP = (KM + 3) & ~3;
+  const ModelParams& p = e.params;
+  const int blocks = (N + APB - 1) / APB;
+  if (filter_bins(p, KP)) {
+    const size_t smem =
+      sizeof(float) * (filter_table_floats(p, KP) + 4 * kBlock * filter_bin_float4(p, KP));
+    k_filter_radial<G, NRM, KM, true><<<blocks, kBlock, smem, s>>>(
+      p, N, e.d_box, e.scratch.sites, e.d_nstate, nb.nn_v, nb.nl_v, nb.mn_v, nb.nn_r, nb.nl_r,
+      nb.mn_r, nb.nn_a, nb.nl_a, nb.mn_a, e.scratch.qrad);
+  } else {
+    const size_t smem = sizeof(float) * filter_table_floats(p, KP);
+    k_filter_radial<G, NRM, KM, false><<<blocks, kBlock, smem, s>>>(
+      p, N, e.d_box, e.scratch.sites, e.d_nstate, nb.nn_v, nb.nl_v, nb.mn_v, nb.nn_r, nb.nl_r,
+      nb.mn_r, nb.nn_a, nb.nl_a, nb.mn_a, e.scratch.qrad);
+  }
 }
 
 template <int G, int KP, int LMAX>
