@@ -60,6 +60,7 @@ struct NeighborState {
   int box_error;       // the device box became unsupported (small in one direction, >10 rc in another)
   int ann_error;       // a tensor-core ANN tile gave up waiting for its MMAs
   double box_scale;    // product of isotropic box factors since the last build (1 = none)
+  double box_def[9];   // product of general box deformations since the last build (I = none)
 };
 
 // Minimum image of a float displacement, the arithmetic of the large-box

@@ -181,6 +181,7 @@ std::string engine_create(Engine& e, const std::string& nep_path, int max_atoms)
   if (!ok) return "cudaMalloc failed (per-atom buffers)";
   NeighborState init{};
   init.box_scale = 1.0;
+  for (int k = 0; k < 9; ++k) init.box_def[k] = (k % 4 == 0) ? 1.0 : 0.0;
   if (cudaMemcpy(e.d_nstate, &init, sizeof(init), cudaMemcpyHostToDevice) != cudaSuccess)
     return "cudaMemcpy failed (neighbour state)";
   if (cudaMemset(nb.nn_a, 0, sizeof(int) * N) != cudaSuccess) return "cudaMemset failed";

@@ -167,6 +167,95 @@ __global__ void k_vv2_thermo(StepParams p, const double* __restrict__ mass,
   block_reduce8(v, partials);
 }
 
+// 3x3 products and inverse, row-major.
+__device__ inline void mat3_mul(const double* a, const double* b, double* c)
+{
+  double t[9];
+  for (int r = 0; r < 3; ++r)
+    for (int q = 0; q < 3; ++q)
+      t[3 * r + q] = a[3 * r] * b[q] + a[3 * r + 1] * b[3 + q] + a[3 * r + 2] * b[6 + q];
+  for (int k = 0; k < 9; ++k) c[k] = t[k];
+}
+
+__device__ inline bool mat3_inverse(const double* a, double* inv)
+{
+  const double c0 = a[4] * a[8] - a[5] * a[7];
+  const double c1 = a[5] * a[6] - a[3] * a[8];
+  const double c2 = a[3] * a[7] - a[4] * a[6];
+  const double det = a[0] * c0 + a[1] * c1 + a[2] * c2;
+  if (!(fabs(det) > 0.0) || !isfinite(det)) return false;
+  const double id = 1.0 / det;
+  inv[0] = c0 * id;
+  inv[1] = (a[2] * a[7] - a[1] * a[8]) * id;
+  inv[2] = (a[1] * a[5] - a[2] * a[4]) * id;
+  inv[3] = c1 * id;
+  inv[4] = (a[0] * a[8] - a[2] * a[6]) * id;
+  inv[5] = (a[2] * a[3] - a[0] * a[5]) * id;
+  inv[6] = c2 * id;
+  inv[7] = (a[1] * a[6] - a[0] * a[7]) * id;
+  inv[8] = (a[0] * a[4] - a[1] * a[3]) * id;
+  return true;
+}
+
+// true when a periodic direction of the box is not thicker than t
+__device__ inline bool box_thinner_than(const Box& b, double t)
+{
+  const double V = fabs(box_volume(b));
+  for (int d = 0; d < 3; ++d) {
+    if (!b.pbc[d]) continue;
+    // thickness along d = V / |a_e x a_f|, a the cell vectors (columns of h)
+    const int e = (d + 1) % 3, f = (d + 2) % 3;
+    const double cx = b.h[3 + e] * b.h[6 + f] - b.h[6 + e] * b.h[3 + f];
+    const double cy = b.h[6 + e] * b.h[f] - b.h[e] * b.h[6 + f];
+    const double cz = b.h[e] * b.h[3 + f] - b.h[3 + e] * b.h[f];
+    if (V / sqrt(cx * cx + cy * cy + cz * cz) <= t) return true;
+  }
+  return false;
+}
+
+// Per-component pressure coupling (the reference has only the isotropic
+// one).  With the pressure tensor P (xx yy zz yz xz xy), targets P0 and
+// couplings c = 1 / (3 tau_p C) (C the component's modulus):
+//   Berendsen  mu_aa = 1 - c_a (P0_a - P_aa);  mu_ab = mu_ba = -c_ab (P0_ab - P_ab)
+//   SCR        the same drift plus sqrt(2 c kT / V) eta on each diagonal strain
+//              ln h_aa and sqrt(c kT / V) eta on each symmetric shear (the
+//              fluctuation-dissipation pairing of each strain with its work
+//              conjugate; with equal couplings and one shared draw the
+//              volume fluctuation equals the isotropic formula's)
+// and h' = mu h, positions with it.  Returns false on a non-positive or
+// non-finite deformation.
+__device__ bool apply_component_coupling(const StepParams& p, Box& b, const double* th,
+                                         double V, double Tt, const double* eta, double* mu,
+                                         NeighborState* nstate)
+{
+  const double P6[6] = {th[2], th[3], th[4], th[7], th[6], th[5]};
+  const int nc = p.baro == kBaroAniso ? 3 : 6;
+  const int slot[6][2] = {{0, 0}, {4, 4}, {8, 8}, {5, 7}, {2, 6}, {1, 3}};
+  for (int c = 0; c < nc; ++c) {
+    double m = -p.pc6[c] * (p.p6[c] - P6[c]);
+    if (p.kind == kNptScr)
+      m += sqrt((c < 3 ? 2.0 : 1.0) * p.pc6[c] * kBoltzmann * Tt / V) * eta[c];
+    mu[slot[c][0]] += m;
+    if (slot[c][1] != slot[c][0]) mu[slot[c][1]] += m;
+  }
+  for (int k = 0; k < 9; ++k)
+    if (!isfinite(mu[k])) return false;
+  if (!(mu[0] > 0.0 && mu[4] > 0.0 && mu[8] > 0.0)) return false;
+  double h[9], hinv[9];
+  mat3_mul(mu, b.h, h);
+  if (!mat3_inverse(h, hinv)) return false;
+  for (int k = 0; k < 9; ++k) {
+    b.h[k] = h[k];
+    b.hinv[k] = hinv[k];
+    b.fh[k] = static_cast<float>(h[k]);
+    b.fh[9 + k] = static_cast<float>(hinv[k]);
+  }
+  b.ortho = h[1] == 0.0 && h[2] == 0.0 && h[3] == 0.0 && h[5] == 0.0 && h[6] == 0.0 &&
+            h[7] == 0.0;
+  mat3_mul(mu, nstate->box_def, nstate->box_def);
+  return true;
+}
+
 // Thermo normalisation, thermostat and barostat scalars, box update and the
 // thermo row of this step (ensemble_control.cpp:180-306, npt_scr.cpp:21-33,
 // box_control.cpp:9-68).  One block: 8 threads reduce the partials in a
@@ -194,7 +283,7 @@ __global__ void k_ensemble(StepParams p, Box* box, MdScalars* sc, const double* 
   const double Tt = target_temperature(p, step);
   double vf = 1.0, bf = 1.0;
   const long long local = step - sc->step0;   // step within this call
-  const double* nz = noise + 3 * local;
+  const double* nz = noise + kNoisePerStep * local;
   switch (p.kind) {
     case kNvtBer:
     case kNptBer: {
@@ -220,7 +309,12 @@ __global__ void k_ensemble(StepParams p, Box* box, MdScalars* sc, const double* 
     default:
       break;
   }
-  if (p.kind == kNptBer || p.kind == kNptScr) {
+  const bool npt = p.kind == kNptBer || p.kind == kNptScr;
+  for (int k = 0; k < 9; ++k) sc->mu[k] = (k % 4 == 0) ? 1.0 : 0.0;
+  if (npt && p.baro != kBaroIso) {
+    if (!apply_component_coupling(p, b, th, V, Tt, nz + 2, sc->mu, nstate)) *status |= 2;
+    else if (p.large_box && box_thinner_than(b, p.thick_min)) *status |= 4;
+  } else if (npt) {
     const double p_inst = (th[2] + th[3] + th[4]) * 0.3333333333333333;
     bf = 1.0 - p.pc * (p.p_target - p_inst);
     if (p.kind == kNptScr)
@@ -287,6 +381,17 @@ __global__ void k_scale(int N, double* vel, double* pos, double* x0,
       pos[d * N + i] *= bf;
       x0[d * N + i] *= bf;
     }
+  const double* mu = sc->mu;
+  if (mu[0] != 1.0 || mu[1] != 0.0 || mu[2] != 0.0 || mu[3] != 0.0 || mu[4] != 1.0 ||
+      mu[5] != 0.0 || mu[6] != 0.0 || mu[7] != 0.0 || mu[8] != 1.0) {
+    double* arrs[2] = {pos, x0};
+    for (double* a : arrs) {
+      const double x = a[i], y = a[N + i], z = a[2 * N + i];
+      a[i] = mu[0] * x + mu[1] * y + mu[2] * z;
+      a[N + i] = mu[3] * x + mu[4] * y + mu[5] * z;
+      a[2 * N + i] = mu[6] * x + mu[7] * y + mu[8] * z;
+    }
+  }
 }
 
 __global__ void k_init_scalars(MdScalars* sc, StepParams p, double T0, double tau)
@@ -296,6 +401,7 @@ __global__ void k_init_scalars(MdScalars* sc, StepParams p, double T0, double ta
   sc->vfactor_pre = 1.0;
   sc->vfactor = 1.0;
   sc->bfactor = 1.0;
+  for (int k = 0; k < 9; ++k) sc->mu[k] = (k % 4 == 0) ? 1.0 : 0.0;
   // Nose-Hoover chain start (thermostat_nhc.cpp:25-41)
   const double kT = kBoltzmann * T0;
   for (int m = 0; m < kChain; ++m) {
@@ -467,6 +573,32 @@ int nepx_md_destroy(nepx_md_t* m)
 
 const char* nepx_md_last_error(const nepx_md_t* m) { return m ? m->error.c_str() : "null handle"; }
 
+int nepx_md_set_barostat(nepx_md_t* m, int coupling, const double* pressure_gpa,
+                         const double* modulus_gpa)
+{
+  if (!m) return NEPX_ERR_ARG;
+  nepx::EnsembleConfig& c = m->md.ens;
+  if (c.kind != nepx::kNptBer && c.kind != nepx::kNptScr)
+    return md_fail(m, NEPX_ERR_ARG, "set an NPT ensemble before its barostat coupling");
+  if (coupling == NEPX_BARO_ISOTROPIC) {
+    c.baro = nepx::kBaroIso;
+    return NEPX_OK;
+  }
+  if (coupling != NEPX_BARO_ANISOTROPIC && coupling != NEPX_BARO_TRICLINIC)
+    return md_fail(m, NEPX_ERR_ARG, "unknown barostat coupling");
+  if (!pressure_gpa || !modulus_gpa) return md_fail(m, NEPX_ERR_ARG, "pressures or moduli missing");
+  const int nc = coupling == NEPX_BARO_ANISOTROPIC ? 3 : 6;
+  for (int k = 0; k < nc; ++k)
+    if (!std::isfinite(pressure_gpa[k]) || !(modulus_gpa[k] > 0.0))
+      return md_fail(m, NEPX_ERR_ARG, "barostat needs finite pressures and moduli > 0");
+  c.baro = coupling == NEPX_BARO_ANISOTROPIC ? nepx::kBaroAniso : nepx::kBaroTri;
+  for (int k = 0; k < 6; ++k) {
+    c.p6_gpa[k] = k < nc ? pressure_gpa[k] : 0.0;
+    c.c6_gpa[k] = k < nc ? modulus_gpa[k] : 1.0e300;   // uncoupled: no deformation
+  }
+  return NEPX_OK;
+}
+
 int nepx_md_set_ensemble(nepx_md_t* m, int kind, const double* params, unsigned seed)
 {
   if (!m || kind < nepx::kNVE || kind > nepx::kNptScr) return NEPX_ERR_ARG;
@@ -485,10 +617,7 @@ int nepx_md_set_ensemble(nepx_md_t* m, int kind, const double* params, unsigned 
       c.tau_p = params[5];
       if (!std::isfinite(c.p_gpa) || !(c.bulk_gpa > 0.0) || !(c.tau_p >= 1.0))
         return md_fail(m, NEPX_ERR_ARG, "NPT needs finite P, B > 0 and tau_p >= 1");
-      const nepx::Box& b = m->md.box;
-      if (!b.ortho || !b.pbc[0] || !b.pbc[1] || !b.pbc[2])
-        return md_fail(m, NEPX_ERR_UNSUPPORTED,
-                       "isotropic NPT needs an orthogonal box periodic in all directions");
+      // the box requirements of the coupling are checked when a run starts
     }
   }
   c.seed = seed;
@@ -511,6 +640,14 @@ int md_enqueue_run(nepx_md* m, int steps, double dt_fs, int thermo_every, double
   nepx::Engine& e = *md.engine;
   const nepx::EnsembleConfig& c = md.ens;
   const int N = md.N;
+  if (c.kind == nepx::kNptBer || c.kind == nepx::kNptScr) {
+    const nepx::Box& b = md.box;
+    if (!b.pbc[0] || !b.pbc[1] || !b.pbc[2])
+      return md_fail(m, NEPX_ERR_UNSUPPORTED, "NPT needs a box periodic in all directions");
+    if (c.baro == nepx::kBaroIso && !b.ortho)
+      return md_fail(m, NEPX_ERR_UNSUPPORTED,
+                     "isotropic NPT needs an orthogonal box (use a triclinic coupling)");
+  }
   e.use_xr = md.xr;
   e.xr.from_box = true;
   nepx::StepParams p{};
@@ -529,6 +666,13 @@ int md_enqueue_run(nepx_md* m, int steps, double dt_fs, int thermo_every, double
     // form pc in 1/GPa, then convert once (ensemble_control.cpp:84-95)
     p.pc = c.bulk_gpa > 2000.0 ? 0.0 : 1.0 / (3.0 * c.tau_p * c.bulk_gpa);
     p.pc *= nepx::kPressureUnit;
+    p.baro = c.baro;
+    for (int k = 0; k < 6; ++k) {
+      p.p6[k] = c.p6_gpa[k] / nepx::kPressureUnit;
+      p.pc6[k] = c.c6_gpa[k] > 2000.0 ? 0.0 : nepx::kPressureUnit / (3.0 * c.tau_p * c.c6_gpa[k]);
+    }
+    p.large_box = md.xr ? 0 : 1;
+    p.thick_min = 2.5 * (e.model.rc_radial_max + 1.0);
   }
   p.bdp_factor = c.Tdamp > 0.1 ? std::exp(-1.0 / c.Tdamp) : 0.0;
   cudaStream_t s = md.stream;
@@ -539,25 +683,28 @@ int md_enqueue_run(nepx_md* m, int steps, double dt_fs, int thermo_every, double
     if (m->h_noise) cudaFreeHost(m->h_noise);
     md.d_noise = nullptr;
     m->h_noise = nullptr;
-    if (!dalloc(md.d_noise, 3 * size_t(steps)) ||
-        cudaMallocHost(reinterpret_cast<void**>(&m->h_noise), sizeof(double) * 3 * steps) !=
-          cudaSuccess)
+    if (!dalloc(md.d_noise, nepx::kNoisePerStep * size_t(steps)) ||
+        cudaMallocHost(reinterpret_cast<void**>(&m->h_noise),
+                       sizeof(double) * nepx::kNoisePerStep * steps) != cudaSuccess)
       return md_cuda(m, "allocate noise buffers");
     md.noise_cap = steps;
   } else {
     cudaEventSynchronize(m->noise_copied);   // previous upload has left the staging buffer
   }
   const bool stochastic_v = c.kind == nepx::kNvtBdp || c.kind == nepx::kNptScr;
+  const int box_draws = c.kind != nepx::kNptScr ? 0
+                        : c.baro == nepx::kBaroIso ? 1 : (c.baro == nepx::kBaroAniso ? 3 : 6);
   for (int k = 0; k < steps; ++k) {
-    double* z = m->h_noise + 3 * k;
-    z[0] = z[1] = z[2] = 0.0;
+    double* z = m->h_noise + nepx::kNoisePerStep * k;
+    for (int q = 0; q < nepx::kNoisePerStep; ++q) z[q] = 0.0;
     if (stochastic_v) {
       z[0] = md.rng.gasdev();
       z[1] = md.rng.sumnoises(3 * N - 1);
     }
-    if (c.kind == nepx::kNptScr) z[2] = md.rng.gasdev();
+    for (int q = 0; q < box_draws; ++q) z[2 + q] = md.rng.gasdev();
   }
-  cudaMemcpyAsync(md.d_noise, m->h_noise, sizeof(double) * 3 * steps, cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(md.d_noise, m->h_noise, sizeof(double) * nepx::kNoisePerStep * steps,
+                  cudaMemcpyHostToDevice, s);
   cudaEventRecord(m->noise_copied, s);
   const int rows = thermo_every > 0 ? steps / thermo_every : 0;
   if (rows > md.rows_cap) {
@@ -625,6 +772,9 @@ int md_finish(nepx_md* m)
   const nepx::NeighborState& st = m->mirror->nstate;
   if (status & 1) return md_fail(m, NEPX_ERR_NONFINITE, "invalid thermostat velocity factor");
   if (status & 2) return md_fail(m, NEPX_ERR_NONFINITE, "invalid barostat box factor");
+  if (status & 4)
+    return md_fail(m, NEPX_ERR_BOX, "the barostat made a periodic direction thinner than "
+                                    "2.5 (rc + 1): the large-box path no longer applies");
   if (st.overflow) return md_fail(m, NEPX_ERR_OVERFLOW, "a neighbour row exceeded its capacity");
   if (st.nonfinite) return md_fail(m, NEPX_ERR_NONFINITE, "non-finite energy or force");
   if (st.box_error)

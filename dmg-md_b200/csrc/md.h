@@ -12,6 +12,13 @@ namespace nepx {
 
 enum EnsembleKind { kNVE = 0, kNvtBer = 1, kNvtNhc = 2, kNvtBdp = 3, kNptBer = 4, kNptScr = 5 };
 
+// Pressure coupling of the NPT ensembles: the reference's isotropic one, and
+// per-component couplings of an orthogonal (xx yy zz) or triclinic
+// (xx yy zz yz xz xy) box, which the reference does not have
+// (box_control.cpp:14-23 rejects them).
+enum BarostatCoupling { kBaroIso = 0, kBaroAniso = 1, kBaroTri = 2 };
+constexpr int kNoisePerStep = 8;   // two thermostat draws, up to six barostat draws
+
 // run.in `ensemble` parameters (reference include/dmgmd/run_ir.hpp:12-117):
 // T0 -> T1 linear ramp, Tdamp coupling in steps; NPT: target pressure (GPa),
 // bulk modulus B (GPa) and pressure coupling tau_p (steps).
@@ -19,6 +26,9 @@ struct EnsembleConfig {
   int kind = kNVE;
   double T0 = 0.0, T1 = 0.0, Tdamp = 100.0;
   double p_gpa = 0.0, bulk_gpa = 0.0, tau_p = 1000.0;
+  int baro = kBaroIso;
+  double p6_gpa[6] = {0, 0, 0, 0, 0, 0};   // component targets, xx yy zz yz xz xy
+  double c6_gpa[6] = {0, 0, 0, 0, 0, 0};   // component moduli
   uint32_t seed = 12345678u;   // reference default (ensemble_control.hpp:12-18)
 };
 
@@ -32,6 +42,7 @@ struct MdScalars {
   double vfactor_pre;  // NHC scale applied before the first half kick
   double vfactor;      // thermostat scale after the second half kick
   double bfactor;      // isotropic box scale of this step
+  double mu[9];        // box deformation of this step, h' = mu h (component couplings)
   double thermo[8];    // T, PE, stresses xx yy zz xy xz yz (natural units, volume-normalised)
   double nhc_pos[kChain], nhc_mom[kChain], nhc_mass[kChain];
 };
@@ -46,6 +57,11 @@ struct StepParams {
   double T0, T1, Tdamp;
   double p_target;     // eV/A^3
   double pc;           // Berendsen pressure coupling, (eV/A^3)^-1
+  int baro;            // BarostatCoupling
+  int large_box;       // the force path is the large-box one (box must stay thick)
+  double p6[6];        // component targets, eV/A^3 (xx yy zz yz xz xy)
+  double pc6[6];       // component couplings, (eV/A^3)^-1
+  double thick_min;    // thinnest periodic thickness the large-box path accepts
   double bdp_factor;   // exp(-1/Tdamp) (0 when Tdamp <= 0.1)
   double rc_v;         // rc + skin, for the NPT rebuild criterion
   double skin;

@@ -49,7 +49,9 @@ __device__ __forceinline__ void cell_coords(const Box& b, const NeighborState& s
 // an isotropic box scaling s since the build (x0 scaled along, so
 // displacements are co-moving) a pair distance also drifts by up to
 // |1 - s| (rc + skin), which shrinks the allowed displacement to
-// (skin - |1 - s| (rc + skin)) / 2.
+// (skin - |1 - s| (rc + skin)) / 2.  A general deformation M since the build
+// moves a pair by at most ||M - I||_2 (rc + skin); the bound used is
+// sqrt(||M - I||_1 ||M - I||_inf) >= ||M - I||_2.
 __global__ void k_skin_check(int N, const Box* __restrict__ box, const double* __restrict__ pos,
                              const int* __restrict__ type, const double* __restrict__ x0,
                              NeighborState* st, Site* __restrict__ sites, double skin,
@@ -63,7 +65,19 @@ __global__ void k_skin_check(int N, const Box* __restrict__ box, const double* _
     if (i == 0) st->rebuild = 1;
     return;
   }
-  const double half = 0.5 * (skin - fabs(1.0 - st->box_scale) * rc_v);
+  double col[3] = {0.0, 0.0, 0.0}, row_max = 0.0;
+  for (int r = 0; r < 3; ++r) {
+    double row = 0.0;
+    for (int c = 0; c < 3; ++c) {
+      const double a = fabs(st->box_def[3 * r + c] - (r == c ? 1.0 : 0.0));
+      row += a;
+      col[c] += a;
+    }
+    row_max = fmax(row_max, row);
+  }
+  const double def = sqrt(fmax(fmax(col[0], col[1]), col[2]) * row_max);
+  const double strain = fmax(fabs(1.0 - st->box_scale), def);
+  const double half = 0.5 * (skin - strain * rc_v);
   if (half <= 0.0) {
     st->rebuild = 1;
     return;
@@ -85,6 +99,7 @@ __global__ void k_cell_setup(const Box* __restrict__ box, NeighborState* st, int
   if (!st->rebuild) return;
   if (threadIdx.x == 0) {
     st->box_scale = 1.0;
+    for (int k = 0; k < 9; ++k) st->box_def[k] = (k % 4 == 0) ? 1.0 : 0.0;
     const Box& b = *box;
     double vol = fabs(b.h[0] * (b.h[4] * b.h[8] - b.h[5] * b.h[7]) +
                       b.h[1] * (b.h[5] * b.h[6] - b.h[3] * b.h[8]) +

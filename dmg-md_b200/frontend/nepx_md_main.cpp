@@ -301,6 +301,9 @@ struct Job {
     const double params[6] = {ens.T0, ens.T1, ens.Tdamp, ens.p_gpa, ens.bulk_gpa, ens.tau_p};
     check(nepx_md_set_ensemble(md, static_cast<int>(ens.kind), params, seed),
           "nepx_md_set_ensemble", nepx_md_last_error(md));
+    if (ens.baro)
+      check(nepx_md_set_barostat(md, ens.baro, ens.p6_gpa, ens.c6_gpa), "nepx_md_set_barostat",
+            nepx_md_last_error(md));
     // stop at every multiple of the gcd of the output intervals
     int g = 0;
     for (int v : thermo) g = std::gcd(g, v);

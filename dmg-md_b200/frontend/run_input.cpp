@@ -120,15 +120,34 @@ EnsembleCmd ensemble(const std::vector<std::string>& t, const Source& s)
     return c;
   }
   if (name == "npt_ber" || name == "npt_scr") {
-    if (t.size() > 8) fail(s, name + ": v1 supports isotropic 8-token syntax only");
-    need(t, 8, s, "ensemble " + name + " should have 6 parameters (isotropic 8-token syntax)");
+    // the reference's isotropic 8-token form, plus GPUMD's anisotropic
+    // (Pxx Pyy Pzz Cxx Cyy Czz) and triclinic (Pxx Pyy Pzz Pyz Pxz Pxy, six
+    // moduli) forms, which the reference rejects
+    if (t.size() > 8 && t.size() != 12 && t.size() != 18)
+      fail(s, name + ": v1 supports isotropic 8-token syntax only (and the anisotropic 12-token "
+                     "and triclinic 18-token forms of this engine)");
+    need(t, t.size() > 8 ? t.size() : 8, s,
+         "ensemble " + name + " should have 6 parameters (isotropic 8-token syntax)");
     c.kind = name == "npt_ber" ? Ensemble::npt_ber : Ensemble::npt_scr;
     c.T0 = to_real(t[2], s, "initial temperature");
     c.T1 = to_real(t[3], s, "final temperature");
     c.Tdamp = to_real(t[4], s, "temperature coupling");
-    c.p_gpa = to_real(t[5], s, "target pressure (GPa)");
-    c.bulk_gpa = to_real(t[6], s, "bulk modulus (GPa)");
-    c.tau_p = to_real(t[7], s, "pressure coupling time");
+    if (t.size() == 8) {
+      c.p_gpa = to_real(t[5], s, "target pressure (GPa)");
+      c.bulk_gpa = to_real(t[6], s, "bulk modulus (GPa)");
+    } else {
+      const int nc = t.size() == 12 ? 3 : 6;
+      c.baro = nc == 3 ? 1 : 2;
+      for (int k = 0; k < nc; ++k) {
+        c.p6_gpa[k] = to_real(t[5 + k], s, "target pressure component (GPa)");
+        c.c6_gpa[k] = to_real(t[5 + nc + k], s, "elastic modulus component (GPa)");
+        if (c.c6_gpa[k] <= 0.0) fail(s, "elastic moduli should be > 0");
+      }
+      // the isotropic fields stay valid for the ensemble call
+      c.p_gpa = (c.p6_gpa[0] + c.p6_gpa[1] + c.p6_gpa[2]) / 3.0;
+      c.bulk_gpa = c.c6_gpa[0];
+    }
+    c.tau_p = to_real(t.back(), s, "pressure coupling time");
     if (c.T0 <= 0.0 || c.T1 <= 0.0) fail(s, "initial and final temperatures should be > 0");
     if (c.Tdamp < 1.0) fail(s, "temperature coupling should be >= 1");
     if (c.bulk_gpa <= 0.0) fail(s, "bulk modulus should be > 0");

@@ -40,6 +40,9 @@ struct EnsembleCmd {
   Ensemble kind = Ensemble::nve;
   double T0 = 0, T1 = 0, Tdamp = 0;        // temperatures (K), coupling (steps)
   double p_gpa = 0, bulk_gpa = 0, tau_p = 0;
+  int baro = 0;                  // 0 isotropic, 1 anisotropic (xx yy zz), 2 triclinic
+  double p6_gpa[6] = {0, 0, 0, 0, 0, 0};   // component targets, xx yy zz yz xz xy
+  double c6_gpa[6] = {0, 0, 0, 0, 0, 0};   // component moduli
 };
 struct CorrectVelocityCmd { int interval = 0; std::optional<int> grouping; };
 struct DumpThermoCmd { int interval = 0; };

@@ -34,9 +34,11 @@ EXPORTED = ["nepx_create", "nepx_destroy", "nepx_last_error", "nepx_info", "nepx
             "nepx_md_run_async", "nepx_md_sync", "nepx_compute_noalloc", "nepx_compute_batch",
             "nepx_server_create", "nepx_server_destroy", "nepx_server_last_error",
             "nepx_server_submit", "nepx_server_poll", "nepx_server_wait", "nepx_server_drain",
-            "nepx_server_stats", "nepx_set_precision", "nepx_md_run_segment"]
+            "nepx_server_stats", "nepx_set_precision", "nepx_md_run_segment",
+            "nepx_md_set_barostat"]
 
 ENSEMBLES = {"nve": 0, "nvt_ber": 1, "nvt_nhc": 2, "nvt_bdp": 3, "npt_ber": 4, "npt_scr": 5}
+BAROSTATS = {"isotropic": 0, "anisotropic": 1, "triclinic": 2}
 THERMO_COLUMNS = ["T", "KE", "PE", "sxx", "syy", "szz", "syz", "sxz", "sxy", "ax", "ay", "az",
                   "bx", "by", "bz", "cx", "cy", "cz", "velocity_factor", "box_factor"]
 
@@ -100,6 +102,7 @@ def lib():
         L.nepx_md_last_error.argtypes = [vp]
         L.nepx_md_last_error.restype = ctypes.c_char_p
         L.nepx_md_set_ensemble.argtypes = [vp, ctypes.c_int, dp, ctypes.c_uint]
+        L.nepx_md_set_barostat.argtypes = [vp, ctypes.c_int, dp, dp]
         L.nepx_md_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, dp]
         L.nepx_md_get.argtypes = [vp, dp, dp, dp, dp, dp, ctypes.POINTER(Box)]
         L.nepx_compute_noalloc.argtypes = [vp, ctypes.POINTER(Box), ctypes.c_int, vp, vp, vp, vp,
@@ -325,6 +328,21 @@ class MD:
         T1 = T0 if T1 is None else T1
         params = np.array([T0, T1, Tdamp, p_gpa, bulk_gpa, tau_p], dtype=np.float64)
         self._check(lib().nepx_md_set_ensemble(self._h, ENSEMBLES[kind], _dp(params), seed))
+
+    def set_barostat(self, coupling, pressure_gpa=None, modulus_gpa=None):
+        """Pressure coupling of the NPT ensemble: "isotropic", "anisotropic"
+        (xx yy zz) or "triclinic" (xx yy zz yz xz xy) targets and moduli in GPa."""
+        import numpy as np
+        code = BAROSTATS[coupling]
+        if code == 0:
+            self._check(lib().nepx_md_set_barostat(self._h, 0, None, None))
+            return
+        pr = np.ascontiguousarray(pressure_gpa, dtype=np.float64)
+        mo = np.ascontiguousarray(modulus_gpa, dtype=np.float64)
+        if pr.size != (3 if code == 1 else 6) or mo.size != pr.size:
+            raise ValueError("%s coupling takes %d pressures and moduli"
+                             % (coupling, 3 if code == 1 else 6))
+        self._check(lib().nepx_md_set_barostat(self._h, code, _dp(pr), _dp(mo)))
 
     def run(self, steps, dt_fs, thermo_every=0):
         """Runs `steps` steps; returns the thermo rows (rows, 20) or None."""

@@ -186,6 +186,26 @@ const char* nepx_md_last_error(const nepx_md_t* md);
 int nepx_md_set_ensemble(nepx_md_t* md, int kind, const double* params, unsigned seed);
 
 /*
+ * Pressure coupling of the NPT ensemble set last (nepx_md_set_ensemble
+ * selects NEPX_BARO_ISOTROPIC, the reference's only one).  The other two
+ * have no counterpart in the reference, which rejects them
+ * (src/box_control.cpp:14-23); they follow GPUMD's component syntax:
+ *   NEPX_BARO_ANISOTROPIC  pressure_gpa[3], modulus_gpa[3]: xx yy zz
+ *   NEPX_BARO_TRICLINIC    pressure_gpa[6], modulus_gpa[6]: xx yy zz yz xz xy
+ * Each component a deforms the box by mu_a = 1 - (P0_a - P_a) / (3 tau_p C_a)
+ * per step (npt_scr adds its component noise), h' = mu h with positions
+ * following; a modulus above 2000 GPa leaves the component uncoupled.  A run
+ * needs a box periodic in all three directions (and an orthogonal one for
+ * the isotropic coupling); a run whose box becomes thinner than the
+ * large-box criterion returns NEPX_ERR_BOX.
+ */
+#define NEPX_BARO_ISOTROPIC 0
+#define NEPX_BARO_ANISOTROPIC 1
+#define NEPX_BARO_TRICLINIC 2
+int nepx_md_set_barostat(nepx_md_t* md, int coupling, const double* pressure_gpa,
+                         const double* modulus_gpa);
+
+/*
  * `steps` steps of dt_fs femtoseconds.  Every thermo_every steps (0 = never)
  * one row of 20 doubles is written to h_thermo (rows = steps / thermo_every,
  * may be NULL): the 18 thermo.out columns (T KE PE sxx syy szz syz sxz sxy

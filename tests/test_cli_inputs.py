@@ -83,3 +83,17 @@ def test_model_rejections(tmp_path, edit, message):
     (tmp_path / "model.xyz").write_text(edit(st["model_xyz"]))
     r = _check(tmp_path)
     assert r.returncode == 1 and message in r.stderr, r.stderr
+
+
+@pytest.mark.parametrize("line,ok", [
+    ("ensemble npt_ber 300 300 100 0 0 0 100 120 140 1000", True),
+    ("ensemble npt_scr 300 300 100 0 0 0 0 0 0 100 100 100 50 50 50 1000", True),
+    ("ensemble npt_ber 300 300 100 0 0 0 100 120 -140 1000", False),
+    ("ensemble npt_ber 300 300 100 0 0 0 100 120 140 1000 7", False),
+    ("ensemble npt_ber 300 300 100 0 0 0 0 100 120 140 1000", False),
+])
+def test_component_barostat_syntax(tmp_path, line, ok):
+    """The anisotropic (12-token) and triclinic (18-token) npt forms."""
+    _stage(tmp_path, run_in="potential nep.txt\nvelocity 300\ntime_step 1\n%s\nrun 10\n" % line)
+    r = _check(tmp_path)
+    assert (r.returncode == 0) == ok, r.stderr
