@@ -71,10 +71,12 @@ __device__ __forceinline__ float zpoly_any(int L, int m, const float* zp, float*
   return f;
 }
 
-// Harmonics Y[0 .. (L_max + 1)^2 - 1) at the unit vector u, degrees up to
-// LMAX (the instance's bound) and L_max (the model's).
-template <int LMAX>
-__device__ __forceinline__ void harmonics(int L_max, float ux, float uy, float uz, float* Y)
+// Harmonics Y[lm], lm < (L_max + 1)^2 - 1, at the unit vector u, degrees up
+// to LMAX (the instance's bound) and L_max (the model's), handed one at a
+// time to f(lm, Y[lm]) with lm a compile-time index once unrolled (no array
+// of all harmonics stays live).
+template <int LMAX, typename F>
+__device__ __forceinline__ void for_each_harmonic(int L_max, float ux, float uy, float uz, F&& f)
 {
   float zp[LMAX + 1];
   zp[0] = 1.0f;
@@ -90,10 +92,10 @@ __device__ __forceinline__ void harmonics(int L_max, float ux, float uy, float u
       float dzf;
       const float zf = zpoly_any(L, m, zp, &dzf);
       if (m == 0) {
-        Y[idx++] = zf;
+        f(idx++, zf);
       } else {
-        Y[idx++] = zf * re;
-        Y[idx++] = zf * im;
+        f(idx++, zf * re);
+        f(idx++, zf * im);
         const float r2 = ux * re - uy * im;
         im = ux * im + uy * re;
         re = r2;
@@ -596,14 +598,10 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
         for (int n = 0; n < CN; ++n)
           g[n] = (nc + n < nA) ? dot_basis<KM>(c + n * Lay.kpa, fn) : 0.0f;
         const float dinv = 1.0f / d;
-        float Y[NLM];
+        for_each_harmonic<LMAX>(p.L_max, dx * dinv, dy * dinv, dz * dinv, [&](int lm, float y) {
 #pragma unroll
-        for (int lm = 0; lm < NLM; ++lm) Y[lm] = 0.0f;
-        harmonics<LMAX>(p.L_max, dx * dinv, dy * dinv, dz * dinv, Y);
-#pragma unroll
-        for (int n = 0; n < CN; ++n)
-#pragma unroll
-          for (int lm = 0; lm < NLM; ++lm) v[n * NLM + lm] += g[n] * Y[lm];
+          for (int n = 0; n < CN; ++n) v[n * NLM + lm] += g[n] * y;
+        });
       }
     }
     const int at = reduce_scatter<G, CN * NLM>(v, gl);
