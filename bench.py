@@ -62,7 +62,7 @@ K_B = 8.617343e-5
 # DRAM bytes per force call of the descriptor stage from the committed ncu
 # captures (profiles/descriptor_kernels_water24k.md): k_filter_radial +
 # k_nep_fused + k_angular_f12
-TRAFFIC = {"water": 18.72e6 + 6.93e6 + 17.97e6}
+TRAFFIC = {"water": 18.78e6 + 6.94e6 + 17.97e6}
 FP32_LANES = 148 * 128          # B200: SMs x FP32 lanes
 SM_MAX_MHZ = 1965.0
 
@@ -449,6 +449,43 @@ def run_reference_arm(args, rank):
     return 0
 
 
+
+class Ranks:
+    """Rank plumbing of the replica runs (one independent system per GPU, no
+    collective on the data path): barriers and the max / sum over ranks of a
+    scalar, on the initialised process group (NCCL on GPUs, gloo on CPU).
+    With no group every operation is the identity."""
+
+    def __init__(self, dist=None, device="cpu"):
+        self.dist = dist
+        self.device = device
+
+    def barrier(self):
+        if self.dist:
+            self.dist.barrier()
+
+    def _reduce(self, x, op):
+        if not self.dist:
+            return float(x)
+        import torch
+        t = torch.tensor([float(x)], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    def max(self, x):
+        return self._reduce(x, self.dist.ReduceOp.MAX if self.dist else None)
+
+    def sum(self, x):
+        return self._reduce(x, self.dist.ReduceOp.SUM if self.dist else None)
+
+
+def replica_rate(units_per_rank, steps, ms_per_rank, ranks):
+    """Whole-job throughput of N replicas: every rank's units over the
+    slowest rank's time (max over ranks)."""
+    total = ranks.sum(units_per_rank)
+    ms = ranks.max(ms_per_rank)
+    return total * steps / (ms / 1e3), ms
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -487,6 +524,7 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
+    ranks = Ranks(dist, "cuda")
     import nepx
 
     spec = WORKLOADS[args.workload]
@@ -516,8 +554,7 @@ def main():
     gpu_id = getattr(props, "uuid", None)
     gpu_id = ("GPU-" + str(gpu_id)) if gpu_id is not None else local
     clocks = ClockSampler(gpu_id)
-    if dist:
-        dist.barrier()
+    ranks.barrier()
     torch.cuda.synchronize()
     clocks.start()
     time.sleep(0.2)
@@ -530,32 +567,21 @@ def main():
     md.sync()
     torch.cuda.synchronize()
     clock_info = clocks.stop()
-    if dist:
-        dist.barrier()
-    dev_ms = sum(a.elapsed_time(b) for a, b in ev)
+    ranks.barrier()
+    value, dev_ms = replica_rate(n, K, sum(a.elapsed_time(b) for a, b in ev), ranks)
     atoms_total = n * world
-    if dist:
-        tt = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        dev_ms = float(tt.item())
-    value = atoms_total * K / (dev_ms / 1e3)
     kernels_per_step = 13 + (2 if kind == "nvt_nhc" else 0)
     launches = K * kernels_per_step + len(chunks)
 
     # end to end through the public API: one nepx_md_run per step
     rows = np.zeros((1, len(nepx.THERMO_COLUMNS)))
-    if dist:
-        dist.barrier()
+    ranks.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(K):
         rows = md.run(1, dt, thermo_every=1)
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        tt = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
-    e2e = {"value": atoms_total * K / e2e_s, "unit": "atom-steps/s",
+    e2e_value, _ = replica_rate(n, K, (time.perf_counter() - t0) * 1e3, ranks)
+    e2e = {"value": e2e_value, "unit": "atom-steps/s",
            "h2d_bytes_per_step": 3 * 8,           # the step's stochastic draws
            "d2h_bytes_per_step": 20 * 8 + 4 + 232 + 56,   # thermo row, status, box, flags
            "api": "nepx_md_run(steps=1, thermo_every=1) per step"}
@@ -572,8 +598,7 @@ def main():
     stream = torch.cuda.ExternalStream(stream_ptr)
     ev_m = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
             for _ in chunks]
-    if dist:
-        dist.barrier()
+    ranks.barrier()
     torch.cuda.synchronize()
     for c, steps in enumerate(chunks):
         with torch.cuda.stream(stream):
@@ -583,12 +608,7 @@ def main():
         ev_m[c][1].record(stream)
     md.sync()
     torch.cuda.synchronize()
-    dev_ms_m = sum(a.elapsed_time(b) for a, b in ev_m)
-    if dist:
-        tt = torch.tensor([dev_ms_m], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        dev_ms_m = float(tt.item())
-    value_mixed = atoms_total * K / (dev_ms_m / 1e3)
+    value_mixed, dev_ms_m = replica_rate(n, K, sum(a.elapsed_time(b) for a, b in ev_m), ranks)
     launches += K * (kernels_per_step + 5) + len(chunks)   # + type sort, tcgen05 ANN, k_acoef
 
     # per-kernel profile of the force path on the final state of the FP32
