@@ -419,6 +419,37 @@ def gpu_reference_rate(nep_path, t, h, p, reps=50):
                       % (reps, n)}
 
 
+def mixed_sweep():
+    """Force-call time of the FP32 and mixed-precision paths on the water
+    system (24,000 atoms) for NEP models of growing descriptor and ANN size
+    (two types, basis 8/8, l_max 4 2 1, the water workload's cutoffs and
+    weight distribution): where the tensor-core ANN starts to pay.  Device
+    time per call from nepx_profile (best of three sets of 30 calls, L2 warm)."""
+    import torch
+    import nepx
+    t, h, p = build_system("water", seed=1)
+    tt = torch.as_tensor(np.asarray(t, dtype=np.int32), device="cuda")
+    pp = torch.as_tensor(np.ascontiguousarray(p), device="cuda")
+    out = []
+    for nmax, H in [((4, 4), 50), ((4, 4), 100), ((8, 8), 64), ((8, 8), 100), ((8, 8), 200),
+                    ((12, 8), 120)]:
+        spec = dict(WORKLOADS["water"]["nep"], n_max=nmax, H=H, l_max=(4, 2, 1))
+        path = workloads.write_nep(os.path.join(tempfile.mkdtemp(), "nep.txt"), **spec)
+        pot = nepx.Potential(path, max_atoms=len(t))
+        us = {}
+        for prec in ("fp32", "mixed"):
+            pot.set_precision(prec)
+            pot.compute(tt, h, pp, sync_check=True)
+            best = min((pot.profile(tt, h, pp, reps=30) for _ in range(3)),
+                       key=lambda d: d["total"])
+            us[prec] = best["total"] * 1000.0
+        out.append({"n_max": list(nmax), "H": H, "dim": pot.info["dim"],
+                    "fp32_us": round(us["fp32"], 1), "mixed_us": round(us["mixed"], 1),
+                    "mixed_over_fp32": round(us["fp32"] / us["mixed"], 3)})
+        pot.close()
+    return {"mixed_sweep": out, "workload": WORKLOADS["water"]["desc"]}
+
+
 def run_reference_arm(args, rank):
     if rank != 0:
         return 0
@@ -498,6 +529,8 @@ def main():
     ap.add_argument("--plain-sample", type=int, default=200)
     ap.add_argument("--chunk", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mixed-sweep", action="store_true",
+                    help="print FP32 vs mixed force-call times over NEP model sizes and exit")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the NVE-drift and serving-sample measurements")
     ap.add_argument("--serving-sample", type=int, default=600)
@@ -514,6 +547,10 @@ def main():
     if args.workload == "serving":
         if rank == 0:
             print(json.dumps(run_serving(args)))
+        return 0
+    if args.mixed_sweep:
+        if rank == 0:
+            print(json.dumps(mixed_sweep()))
         return 0
 
     import torch
