@@ -33,6 +33,7 @@
 //    gpu_find_force_many_body (potential.cu:81-210), find_force_ZBL
 //    (nep.cu:996-1111).
 #include <cstdio>
+#include <mutex>
 
 #include "engine.h"
 #include "harmonic_tables.h"
