@@ -72,6 +72,7 @@ std::string engine_create(Engine& e, const std::string& nep_path, int max_atoms)
 {
   std::string err = load_nep(nep_path, e.model);
   if (!err.empty()) return err;
+  if (cudaGetDevice(&e.device) != cudaSuccess) return "no CUDA device";
   const NepModel& m = e.model;
   ModelParams& p = e.params;
   std::memset(&p, 0, sizeof(p));

@@ -64,6 +64,7 @@ struct Engine {
   NepModel model;
   ModelParams params{};
   int capacity = 0;          // atoms the buffers are sized for
+  int device = 0;            // the CUDA device current at creation, which owns every buffer
   double skin = 1.0;         // Verlet skin (A), the reference's default
   // device copies of the model
   float* d_params = nullptr; // one allocation holding all parameter blocks

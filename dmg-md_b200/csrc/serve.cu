@@ -300,6 +300,8 @@ void nepx_server::run()
 {
   using namespace nepx;
   Engine& e = h->engine;
+  // a new host thread starts on device 0: work on the handle's device
+  cudaSetDevice(e.device);
   cudaStream_t s = stream;
   std::vector<Resident> res;   // arena order
   int T = 0;                   // atoms in the current arena

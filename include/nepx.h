@@ -1,9 +1,12 @@
 /*
  * nepx.h -- C ABI of the B200-native NEP molecular-dynamics engine.
  *
- * Plain pointers and sizes only.  Device pointers are CUDA device memory of
- * the calling process's current device; `stream` is a cudaStream_t (NULL =
- * legacy default stream).  Every function returns 0 (NEPX_OK) or a positive
+ * Plain pointers and sizes only.  A handle belongs to the CUDA device that is
+ * current when it is created; calls on it expect that device to be current
+ * (as cuBLAS handles do), and device pointers are memory of that device.
+ * Handles are independent: different host threads may use different handles
+ * at the same time.  `stream` is a cudaStream_t (NULL = legacy default
+ * stream).  Every function returns 0 (NEPX_OK) or a positive
  * NEPX_ERR_* code; nepx_last_error() gives the message.  No function exits
  * the process.
  *
