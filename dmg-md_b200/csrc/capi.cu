@@ -55,16 +55,27 @@ int check_state(nepx_handle* h, bool wait)
 
 }  // namespace
 
+// Why the last nepx_create of this thread failed (no handle to hold it).
+thread_local std::string t_create_error;
+
 extern "C" {
 
 int nepx_create(const char* nep_path, int max_atoms, nepx_t** out)
 {
-  if (!nep_path || !out || max_atoms < 1) return NEPX_ERR_ARG;
+  t_create_error.clear();
+  if (!nep_path || !out || max_atoms < 1) {
+    t_create_error = "nepx_create: null path or handle pointer, or max_atoms < 1";
+    return NEPX_ERR_ARG;
+  }
   *out = nullptr;
   auto* h = new (std::nothrow) nepx_handle();
-  if (!h) return NEPX_ERR_ARG;
+  if (!h) {
+    t_create_error = "nepx_create: out of host memory";
+    return NEPX_ERR_CAPACITY;
+  }
   std::string err = nepx::engine_create(h->engine, nep_path, max_atoms);
   if (!err.empty()) {
+    t_create_error = "nepx_create: " + err;
     int code = NEPX_ERR_FILE;
     if (err.find("cuda") != std::string::npos || err.find("CUDA") != std::string::npos)
       code = NEPX_ERR_CUDA;
@@ -79,6 +90,7 @@ int nepx_create(const char* nep_path, int max_atoms, nepx_t** out)
       cudaEventCreateWithFlags(&h->state_ready, cudaEventDisableTiming) != cudaSuccess) {
     nepx::engine_destroy(h->engine);
     delete h;
+    t_create_error = "nepx_create: pinned host buffer or event creation failed";
     return NEPX_ERR_CUDA;
   }
   std::memset(h->h_state, 0, sizeof(nepx::NeighborState));
@@ -99,7 +111,7 @@ int nepx_destroy(nepx_t* h)
 
 const char* nepx_last_error(const nepx_t* h)
 {
-  if (!h) return "null handle";
+  if (!h) return t_create_error.empty() ? "null handle" : t_create_error.c_str();
   return h->error.c_str();
 }
 

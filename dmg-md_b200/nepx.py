@@ -166,7 +166,7 @@ class Potential:
         self._h = ctypes.c_void_p()
         rc = lib().nepx_create(os.fsencode(path), int(max_atoms), ctypes.byref(self._h))
         if rc:
-            raise NepxError(rc, "nepx_create(%s) failed" % path)
+            raise NepxError(rc, lib().nepx_last_error(None).decode())
         info = (ctypes.c_int * 16)()
         rcs = (ctypes.c_double * 32)()
         lib().nepx_info(self._h, info, rcs)

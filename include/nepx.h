@@ -60,7 +60,8 @@ int nepx_create(const char* nep_path, int max_atoms, nepx_t** out);
 /* Frees the handle and its device memory.  Replaces NEP::~NEP (nep.cu:397). */
 int nepx_destroy(nepx_t* handle);
 
-/* Message of the last error of this handle (never NULL). */
+/* Message of the last error of this handle (never NULL).  With handle NULL:
+ * why this thread's last nepx_create failed ("null handle" if it did not). */
 const char* nepx_last_error(const nepx_t* handle);
 
 /*

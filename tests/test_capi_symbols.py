@@ -29,4 +29,8 @@ def test_create_rejects_bad_arguments():
     h = ctypes.c_void_p()
     assert lib.nepx_create(None, 10, ctypes.byref(h)) == 1
     assert lib.nepx_create(b"/nonexistent/nep.txt", 0, ctypes.byref(h)) == 1
-    assert lib.nepx_last_error(None) == b"null handle"
+    assert b"max_atoms" in lib.nepx_last_error(None)
+    # the reason of a failed create is kept for this thread (no handle exists)
+    assert lib.nepx_create(b"/nonexistent/nep.txt", 10, ctypes.byref(h)) == 2
+    msg = lib.nepx_last_error(None)
+    assert msg.startswith(b"nepx_create: ") and b"/nonexistent/nep.txt" in msg
