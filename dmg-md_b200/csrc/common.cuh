@@ -148,6 +148,51 @@ __device__ __forceinline__ void site_displacement(const Box& b, const Site* __re
   site_delta(b, a, c, xi, yi, zi, dx, dy, dz, tj);
 }
 
+// Skin criterion of atom i at its new position (reference
+// neighbor.cu:446-533, without the host round trip): packs its Site record
+// for this step's neighbour sweeps and marks a rebuild when forced or when
+// it moved more than skin/2 since the build.  Under an isotropic box scaling
+// s since the build (x0 scaled along, so displacements are co-moving) a pair
+// distance also drifts by up to |1 - s| (rc + skin), which shrinks the
+// allowed displacement to (skin - |1 - s| (rc + skin)) / 2.  A general
+// deformation M since the build moves a pair by at most ||M - I||_2
+// (rc + skin); the bound used is sqrt(||M - I||_1 ||M - I||_inf) >= ||M - I||_2.
+__device__ __forceinline__ void skin_check_atom(int N, int i, const Box& b, double xi, double yi,
+                                                double zi, int type_i,
+                                                const double* __restrict__ x0, NeighborState* st,
+                                                Site* __restrict__ sites, double skin,
+                                                double rc_v, int force)
+{
+  sites[i] = Site{xi, yi, zi, static_cast<long long>(type_i)};
+  if (force) {
+    if (i == 0) st->rebuild = 1;
+    return;
+  }
+  double col[3] = {0.0, 0.0, 0.0}, row_max = 0.0;
+  for (int r = 0; r < 3; ++r) {
+    double row = 0.0;
+    for (int c = 0; c < 3; ++c) {
+      const double a = fabs(st->box_def[3 * r + c] - (r == c ? 1.0 : 0.0));
+      row += a;
+      col[c] += a;
+    }
+    row_max = fmax(row_max, row);
+  }
+  const double def = sqrt(fmax(fmax(col[0], col[1]), col[2]) * row_max);
+  const double strain = fmax(fabs(1.0 - st->box_scale), def);
+  const double half = 0.5 * (skin - strain * rc_v);
+  if (half <= 0.0) {
+    st->rebuild = 1;
+    return;
+  }
+  const double half_skin_sq = half * half;
+  float dx = xi - x0[i];
+  float dy = yi - x0[N + i];
+  float dz = zi - x0[2 * N + i];
+  mic_f32(b, dx, dy, dz);
+  if ((dx * dx + dy * dy + dz * dz) > half_skin_sq) st->rebuild = 1;
+}
+
 // Cutoff function fc = (1 + cos(pi d / rc)) / 2 and its d-derivative.
 __device__ __forceinline__ void cutoff_fc(float rc, float rcinv, float d, float& fc, float& fcp)
 {

@@ -118,8 +118,10 @@ void launch_set_box(Engine& e, const Box& b, cudaStream_t stream);
 // Site packing, skin check and conditional Verlet rebuild.  The force
 // launches read positions and types from the packed sites, so every force
 // launch follows a neighbour update at the same positions.
+// skin_done: the caller has packed the site records and applied the skin
+// criterion itself (the MD step does it in its first half kick).
 void launch_neighbor_update(Engine& e, int N, const double* pos, const int* type, bool force,
-                            cudaStream_t stream);
+                            cudaStream_t stream, bool skin_done = false);
 
 // Explicit rows: allocates them for the handle's capacity and max_struct
 // structures (once; later calls only check the size).

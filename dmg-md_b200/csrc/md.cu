@@ -106,11 +106,23 @@ __global__ void k_nhc_pre(StepParams p, MdScalars* sc, const double* __restrict_
                                   3.0 * p.N, p.dt * 0.5);
 }
 
+// Skin check of the large-box neighbour path, done by k_vv1 on the new
+// positions (enabled = 0: explicit rows, nothing to check).
+struct SkinArgs {
+  const int* type;
+  const double* x0;
+  NeighborState* st;
+  Site* sites;
+  double skin, rc_v;
+  int enabled;
+};
+
 // v = v * f_pre + F/m dt/2 ; x += v dt ; wrap into the cell
-// (runtime.cu:392-421, runtime_internal.hpp:648-681)
+// (runtime.cu:392-421, runtime_internal.hpp:648-681); then the skin check
+// of the new position.
 __global__ void k_vv1(StepParams p, const Box* __restrict__ box, const double* __restrict__ mass,
                       const double* __restrict__ force, double* pos, double* vel,
-                      const MdScalars* __restrict__ sc)
+                      const MdScalars* __restrict__ sc, SkinArgs sk)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= p.N) return;
@@ -133,8 +145,14 @@ __global__ void k_vv1(StepParams p, const Box* __restrict__ box, const double* _
       else if (s[d] > 1.0) s[d] -= 1.0;
     }
   }
-  for (int d = 0; d < 3; ++d)
-    pos[d * N + i] = b.h[3 * d] * s[0] + b.h[3 * d + 1] * s[1] + b.h[3 * d + 2] * s[2];
+  double x[3];
+  for (int d = 0; d < 3; ++d) {
+    x[d] = b.h[3 * d] * s[0] + b.h[3 * d + 1] * s[1] + b.h[3 * d + 2] * s[2];
+    pos[d * N + i] = x[d];
+  }
+  if (sk.enabled)
+    skin_check_atom(N, i, b, x[0], x[1], x[2], sk.type[i], sk.x0, sk.st, sk.sites, sk.skin,
+                    sk.rc_v, 0);
 }
 
 // second half kick and the FP64 thermo partial sums (runtime.cu:442-493)
@@ -258,17 +276,24 @@ __device__ bool apply_component_coupling(const StepParams& p, Box& b, const doub
 
 // Thermo normalisation, thermostat and barostat scalars, box update and the
 // thermo row of this step (ensemble_control.cpp:180-306, npt_scr.cpp:21-33,
-// box_control.cpp:9-68).  One block: 8 threads reduce the partials in a
-// fixed order, thread 0 does the scalar work.
-__global__ void k_ensemble(StepParams p, Box* box, MdScalars* sc, const double* __restrict__ partials,
-                           int nblocks, const double* __restrict__ noise, double* rows,
-                           int rows_cap, NeighborState* nstate, int* status)
+// box_control.cpp:9-68).  One block of 8 warps: warp q reduces quantity q
+// of the block partials (lane l takes blocks l, l + 32, ..., then a fixed
+// shuffle tree: a fixed order, so the sums are reproducible), thread 0 does
+// the scalar work.
+constexpr int kEnsembleThreads = 256;
+__global__ void __launch_bounds__(kEnsembleThreads)
+k_ensemble(StepParams p, Box* box, MdScalars* sc, const double* __restrict__ partials,
+           int nblocks, const double* __restrict__ noise, double* rows, int rows_cap,
+           NeighborState* nstate, int* status)
 {
   __shared__ double s_sum[8];
-  if (threadIdx.x < 8) {
+  {
+    const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double acc = 0.0;
-    for (int b = 0; b < nblocks; ++b) acc += partials[b * 8 + threadIdx.x];
-    s_sum[threadIdx.x] = acc;
+    for (int b = lane; b < nblocks; b += 32) acc += partials[b * 8 + q];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if (lane == 0) s_sum[q] = acc;
   }
   __syncthreads();
   if (threadIdx.x != 0) return;
@@ -425,13 +450,17 @@ void md_enqueue_step(Md& md, const StepParams& p, int* d_status)
     k_ke_partials<<<blocks, kThreads, 0, s>>>(N, md.d_mass, md.d_vel, md.d_partials);
     k_nhc_pre<<<1, 1, 0, s>>>(p, md.d_sc, md.d_partials, blocks);
   }
-  k_vv1<<<blocks, kThreads, 0, s>>>(p, e.d_box, md.d_mass, md.d_force, md.d_pos, md.d_vel, md.d_sc);
-  launch_neighbor_update(e, N, md.d_pos, md.d_type, false, s);
+  const SkinArgs sk{md.d_type, e.nbr.x0, e.d_nstate, e.scratch.sites, e.skin,
+                    static_cast<double>(e.model.rc_max) + e.skin, e.use_xr ? 0 : 1};
+  k_vv1<<<blocks, kThreads, 0, s>>>(p, e.d_box, md.d_mass, md.d_force, md.d_pos, md.d_vel, md.d_sc,
+                                    sk);
+  launch_neighbor_update(e, N, md.d_pos, md.d_type, false, s, sk.enabled != 0);
   launch_force(e, N, md.d_pos, md.d_type, md.d_pe, md.d_force, md.d_virial, false, s);
   k_vv2_thermo<<<blocks, kThreads, 0, s>>>(p, md.d_mass, md.d_force, md.d_vel, md.d_pe,
                                           md.d_virial, md.d_partials);
-  k_ensemble<<<1, 32, 0, s>>>(p, e.d_box, md.d_sc, md.d_partials, blocks, md.d_noise, md.d_rows,
-                              md.rows_cap, e.d_nstate, d_status);
+  k_ensemble<<<1, kEnsembleThreads, 0, s>>>(p, e.d_box, md.d_sc, md.d_partials, blocks,
+                                            md.d_noise, md.d_rows, md.rows_cap, e.d_nstate,
+                                            d_status);
   k_scale<<<blocks, kThreads, 0, s>>>(N, md.d_vel, md.d_pos, e.nbr.x0, md.d_sc);
 }
 

@@ -44,14 +44,8 @@ __device__ __forceinline__ void cell_coords(const Box& b, const NeighborState& s
 }
 
 // Packs each atom into its Site record for the neighbour sweeps of this
-// step, and marks a rebuild when forced or when an atom moved more than
-// skin/2 (reference neighbor.cu:446-533, without the host round trip).  Under
-// an isotropic box scaling s since the build (x0 scaled along, so
-// displacements are co-moving) a pair distance also drifts by up to
-// |1 - s| (rc + skin), which shrinks the allowed displacement to
-// (skin - |1 - s| (rc + skin)) / 2.  A general deformation M since the build
-// moves a pair by at most ||M - I||_2 (rc + skin); the bound used is
-// sqrt(||M - I||_1 ||M - I||_inf) >= ||M - I||_2.
+// step and applies the skin criterion (skin_check_atom, common.cuh).  The MD
+// step does the same inside its first half kick instead.
 __global__ void k_skin_check(int N, const Box* __restrict__ box, const double* __restrict__ pos,
                              const int* __restrict__ type, const double* __restrict__ x0,
                              NeighborState* st, Site* __restrict__ sites, double skin,
@@ -59,35 +53,8 @@ __global__ void k_skin_check(int N, const Box* __restrict__ box, const double* _
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
-  const double xi = pos[i], yi = pos[N + i], zi = pos[2 * N + i];
-  sites[i] = Site{xi, yi, zi, static_cast<long long>(type[i])};
-  if (force) {
-    if (i == 0) st->rebuild = 1;
-    return;
-  }
-  double col[3] = {0.0, 0.0, 0.0}, row_max = 0.0;
-  for (int r = 0; r < 3; ++r) {
-    double row = 0.0;
-    for (int c = 0; c < 3; ++c) {
-      const double a = fabs(st->box_def[3 * r + c] - (r == c ? 1.0 : 0.0));
-      row += a;
-      col[c] += a;
-    }
-    row_max = fmax(row_max, row);
-  }
-  const double def = sqrt(fmax(fmax(col[0], col[1]), col[2]) * row_max);
-  const double strain = fmax(fabs(1.0 - st->box_scale), def);
-  const double half = 0.5 * (skin - strain * rc_v);
-  if (half <= 0.0) {
-    st->rebuild = 1;
-    return;
-  }
-  const double half_skin_sq = half * half;
-  float dx = xi - x0[i];
-  float dy = yi - x0[N + i];
-  float dz = zi - x0[2 * N + i];
-  mic_f32(*box, dx, dy, dz);
-  if ((dx * dx + dy * dy + dz * dz) > half_skin_sq) st->rebuild = 1;
+  skin_check_atom(N, i, *box, pos[i], pos[N + i], pos[2 * N + i], type[i], x0, st, sites, skin,
+                  rc_v, force);
 }
 
 // Cell grid from the current box (cells at least rc_v/2 thick, at most
@@ -276,7 +243,7 @@ __global__ void k_verlet_build(int N, const Box* __restrict__ box, const Site* _
 }  // namespace
 
 void launch_neighbor_update(Engine& e, int N, const double* pos, const int* type, bool force,
-                            cudaStream_t stream)
+                            cudaStream_t stream, bool skin_done)
 {
   if (e.use_xr) {
     launch_explicit_rows(e, N, pos, type, stream);
@@ -287,8 +254,9 @@ void launch_neighbor_update(Engine& e, int N, const double* pos, const int* type
   const int grid = (N + threads - 1) / threads;
   const float rc_v = e.model.rc_max + static_cast<float>(e.skin);
   const double rc_v_d = static_cast<double>(e.model.rc_max) + e.skin;
-  k_skin_check<<<grid, threads, 0, stream>>>(N, e.d_box, pos, type, nb.x0, e.d_nstate,
-                                              e.scratch.sites, e.skin, rc_v_d, force ? 1 : 0);
+  if (!skin_done)
+    k_skin_check<<<grid, threads, 0, stream>>>(N, e.d_box, pos, type, nb.x0, e.d_nstate,
+                                                e.scratch.sites, e.skin, rc_v_d, force ? 1 : 0);
   k_cell_setup<<<1, 1024, 0, stream>>>(e.d_box, e.d_nstate, nb.cell_count, rc_v_d, nb.cell_cap);
   k_cell_count<<<grid, threads, 0, stream>>>(N, e.d_box, pos, e.d_nstate, nb.cell_of,
                                              nb.cell_count);
