@@ -587,6 +587,7 @@ int nepx_md_destroy(nepx_md_t* m)
   nepx::Md& md = m->md;
   if (md.stream) cudaStreamSynchronize(md.stream);
   if (md.graph) cudaGraphExecDestroy(md.graph);
+  if (md.graph_multi) cudaGraphExecDestroy(md.graph_multi);
   void* ptrs[] = {md.d_type, md.d_mass, md.d_pos, md.d_vel, md.d_force, md.d_pe, md.d_virial,
                   md.d_partials, md.d_sc, md.d_noise, md.d_rows};
   for (void* p : ptrs)
@@ -760,25 +761,35 @@ int md_enqueue_run(nepx_md* m, int steps, double dt_fs, int thermo_every, double
   e.force_rebuild = true;     // a later nepx_compute on this handle rebuilds
   e.have_box = false;
   int* d_status = status_buffer(m);
-  // capture one step as a graph (re-captured when the per-run constants change)
+  // capture one step, and kGraphSteps steps back to back, as graphs (the step
+  // counter lives on the device, so consecutive steps are the same kernels;
+  // re-captured when the per-run constants change)
   if (!md.graph || std::memcmp(&p, &md.graph_params, sizeof(p)) != 0 ||
       md.graph_precision != e.precision) {
-    if (md.graph) cudaGraphExecDestroy(md.graph);
-    md.graph = nullptr;
-    cudaGraph_t g;
-    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
-      return md_cuda(m, "begin capture");
-    nepx::md_enqueue_step(md, p, d_status);
-    if (cudaStreamEndCapture(s, &g) != cudaSuccess) return md_cuda(m, "end capture");
-    if (cudaGraphInstantiate(&md.graph, g, 0) != cudaSuccess) {
-      cudaGraphDestroy(g);
-      return md_cuda(m, "instantiate graph");
+    for (cudaGraphExec_t* x : {&md.graph, &md.graph_multi}) {
+      if (*x) cudaGraphExecDestroy(*x);
+      *x = nullptr;
     }
-    cudaGraphDestroy(g);
+    for (int reps : {1, nepx::kGraphSteps}) {
+      cudaGraph_t g;
+      if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return md_cuda(m, "begin capture");
+      for (int r = 0; r < reps; ++r) nepx::md_enqueue_step(md, p, d_status);
+      if (cudaStreamEndCapture(s, &g) != cudaSuccess) return md_cuda(m, "end capture");
+      cudaGraphExec_t& x = reps == 1 ? md.graph : md.graph_multi;
+      if (cudaGraphInstantiate(&x, g, 0) != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return md_cuda(m, "instantiate graph");
+      }
+      cudaGraphDestroy(g);
+    }
     md.graph_params = p;
     md.graph_precision = e.precision;
   }
-  for (int k = 0; k < steps; ++k)
+  int k = 0;
+  for (; k + nepx::kGraphSteps <= steps; k += nepx::kGraphSteps)
+    if (cudaGraphLaunch(md.graph_multi, s) != cudaSuccess) return md_cuda(m, "graph launch");
+  for (; k < steps; ++k)
     if (cudaGraphLaunch(md.graph, s) != cudaSuccess) return md_cuda(m, "graph launch");
   // device-side status, box and neighbour flags land in pinned memory
   cudaMemcpyAsync(&m->mirror->box, e.d_box, sizeof(nepx::Box), cudaMemcpyDeviceToHost, s);

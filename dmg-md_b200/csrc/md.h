@@ -33,6 +33,7 @@ struct EnsembleConfig {
 };
 
 constexpr int kChain = 4;      // Nose-Hoover chain length
+constexpr int kGraphSteps = 8;   // steps per replay of the multi-step graph
 constexpr int kThermoCols = 20;  // thermo.out's 18 columns + velocity and box factors
 
 // Scalars the per-step kernels share, resident on the device.
@@ -87,10 +88,10 @@ struct Md {
   bool forces_valid = false;
   bool xr = false;                // explicit-row (small-box) force path
   cudaStream_t stream = nullptr;
-  cudaGraphExec_t graph = nullptr;
+  cudaGraphExec_t graph = nullptr;        // one step
+  cudaGraphExec_t graph_multi = nullptr;  // kGraphSteps steps back to back
   StepParams graph_params{};
   int graph_precision = -1;       // ANN precision the graph's kernels were captured with
-  int graph_steps = 0;
 };
 
 }  // namespace nepx
