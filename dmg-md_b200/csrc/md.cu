@@ -749,6 +749,10 @@ int md_enqueue_run(nepx_md* m, int steps, double dt_fs, int thermo_every, double
   if (e.box_owner != &md) {
     nepx::launch_set_box(e, md.box, s);
     e.box_owner = &md;
+    // the engine served another caller: its Verlet rows and type order
+    // belong to that system
+    if (md.forces_valid) nepx::launch_neighbor_update(e, N, md.d_pos, md.d_type, true, s);
+    e.order_valid = false;
   }
   if (first_step == 0) nepx::md_init_scalars(md, p, c.T0, p.dt * c.Tdamp);
   else nepx::md_continue_scalars(md);
@@ -757,6 +761,12 @@ int md_enqueue_run(nepx_md* m, int steps, double dt_fs, int thermo_every, double
     if (!e.tuned) nepx::engine_autotune(e, N, md.d_pos, md.d_type, s);
     nepx::launch_force(e, N, md.d_pos, md.d_type, md.d_pe, md.d_force, md.d_virial, false, s);
     md.forces_valid = true;
+  }
+  // a valid type order before the step graph is captured, whose sort then
+  // runs only on rebuild steps
+  if (e.precision == 1 && !md.xr && !e.order_valid) {
+    nepx::launch_type_order(e, N, true, s);
+    e.order_valid = true;
   }
   e.force_rebuild = true;     // a later nepx_compute on this handle rebuilds
   e.have_box = false;
