@@ -26,8 +26,9 @@ roofline -- the dominant kernel (fused descriptor/ANN/angular-force kernel),
           FMA peak of B200 (148 SMs x 128 lanes x 2 FLOP x max SM clock).
 cpu_baseline -- the reference's own FP64 CPU NEP evaluator (NEP3_CPU,
           oracle/_ref) over the full system on all host cores, force call,
-          on the final MD state; the same FP64 values give err_vs_fp64 (force
-          RMSE and energy error of the FP32 and mixed paths).
+          on the final MD state (md_step: with a CPU velocity-Verlet update
+          around it); the same FP64 values give err_vs_fp64 (force RMSE and
+          energy error of the FP32 and mixed paths).
 mixed_precision -- the same MD with the ANN on the tcgen05 tensor cores.
 nve_drift -- NVE energy drift (eV/atom/ns) of 4096-atom diamond carbon,
           20,000 steps of 1 fs, both precisions.
@@ -325,6 +326,26 @@ def cpu_reference_rate(nep_path, t, h, p, budget_s=8.0, max_reps=5, want_result=
     line = {"value": len(t) / sec, "unit": "atom-steps/s", "cores": threads, "kind": "reference",
             "sample": "NEP3_CPU (reference FP64 CPU evaluator) force call on all %d atoms, "
                       "median of %d calls, %d threads" % (len(t), len(times), threads)}
+    # with a CPU velocity-Verlet loop around it: both half kicks, the drift and
+    # the wrap into the box (FP64, vectorised over atoms)
+    n = len(t)
+    L = np.diag(np.asarray(h, dtype=np.float64).reshape(3, 3))[:, None]
+    x = np.array(p, dtype=np.float64)
+    v = np.zeros_like(x)
+    f = np.asarray(result[1]) if result is not None else np.zeros_like(x)
+    inv_m = np.ones(n)
+    vv = []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        v += 0.5 * 1e-3 * f * inv_m
+        x += 1e-3 * v
+        x -= np.floor(x / L) * L
+        v += 0.5 * 1e-3 * f * inv_m
+        vv.append(time.perf_counter() - t0)
+    vv_s = statistics.median(vv)
+    line["md_step"] = {"value": n / (sec + vv_s), "unit": "atom-steps/s",
+                       "what": "force call plus a CPU velocity-Verlet update (numpy, FP64)",
+                       "vv_ms": vv_s * 1e3}
     return (line, result) if want_result else line
 
 
