@@ -628,6 +628,9 @@ def main():
     ranks.barrier()
     value, dev_ms = replica_rate(n, K, sum(a.elapsed_time(b) for a, b in ev), ranks)
     atoms_total = n * world
+    # k_vv1 (with the skin check), five Verlet-rebuild kernels (each returns at
+    # once unless a rebuild is due), k_filter_radial, k_nep_fused,
+    # k_angular_f12, k_gather, k_vv2_thermo, k_ensemble, k_scale; NHC adds two
     kernels_per_step = 13 + (2 if kind == "nvt_nhc" else 0)
     launches = K * kernels_per_step + len(chunks)
 
@@ -667,7 +670,8 @@ def main():
     md.sync()
     torch.cuda.synchronize()
     value_mixed, dev_ms_m = replica_rate(n, K, sum(a.elapsed_time(b) for a, b in ev_m), ranks)
-    launches += K * (kernels_per_step + 5) + len(chunks)   # + type sort, tcgen05 ANN, k_acoef
+    # + four type-sort kernels, the tcgen05 ANN and k_acoef
+    launches += K * (kernels_per_step + 6) + len(chunks)
 
     # per-kernel profile of the force path on the final state of the FP32
     # run, both precisions
