@@ -632,7 +632,7 @@ def main():
     # once unless a rebuild is due), k_filter_radial, k_nep_fused,
     # k_angular_f12, k_gather, k_vv2_thermo, k_ensemble, k_scale; NHC adds two
     kernels_per_step = 13 + (2 if kind == "nvt_nhc" else 0)
-    launches = K * kernels_per_step + len(chunks)
+    launches = K * kernels_per_step   # the L2-flush fills are torch's, not counted
 
     # end to end through the public API: one nepx_md_run per step
     rows = np.zeros((1, len(nepx.THERMO_COLUMNS)))
@@ -671,7 +671,7 @@ def main():
     torch.cuda.synchronize()
     value_mixed, dev_ms_m = replica_rate(n, K, sum(a.elapsed_time(b) for a, b in ev_m), ranks)
     # + four type-sort kernels, the tcgen05 ANN and k_acoef
-    launches += K * (kernels_per_step + 6) + len(chunks)
+    launches += K * (kernels_per_step + 6)
 
     # per-kernel profile of the force path on the final state of the FP32
     # run, both precisions
