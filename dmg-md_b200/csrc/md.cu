@@ -1,6 +1,7 @@
 // md.cu -- device-resident molecular dynamics: velocity Verlet in FP64 with
 // the reference's ensembles (NVE, Berendsen / Nose-Hoover chain / Bussi
-// NVT, isotropic Berendsen and stochastic-cell-rescaling NPT).
+// NVT, Berendsen and stochastic-cell-rescaling NPT with the reference's
+// isotropic coupling, plus anisotropic and triclinic couplings).
 //
 // Step order of the reference's single-rank loop (src/runtime.cu:747-848):
 //   [NHC: scale v by the pre-force chain factor]
@@ -10,7 +11,8 @@
 // are computed on the device from the FP64 thermo sums, with the stochastic
 // draws generated ahead on the host from the reference's random stream
 // (svr_rng.h).  A step therefore never synchronises with the host, and a run
-// is a CUDA graph of captured steps replayed back to back.
+// replays CUDA graphs of captured steps (eight, then single ones) back to
+// back.  The large-box path's skin check runs inside the first half kick.
 #include <cmath>
 #include <cstring>
 #include <new>

@@ -252,7 +252,6 @@ void launch_neighbor_update(Engine& e, int N, const double* pos, const int* type
   NeighborBuffers& nb = e.nbr;
   const int threads = 256;
   const int grid = (N + threads - 1) / threads;
-  const float rc_v = e.model.rc_max + static_cast<float>(e.skin);
   const double rc_v_d = static_cast<double>(e.model.rc_max) + e.skin;
   if (!skin_done)
     k_skin_check<<<grid, threads, 0, stream>>>(N, e.d_box, pos, type, nb.x0, e.d_nstate,
@@ -272,8 +271,7 @@ void launch_neighbor_update(Engine& e, int N, const double* pos, const int* type
   k_verlet_build<<<vblocks, warps * 32, smem, stream>>>(
     N, e.d_box, e.scratch.sites, e.d_nstate, nb.cell_count, nb.cell_start, nb.cell_atoms, nb.cell_of,
     nb.nn_v, nb.nl_v, nb.mn_v, nb.pow2_v, static_cast<float>(rc_v_d * rc_v_d), nb.x0);
-  (void)rc_v;
-  // the typewise radial / angular filter runs inside the fused force kernel
+  // the typewise radial / angular filter follows in k_filter_radial
 }
 
 }  // namespace nepx

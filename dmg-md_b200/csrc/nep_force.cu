@@ -1,37 +1,42 @@
-// nep_force.cu -- NEP energy, force and virial on sm_100a (plain FP32 path).
+// nep_force.cu -- NEP energy, force and virial on sm_100a.
 //
-// Two kernels per force call, each giving a group of G lanes (G = 4 or 8,
+// Four kernels per force call, each giving a group of G lanes (G = 4 or 8,
 // chosen by the autotuner in engine.cu) to one center; every phase is local
 // to the group, so no CTA-wide barrier follows the set-up.
 //
-//  k_nep_fused  (typewise filter + descriptor + ANN + angular partial forces)
-//    1. one sweep over the center's sorted Verlet row applies the reference's
-//       FP32 typewise predicate (nep.cu:503-561) and writes the radial and
-//       angular rows in order (group ballot + popcount), accumulating the
-//       radial descriptors q_n = sum_j sum_k c(ti,tj)[n][k] f_k(d_ij) on the way;
+//  k_filter_radial  one sweep over the center's sorted Verlet row applies the
+//    reference's FP32 typewise predicate (nep.cu:503-561), writes the radial
+//    and angular rows in order (group ballot + popcount) and sums the radial
+//    descriptors q_n = sum_j sum_k c(ti,tj)[n][k] f_k(d_ij) through per-type
+//    bins of the basis values.
+//  k_nep_fused  (descriptors + ANN)
+//    1. the radial descriptors (explicit rows: evaluated here);
 //    2. a sweep over the dense angular row accumulates the moments
 //       s[n][lm] = sum_j g_n(d_ij) Y_lm(r_ij/d) in registers; a register
-//       reduce-scatter across the group (3 x 60/30/15 shuffles) lands each
-//       lane's share in shared memory;
+//       reduce-scatter across the group lands each lane's share in shared
+//       memory;
 //    3. per center: invariants q_L and q_222/q_1111/q_112/q_123/q_233/q_134,
 //       the one-hidden-layer ANN (site energy, dE/dq), the moment derivatives
 //       a[n][lm] = dE/ds[n][lm], and the radial force coefficients
-//       alpha[t][k] = sum_n dE/dq_n c(ti,t)[n][k] (stored for the gather);
-//    4. a sweep over the angular row writes each directed partial force
+//       alpha[t][k] = sum_n dE/dq_n c(ti,t)[n][k] (stored for the gather).
+//    Mixed precision hands q and s to the tensor-core ANN (ann_tc.cu) and
+//    k_acoef forms a and alpha.  Reference: find_descriptor (nep.cu:569-748).
+//  k_angular_f12  each directed partial force
 //       f12(i,j) = (sum_lm B_lm Y_lm) r^ + (1/d)(I - r^r^T) sum_lm A_lm dY_lm/dr^
-//       with A_lm = sum_n a[n][lm] g_n and B_lm = sum_n a[n][lm] g'_n: the
-//       harmonic ladder runs once per edge, not once per (edge, n) as in
-//       accumulate_f12 (nep_utilities.cuh:1240-1491).
-//    Reference: find_descriptor (nep.cu:569-748), find_partial_force_angular
-//    (nep.cu:890-991).
-//
+//    with A_lm = sum_n a[n][lm] g_n and B_lm = sum_n a[n][lm] g'_n: the
+//    harmonic ladder runs once per edge, not once per (edge, n) as in
+//    accumulate_f12 (nep_utilities.cuh:1240-1491).  Reference:
+//    find_partial_force_angular (nep.cu:890-991).
 //  k_gather  radial pair force from both site energies with the per-atom
 //    alpha coefficients (w_ij = sum_k f'_k(d) alpha_i[tj][k]), the angular
 //    exchange F_i += f12(i,j) - f12(j,i) with the reverse slot found by binary
-//    search in j's sorted row, ZBL, and the per-atom virial
-//    W_i = sum_j r_ij (x) f_ji.  Reference: find_force_radial (nep.cu:756-881),
-//    gpu_find_force_many_body (potential.cu:81-210), find_force_ZBL
-//    (nep.cu:996-1111).
+//    search in j's sorted row (explicit rows: both directed forces evaluated
+//    here), ZBL, and the per-atom virial W_i = sum_j r_ij (x) f_ji.
+//    Reference: find_force_radial (nep.cu:756-881), gpu_find_force_many_body
+//    (potential.cu:81-210), find_force_ZBL (nep.cu:996-1111).
+//
+// Harmonic degree: instances for l_max <= 4 (24 moment components per n) and
+// l_max 5..8 (80 components).
 #include <cstdio>
 #include <mutex>
 
