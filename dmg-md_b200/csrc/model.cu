@@ -1,4 +1,4 @@
-// model.cpp -- NEP potential file loader.
+// model.cu -- NEP potential file loader.
 //
 // Accepts the GPUMD nep.txt format the reference reads in
 // src/gpumd_compat/nep.cu:135-415 (nep4, nep4_zbl, nep5, nep5_zbl; global or

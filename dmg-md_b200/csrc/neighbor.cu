@@ -1,5 +1,6 @@
-// neighbor.cu -- Verlet list (cutoff + skin) on a cell grid, and the per-step
-// typewise radial / angular filter.
+// neighbor.cu -- Verlet list (cutoff + skin) on a cell grid; the per-step
+// typewise radial / angular filter of its rows is k_filter_radial
+// (nep_force.cu).
 //
 // Reference behaviour (src/gpumd_compat/neighbor.cu:90-582, nep.cu:503-561):
 // the Verlet list of all pairs with float d^2 < (rc + skin)^2 is rebuilt when
