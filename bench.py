@@ -105,7 +105,8 @@ def _percentile_ms(xs, q):
 
 
 def run_serving(args):
-    """Served structures/s and p50/p99 latency of the continuous-batching
+    """Served structures/s (saturation) and p50/p99 latency (Poisson arrivals
+    at 30, 60 and 90% of saturation) of the continuous-batching
     server on a stream of independent structures (log-uniform 16..8192
     atoms; diamond C, FCC Cu, random-packed C/H/O/Cu; a fifth of the
     requests are 100-step NVE segments at dt 1 fs), next to the same
@@ -142,25 +143,34 @@ def run_serving(args):
     st = srv.stats()
     srv.close()
     rate_sat = count / wall
-    # 2. Poisson arrivals at 60% of the saturation rate: latency
-    rate = 0.6 * rate_sat
-    rng = np.random.default_rng(5)
-    arrivals = np.cumsum(rng.exponential(1.0 / rate, count))
-    srv = nepx.Server(pot, max_atoms=arena, max_struct=slots)
-    t0 = time.perf_counter()
-    tickets = []
-    for r, ta in zip(stream, arrivals):
-        dt_wait = ta - (time.perf_counter() - t0)
-        if dt_wait > 0:
-            time.sleep(dt_wait)
-        tickets.append(submit(srv, r))
-    srv.drain()
-    wall_p = time.perf_counter() - t0
-    res = [srv.wait(tk) for tk in tickets]
-    srv.close()
-    lat = [x["t_done"] - x["t_submit"] for x in res]
-    lat_sp = [x for x, r in zip(lat, stream) if r["md_steps"] == 0]
-    lat_md = [x for x, r in zip(lat, stream) if r["md_steps"] > 0]
+    # 2. Poisson arrivals at 30%, 60% and 90% of the saturation rate: latency
+    def poisson(fraction, seed):
+        rate = fraction * rate_sat
+        rng = np.random.default_rng(seed)
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, count))
+        srv = nepx.Server(pot, max_atoms=arena, max_struct=slots)
+        t0 = time.perf_counter()
+        tickets = []
+        for r, ta in zip(stream, arrivals):
+            dt_wait = ta - (time.perf_counter() - t0)
+            if dt_wait > 0:
+                time.sleep(dt_wait)
+            tickets.append(submit(srv, r))
+        srv.drain()
+        wall_p = time.perf_counter() - t0
+        res = [srv.wait(tk) for tk in tickets]
+        srv.close()
+        lat = [x["t_done"] - x["t_submit"] for x in res]
+        lat_sp = [x for x, r in zip(lat, stream) if r["md_steps"] == 0]
+        lat_md = [x for x, r in zip(lat, stream) if r["md_steps"] > 0]
+        return {"rate_fraction": fraction, "arrival_rate_per_s": rate, "wall_s": wall_p,
+                "p50": _percentile_ms(lat, 50), "p99": _percentile_ms(lat, 99),
+                "single_point_p50": _percentile_ms(lat_sp, 50),
+                "single_point_p99": _percentile_ms(lat_sp, 99),
+                "nve100_p50": _percentile_ms(lat_md, 50),
+                "nve100_p99": _percentile_ms(lat_md, 99)}
+
+    sweep = [poisson(f, 5 + k) for k, f in enumerate((0.3, 0.6, 0.9))]
     # 3. the plain path on a sample: one request at a time, host buffers in and out
     plain_pot = nepx.Potential(path, max_atoms=8192)
     step = max(1, count // max(1, args.plain_sample))
@@ -198,12 +208,8 @@ def run_serving(args):
         "atom_steps_per_s": served_rate,
         "saturation": {"wall_s": wall, "steps": st["steps"], "mean_resident_atoms":
                        st["mean_atoms"], "mean_resident_structs": st["mean_structs"]},
-        "latency_ms": {"arrival_rate_per_s": rate, "wall_s": wall_p,
-                       "p50": _percentile_ms(lat, 50), "p99": _percentile_ms(lat, 99),
-                       "single_point_p50": _percentile_ms(lat_sp, 50),
-                       "single_point_p99": _percentile_ms(lat_sp, 99),
-                       "nve100_p50": _percentile_ms(lat_md, 50),
-                       "nve100_p99": _percentile_ms(lat_md, 99)},
+        "latency_ms": sweep[1],   # Poisson arrivals at 60% of saturation
+        "latency_sweep_ms": sweep,
         "plain_fp32_one_at_a_time": {"atom_steps_per_s": plain_rate, "requests": len(sample),
                                      "wall_s": plain_wall},
         "batched_over_plain": served_rate / plain_rate,
