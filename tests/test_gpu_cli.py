@@ -124,3 +124,49 @@ def test_golden_program(tmp_path, case):
             else:
                 compare_xyz(ours, gold, restart=name == "restart.xyz")
         previous = d
+
+
+def _diamond_xyz(ncell, shear=(0.0, 0.0, 0.0)):
+    a = 3.567
+    base = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0],
+                     [.25, .25, .25], [.25, .75, .75], [.75, .25, .75], [.75, .75, .25]])
+    g = np.stack(np.meshgrid(*[np.arange(ncell)] * 3, indexing="ij"), -1).reshape(-1, 3)
+    frac = ((g[:, None, :] + base[None, :, :]).reshape(-1, 3) + 0.01) / ncell
+    L = a * ncell
+    # cell vectors as columns: a = (L, 0, 0), b = (sxy, L, 0), c = (sxz, syz, L)
+    H = np.array([[L, shear[0], shear[1]], [0.0, L, shear[2]], [0.0, 0.0, L]])
+    pos = frac @ H.T
+    lat = " ".join("%.10g" % x for x in H.T.reshape(-1))   # a, b, c vectors in turn
+    lines = ["%d" % len(pos), 'pbc="T T T" Lattice="%s" Properties=species:S:1:pos:R:3' % lat]
+    lines += ["C %.10f %.10f %.10f" % tuple(r) for r in pos]
+    return "\n".join(lines) + "\n"
+
+
+@pytest.mark.parametrize("coupling", ["anisotropic", "triclinic"])
+def test_component_barostat_program(tmp_path, coupling):
+    """nepx-md runs the 12- and 18-token npt_ber forms: the anisotropic one moves
+    the three box lengths independently and keeps the box orthogonal, the
+    triclinic one also moves the shears."""
+    shutil.copyfile(os.path.join(GOLD, "potentials", "nep_C.txt"), tmp_path / "nep.txt")
+    if coupling == "anisotropic":
+        ens = "ensemble npt_ber 300 300 100 1 0 -1 400 400 400 100"
+        model = _diamond_xyz(6)
+    else:
+        ens = "ensemble npt_ber 300 300 100 0 0 0 0.5 -0.5 0.5 400 400 400 200 200 200 100"
+        model = _diamond_xyz(6, shear=(0.8, 0.3, 0.5))
+    (tmp_path / "run.in").write_text("potential nep.txt\nvelocity 300\ntime_step 1\n%s\n"
+                                     "dump_thermo 10\nrun 100\n" % ens)
+    (tmp_path / "model.xyz").write_text(model)
+    r = subprocess.run([CLI], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    rows = np.array(thermo_rows((tmp_path / "thermo.out").read_text()))
+    assert rows.shape == (10, 18) and np.isfinite(rows).all()
+    box = rows[:, 9:18]   # ax ay az bx by bz cx cy cz
+    lengths = box[:, [0, 4, 8]]
+    assert np.ptp(lengths, axis=0).min() > 0.0          # every length moved
+    off = box[:, [1, 2, 3, 5, 6, 7]]
+    if coupling == "anisotropic":
+        assert np.all(off == 0.0)
+        assert np.ptp(lengths[-1]) > 0.0                 # the lengths moved apart
+    else:
+        assert np.ptp(box[:, 3], axis=0) > 0.0           # the shears moved
