@@ -665,64 +665,81 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
   }
   float e_part = 0.0f;
   if (active) {
-    // hidden layer: each lane owns groups of four consecutive hidden units
-    // (float4 rows of the transposed w0, four independent FMA chains,
-    // sequential in d as in the reference)
+    // hidden layer: each lane owns two groups of four consecutive hidden units
+    // (float4 rows of the transposed w0; eight independent FMA chains in one
+    // pass, each sequential in d as in the reference)
     const int hq = p.H4 / 4;
     const float4* wt =
       reinterpret_cast<const float4*>(w0t + static_cast<size_t>(t1) * dim * p.H4);
-    for (int h4 = gl; h4 < hq; h4 += G) {
+    auto finish = [&](int h, float z) {
+      if (h < H) {
+        const float x1 = tanhf(z - __ldg(p.b0 + t1 * H + h));
+        const float w1 = __ldg(p.w1 + t1 * H + h);
+        e_part += w1 * x1;
+        s_gh[h] = w1 * (1.0f - x1 * x1);
+      }
+    };
+    for (int h4 = gl; h4 < hq; h4 += 2 * G) {
+      const bool has_b = h4 + G < hq;
+      const int h4b = has_b ? h4 + G : h4;   // past the end: computed, dropped
       float z0 = 0.0f, z1 = 0.0f, z2 = 0.0f, z3 = 0.0f;
-#pragma unroll 4
+      float z4 = 0.0f, z5 = 0.0f, z6 = 0.0f, z7 = 0.0f;
+#pragma unroll 2
       for (int d = 0; d < dim; ++d) {
         const float q = s_q[d];
-        const float4 w = wt[d * hq + h4];
-        z0 = fmaf(w.x, q, z0);
-        z1 = fmaf(w.y, q, z1);
-        z2 = fmaf(w.z, q, z2);
-        z3 = fmaf(w.w, q, z3);
+        const float4 wa = wt[d * hq + h4];
+        const float4 wb = wt[d * hq + h4b];
+        z0 = fmaf(wa.x, q, z0);
+        z1 = fmaf(wa.y, q, z1);
+        z2 = fmaf(wa.z, q, z2);
+        z3 = fmaf(wa.w, q, z3);
+        z4 = fmaf(wb.x, q, z4);
+        z5 = fmaf(wb.y, q, z5);
+        z6 = fmaf(wb.z, q, z6);
+        z7 = fmaf(wb.w, q, z7);
       }
-      auto finish = [&](int h, float z) {
-        if (h < H) {
-          const float x1 = tanhf(z - __ldg(p.b0 + t1 * H + h));
-          const float w1 = __ldg(p.w1 + t1 * H + h);
-          e_part += w1 * x1;
-          s_gh[h] = w1 * (1.0f - x1 * x1);
-        }
-      };
       finish(4 * h4, z0);
       finish(4 * h4 + 1, z1);
       finish(4 * h4 + 2, z2);
       finish(4 * h4 + 3, z3);
+      if (has_b) {
+        finish(4 * h4b, z4);
+        finish(4 * h4b + 1, z5);
+        finish(4 * h4b + 2, z6);
+        finish(4 * h4b + 3, z7);
+      }
     }
   }
   e_part = group_sum<G>(e_part);
   if (active && gl == 0) pe_ann[i] = static_cast<double>(e_part - __ldg(p.out_bias + t1));
   __syncwarp();
   if (active) {
-    // dE/dq: two descriptor components per lane at once, float4 over h
+    // dE/dq: four descriptor components per lane at once (d0, d0 + G,
+    // d0 + 2G, d0 + 3G), float4 over h, each sum in the same order as before
     const int hq = p.H4 / 4;
     const float4* g4 = reinterpret_cast<const float4*>(s_gh);
     const float4* wt =
       reinterpret_cast<const float4*>(w0t + static_cast<size_t>(t1) * dim * p.H4);
-    for (int d0 = gl; d0 < dim; d0 += 2 * G) {
-      const int da = d0, db = min(d0 + G, dim - 1);   // db past dim: computed, dropped
-      float aa = 0.0f, ab = 0.0f;
+    for (int d0 = gl; d0 < dim; d0 += 4 * G) {
+      int dd[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) dd[k] = min(d0 + k * G, dim - 1);   // past dim: dropped
+      float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll 2
       for (int h = 0; h < hq; ++h) {
         const float4 g = g4[h];
-        const float4 wa = wt[da * hq + h], wb = wt[db * hq + h];
-        aa = fmaf(g.x, wa.x, aa);
-        ab = fmaf(g.x, wb.x, ab);
-        aa = fmaf(g.y, wa.y, aa);
-        ab = fmaf(g.y, wb.y, ab);
-        aa = fmaf(g.z, wa.z, aa);
-        ab = fmaf(g.z, wb.z, ab);
-        aa = fmaf(g.w, wa.w, aa);
-        ab = fmaf(g.w, wb.w, ab);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const float4 w = wt[dd[k] * hq + h];
+          acc[k] = fmaf(g.x, w.x, acc[k]);
+          acc[k] = fmaf(g.y, w.y, acc[k]);
+          acc[k] = fmaf(g.z, w.z, acc[k]);
+          acc[k] = fmaf(g.w, w.w, acc[k]);
+        }
       }
-      s_fp[da] = aa * __ldg(p.q_scaler + da);
-      if (d0 + G < dim) s_fp[d0 + G] = ab * __ldg(p.q_scaler + d0 + G);
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        if (d0 + k * G < dim) s_fp[d0 + k * G] = acc[k] * __ldg(p.q_scaler + d0 + k * G);
     }
   }
   __syncwarp();
