@@ -71,3 +71,42 @@ def test_neighbor_rows_bit_exact(tmp_path):
         b = pot.neighbors(which, len(t))
         for i in range(len(t)):
             assert np.array_equal(a[i], b[i]), (which, i)
+
+
+def _perovskite(ncell=8, a=4.0, jitter=0.05, seed=0):
+    """BaTiO3 perovskite supercell: types Ba 0, Ti 1, O 2."""
+    base = np.array([[0, 0, 0], [.5, .5, .5], [.5, .5, 0], [.5, 0, .5], [0, .5, .5]])
+    kinds = np.array([0, 1, 2, 2, 2], dtype=np.int32)
+    g = np.stack(np.meshgrid(*[np.arange(ncell)] * 3, indexing="ij"), -1).reshape(-1, 3)
+    frac = (g[:, None, :] + base[None, :, :]).reshape(-1, 3) / ncell
+    L = a * ncell
+    rng = np.random.default_rng(seed)
+    pos = (frac * L + rng.normal(0.0, jitter, frac.shape)) % L
+    t = np.tile(kinds, len(g))
+    return t, np.array([L, 0, 0, 0, L, 0, 0, 0, L], dtype=np.float64), np.ascontiguousarray(pos.T)
+
+
+@pytest.mark.parametrize("case", ["nep5_four_types", "zbl_universal", "zbl_typewise",
+                                  "batio3_nep_zbl"])
+def test_more_models_match_reference_fp32(case, tmp_path):
+    """NEP5 with four types, NEP4-ZBL with the universal and the typewise ZBL
+    cutoffs (close contacts down to 0.9 A), and the reference suite's BaTiO3
+    NEP-ZBL potential on a perovskite supercell."""
+    syms = ("C", "H", "O", "Cu")
+    if case == "batio3_nep_zbl":
+        path = potential("nep_BaTiO3_zbl.txt")
+        t, h, p = _perovskite(seed=3)
+    else:
+        zbl = {"nep5_four_types": None, "zbl_universal": (1.0, 2.0),
+               "zbl_typewise": (1.0, 2.0, 0.7)}[case]
+        path = workloads.write_nep(str(tmp_path / "nep.txt"), version=5 if zbl is None else 4,
+                                   symbols=syms, zbl=zbl, rc=(5.0, 4.0), mn=(160, 80),
+                                   l_max=(4, 2, 1), H=32, seed=17, q_scaler=0.1)
+        t, h, p = workloads.random_packed(n=2000, num_types=4, density=0.08, seed=19)
+    _, _, (pe0, f0, w0), (pe1, f1, w1) = _both(path, t, h, p, tmp_path)
+    n = len(t)
+    rel_f = np.linalg.norm(f1 - f0) / np.linalg.norm(f0)
+    assert rel_f <= 1e-5, rel_f
+    assert abs(pe1.sum() - pe0.sum()) / n <= 1e-6
+    assert np.abs(pe1 - pe0).max() <= 2e-5
+    assert np.linalg.norm(w1 - w0) / np.linalg.norm(w0) <= 2e-5
