@@ -103,7 +103,8 @@ def test_triclinic_box():
     assert_close(ref, (pe, f, w), "triclinic")
 
 
-@pytest.mark.parametrize("version,zbl", [(5, None), (4, (1.0, 2.0)), (5, (0.8, 1.6, 0.7))])
+@pytest.mark.parametrize("version,zbl", [(5, None), (4, (1.0, 2.0)), (5, (0.8, 1.6, 0.7)),
+                                         (4, "flexible"), (5, "flexible")])
 def test_synthetic_multitype(tmp_path, version, zbl):
     syms = ("C", "H", "O", "Cu")
     path = workloads.write_nep(str(tmp_path / "nep.txt"), version=version, symbols=syms, zbl=zbl,

@@ -87,18 +87,18 @@ def _perovskite(ncell=8, a=4.0, jitter=0.05, seed=0):
 
 
 @pytest.mark.parametrize("case", ["nep5_four_types", "zbl_universal", "zbl_typewise",
-                                  "batio3_nep_zbl"])
+                                  "zbl_flexible", "batio3_nep_zbl"])
 def test_more_models_match_reference_fp32(case, tmp_path):
-    """NEP5 with four types, NEP4-ZBL with the universal and the typewise ZBL
-    cutoffs (close contacts down to 0.9 A), and the reference suite's BaTiO3
-    NEP-ZBL potential on a perovskite supercell."""
+    """NEP5 with four types, NEP4-ZBL with the universal, the typewise and the
+    flexible (fitted per-pair) ZBL (close contacts down to 0.9 A), and the
+    reference suite's BaTiO3 NEP-ZBL potential on a perovskite supercell."""
     syms = ("C", "H", "O", "Cu")
     if case == "batio3_nep_zbl":
         path = potential("nep_BaTiO3_zbl.txt")
         t, h, p = _perovskite(seed=3)
     else:
         zbl = {"nep5_four_types": None, "zbl_universal": (1.0, 2.0),
-               "zbl_typewise": (1.0, 2.0, 0.7)}[case]
+               "zbl_typewise": (1.0, 2.0, 0.7), "zbl_flexible": "flexible"}[case]
         path = workloads.write_nep(str(tmp_path / "nep.txt"), version=5 if zbl is None else 4,
                                    symbols=syms, zbl=zbl, rc=(5.0, 4.0), mn=(160, 80),
                                    l_max=(4, 2, 1), H=32, seed=17, q_scaler=0.1)

@@ -70,3 +70,31 @@ def test_oracle_virial_sum_is_pair_virial():
         e0.append(m.compute(types, hs, pos * s)[0].sum())
     dE = (e0[0] - e0[1]) / (2 * eps)
     assert abs(-dE - w[:3].sum()) < 1e-5 * max(1.0, abs(dE))
+
+
+def test_oracle_flexible_zbl_forces(tmp_path):
+    """Flexible (per-pair fitted) ZBL: the oracle's forces are -dE/dr, with
+    close contacts inside every pair's inner and outer ZBL cutoff."""
+    import workloads
+    path = workloads.write_nep(str(tmp_path / "nep.txt"), version=4, symbols=("C", "O"),
+                               zbl="flexible", rc=(4.0, 3.5), mn=(80, 60), H=8, seed=21)
+    rng = np.random.default_rng(5)
+    n, L = 30, 9.0
+    pos = rng.uniform(0, L, (3, n))
+    pos[:, 1] = pos[:, 0] + [0.7, 0.2, 0.1]      # pairs at 0.7 A and 1.5 A
+    pos[:, 3] = pos[:, 2] + [1.4, 0.4, 0.3]
+    types = rng.integers(0, 2, n)
+    h = [L, 0, 0, 0, L, 0, 0, 0, L]
+    m = oracle.OracleModel(path)
+    _, f, _ = m.compute(types, h, pos)
+    eps = 1e-6
+    for i in (0, 1, 2, 3):
+        for d in range(3):
+            p1 = pos.copy()
+            p1[d, i] += eps
+            p2 = pos.copy()
+            p2[d, i] -= eps
+            e1 = m.compute(types, h, p1)[0].sum()
+            e2 = m.compute(types, h, p2)[0].sum()
+            assert abs(-(e1 - e2) / (2 * eps) - f[d, i]) < 1e-5 * max(1.0, abs(f[d, i]))
+

@@ -26,7 +26,10 @@ def write_nep(path, version=4, symbols=("C",), zbl=None, rc=(4.2, 3.7), mn=(100,
               q_scaler=1.0):
     """Write a synthetic NEP file; returns its path.
 
-    zbl: None, (rc_inner, rc_outer) or (rc_inner, rc_outer, factor).
+    zbl: None, (rc_inner, rc_outer), (rc_inner, rc_outer, factor) or
+    "flexible" (the "zbl 0 0" form: per type pair rc_inner, rc_outer and four
+    screening pairs (a_k, b_k) after the descriptor scales, drawn near the
+    universal ZBL values).
     """
     T = len(symbols)
     nR, nA = n_max[0] + 1, n_max[1] + 1
@@ -42,7 +45,9 @@ def write_nep(path, version=4, symbols=("C",), zbl=None, rc=(4.2, 3.7), mn=(100,
     params = rng.normal(0.0, std, num_ann + num_desc)
     tag = "nep%d%s" % (version, "_zbl" if zbl else "")
     lines = ["%s %d %s" % (tag, T, " ".join(symbols))]
-    if zbl:
+    if zbl == "flexible":
+        lines.append("zbl 0 0")
+    elif zbl:
         lines.append("zbl " + " ".join("%g" % v for v in zbl))
     lines.append("cutoff %g %g %d %d" % (rc[0], rc[1], mn[0], mn[1]))
     lines.append("n_max %d %d" % n_max)
@@ -52,6 +57,12 @@ def write_nep(path, version=4, symbols=("C",), zbl=None, rc=(4.2, 3.7), mn=(100,
     lines += ["%.8e" % v for v in params]
     qs = np.full(dim, q_scaler) if np.isscalar(q_scaler) else np.asarray(q_scaler)
     lines += ["%.8e" % v for v in qs]
+    if zbl == "flexible":
+        universal = [0.18175, 3.1998, 0.50986, 0.94229, 0.28022, 0.4029, 0.02817, 0.20162]
+        for _ in range(T * (T + 1) // 2):
+            pair = [rng.uniform(0.8, 1.2), rng.uniform(1.8, 2.2)]
+            pair += [c * rng.uniform(0.9, 1.1) for c in universal]
+            lines += ["%.8e" % v for v in pair]
     os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
     with open(path, "w") as f:
         f.write("\n".join(lines) + "\n")
