@@ -115,6 +115,18 @@ def test_synthetic_multitype(tmp_path, version, zbl):
     assert_close(ref, (pe, f, w), "nep%d zbl=%s" % (version, zbl))
 
 
+@pytest.mark.parametrize("box", ["large", "small"])
+def test_typewise_cutoffs(tmp_path, box):
+    """Per-type cutoffs against the oracle, on the large-box and the small-box path."""
+    path = workloads.write_nep(str(tmp_path / "nep.txt"), version=5, symbols=("O", "H"),
+                               rc=((6.0, 4.0), (5.0, 3.5)), mn=(250, 100), l_max=(4, 2, 1),
+                               H=20, seed=31, q_scaler=0.1)
+    t, h, p = workloads.water(n_mol=400 if box == "large" else 30, seed=37)
+    ref = oracle.OracleModel(path).compute(t, h, p)
+    _, pe, f, w = run_gpu(path, t, h, p)
+    assert_close(ref, (pe, f, w), "typewise cutoffs, %s box" % box)
+
+
 def test_all_many_body_invariants(tmp_path):
     """l_max line with q_222, q_1111, q_112, q_123, q_233 and q_134 all on."""
     path = str(tmp_path / "nep_inv.txt")

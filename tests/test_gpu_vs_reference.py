@@ -110,3 +110,24 @@ def test_more_models_match_reference_fp32(case, tmp_path):
     assert abs(pe1.sum() - pe0.sum()) / n <= 1e-6
     assert np.abs(pe1 - pe0).max() <= 2e-5
     assert np.linalg.norm(w1 - w0) / np.linalg.norm(w0) <= 2e-5
+
+
+def test_typewise_cutoffs_match_reference(tmp_path):
+    """Per-type cutoffs (O 6.0/4.0 A, H 5.0/3.5 A; a pair uses the mean of
+    its two types' cutoffs, nep.cu:503-561): forces and energies within the
+    FP32 tolerances and typewise rows identical to the reference's."""
+    path = workloads.write_nep(str(tmp_path / "nep.txt"), version=4, symbols=("O", "H"),
+                               rc=((6.0, 4.0), (5.0, 3.5)), mn=(250, 100), l_max=(4, 2, 0),
+                               H=30, seed=23, q_scaler=0.1)
+    t, h, p = workloads.water(n_mol=900, seed=29)
+    ref, pot, (pe0, f0, w0), (pe1, f1, w1) = _both(path, t, h, p, tmp_path)
+    n = len(t)
+    assert np.linalg.norm(f1 - f0) / np.linalg.norm(f0) <= 1e-5
+    assert abs(pe1.sum() - pe0.sum()) / n <= 1e-6
+    assert np.linalg.norm(w1 - w0) / np.linalg.norm(w0) <= 2e-5
+    for which, mn in ((0, pot.info["MN_r"]), (1, pot.info["MN_a"])):
+        a = ref.neighbors(which, mn)
+        b = pot.neighbors(which, n)
+        for i in range(n):
+            assert np.array_equal(a[i], b[i]), (which, i)
+

@@ -26,6 +26,7 @@ def write_nep(path, version=4, symbols=("C",), zbl=None, rc=(4.2, 3.7), mn=(100,
               q_scaler=1.0):
     """Write a synthetic NEP file; returns its path.
 
+    rc: (rc_radial, rc_angular), or one such pair per type (typewise cutoffs).
     zbl: None, (rc_inner, rc_outer), (rc_inner, rc_outer, factor) or
     "flexible" (the "zbl 0 0" form: per type pair rc_inner, rc_outer and four
     screening pairs (a_k, b_k) after the descriptor scales, drawn near the
@@ -49,7 +50,11 @@ def write_nep(path, version=4, symbols=("C",), zbl=None, rc=(4.2, 3.7), mn=(100,
         lines.append("zbl 0 0")
     elif zbl:
         lines.append("zbl " + " ".join("%g" % v for v in zbl))
-    lines.append("cutoff %g %g %d %d" % (rc[0], rc[1], mn[0], mn[1]))
+    if np.ndim(rc) == 2:   # per-type cutoffs: (rc_radial, rc_angular) of each type
+        lines.append("cutoff " + " ".join("%g %g" % tuple(c) for c in rc) +
+                     " %d %d" % (mn[0], mn[1]))
+    else:
+        lines.append("cutoff %g %g %d %d" % (rc[0], rc[1], mn[0], mn[1]))
     lines.append("n_max %d %d" % n_max)
     lines.append("basis_size %d %d" % basis)
     lines.append("l_max %d %d %d" % tuple(l_max))
