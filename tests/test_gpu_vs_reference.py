@@ -131,3 +131,20 @@ def test_typewise_cutoffs_match_reference(tmp_path):
         for i in range(n):
             assert np.array_equal(a[i], b[i]), (which, i)
 
+
+def test_all_many_body_invariants_match_reference(tmp_path):
+    """q_222, q_1111, q_112, q_123, q_233 and q_134 all on: the engine's and the
+    oracle's monomial tables of these invariants are both transcriptions of
+    find_q (nep_utilities.cuh:1602-1730), so the reference's own kernels are
+    the independent check."""
+    path = workloads.write_nep(str(tmp_path / "nep.txt"), version=4, symbols=("C", "O"),
+                               rc=(4.6, 4.0), mn=(90, 60), l_max=(4, 1, 1, 1, 1, 1, 1), H=16,
+                               seed=41, q_scaler=0.1)
+    t, h, p = workloads.random_packed(2000, 2, density=0.09, seed=43)
+    _, _, (pe0, f0, w0), (pe1, f1, w1) = _both(path, t, h, p, tmp_path)
+    n = len(t)
+    assert np.linalg.norm(f1 - f0) / np.linalg.norm(f0) <= 1e-5
+    assert abs(pe1.sum() - pe0.sum()) / n <= 1e-6
+    assert np.abs(pe1 - pe0).max() <= 2e-5
+    assert np.linalg.norm(w1 - w0) / np.linalg.norm(w0) <= 2e-5
+

@@ -35,7 +35,8 @@ def write_nep(path, version=4, symbols=("C",), zbl=None, rc=(4.2, 3.7), mn=(100,
     T = len(symbols)
     nR, nA = n_max[0] + 1, n_max[1] + 1
     kR, kA = basis[0] + 1, basis[1] + 1
-    num_L = l_max[0] + (1 if l_max[1] else 0) + (1 if l_max[2] else 0)
+    # l_max: (L, has_q_222, has_q_1111[, has_q_112, has_q_123, has_q_233, has_q_134])
+    num_L = l_max[0] + sum(1 for flag in l_max[1:] if flag)
     dim = nR + nA * num_L
     if version == 4:
         num_ann = (dim + 2) * H * T + 1
@@ -57,7 +58,7 @@ def write_nep(path, version=4, symbols=("C",), zbl=None, rc=(4.2, 3.7), mn=(100,
         lines.append("cutoff %g %g %d %d" % (rc[0], rc[1], mn[0], mn[1]))
     lines.append("n_max %d %d" % n_max)
     lines.append("basis_size %d %d" % basis)
-    lines.append("l_max %d %d %d" % tuple(l_max))
+    lines.append("l_max " + " ".join("%d" % v for v in l_max))
     lines.append("ANN %d 0" % H)
     lines += ["%.8e" % v for v in params]
     qs = np.full(dim, q_scaler) if np.isscalar(q_scaler) else np.asarray(q_scaler)
