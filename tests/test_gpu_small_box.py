@@ -86,14 +86,11 @@ def test_unsupported_thin_and_thick_box():
     assert err.value.code == 8
 
 
-@pytest.mark.skipif(not oracle.ref_gpu_available(), reason="reference GPU library not built")
-def test_small_box_matches_reference_gpu(tmp_path):
+def _small_vs_reference(path, t, h, p, tmp_path):
     import nepx
-    t, h, p = workloads.water(n_mol=40, seed=11)          # L ~ 10.6 A
-    path = potential("nep_water.txt")
     n = len(t)
     cwd = os.getcwd()
-    os.chdir(tmp_path)
+    os.chdir(tmp_path)   # the reference appends neighbor.out to the working directory
     try:
         tt = torch.as_tensor(np.asarray(t, dtype=np.int32), device="cuda")
         pp = torch.as_tensor(np.ascontiguousarray(p), device="cuda")
@@ -118,6 +115,29 @@ def test_small_box_matches_reference_gpu(tmp_path):
                 assert np.array_equal(a[i], b[i]), (which, i)
     finally:
         os.chdir(cwd)
+
+
+@pytest.mark.skipif(not oracle.ref_gpu_available(), reason="reference GPU library not built")
+def test_small_box_matches_reference_gpu(tmp_path):
+    t, h, p = workloads.water(n_mol=40, seed=11)          # L ~ 10.6 A
+    _small_vs_reference(potential("nep_water.txt"), t, h, p, tmp_path)
+
+
+@pytest.mark.skipif(not oracle.ref_gpu_available(), reason="reference GPU library not built")
+@pytest.mark.parametrize("case", ["zbl_universal", "zbl_flexible", "typewise_cutoffs"])
+def test_small_box_models_match_reference_gpu(tmp_path, case):
+    """The small-box path of the reference (its image rows and its small-box
+    ZBL) for four-type NEP5 with universal or flexible ZBL, and for per-type
+    cutoffs."""
+    syms = ("C", "H", "O", "Cu")
+    zbl = {"zbl_universal": (1.0, 2.0), "zbl_flexible": "flexible",
+           "typewise_cutoffs": None}[case]
+    rc = ((5.0, 4.0), (4.2, 3.6), (4.6, 3.8), (5.0, 4.0)) if case == "typewise_cutoffs" \
+        else (5.0, 4.0)
+    path = workloads.write_nep(str(tmp_path / "nep.txt"), version=5, symbols=syms, zbl=zbl,
+                               rc=rc, mn=(200, 100), H=24, seed=47, q_scaler=0.1)
+    t, h, p = workloads.random_packed(n=60, num_types=4, density=0.08, seed=53)
+    _small_vs_reference(path, t, h, p, tmp_path)
 
 
 def test_small_box_nve_conserves_energy():
