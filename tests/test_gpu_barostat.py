@@ -118,3 +118,27 @@ def test_isotropic_coupling_rejects_triclinic_box():
         md.run(5, 1.0)
     md.close()
     pot.close()
+
+
+def test_isotropic_berendsen_against_the_reference_formulas():
+    """The reference's isotropic npt_ber (ensemble_control.cpp:180-306,
+    box_control.cpp:9-68), restated from the thermo rows: each step's box
+    factor is 1 - (P0 - P)/(3 tau_p B) with P the mean of the three normal
+    stresses, the box scales by it, and the Berendsen velocity factor is
+    sqrt(1 + (T0 / T - 1) / Tdamp) with T the step's temperature."""
+    pot, md, n = _md("npt_ber", CUBE)
+    tau, bulk, p0, t0, tdamp = 150.0, 300.0, 0.5, 300.0, 80.0
+    md.set_ensemble("npt_ber", T0=t0, Tdamp=tdamp, p_gpa=p0, bulk_gpa=bulk, tau_p=tau)
+    rows = md.run(50, 1.0, thermo_every=1)
+    prev = np.asarray(CUBE, dtype=np.float64).reshape(3, 3)
+    for row in rows:
+        p_inst = (row[COLS["sxx"]] + row[COLS["syy"]] + row[COLS["szz"]]) / 3.0
+        bf = 1.0 - (p0 - p_inst) / (3.0 * tau * bulk)
+        assert row[19] == pytest.approx(bf, rel=1e-13, abs=1e-15)
+        got = _box(row)
+        assert np.allclose(got, bf * prev, rtol=1e-13, atol=1e-13)
+        vf = np.sqrt(1.0 + (t0 / row[0] - 1.0) / tdamp)
+        assert row[18] == pytest.approx(vf, rel=1e-12)
+        prev = got
+    md.close()
+    pot.close()
