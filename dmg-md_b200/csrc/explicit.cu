@@ -123,14 +123,21 @@ k_rows_explicit(const ModelParams p, int total, const StructInfo* __restrict__ s
         }
       };
       if (s.nc[0] > 0) {
-        // the 3x3x3 cells around the center's (every cell once where the grid is narrower)
+        // the 3x3x3 cells around the center's (every cell once where the grid
+        // is narrower): lane q takes stencil cell q, a warp prefix sum of the
+        // cell counts flattens their atoms into one range, and the warp
+        // sweeps that range 32 candidates at a time (a cell holds about ten
+        // atoms, so one cell per pass would leave most lanes idle)
         const int nc0 = s.nc[0], nc1 = s.nc[1], nc2 = s.nc[2];
         const int lc = cell_of[i] - s.cell_base;
         const int cx = lc % nc0, cy = (lc / nc0) % nc1, cz = lc / (nc0 * nc1);
         const int sp0 = (s.box.pbc[0] && nc0 >= 3) ? 3 : nc0;
         const int sp1 = (s.box.pbc[1] && nc1 >= 3) ? 3 : nc1;
         const int sp2 = (s.box.pbc[2] && nc2 >= 3) ? 3 : nc2;
-        for (int q = 0; q < sp0 * sp1 * sp2; ++q) {
+        const int ns = sp0 * sp1 * sp2;   // at most 27 (grids below 27 cells scan all atoms)
+        int my_start = 0, my_cnt = 0;
+        if (lane < ns) {
+          const int q = lane;
           const int q0 = q % sp0, q1 = (q / sp0) % sp1, q2 = q / (sp0 * sp1);
           int gx = sp0 == 3 ? cx + q0 - 1 : q0;
           int gy = sp1 == 3 ? cy + q1 - 1 : q1;
@@ -139,9 +146,31 @@ k_rows_explicit(const ModelParams p, int total, const StructInfo* __restrict__ s
           if (gy < 0) gy += nc1; else if (gy >= nc1) gy -= nc1;
           if (gz < 0) gz += nc2; else if (gz >= nc2) gz -= nc2;
           const int c = s.cell_base + (gz * nc1 + gy) * nc0 + gx;
-          const int start = cell_start[c], cnt = cell_count[c];
-          for (int m = lane; m < cnt; m += 32) {
-            const int j = cell_atoms[start + m];
+          my_start = cell_start[c];
+          my_cnt = cell_count[c];
+        }
+        int incl = my_cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int v = __shfl_up_sync(kFull, incl, o);
+          if (lane >= o) incl += v;
+        }
+        const int total_c = __shfl_sync(kFull, incl, 31);
+        for (int base = 0; base < total_c; base += 32) {
+          const int k = base + lane;
+          // stencil cell of candidate k: the first lane whose inclusive count exceeds k
+          int lo = 0;
+#pragma unroll
+          for (int step = 16; step > 0; step >>= 1) {
+            const int probe = lo + step - 1;
+            const int v = __shfl_sync(kFull, incl, probe < 31 ? probe : 31);
+            if (probe < 31 && v <= k) lo += step;
+          }
+          const int cstart = __shfl_sync(kFull, my_start, lo);
+          const int cincl = __shfl_sync(kFull, incl, lo);
+          const int ccnt = __shfl_sync(kFull, my_cnt, lo);
+          if (k < total_c) {
+            const int j = cell_atoms[cstart + (k - (cincl - ccnt))];
             if (j != i) consider(j);
           }
         }
