@@ -86,7 +86,7 @@ k_rows_explicit(const ModelParams p, int total, const StructInfo* __restrict__ s
                 int mn_r, int* __restrict__ nn_a, float4* __restrict__ ea, int mn_a,
                 const int* __restrict__ cell_count, const int* __restrict__ cell_start,
                 const int* __restrict__ cell_atoms, const int* __restrict__ cell_of, int p2r,
-                NeighborState* st)
+                const Site* __restrict__ sites, NeighborState* st)
 {
   extern __shared__ int s_rows[];   // per warp: p2r row slots + a counter
   const int lane = threadIdx.x & 31;
@@ -108,15 +108,18 @@ k_rows_explicit(const ModelParams p, int total, const StructInfo* __restrict__ s
     int cr = 0, ca = 0;
     if (!s.small) {
       const double xi = pos[i], yi = pos[total + i], zi = pos[2 * total + i];
+      const Box b = s.box;   // the structure's box, held in registers for this center
       int* buf = s_rows + (threadIdx.x >> 5) * (p2r + 1);
       int* count = buf + p2r;
       if (lane == 0) *count = 0;
       __syncwarp();
       auto consider = [&](int j) {
-        float x12 = pos[j] - xi, y12 = pos[total + j] - yi, z12 = pos[2 * total + j] - zi;
-        mic_f32(s.box, x12, y12, z12);
+        // the site record: position and type in one 32-byte sector
+        float x12, y12, z12;
+        int tj;
+        site_displacement(b, sites, xi, yi, zi, j, x12, y12, z12, tj);
         const float d12_square = x12 * x12 + y12 * y12 + z12 * z12;
-        const float rc_radial = (rr1 + p.rc_r[type[j]]) * 0.5f;
+        const float rc_radial = (rr1 + p.rc_r[tj]) * 0.5f;
         if (d12_square < rc_radial * rc_radial) {
           const int slot = atomicAdd(count, 1);
           if (slot < p2r) buf[slot] = j;
@@ -208,10 +211,10 @@ k_rows_explicit(const ModelParams p, int total, const StructInfo* __restrict__ s
         float4 entry = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         if (k < used) {
           const int j = buf[k];
-          float x12 = pos[j] - xi, y12 = pos[total + j] - yi, z12 = pos[2 * total + j] - zi;
-          mic_f32(s.box, x12, y12, z12);
+          float x12, y12, z12;
+          int t2;
+          site_displacement(b, sites, xi, yi, zi, j, x12, y12, z12, t2);
           const float d12_square = x12 * x12 + y12 * y12 + z12 * z12;
-          const int t2 = type[j];
           const float rc_angular = (ra1 + p.rc_a[t2]) * 0.5f;
           in_a = d12_square < rc_angular * rc_angular;
           entry = row_entry(x12, y12, z12, j, t2);
@@ -472,7 +475,7 @@ void launch_explicit_rows(Engine& e, int N, const double* pos, const int* type,
   k_rows_explicit<<<blocks, threads, smem, stream>>>(
     e.params, N, x.d_si, x.d_soff, x.n_struct, pos, type, e.nbr.nn_r, x.er, e.nbr.mn_r,
     e.nbr.nn_a, x.ea, e.nbr.mn_a, x.cell_count, x.cell_start, x.cell_atoms, x.cell_of, p2r,
-    e.d_nstate);
+    e.scratch.sites, e.d_nstate);
 }
 
 void launch_explicit_row_indices(const Engine& e, int which, int n, int* nn, int* nl, int mn,
