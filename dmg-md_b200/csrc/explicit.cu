@@ -17,7 +17,7 @@
 // its structure by binary search over the structure offsets.  Structures
 // that are not small use the large-box arithmetic (double difference rounded
 // to float, float minimum image, reference nep.cu:503-561); their candidates
-// come from a cell grid of their own (cells at least rc thick, 3x3x3 stencil,
+// come from a cell grid of their own (cells at least rc/2 thick, 5x5x5 stencil,
 // one counting sort over the whole batch), and each row is sorted in shared
 // memory, which yields the large-box path's typewise rows exactly.
 //
@@ -126,55 +126,57 @@ k_rows_explicit(const ModelParams p, int total, const StructInfo* __restrict__ s
         }
       };
       if (s.nc[0] > 0) {
-        // the 3x3x3 cells around the center's (every cell once where the grid
-        // is narrower): lane q takes stencil cell q, a warp prefix sum of the
-        // cell counts flattens their atoms into one range, and the warp
-        // sweeps that range 32 candidates at a time (a cell holds about ten
-        // atoms, so one cell per pass would leave most lanes idle)
+        // the 5x5x5 cells (at least rc/2 wide) around the center's, every cell
+        // once where the grid is narrower.  In rounds of 32 stencil cells:
+        // lane q takes a cell, a warp prefix sum of the cell counts flattens
+        // their atoms into one range, and the warp sweeps that range 32
+        // candidates at a time (one cell per pass would leave most lanes idle)
         const int nc0 = s.nc[0], nc1 = s.nc[1], nc2 = s.nc[2];
         const int lc = cell_of[i] - s.cell_base;
         const int cx = lc % nc0, cy = (lc / nc0) % nc1, cz = lc / (nc0 * nc1);
-        const int sp0 = (s.box.pbc[0] && nc0 >= 3) ? 3 : nc0;
-        const int sp1 = (s.box.pbc[1] && nc1 >= 3) ? 3 : nc1;
-        const int sp2 = (s.box.pbc[2] && nc2 >= 3) ? 3 : nc2;
-        const int ns = sp0 * sp1 * sp2;   // at most 27 (grids below 27 cells scan all atoms)
-        int my_start = 0, my_cnt = 0;
-        if (lane < ns) {
-          const int q = lane;
-          const int q0 = q % sp0, q1 = (q / sp0) % sp1, q2 = q / (sp0 * sp1);
-          int gx = sp0 == 3 ? cx + q0 - 1 : q0;
-          int gy = sp1 == 3 ? cy + q1 - 1 : q1;
-          int gz = sp2 == 3 ? cz + q2 - 1 : q2;
-          if (gx < 0) gx += nc0; else if (gx >= nc0) gx -= nc0;
-          if (gy < 0) gy += nc1; else if (gy >= nc1) gy -= nc1;
-          if (gz < 0) gz += nc2; else if (gz >= nc2) gz -= nc2;
-          const int c = s.cell_base + (gz * nc1 + gy) * nc0 + gx;
-          my_start = cell_start[c];
-          my_cnt = cell_count[c];
-        }
-        int incl = my_cnt;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const int v = __shfl_up_sync(kFull, incl, o);
-          if (lane >= o) incl += v;
-        }
-        const int total_c = __shfl_sync(kFull, incl, 31);
-        for (int base = 0; base < total_c; base += 32) {
-          const int k = base + lane;
-          // stencil cell of candidate k: the first lane whose inclusive count exceeds k
-          int lo = 0;
-#pragma unroll
-          for (int step = 16; step > 0; step >>= 1) {
-            const int probe = lo + step - 1;
-            const int v = __shfl_sync(kFull, incl, probe < 31 ? probe : 31);
-            if (probe < 31 && v <= k) lo += step;
+        const int sp0 = (b.pbc[0] && nc0 >= 5) ? 5 : nc0;
+        const int sp1 = (b.pbc[1] && nc1 >= 5) ? 5 : nc1;
+        const int sp2 = (b.pbc[2] && nc2 >= 5) ? 5 : nc2;
+        const int ns = sp0 * sp1 * sp2;   // at most 125
+        for (int r0 = 0; r0 < ns; r0 += 32) {
+          int my_start = 0, my_cnt = 0;
+          if (r0 + lane < ns) {
+            const int q = r0 + lane;
+            const int q0 = q % sp0, q1 = (q / sp0) % sp1, q2 = q / (sp0 * sp1);
+            int gx = sp0 == 5 ? cx + q0 - 2 : q0;
+            int gy = sp1 == 5 ? cy + q1 - 2 : q1;
+            int gz = sp2 == 5 ? cz + q2 - 2 : q2;
+            if (gx < 0) gx += nc0; else if (gx >= nc0) gx -= nc0;
+            if (gy < 0) gy += nc1; else if (gy >= nc1) gy -= nc1;
+            if (gz < 0) gz += nc2; else if (gz >= nc2) gz -= nc2;
+            const int c = s.cell_base + (gz * nc1 + gy) * nc0 + gx;
+            my_start = cell_start[c];
+            my_cnt = cell_count[c];
           }
-          const int cstart = __shfl_sync(kFull, my_start, lo);
-          const int cincl = __shfl_sync(kFull, incl, lo);
-          const int ccnt = __shfl_sync(kFull, my_cnt, lo);
-          if (k < total_c) {
-            const int j = cell_atoms[cstart + (k - (cincl - ccnt))];
-            if (j != i) consider(j);
+          int incl = my_cnt;
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += v;
+          }
+          const int total_c = __shfl_sync(kFull, incl, 31);
+          for (int base = 0; base < total_c; base += 32) {
+            const int k = base + lane;
+            // stencil cell of candidate k: the first lane whose inclusive count exceeds k
+            int lo = 0;
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1) {
+              const int probe = lo + step - 1;
+              const int v = __shfl_sync(kFull, incl, probe);
+              if (v <= k) lo += step;
+            }
+            const int cstart = __shfl_sync(kFull, my_start, lo);
+            const int cincl = __shfl_sync(kFull, incl, lo);
+            const int ccnt = __shfl_sync(kFull, my_cnt, lo);
+            if (k < total_c) {
+              const int j = cell_atoms[cstart + (k - (cincl - ccnt))];
+              if (j != i) consider(j);
+            }
           }
         }
       } else {
@@ -399,10 +401,12 @@ int assign_cells(const Engine& e, StructInfo* si, int n)
     for (int d = 0; d < 3; ++d) {
       const double* r = s.box.hinv + 3 * d;
       const double thick = 1.0 / std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
-      nc[d] = s.box.pbc[d] ? std::max(1, static_cast<int>(thick / rc)) : 1;
+      nc[d] = s.box.pbc[d] ? std::max(1, static_cast<int>(thick / (0.5 * rc))) : 1;
       cells *= nc[d];
     }
-    if (cells < 27 || used + cells > e.xr.cell_cap) continue;   // scan all atoms instead
+    // a 5x5x5 stencil of cells at least rc/2 wide covers the cutoff; grids
+    // of fewer than 125 cells scan all the structure's atoms instead
+    if (cells < 125 || used + cells > e.xr.cell_cap) continue;
     for (int d = 0; d < 3; ++d) s.nc[d] = nc[d];
     s.cell_base = used;
     used += cells;
