@@ -647,7 +647,9 @@ def main():
     # once unless a rebuild is due), k_filter_radial, k_nep_fused,
     # k_angular_f12, k_gather, k_vv2_thermo, k_ensemble, k_scale; NHC adds two
     kernels_per_step = 13 + (2 if kind == "nvt_nhc" else 0)
-    launches = K * kernels_per_step   # the L2-flush fills are torch's, not counted
+    # per call (chunk): k_mark_call before the step graphs and k_publish after
+    # them; the L2-flush fills are torch's, not counted
+    launches = K * kernels_per_step + 2 * len(chunks)
 
     st = md.state()     # the final state of the timed run
     md.close()
@@ -694,7 +696,7 @@ def main():
     torch.cuda.synchronize()
     value_mixed, dev_ms_m = replica_rate(n, K, sum(a.elapsed_time(b) for a, b in ev_m), ranks)
     # + four type-sort kernels, the tcgen05 ANN and k_acoef
-    launches += K * (kernels_per_step + 6)
+    launches += K * (kernels_per_step + 6) + 2 * len(chunks)
 
     # per-kernel profile of the force path on the final state of the FP32
     # run, both precisions

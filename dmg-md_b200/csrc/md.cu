@@ -13,6 +13,7 @@
 // (svr_rng.h).  A step therefore never synchronises with the host, and a run
 // replays CUDA graphs of captured steps (eight, then single ones) back to
 // back.  The large-box path's skin check runs inside the first half kick.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -35,6 +36,9 @@ struct nepx_md {
   MdMirror* mirror = nullptr;   // pinned host copy of the device status
   nepx_handle* pot = nullptr;
   double* h_noise = nullptr;   // pinned staging of the stochastic draws
+  double* h_rows = nullptr;    // pinned staging of the thermo rows (rows_cap rows)
+  double* pending_thermo = nullptr;   // the caller's row buffer, filled by md_finish
+  int pending_rows = 0;
   cudaEvent_t noise_copied = nullptr;
   bool own_stream = false;
   std::string error;
@@ -472,6 +476,39 @@ __global__ void k_mark_call(MdScalars* sc) { sc->step0 = sc->step; }
 
 void md_continue_scalars(Md& md) { k_mark_call<<<1, 1, 0, md.stream>>>(md.d_sc); }
 
+// End of a call: the box, the status word, the neighbour state and the thermo
+// rows, written straight into pinned host memory (device-addressable under
+// unified addressing) -- one launch in place of four small copies.
+__global__ void k_publish(const Box* __restrict__ box, const int* __restrict__ status,
+                          const NeighborState* __restrict__ nstate, Box* h_box, int* h_status,
+                          NeighborState* h_nstate, const double* __restrict__ rows, double* h_rows,
+                          int n_vals)
+{
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (blockIdx.x == 0) {
+    constexpr int kBoxWords = sizeof(Box) / sizeof(int);
+    constexpr int kStateWords = sizeof(NeighborState) / sizeof(int);
+    static_assert(sizeof(Box) % sizeof(int) == 0 && sizeof(NeighborState) % sizeof(int) == 0,
+                  "word copies");
+    const int* b = reinterpret_cast<const int*>(box);
+    const int* n = reinterpret_cast<const int*>(nstate);
+    for (int k = threadIdx.x; k < kBoxWords; k += blockDim.x) reinterpret_cast<int*>(h_box)[k] = b[k];
+    for (int k = threadIdx.x; k < kStateWords; k += blockDim.x)
+      reinterpret_cast<int*>(h_nstate)[k] = n[k];
+    if (threadIdx.x == 0) *h_status = *status;
+  }
+  for (int k = tid; k < n_vals; k += gridDim.x * blockDim.x) h_rows[k] = rows[k];
+}
+
+void launch_publish(const Engine& e, const Md& md, const int* d_status, Box* h_box,
+                    int* h_status, NeighborState* h_nstate, double* h_rows, int rows)
+{
+  const int n_vals = rows * kThermoCols;
+  const int blocks = std::max(1, std::min(148, (n_vals + 255) / 256));
+  k_publish<<<blocks, 256, 0, md.stream>>>(e.d_box, d_status, e.d_nstate, h_box, h_status,
+                                           h_nstate, md.d_rows, h_rows, n_vals);
+}
+
 void md_init_scalars(Md& md, const StepParams& p, double T0, double tau)
 {
   k_init_scalars<<<1, 1, 0, md.stream>>>(md.d_sc, p, T0, tau);
@@ -502,6 +539,24 @@ bool dalloc(T*& p, size_t n)
 {
   return cudaMalloc(reinterpret_cast<void**>(&p), std::max<size_t>(n, 1) * sizeof(T)) ==
          cudaSuccess;
+}
+
+// Pinned host memory that kernels write directly: mapped into the device's
+// address space under the same pointer (unified addressing), checked here.
+template <typename T>
+bool pinned_mapped(T*& p, size_t count)
+{
+  p = nullptr;
+  if (cudaHostAlloc(reinterpret_cast<void**>(&p), std::max<size_t>(count, 1) * sizeof(T),
+                    cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess)
+    return false;
+  void* dp = nullptr;
+  if (cudaHostGetDevicePointer(&dp, p, 0) != cudaSuccess || dp != p) {
+    cudaFreeHost(p);
+    p = nullptr;
+    return false;
+  }
+  return true;
 }
 
 int* status_buffer(nepx_md* m)
@@ -560,7 +615,7 @@ int nepx_md_create(nepx_t* pot, int n, const int* h_type, const double* h_mass,
        dalloc(md.d_pe, n) && dalloc(md.d_virial, 9 * size_t(n)) &&
        dalloc(md.d_partials, 8 * size_t(md.partial_blocks) + 2) && dalloc(md.d_sc, 1);
   ok = ok && cudaEventCreateWithFlags(&m->noise_copied, cudaEventDisableTiming) == cudaSuccess;
-  ok = ok && cudaMallocHost(reinterpret_cast<void**>(&m->mirror), sizeof(MdMirror)) == cudaSuccess;
+  ok = ok && pinned_mapped(m->mirror, 1);
   if (ok) {
     std::memset(m->mirror, 0, sizeof(MdMirror));
     m->mirror->box = md.box;
@@ -595,6 +650,7 @@ int nepx_md_destroy(nepx_md_t* m)
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (m->h_noise) cudaFreeHost(m->h_noise);
+  if (m->h_rows) cudaFreeHost(m->h_rows);
   if (m->mirror) cudaFreeHost(m->mirror);
   if (m->noise_copied) cudaEventDestroy(m->noise_copied);
   if (md.engine && md.engine->box_owner == &md) md.engine->box_owner = nullptr;
@@ -742,8 +798,12 @@ int md_enqueue_run(nepx_md* m, int steps, double dt_fs, int thermo_every, double
   if (rows > md.rows_cap) {
     cudaStreamSynchronize(s);
     if (md.d_rows) cudaFree(md.d_rows);
+    if (m->h_rows) cudaFreeHost(m->h_rows);
     md.d_rows = nullptr;
-    if (!dalloc(md.d_rows, size_t(rows) * nepx::kThermoCols)) return md_cuda(m, "allocate rows");
+    m->h_rows = nullptr;
+    if (!dalloc(md.d_rows, size_t(rows) * nepx::kThermoCols) ||
+        !pinned_mapped(m->h_rows, size_t(rows) * nepx::kThermoCols))
+      return md_cuda(m, "allocate rows");
     md.rows_cap = rows;
   }
   // the device box is authoritative while this md owns the engine; it is
@@ -803,14 +863,12 @@ int md_enqueue_run(nepx_md* m, int steps, double dt_fs, int thermo_every, double
     if (cudaGraphLaunch(md.graph_multi, s) != cudaSuccess) return md_cuda(m, "graph launch");
   for (; k < steps; ++k)
     if (cudaGraphLaunch(md.graph, s) != cudaSuccess) return md_cuda(m, "graph launch");
-  // device-side status, box and neighbour flags land in pinned memory
-  cudaMemcpyAsync(&m->mirror->box, e.d_box, sizeof(nepx::Box), cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(&m->mirror->status, d_status, sizeof(int), cudaMemcpyDeviceToHost, s);
-  cudaMemcpyAsync(&m->mirror->nstate, e.d_nstate, sizeof(nepx::NeighborState),
-                  cudaMemcpyDeviceToHost, s);
-  if (h_thermo && rows > 0)
-    cudaMemcpyAsync(h_thermo, md.d_rows, sizeof(double) * rows * nepx::kThermoCols,
-                    cudaMemcpyDeviceToHost, s);
+  // device-side status, box, neighbour flags and thermo rows land in pinned memory
+  const int publish_rows = h_thermo ? rows : 0;
+  nepx::launch_publish(e, md, d_status, &m->mirror->box, &m->mirror->status,
+                       &m->mirror->nstate, m->h_rows, publish_rows);
+  m->pending_thermo = publish_rows > 0 ? h_thermo : nullptr;
+  m->pending_rows = publish_rows;
   if (cudaPeekAtLastError() != cudaSuccess) return md_cuda(m, "enqueue run");
   return NEPX_OK;
 }
@@ -819,6 +877,11 @@ int md_finish(nepx_md* m)
 {
   nepx::Md& md = m->md;
   if (cudaStreamSynchronize(md.stream) != cudaSuccess) return md_cuda(m, "run");
+  if (m->pending_thermo) {
+    std::memcpy(m->pending_thermo, m->h_rows,
+                sizeof(double) * size_t(m->pending_rows) * nepx::kThermoCols);
+    m->pending_thermo = nullptr;
+  }
   md.box = m->mirror->box;
   const int status = m->mirror->status;
   const nepx::NeighborState& st = m->mirror->nstate;
