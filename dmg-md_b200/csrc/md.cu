@@ -40,6 +40,15 @@ struct nepx_md {
   double* pending_thermo = nullptr;   // the caller's row buffer, filled by md_finish
   int pending_rows = 0;
   cudaEvent_t noise_copied = nullptr;
+  // one-step calls replay one graph: draws' upload, the call's scalar kernel,
+  // the step and the publish; re-captured when any of its inputs changes
+  cudaGraphExec_t graph_call = nullptr;
+  struct CallKey {
+    nepx::StepParams p;
+    int precision, init, rows;
+    double T0, tau;
+    const void* bufs[5];
+  } call_key{};
   bool own_stream = false;
   std::string error;
 };
@@ -651,6 +660,7 @@ int nepx_md_destroy(nepx_md_t* m)
     if (p) cudaFree(p);
   if (m->h_noise) cudaFreeHost(m->h_noise);
   if (m->h_rows) cudaFreeHost(m->h_rows);
+  if (m->graph_call) cudaGraphExecDestroy(m->graph_call);
   if (m->mirror) cudaFreeHost(m->mirror);
   if (m->noise_copied) cudaEventDestroy(m->noise_copied);
   if (md.engine && md.engine->box_owner == &md) md.engine->box_owner = nullptr;
@@ -791,14 +801,19 @@ int md_enqueue_run(nepx_md* m, int steps, double dt_fs, int thermo_every, double
     }
     for (int q = 0; q < box_draws; ++q) z[2 + q] = md.rng.gasdev();
   }
-  cudaMemcpyAsync(md.d_noise, m->h_noise, sizeof(double) * nepx::kNoisePerStep * steps,
-                  cudaMemcpyHostToDevice, s);
-  cudaEventRecord(m->noise_copied, s);
+  // a one-step call uploads its draws inside the call graph
+  const bool fold = steps == 1;
+  if (!fold) {
+    cudaMemcpyAsync(md.d_noise, m->h_noise, sizeof(double) * nepx::kNoisePerStep * steps,
+                    cudaMemcpyHostToDevice, s);
+    cudaEventRecord(m->noise_copied, s);
+  }
   const int rows = thermo_every > 0 ? steps / thermo_every : 0;
   if (rows > md.rows_cap) {
     cudaStreamSynchronize(s);
     if (md.d_rows) cudaFree(md.d_rows);
     if (m->h_rows) cudaFreeHost(m->h_rows);
+  if (m->graph_call) cudaGraphExecDestroy(m->graph_call);
     md.d_rows = nullptr;
     m->h_rows = nullptr;
     if (!dalloc(md.d_rows, size_t(rows) * nepx::kThermoCols) ||
@@ -816,8 +831,11 @@ int md_enqueue_run(nepx_md* m, int steps, double dt_fs, int thermo_every, double
     if (md.forces_valid) nepx::launch_neighbor_update(e, N, md.d_pos, md.d_type, true, s);
     e.order_valid = false;
   }
-  if (first_step == 0) nepx::md_init_scalars(md, p, c.T0, p.dt * c.Tdamp);
-  else nepx::md_continue_scalars(md);
+  const double tau = p.dt * c.Tdamp;
+  if (!fold) {
+    if (first_step == 0) nepx::md_init_scalars(md, p, c.T0, tau);
+    else nepx::md_continue_scalars(md);
+  }
   if (!md.forces_valid) {
     nepx::launch_neighbor_update(e, N, md.d_pos, md.d_type, true, s);
     if (!e.tuned) nepx::engine_autotune(e, N, md.d_pos, md.d_type, s);
@@ -858,15 +876,55 @@ int md_enqueue_run(nepx_md* m, int steps, double dt_fs, int thermo_every, double
     md.graph_params = p;
     md.graph_precision = e.precision;
   }
-  int k = 0;
-  for (; k + nepx::kGraphSteps <= steps; k += nepx::kGraphSteps)
-    if (cudaGraphLaunch(md.graph_multi, s) != cudaSuccess) return md_cuda(m, "graph launch");
-  for (; k < steps; ++k)
-    if (cudaGraphLaunch(md.graph, s) != cudaSuccess) return md_cuda(m, "graph launch");
   // device-side status, box, neighbour flags and thermo rows land in pinned memory
   const int publish_rows = h_thermo ? rows : 0;
-  nepx::launch_publish(e, md, d_status, &m->mirror->box, &m->mirror->status,
-                       &m->mirror->nstate, m->h_rows, publish_rows);
+  if (fold) {
+    nepx_md::CallKey key{};
+    key.p = p;
+    key.precision = e.precision;
+    key.init = first_step == 0;
+    key.rows = publish_rows;
+    key.T0 = c.T0;
+    key.tau = tau;
+    key.bufs[0] = m->h_noise;
+    key.bufs[1] = md.d_noise;
+    key.bufs[2] = m->h_rows;
+    key.bufs[3] = md.d_rows;
+    key.bufs[4] = m->mirror;
+    if (!m->graph_call || std::memcmp(&key, &m->call_key, sizeof(key)) != 0) {
+      if (m->graph_call) cudaGraphExecDestroy(m->graph_call);
+      m->graph_call = nullptr;
+      cudaGraph_t g;
+      if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return md_cuda(m, "begin capture");
+      cudaMemcpyAsync(md.d_noise, m->h_noise, sizeof(double) * nepx::kNoisePerStep,
+                      cudaMemcpyHostToDevice, s);
+      if (key.init) nepx::md_init_scalars(md, p, c.T0, tau);
+      else nepx::md_continue_scalars(md);
+      nepx::md_enqueue_step(md, p, d_status);
+      nepx::launch_publish(e, md, d_status, &m->mirror->box, &m->mirror->status,
+                           &m->mirror->nstate, m->h_rows, publish_rows);
+      if (cudaStreamEndCapture(s, &g) != cudaSuccess) return md_cuda(m, "end capture");
+      if (cudaGraphInstantiate(&m->graph_call, g, 0) != cudaSuccess) {
+        cudaGraphDestroy(g);
+        m->graph_call = nullptr;
+        return md_cuda(m, "instantiate graph");
+      }
+      cudaGraphDestroy(g);
+      m->call_key = key;
+    }
+    if (cudaGraphLaunch(m->graph_call, s) != cudaSuccess) return md_cuda(m, "graph launch");
+    // the staging buffer of the draws is free again once the graph has run
+    cudaEventRecord(m->noise_copied, s);
+  } else {
+    int k = 0;
+    for (; k + nepx::kGraphSteps <= steps; k += nepx::kGraphSteps)
+      if (cudaGraphLaunch(md.graph_multi, s) != cudaSuccess) return md_cuda(m, "graph launch");
+    for (; k < steps; ++k)
+      if (cudaGraphLaunch(md.graph, s) != cudaSuccess) return md_cuda(m, "graph launch");
+    nepx::launch_publish(e, md, d_status, &m->mirror->box, &m->mirror->status,
+                         &m->mirror->nstate, m->h_rows, publish_rows);
+  }
   m->pending_thermo = publish_rows > 0 ? h_thermo : nullptr;
   m->pending_rows = publish_rows;
   if (cudaPeekAtLastError() != cudaSuccess) return md_cuda(m, "enqueue run");

@@ -114,6 +114,33 @@ def test_bdp_velocity_factor_bit_exact(tmp_path):
         assert np.sqrt(new / old) == rows[k, 18], k
 
 
+@pytest.mark.parametrize("kind,ens", [("nvt_bdp", dict(T0=300.0, T1=330.0, Tdamp=20.0)),
+                                      ("nvt_nhc", dict(T0=300.0, T1=300.0, Tdamp=50.0)),
+                                      ("npt_scr", dict(T0=300.0, T1=300.0, Tdamp=50.0,
+                                                       p_gpa=0.0, bulk_gpa=2.0, tau_p=500.0))])
+def test_one_step_calls_equal_one_run(kind, ens):
+    """A segment driven one step per call (each call one graph: the draws'
+    upload, the segment bookkeeping, the step and the status readback) is the
+    same trajectory, bit for bit, as the segment run in a single call."""
+    steps = 24
+    out = []
+    for per_step in (False, True):
+        pot, md, t, h = _water_md(150, 300.0, 9, kind=kind, seed=77, **ens)
+        if per_step:
+            rows = np.concatenate([md.run_segment(1, 0.5, k, steps, thermo_every=1)
+                                   for k in range(steps)])
+        else:
+            rows = md.run_segment(steps, 0.5, 0, steps, thermo_every=1)
+        s = md.state()
+        out.append((rows, s["pos"], s["vel"], s["h"]))
+        md.close()
+        pot.close()
+    (r0, p0, v0, h0), (r1, p1, v1, h1) = out
+    assert r0.shape == (steps, 20) and np.isfinite(r0).all()
+    assert np.array_equal(r0, r1)
+    assert np.array_equal(p0, p1) and np.array_equal(v0, v1) and np.array_equal(h0, h1)
+
+
 @pytest.mark.parametrize("kind", ["nvt_ber", "nvt_nhc", "nvt_bdp"])
 def test_thermostats_reach_target(kind):
     """Diamond carbon started at 200 K is driven to 500 K (Tdamp 50 steps)."""
