@@ -300,7 +300,7 @@ void engine_destroy(Engine& e)
                   nb.x0, e.scratch.alpha, e.scratch.f12, e.scratch.pe_ann, e.scratch.q,
                   e.scratch.tune_out, e.scratch.acoef, e.scratch.sites, e.scratch.qrad,
                   e.scratch.fp,
-                  e.scratch.order, e.scratch.type_counts, e.xr.er, e.xr.ea,
+                  e.scratch.order, e.scratch.type_counts, e.xr.er, e.xr.ea, e.xr.large,
                   e.xr.d_si, e.xr.d_soff};
   for (void* q : ptrs)
     if (q) cudaFree(q);

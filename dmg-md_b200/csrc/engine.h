@@ -58,6 +58,10 @@ struct ExplicitRows {
   int* cell_of = nullptr;     // [N], -1: the atom's structure scans all its atoms
   int cell_cap = 0;
   int n_cells = 0;            // cells in use (set with the structure table)
+  // [N] 1: the center's structure is not small (a batch only), so its rows
+  // hold each neighbour once, ascending, and its angular forces take the
+  // directed-f12 scheme of the large-box path
+  unsigned char* large = nullptr;
 };
 
 struct Engine {

@@ -86,7 +86,8 @@ k_rows_explicit(const ModelParams p, int total, const StructInfo* __restrict__ s
                 int mn_r, int* __restrict__ nn_a, float4* __restrict__ ea, int mn_a,
                 const int* __restrict__ cell_count, const int* __restrict__ cell_start,
                 const int* __restrict__ cell_atoms, const int* __restrict__ cell_of, int p2r,
-                const Site* __restrict__ sites, NeighborState* st)
+                const Site* __restrict__ sites, unsigned char* __restrict__ large, int mark_large,
+                NeighborState* st)
 {
   extern __shared__ int s_rows[];   // per warp: p2r row slots + a counter
   const int lane = threadIdx.x & 31;
@@ -294,6 +295,7 @@ k_rows_explicit(const ModelParams p, int total, const StructInfo* __restrict__ s
     if (lane == 0) {
       nn_r[i] = min(cr, mn_r);
       nn_a[i] = min(ca, mn_a);
+      large[i] = mark_large && !s.small ? 1 : 0;
       if (cr > mn_r) atomicOr(&st->overflow, 2);
       if (ca > mn_a) atomicOr(&st->overflow, 4);
       atomicMax(&st->max_nn[1], cr);
@@ -436,6 +438,7 @@ std::string engine_enable_xr(Engine& e, int max_struct)
     ok &= dalloc(x.cell_start, x.cell_cap) == cudaSuccess;
     ok &= dalloc(x.cell_atoms, N) == cudaSuccess;
     ok &= dalloc(x.cell_of, N) == cudaSuccess;
+    ok &= dalloc(x.large, N) == cudaSuccess;
     if (!ok) return "cudaMalloc failed (explicit neighbour rows)";
   }
   if (x.max_struct < max_struct) {
@@ -479,7 +482,7 @@ void launch_explicit_rows(Engine& e, int N, const double* pos, const int* type,
   k_rows_explicit<<<blocks, threads, smem, stream>>>(
     e.params, N, x.d_si, x.d_soff, x.n_struct, pos, type, e.nbr.nn_r, x.er, e.nbr.mn_r,
     e.nbr.nn_a, x.ea, e.nbr.mn_a, x.cell_count, x.cell_start, x.cell_atoms, x.cell_of, p2r,
-    e.scratch.sites, e.d_nstate);
+    e.scratch.sites, x.large, x.from_box ? 0 : 1, e.d_nstate);
 }
 
 void launch_explicit_row_indices(const Engine& e, int which, int n, int* nn, int* nl, int mn,

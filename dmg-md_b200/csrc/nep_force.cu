@@ -905,11 +905,14 @@ __device__ __forceinline__ void load_angular_tables(const ModelParams& p, float*
 
 // One group of G lanes per center: the directed angular partial force of
 // every edge of the center's angular row, f12[i][k] (float4, w unused).
-template <int G, int KM, int NAM, int LMAX>
+// XR: explicit rows of a batch; only the centers of structures that are not
+// small (each neighbour once in their rows) take this scheme.
+template <int G, int KM, int NAM, bool XR, int LMAX>
 __global__ void __launch_bounds__(kBlock)
 k_angular_f12(const ModelParams p, int N, const Box* __restrict__ box,
               const Site* __restrict__ sites,
               const int* __restrict__ nn_a, const int* __restrict__ nl_a, int mn_a,
+              const float4* __restrict__ ea, const unsigned char* __restrict__ large,
               const float* __restrict__ acoef, float4* __restrict__ f12)
 {
   constexpr int KP = (KM + 3) & ~3;
@@ -921,6 +924,9 @@ k_angular_f12(const ModelParams p, int N, const Box* __restrict__ box,
   const int gl = tid % G;
   const int i = blockIdx.x * (kBlock / G) + tid / G;
   if (i >= N) return;
+  if constexpr (XR) {
+    if (!large[i]) return;
+  }
   const Box b = *box;
   const Site me = sites[i];
   const double xi = me.x, yi = me.y, zi = me.z;
@@ -932,7 +938,15 @@ k_angular_f12(const ModelParams p, int N, const Box* __restrict__ box,
   for (int k = gl; k < na; k += G) {
     int t2;
     float dx, dy, dz;
-    site_displacement(b, sites, xi, yi, zi, arow[k], dx, dy, dz, t2);
+    if constexpr (XR) {
+      const float4 e = ea[static_cast<size_t>(i) * mn_a + k];
+      t2 = static_cast<int>(static_cast<unsigned>(__float_as_int(e.w)) >> kRowTypeShift);
+      dx = e.x;
+      dy = e.y;
+      dz = e.z;
+    } else {
+      site_displacement(b, sites, xi, yi, zi, arow[k], dx, dy, dz, t2);
+    }
     const float rc = (ra1 + p.rc_a[t2]) * 0.5f;
     const float3 f = angular_edge_force<KM, NAM, LMAX>(p, sm + (t1 * T + t2) * nA * KP, ai, rc,
                                                        dx, dy, dz);
@@ -955,7 +969,8 @@ k_gather(const ModelParams p, int N, const Box* __restrict__ box,
          int mn_r, const int* __restrict__ nn_a, const int* __restrict__ nl_a, int mn_a,
          const float4* __restrict__ er, const float4* __restrict__ ea,
          const float* __restrict__ acoef, const float* __restrict__ alpha,
-         const float4* __restrict__ f12, const double* __restrict__ pe_ann,
+         const float4* __restrict__ f12, const unsigned char* __restrict__ large,
+         const double* __restrict__ pe_ann,
          double* __restrict__ pe, double* __restrict__ force, double* __restrict__ virial,
          int accumulate, NeighborState* st)
 {
@@ -1031,6 +1046,7 @@ k_gather(const ModelParams p, int N, const Box* __restrict__ box,
     // angular exchange and ZBL
     const int na = nn_a[i];
     const int* arow = nl_a + static_cast<size_t>(i) * mn_a;
+    const bool large_i = XR && large[i];
     const int zi_ = p.Z[t1];
     const float pow_zi = p.zbl ? powf(static_cast<float>(zi_), 0.23f) : 0.0f;
     for (int k = gl; k < na; k += G) {
@@ -1045,17 +1061,36 @@ k_gather(const ModelParams p, int N, const Box* __restrict__ box,
         dx = e.x;
         dy = e.y;
         dz = e.z;
-        const float rc = (p.rc_a[t1] + p.rc_a[t2]) * 0.5f;
-        const int nA = p.nA;
-        constexpr int NLM = num_lm<LMAX>();
-        const float3 fij = angular_edge_force<KM, NAM, LMAX>(
-          p, sm + (t1 * T + t2) * nA * KP, acoef + static_cast<size_t>(i) * nA * NLM, rc, dx,
-          dy, dz);
-        const float3 fji = angular_edge_force<KM, NAM, LMAX>(
-          p, sm + (t2 * T + t1) * nA * KP, acoef + static_cast<size_t>(j) * nA * NLM, rc, -dx,
-          -dy, -dz);
-        a12 = make_float4(fij.x, fij.y, fij.z, 0.0f);
-        a21 = make_float4(fji.x, fji.y, fji.z, 0.0f);
+        if (large_i) {
+          // a structure that is not small: j once in i's row and i once in
+          // j's (rows ascend by the packed index), f12 from k_angular_f12
+          a12 = f12[static_cast<size_t>(i) * mn_a + k];
+          const int* jw = reinterpret_cast<const int*>(ea + static_cast<size_t>(j) * mn_a) + 3;
+          const int nj = nn_a[j];
+          int lo = 0, hi = nj - 1;
+          while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if ((__ldg(jw + 4 * mid) & kRowIndexMask) < i) lo = mid + 1; else hi = mid;
+          }
+          a21 = f12[static_cast<size_t>(j) * mn_a + lo];
+          if (nj == 0 || (__ldg(jw + 4 * lo) & kRowIndexMask) != i) {
+            // only a truncated (overflowed) row can lose the reverse edge
+            a21 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            atomicOr(&st->overflow, 4);
+          }
+        } else {
+          const float rc = (p.rc_a[t1] + p.rc_a[t2]) * 0.5f;
+          const int nA = p.nA;
+          constexpr int NLM = num_lm<LMAX>();
+          const float3 fij = angular_edge_force<KM, NAM, LMAX>(
+            p, sm + (t1 * T + t2) * nA * KP, acoef + static_cast<size_t>(i) * nA * NLM, rc, dx,
+            dy, dz);
+          const float3 fji = angular_edge_force<KM, NAM, LMAX>(
+            p, sm + (t2 * T + t1) * nA * KP, acoef + static_cast<size_t>(j) * nA * NLM, rc, -dx,
+            -dy, -dz);
+          a12 = make_float4(fij.x, fij.y, fij.z, 0.0f);
+          a21 = make_float4(fji.x, fji.y, fji.z, 0.0f);
+        }
       } else {
         const int j = arow[k];
         site_displacement(b, sites, xi, yi, zi, j, dx, dy, dz, t2);
@@ -1224,9 +1259,14 @@ void launch_f12_t(Engine& e, int N, cudaStream_t s)
   const int blocks = (N + APB - 1) / APB;
   const size_t smem =
     sizeof(float) * e.params.T * e.params.T * e.params.nA * ((KM + 3) & ~3);
-  k_angular_f12<G, KM, NAM, LMAX><<<blocks, kBlock, smem, s>>>(
-    e.params, N, e.d_box, e.scratch.sites, nb.nn_a, nb.nl_a, nb.mn_a, e.scratch.acoef,
-    e.scratch.f12);
+  if (e.use_xr)
+    k_angular_f12<G, KM, NAM, true, LMAX><<<blocks, kBlock, smem, s>>>(
+      e.params, N, e.d_box, e.scratch.sites, nb.nn_a, nb.nl_a, nb.mn_a, e.xr.ea, e.xr.large,
+      e.scratch.acoef, e.scratch.f12);
+  else
+    k_angular_f12<G, KM, NAM, false, LMAX><<<blocks, kBlock, smem, s>>>(
+      e.params, N, e.d_box, e.scratch.sites, nb.nn_a, nb.nl_a, nb.mn_a, e.xr.ea, e.xr.large,
+      e.scratch.acoef, e.scratch.f12);
 }
 
 template <int G, int NRM, int KM, int NAM, int LMAX>
@@ -1249,7 +1289,8 @@ void launch_gather_t(Engine& e, int N, double* pe, double* force, double* virial
     XR ? sizeof(float) * e.params.T * e.params.T * e.params.nA * ((KM + 3) & ~3) : 0;
   k_gather<G, KM, NAM, XR, LMAX><<<blocks, threads, smem, s>>>(
     e.params, N, e.d_box, e.scratch.sites, nb.nn_r, nb.nl_r, nb.mn_r, nb.nn_a, nb.nl_a, nb.mn_a,
-    e.xr.er, e.xr.ea, e.scratch.acoef, e.scratch.alpha, e.scratch.f12, e.scratch.pe_ann, pe,
+    e.xr.er, e.xr.ea, e.scratch.acoef, e.scratch.alpha, e.scratch.f12, e.xr.large,
+    e.scratch.pe_ann, pe,
     force, virial, accumulate ? 1 : 0, e.d_nstate);
 }
 
@@ -1344,7 +1385,9 @@ void launch_descriptor(Engine& e, int N, const double*, const int*, cudaStream_t
     else if (small) launch_acoef_t<4, round4(kSmallK), 4>(e, N, stream);
     else launch_acoef_t<4, round4(kMaxBasis), 4>(e, N, stream);
   }
-  if (e.use_xr) return;   // the explicit-row gather evaluates the angular forces itself
+  // a single explicit-row system: the gather evaluates both directed angular
+  // forces itself; a batch's structures that are not small take f12 here
+  if (e.use_xr && e.xr.from_box) return;
   if (high) launch_f12_t<kHighGroup, kMaxBasis, kMaxN, 8>(e, N, stream);
   else if (e.f12_group == 8) {
     if (small) launch_f12_t<8, kSmallK, kSmallN, 4>(e, N, stream);
