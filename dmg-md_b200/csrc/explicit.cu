@@ -335,28 +335,48 @@ __global__ void k_xcell_assign(int total, const StructInfo* __restrict__ si,
   atomicAdd(cell_count + cell, 1);
 }
 
-// Exclusive scan of the cell counts (one block); counts reset as fill cursors.
-__global__ void k_xcell_scan(int ncells, int* cell_count, int* cell_start)
+// Exclusive scan of the cell counts, one block per structure: a structure's
+// cells are contiguous and its atoms fill [off, off + n) of cell_atoms, so
+// its cells start at off plus the scan of its own counts (coalesced chunks
+// of blockDim.x cells with a running carry).  Counts reset as fill cursors.
+__global__ void k_xcell_scan(const StructInfo* __restrict__ si, int* cell_count, int* cell_start)
 {
-  __shared__ int part[1024];
-  const int per = (ncells + blockDim.x - 1) / blockDim.x;
-  const int lo = threadIdx.x * per, hi = min(ncells, lo + per);
-  int sum = 0;
-  for (int c = lo; c < hi; ++c) sum += cell_count[c];
-  part[threadIdx.x] = sum;
-  __syncthreads();
-  for (int o = 1; o < blockDim.x; o <<= 1) {
-    const int v = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+  __shared__ int warp_sum[32];
+  __shared__ int carry_s;
+  const StructInfo& s = si[blockIdx.x];
+  if (s.nc[0] == 0) return;   // block-uniform: the structure scans all its atoms
+  const int ncs = s.nc[0] * s.nc[1] * s.nc[2];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int carry = s.off;
+  for (int c0 = 0; c0 < ncs; c0 += blockDim.x) {
+    const int c = c0 + threadIdx.x;
+    const int v = c < ncs ? cell_count[s.cell_base + c] : 0;
+    int incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += u;
+    }
+    if (lane == 31) warp_sum[warp] = incl;
     __syncthreads();
-    part[threadIdx.x] += v;
+    if (warp == 0) {
+      int w = lane < nw ? warp_sum[lane] : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(kFull, w, o);
+        if (lane >= o) w += u;
+      }
+      if (lane < nw) warp_sum[lane] = w;   // inclusive over warps
+      if (lane == 31) carry_s = w;         // chunk total
+    }
     __syncthreads();
-  }
-  int run = part[threadIdx.x] - sum;
-  for (int c = lo; c < hi; ++c) {
-    const int k = cell_count[c];
-    cell_start[c] = run;
-    run += k;
-    cell_count[c] = 0;
+    const int before = (warp > 0 ? warp_sum[warp - 1] : 0) + incl - v;
+    if (c < ncs) {
+      cell_start[s.cell_base + c] = carry + before;
+      cell_count[s.cell_base + c] = 0;
+    }
+    carry += carry_s;
+    __syncthreads();   // warp_sum and carry_s are rewritten by the next chunk
   }
 }
 
@@ -470,7 +490,7 @@ void launch_explicit_rows(Engine& e, int N, const double* pos, const int* type,
     cudaMemsetAsync(x.cell_count, 0, sizeof(int) * x.n_cells, stream);
     k_xcell_assign<<<(N + threads - 1) / threads, threads, 0, stream>>>(
       N, x.d_si, x.d_soff, x.n_struct, pos, x.cell_count, x.cell_of);
-    k_xcell_scan<<<1, 1024, 0, stream>>>(x.n_cells, x.cell_count, x.cell_start);
+    k_xcell_scan<<<x.n_struct, 1024, 0, stream>>>(x.d_si, x.cell_count, x.cell_start);
     k_xcell_fill<<<(N + threads - 1) / threads, threads, 0, stream>>>(
       N, x.cell_of, x.cell_count, x.cell_start, x.cell_atoms);
   }
