@@ -139,11 +139,21 @@ k_rows_explicit(const ModelParams p, int total, const StructInfo* __restrict__ s
         const int sp1 = (b.pbc[1] && nc1 >= 5) ? 5 : nc1;
         const int sp2 = (b.pbc[2] && nc2 >= 5) ? 5 : nc2;
         const int ns = sp0 * sp1 * sp2;   // at most 125
+        const bool full = sp0 == 5 && sp1 == 5 && sp2 == 5;   // usual: constant divisors
         for (int r0 = 0; r0 < ns; r0 += 32) {
           int my_start = 0, my_cnt = 0;
           if (r0 + lane < ns) {
             const int q = r0 + lane;
-            const int q0 = q % sp0, q1 = (q / sp0) % sp1, q2 = q / (sp0 * sp1);
+            int q0, q1, q2;
+            if (full) {
+              q0 = q % 5;
+              q1 = (q / 5) % 5;
+              q2 = q / 25;
+            } else {
+              q0 = q % sp0;
+              q1 = (q / sp0) % sp1;
+              q2 = q / (sp0 * sp1);
+            }
             int gx = sp0 == 5 ? cx + q0 - 2 : q0;
             int gy = sp1 == 5 ? cy + q1 - 2 : q1;
             int gz = sp2 == 5 ? cz + q2 - 2 : q2;
