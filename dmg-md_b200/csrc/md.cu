@@ -568,6 +568,17 @@ bool pinned_mapped(T*& p, size_t count)
   return true;
 }
 
+// The captured graphs hold the draw, row and status buffers' addresses as
+// kernel and copy parameters: dropped (and captured again on the next run)
+// whenever one of those buffers is reallocated.
+void drop_graphs(nepx_md* m)
+{
+  for (cudaGraphExec_t* x : {&m->md.graph, &m->md.graph_multi, &m->graph_call}) {
+    if (*x) cudaGraphExecDestroy(*x);
+    *x = nullptr;
+  }
+}
+
 int* status_buffer(nepx_md* m)
 {
   // one int of device status behind the partials (allocated with them)
@@ -652,15 +663,13 @@ int nepx_md_destroy(nepx_md_t* m)
   if (!m) return NEPX_ERR_ARG;
   nepx::Md& md = m->md;
   if (md.stream) cudaStreamSynchronize(md.stream);
-  if (md.graph) cudaGraphExecDestroy(md.graph);
-  if (md.graph_multi) cudaGraphExecDestroy(md.graph_multi);
+  drop_graphs(m);
   void* ptrs[] = {md.d_type, md.d_mass, md.d_pos, md.d_vel, md.d_force, md.d_pe, md.d_virial,
                   md.d_partials, md.d_sc, md.d_noise, md.d_rows};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (m->h_noise) cudaFreeHost(m->h_noise);
   if (m->h_rows) cudaFreeHost(m->h_rows);
-  if (m->graph_call) cudaGraphExecDestroy(m->graph_call);
   if (m->mirror) cudaFreeHost(m->mirror);
   if (m->noise_copied) cudaEventDestroy(m->noise_copied);
   if (md.engine && md.engine->box_owner == &md) md.engine->box_owner = nullptr;
@@ -779,6 +788,7 @@ int md_enqueue_run(nepx_md* m, int steps, double dt_fs, int thermo_every, double
     cudaStreamSynchronize(s);
     if (md.d_noise) cudaFree(md.d_noise);
     if (m->h_noise) cudaFreeHost(m->h_noise);
+    drop_graphs(m);   // they hold the old buffers' addresses
     md.d_noise = nullptr;
     m->h_noise = nullptr;
     if (!dalloc(md.d_noise, nepx::kNoisePerStep * size_t(steps)) ||
@@ -813,7 +823,7 @@ int md_enqueue_run(nepx_md* m, int steps, double dt_fs, int thermo_every, double
     cudaStreamSynchronize(s);
     if (md.d_rows) cudaFree(md.d_rows);
     if (m->h_rows) cudaFreeHost(m->h_rows);
-  if (m->graph_call) cudaGraphExecDestroy(m->graph_call);
+    drop_graphs(m);   // they hold the old buffers' addresses
     md.d_rows = nullptr;
     m->h_rows = nullptr;
     if (!dalloc(md.d_rows, size_t(rows) * nepx::kThermoCols) ||

@@ -141,6 +141,35 @@ def test_one_step_calls_equal_one_run(kind, ens):
     assert np.array_equal(p0, p1) and np.array_equal(v0, v1) and np.array_equal(h0, h1)
 
 
+def test_buffers_regrow_inside_a_segment():
+    """Calls of 1, 9 and 20 steps inside one 30-step segment: the draw and
+    row buffers grow between calls while the step parameters stay the same,
+    so the captured graphs must follow the new buffers.  The trajectory is
+    the one-call segment's, bit for bit, and a second MD on the same handle
+    afterwards runs cleanly."""
+    ens = dict(T0=300.0, T1=320.0, Tdamp=20.0, seed=5)
+    out = []
+    for calls in ([30], [1, 9, 20]):
+        pot, md, t, h = _water_md(150, 300.0, 12, kind="nvt_bdp", **ens)
+        rows, first = [], 0
+        for c in calls:
+            rows.append(md.run_segment(c, 0.5, first, 30, thermo_every=1))
+            first += c
+        s = md.state()
+        out.append((np.concatenate(rows), s["pos"], s["vel"]))
+        md.close()
+        md2 = _nepx().MD(pot, t, np.where(t == 0, 15.999, 1.008), s["pos"], s["vel"], h)
+        md2.set_ensemble("nve")
+        r2 = md2.run(4, 0.5, thermo_every=2)
+        assert np.isfinite(r2).all()
+        md2.close()
+        pot.close()
+    (r0, p0, v0), (r1, p1, v1) = out
+    assert r0.shape == (30, 20)
+    assert np.array_equal(r0, r1)
+    assert np.array_equal(p0, p1) and np.array_equal(v0, v1)
+
+
 @pytest.mark.parametrize("kind", ["nvt_ber", "nvt_nhc", "nvt_bdp"])
 def test_thermostats_reach_target(kind):
     """Diamond carbon started at 200 K is driven to 500 K (Tdamp 50 steps)."""
