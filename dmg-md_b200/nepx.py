@@ -103,7 +103,8 @@ def lib():
         L.nepx_md_last_error.restype = ctypes.c_char_p
         L.nepx_md_set_ensemble.argtypes = [vp, ctypes.c_int, dp, ctypes.c_uint]
         L.nepx_md_set_barostat.argtypes = [vp, ctypes.c_int, dp, dp]
-        L.nepx_md_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, dp]
+        # the thermo buffer goes as an address (one-step calls are a hot loop)
+        L.nepx_md_run.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, vp]
         L.nepx_md_get.argtypes = [vp, dp, dp, dp, dp, dp, ctypes.POINTER(Box)]
         L.nepx_compute_noalloc.argtypes = [vp, ctypes.POINTER(Box), ctypes.c_int, vp, vp, vp, vp,
                                            vp, vp]
@@ -115,7 +116,7 @@ def lib():
                                            ctypes.POINTER(vp), ctypes.POINTER(vp),
                                            ctypes.POINTER(vp)]
         L.nepx_set_precision.argtypes = [vp, ctypes.c_int]
-        L.nepx_md_run_segment.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, dp,
+        L.nepx_md_run_segment.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, vp,
                                           ctypes.c_int, ctypes.c_int]
         L.nepx_compute_batch.argtypes = [vp, ctypes.POINTER(StructDesc), ctypes.c_int, vp, vp, vp,
                                          vp, vp, ctypes.c_uint, vp]
@@ -350,7 +351,7 @@ class MD:
         rows = steps // thermo_every if thermo_every else 0
         out = np.zeros((max(rows, 1), len(THERMO_COLUMNS)))
         self._check(lib().nepx_md_run(self._h, steps, dt_fs, thermo_every,
-                                      _dp(out) if rows else None))
+                                      out.ctypes.data if rows else None))
         return out[:rows] if rows else None
 
     def run_segment(self, steps, dt_fs, first_step, segment_steps, thermo_every=0):
@@ -359,7 +360,7 @@ class MD:
         rows = steps // thermo_every if thermo_every else 0
         out = np.zeros((max(rows, 1), len(THERMO_COLUMNS)))
         self._check(lib().nepx_md_run_segment(self._h, steps, dt_fs, thermo_every,
-                                              _dp(out) if rows else None, first_step,
+                                              out.ctypes.data if rows else None, first_step,
                                               segment_steps))
         return out[:rows] if rows else None
 
