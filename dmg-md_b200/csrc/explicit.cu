@@ -201,20 +201,51 @@ k_rows_explicit(const ModelParams p, int total, const StructInfo* __restrict__ s
       const int used = min(found, p2r);
       int p2 = 1;
       while (p2 < used) p2 <<= 1;
-      for (int k = used + lane; k < p2; k += 32) buf[k] = INT_MAX;
-      __syncwarp();
-      for (int k = 2; k <= p2; k <<= 1) {   // bitonic sort, one pair per lane and pass
-        for (int jj = k >> 1; jj > 0; jj >>= 1) {
-          for (int q = lane; q < (p2 >> 1); q += 32) {
-            const int t = ((q & ~(jj - 1)) << 1) | (q & (jj - 1));
-            const int u = t | jj;
-            const int a = buf[t], c = buf[u];
-            if ((a > c) == ((t & k) == 0)) {
-              buf[t] = c;
-              buf[u] = a;
+      if (p2 <= 64) {
+        // bitonic sort in registers: element e = lane in a, e = lane + 32 in
+        // c; partners e ^ jj exchange by shuffle (jj < 32) or inside the lane
+        // (jj = 32); e keeps the smaller value when (e < partner) matches the
+        // ascending direction (e & k) == 0 of its block
+        int a = lane < used ? buf[lane] : INT_MAX;
+        int c = lane + 32 < used ? buf[lane + 32] : INT_MAX;
+        const bool two = p2 > 32;   // warp-uniform
+        for (int k = 2; k <= p2; k <<= 1) {
+          for (int jj = k >> 1; jj > 0; jj >>= 1) {
+            if (jj == 32) {
+              const int lo_v = min(a, c);
+              c = max(a, c);
+              a = lo_v;
+            } else {
+              const bool lower = (lane & jj) == 0;
+              const int pa = __shfl_xor_sync(kFull, a, jj);
+              a = (lower == ((lane & k) == 0)) ? min(a, pa) : max(a, pa);
+              if (two) {
+                const int pc = __shfl_xor_sync(kFull, c, jj);
+                c = (lower == (((lane + 32) & k) == 0)) ? min(c, pc) : max(c, pc);
+              }
             }
           }
-          __syncwarp();
+        }
+        __syncwarp();   // every lane has read buf before it is overwritten
+        if (lane < used) buf[lane] = a;
+        if (lane + 32 < used) buf[lane + 32] = c;
+        __syncwarp();
+      } else {
+        for (int k = used + lane; k < p2; k += 32) buf[k] = INT_MAX;
+        __syncwarp();
+        for (int k = 2; k <= p2; k <<= 1) {   // bitonic sort, one pair per lane and pass
+          for (int jj = k >> 1; jj > 0; jj >>= 1) {
+            for (int q = lane; q < (p2 >> 1); q += 32) {
+              const int t = ((q & ~(jj - 1)) << 1) | (q & (jj - 1));
+              const int u = t | jj;
+              const int a = buf[t], c = buf[u];
+              if ((a > c) == ((t & k) == 0)) {
+                buf[t] = c;
+                buf[u] = a;
+              }
+            }
+            __syncwarp();
+          }
         }
       }
       // ascending radial row; the angular row is its subset inside the angular cutoff
