@@ -18,8 +18,11 @@
 // that are not small use the large-box arithmetic (double difference rounded
 // to float, float minimum image, reference nep.cu:503-561); their candidates
 // come from a cell grid of their own (cells at least rc/2 thick, 5x5x5 stencil,
-// one counting sort over the whole batch), and each row is sorted in shared
-// memory, which yields the large-box path's typewise rows exactly.
+// a counting sort per batch scanned per structure), and each row is sorted
+// (warp-shuffle bitonic network up to 64 entries, shared memory above), which
+// yields the large-box path's typewise rows exactly.  Those structures' rows
+// hold each neighbour once, so a batch marks their centers (large[]) for the
+// directed-f12 scheme of the large-box path.
 //
 // Row entry: float4 (x12, y12, z12, bits of j | type(j) << 28), row-major
 // [center][slot]; radial and angular rows are separate.
