@@ -27,19 +27,12 @@ const char* const kUnsupportedBox =
   "box thinner than 2.5 (rc + 1) in one periodic direction and thicker than 10 rc in another "
   "(unsupported, as in the reference)";
 
-// Device flags of the previous call; ready only when its copy has landed
-// (or immediately when `wait`).
-int check_state(nepx_handle* h, bool wait)
+}  // namespace
+
+namespace nepx {
+
+int decode_state(nepx_handle* h, const NeighborState& s)
 {
-  if (!h->state_pending) return NEPX_OK;
-  if (wait) {
-    if (cudaEventSynchronize(h->state_ready) != cudaSuccess) return cuda_fail(h, "event sync");
-  } else if (cudaEventQuery(h->state_ready) != cudaSuccess) {
-    cudaGetLastError();   // clear cudaErrorNotReady
-    return NEPX_OK;
-  }
-  h->state_pending = false;
-  const nepx::NeighborState& s = *h->h_state;
   if (s.overflow) {
     const char* which = (s.overflow & 1) ? "Verlet" : (s.overflow & 2) ? "radial" : "angular";
     return fail(h, NEPX_ERR_OVERFLOW,
@@ -53,7 +46,22 @@ int check_state(nepx_handle* h, bool wait)
   return NEPX_OK;
 }
 
-}  // namespace
+int check_state(nepx_handle* h, bool wait)
+{
+  if (!h->state_pending) return NEPX_OK;
+  if (wait) {
+    if (cudaEventSynchronize(h->state_ready) != cudaSuccess) return cuda_fail(h, "event sync");
+  } else if (cudaEventQuery(h->state_ready) != cudaSuccess) {
+    cudaGetLastError();   // clear cudaErrorNotReady
+    return NEPX_OK;
+  }
+  h->state_pending = false;
+  return decode_state(h, *h->h_state);
+}
+
+}  // namespace nepx
+
+using nepx::check_state;
 
 // Why the last nepx_create of this thread failed (no handle to hold it).
 thread_local std::string t_create_error;

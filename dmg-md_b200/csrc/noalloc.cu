@@ -38,7 +38,9 @@ static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBy
 std::mutex g_setup_mutex;
 void* g_scratch_ptr[kMaxDevices] = {nullptr};
 
-// Device address of g_static_scratch on the current device, resolved once.
+// Device address of g_static_scratch on the current device, resolved once
+// per device (cudaGetSymbolAddress; the host-side name of a __device__ array
+// is only a stand-in, not a device address).
 cudaError_t static_scratch(void** out)
 {
   int dev = 0;
@@ -98,6 +100,38 @@ size_t bytes_needed(const nepx::Engine& e, int n)
   return c.used;
 }
 
+// The handle's engine runs the launches with its per-call buffers pointed
+// into the static array for the duration of one call; the destructor puts the
+// handle's own buffers back on every exit path.  Only plain pointer and
+// scalar fields change hands (the model's host vectors are never copied), so
+// nothing is allocated on the host either.
+struct BorrowedBuffers {
+  nepx::Engine& e;
+  nepx::Box* d_box;
+  nepx::NeighborState* d_nstate;
+  nepx::NeighborBuffers nbr;
+  nepx::ForceScratch scratch;
+  int capacity;
+  bool tuned, use_xr;
+  int precision;
+  explicit BorrowedBuffers(nepx::Engine& eng)
+    : e(eng), d_box(eng.d_box), d_nstate(eng.d_nstate), nbr(eng.nbr), scratch(eng.scratch),
+      capacity(eng.capacity), tuned(eng.tuned), use_xr(eng.use_xr), precision(eng.precision)
+  {
+  }
+  ~BorrowedBuffers()
+  {
+    e.d_box = d_box;
+    e.d_nstate = d_nstate;
+    e.nbr = nbr;
+    e.scratch = scratch;
+    e.capacity = capacity;
+    e.tuned = tuned;
+    e.use_xr = use_xr;
+    e.precision = precision;
+  }
+};
+
 }  // namespace
 
 extern "C" int nepx_compute_noalloc(nepx_t* h, const nepx_box* box, int n, const int* d_type,
@@ -109,81 +143,82 @@ extern "C" int nepx_compute_noalloc(nepx_t* h, const nepx_box* box, int n, const
     h->error = "null pointer or n < 1";
     return NEPX_ERR_ARG;
   }
-  const nepx::Engine& owner = h->engine;
-  if (bytes_needed(owner, n) > kStaticScratchBytes) {
+  nepx::Engine& e = h->engine;
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev != e.device) {
+    cudaGetLastError();
+    h->error = "the current CUDA device is not the one the handle was created on";
+    return NEPX_ERR_ARG;
+  }
+  if (bytes_needed(e, n) > kStaticScratchBytes) {
     h->error = "n = " + std::to_string(n) +
                " needs more than the 16 MiB static scratch of nepx_compute_noalloc";
     return NEPX_ERR_CAPACITY;
   }
   nepx::Box b;
   std::string err = nepx::make_box(box->h, box->pbc, b);
-  if (!err.empty() || !nepx::large_box_ok(owner, b)) {
+  if (!err.empty() || !nepx::large_box_ok(e, b)) {
     h->error = err.empty() ? "box thinner than 2.5 (rc + skin) in a periodic direction" : err;
     return NEPX_ERR_BOX;
   }
   void* base = nullptr;
   if (static_scratch(&base) != cudaSuccess) {
+    cudaGetLastError();
     h->error = "cudaGetSymbolAddress of the static scratch failed";
     return NEPX_ERR_CUDA;
   }
-  // an engine view whose per-atom buffers all live in the static array
-  nepx::Engine view = owner;
-  Carver c{static_cast<unsigned char*>(base)};
-  const size_t N = n;
-  const size_t cells = std::max<size_t>(N, 4096);
-  nepx::NeighborBuffers& nb = view.nbr;
-  view.d_box = c.take<nepx::Box>(1);
-  view.d_nstate = c.take<nepx::NeighborState>(1);
-  nb.nn_v = c.take<int>(N);
-  nb.nl_v = c.take<int>(N * nb.mn_v);
-  nb.nn_r = c.take<int>(N);
-  nb.nl_r = c.take<int>(N * nb.mn_r);
-  nb.nn_a = c.take<int>(N);
-  nb.nl_a = c.take<int>(N * nb.mn_a);
-  nb.cell_count = c.take<int>(cells);
-  nb.cell_start = c.take<int>(cells);
-  nb.cell_atoms = c.take<int>(N);
-  nb.cell_of = c.take<int>(N);
-  nb.x0 = c.take<double>(3 * N);
-  nb.cell_cap = static_cast<int>(cells);
-  view.scratch.sites = c.take<nepx::Site>(N);
-  view.scratch.qrad = c.take<float>(N * view.params.nR);
-  view.scratch.alpha = c.take<float>(N * view.params.T * nepx::basis_stride(view.params));
-  view.scratch.f12 = c.take<float4>(N * nb.mn_a);
-  view.scratch.pe_ann = c.take<double>(N);
-  view.scratch.acoef = c.take<float>(N * view.params.nA * view.params.nlm);
-  view.capacity = n;
-  view.tuned = true;   // keeps the handle's kernel variants; no timing runs here
-  view.precision = 0;  // the mixed path's buffers are not part of the static scratch
-  view.use_xr = false;
+  // an earlier asynchronous nepx_compute on this handle may still have its
+  // flags on the way into the pinned mirror: report its errors before this
+  // call reuses the mirror
+  int rc = nepx::check_state(h, true);
+  if (rc) return rc;
   auto s = static_cast<cudaStream_t>(stream);
-  // the handle's pinned flag mirror may still receive a copy from an earlier
-  // nepx_compute; let it land before this call reuses the mirror
-  if (h->state_pending) cudaEventSynchronize(h->state_ready);
-  // the array keeps the previous call's contents: clear the flags, rebuild
-  cudaMemsetAsync(view.d_nstate, 0, sizeof(nepx::NeighborState), s);
-  nepx::launch_set_box(view, b, s);
-  nepx::launch_neighbor_update(view, n, d_pos, d_type, true, s);
-  nepx::launch_force(view, n, d_pos, d_type, d_pe, d_force, d_virial, false, s);
-  if (cudaPeekAtLastError() != cudaSuccess) {
-    h->error = std::string("kernel launch: ") + cudaGetErrorString(cudaGetLastError());
-    return NEPX_ERR_CUDA;
+  {
+    BorrowedBuffers keep(e);
+    Carver c{static_cast<unsigned char*>(base)};
+    const size_t N = n;
+    const size_t cells = std::max<size_t>(N, 4096);
+    nepx::NeighborBuffers& nb = e.nbr;
+    e.d_box = c.take<nepx::Box>(1);
+    e.d_nstate = c.take<nepx::NeighborState>(1);
+    nb.nn_v = c.take<int>(N);
+    nb.nl_v = c.take<int>(N * nb.mn_v);
+    nb.nn_r = c.take<int>(N);
+    nb.nl_r = c.take<int>(N * nb.mn_r);
+    nb.nn_a = c.take<int>(N);
+    nb.nl_a = c.take<int>(N * nb.mn_a);
+    nb.cell_count = c.take<int>(cells);
+    nb.cell_start = c.take<int>(cells);
+    nb.cell_atoms = c.take<int>(N);
+    nb.cell_of = c.take<int>(N);
+    nb.x0 = c.take<double>(3 * N);
+    nb.cell_cap = static_cast<int>(cells);
+    e.scratch.sites = c.take<nepx::Site>(N);
+    e.scratch.qrad = c.take<float>(N * e.params.nR);
+    e.scratch.alpha = c.take<float>(N * e.params.T * nepx::basis_stride(e.params));
+    e.scratch.f12 = c.take<float4>(N * nb.mn_a);
+    e.scratch.pe_ann = c.take<double>(N);
+    e.scratch.acoef = c.take<float>(N * e.params.nA * e.params.nlm);
+    e.capacity = n;
+    e.tuned = true;      // keeps the handle's kernel variants; no timing runs here
+    e.precision = 0;     // FP32 ANN: the mixed path's buffers are not in the static array
+    e.use_xr = false;
+    // the array keeps the previous call's contents: clear the flags, rebuild
+    cudaMemsetAsync(e.d_nstate, 0, sizeof(nepx::NeighborState), s);
+    nepx::launch_set_box(e, b, s);
+    nepx::launch_neighbor_update(e, n, d_pos, d_type, true, s);
+    nepx::launch_force(e, n, d_pos, d_type, d_pe, d_force, d_virial, false, s);
+    if (cudaPeekAtLastError() != cudaSuccess) {
+      h->error = std::string("kernel launch: ") + cudaGetErrorString(cudaGetLastError());
+      return NEPX_ERR_CUDA;
+    }
+    // h_state is the handle's pinned flag mirror, allocated by nepx_create
+    cudaMemcpyAsync(h->h_state, e.d_nstate, sizeof(nepx::NeighborState),
+                    cudaMemcpyDeviceToHost, s);
   }
-  // h_state is the handle's pinned flag mirror, allocated by nepx_create
-  cudaMemcpyAsync(h->h_state, view.d_nstate, sizeof(nepx::NeighborState),
-                  cudaMemcpyDeviceToHost, s);
   if (cudaStreamSynchronize(s) != cudaSuccess) {
     h->error = std::string("stream: ") + cudaGetErrorString(cudaGetLastError());
     return NEPX_ERR_CUDA;
   }
-  h->state_pending = false;
-  if (h->h_state->overflow) {
-    h->error = "a neighbour row exceeded its capacity; raise MN_radial/MN_angular in nep.txt";
-    return NEPX_ERR_OVERFLOW;
-  }
-  if (h->h_state->nonfinite) {
-    h->error = "non-finite energy or force";
-    return NEPX_ERR_NONFINITE;
-  }
-  return NEPX_OK;
+  return nepx::decode_state(h, *h->h_state);
 }

@@ -11,8 +11,7 @@
  * the process.
  *
  * Each entry point names the reference (DMG-MD, zhangfeifan21/DMG-MD)
- * interface it replaces.  INTEGRATION.md shows the bindings a maintainer of
- * the reference adds (a NepForce adapter in C++ and a ctypes stub).
+ * interface it replaces.
  */
 #ifndef NEPX_H
 #define NEPX_H
@@ -97,18 +96,25 @@ int nepx_compute(nepx_t* handle, const nepx_box* box, int n, const int* d_type,
  * nepx_compute for callers that cannot allocate device memory while they run:
  * codes whose start-up hands all device memory to their own pool allocator,
  * and real-time or safety-reviewed drivers that forbid allocator calls after
- * initialisation.  This call allocates nothing (no cudaMalloc, cudaFree or
- * allocating library routine): all per-call scratch comes from one 16 MiB
- * static device array inside the library, held by every GPU that loads it
- * until the process exits.  n is limited by what fits in those 16 MiB for
- * the handle's neighbour capacities (about 5 KB per atom for MN_radial 250:
- * some 2,500-3,000 atoms); larger n returns NEPX_ERR_CAPACITY.  The handle
- * (nepx_create, max_atoms may be 1) supplies only the model parameters.
- * The first call on a device resolves the array's device address; make it
- * before any stream capture.  Calls share the array: neighbour rows are
- * rebuilt and flags cleared on every call, and calls that overlap on the
- * GPU race.  Synchronises `stream`.  Arguments and outputs as nepx_compute
- * (outputs overwritten).
+ * initialisation.  This call allocates no device memory (no cudaMalloc,
+ * cudaFree or allocating library routine) and, when it succeeds, no host
+ * memory: all per-call scratch comes from one 16 MiB static device array
+ * inside the library, held by every GPU that loads it until the process
+ * exits.  n is limited by what fits in those 16 MiB for the handle's
+ * neighbour capacities (about 5 KB per atom for MN_radial 250: some
+ * 2,500-3,000 atoms); larger n returns NEPX_ERR_CAPACITY.  The handle
+ * (nepx_create, max_atoms may be 1) supplies only the model parameters; the
+ * handle's device must be current (else NEPX_ERR_ARG).  The ANN always runs
+ * in FP32, whatever nepx_set_precision chose for the handle, and only the
+ * large-box path is served (a box thinner than 2.5 (rc + skin) in a periodic
+ * direction returns NEPX_ERR_BOX).  Errors of an earlier asynchronous
+ * nepx_compute on the same handle are returned first, as nepx_compute
+ * would.  The first call on a device resolves the array's device address;
+ * make it before any stream capture.  Calls share the array: neighbour rows
+ * are rebuilt and flags cleared on every call, and calls that overlap on
+ * the GPU race.  Synchronises `stream`.  Arguments and outputs as
+ * nepx_compute (outputs overwritten); error codes and messages as
+ * nepx_compute with NEPX_SYNC_CHECK.
  * This entry point has no counterpart in the reference.
  */
 int nepx_compute_noalloc(nepx_t* handle, const nepx_box* box, int n, const int* d_type,

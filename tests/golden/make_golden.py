@@ -1,7 +1,8 @@
 #!/usr/bin/env python3
 """Regenerate the committed golden fixtures from the DMG-MD reference tree.
 
-Run in a checkout that has the reference mounted (default /root/reference):
+Run in a checkout that has the reference available (--reference, else
+$DMGMD_REFERENCE, else a `reference` directory beside this repository):
 
     python tests/golden/make_golden.py [--reference PATH]
 
@@ -106,7 +107,9 @@ def frame_record(frame, symbols):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    default_ref = os.environ.get("DMGMD_REFERENCE") or os.path.join(
+        os.path.dirname(os.path.dirname(os.path.dirname(HERE))), "reference")
+    ap.add_argument("--reference", default=default_ref)
     args = ap.parse_args()
     base = os.path.join(args.reference, "tests", "baseline")
     out = {"source": "DMG-MD tests/baseline (GPUMD 5.9.1 goldens, FP32 on NVIDIA L20)",
