@@ -2,41 +2,55 @@
 """Benchmark of the nepx NEP molecular-dynamics engine on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload water|carbon|copper]
+                    [--workload carbon8m|water|copper|carbon|serving]
 
-Default workload (the headline config): liquid water, 8000 molecules = 24,000
-atoms at 1.0 g/cm^3, synthetic two-type NEP4 (O/H, rc 6.0/4.0 A, n_max 4/4,
-basis 8/8, l_max 4 2 0, 50 hidden units, weights N(0, 0.1^2), seeded; a
-descriptor scale q_scaler = 0.02 keeps the random-weight landscape gentle so
-the liquid keeps water's density and neighbour counts through the run
-instead of clustering -- the cost per step is that of any NEP of this shape),
-Bussi NVT (nvt_bdp) at 300 K, dt 0.5 fs.  One "step" is one full MD step:
-neighbour update, NEP energy/force/virial, FP64 velocity Verlet, thermo
-reduction and thermostat.  Metric: atom-steps/s, whole job (sum over ranks).
+Default workload (the headline): large carbon NVE -- 8,000,000 atoms, a
+100x100x100-cell diamond supercell (a = 3.567 A, 8 atoms per cubic cell,
+jitter N(0, 0.05 A)) with a random 10% of the atoms displaced by N(0, 0.3 A)
+(amorphous regions); synthetic one-type NEP4 (rc 4.2/3.7 A, n_max 4/4, basis
+8/8, l_max 4 2 1 with the 4- and 5-body invariants, 30 hidden units, weights
+N(0, 0.1^2), seeded; a descriptor scale q_scaler = 0.02 keeps the
+random-weight landscape gentle), Maxwell-Boltzmann velocities at 300 K, NVE,
+dt 1 fs.  One "step" is one full MD step: skin check and conditional Verlet
+rebuild, NEP energy/force/virial, FP64 velocity Verlet, thermo reduction.
+Metric: atom-steps/s, whole job (sum over ranks).
 
 value  -- device time (CUDA events on the MD stream) of K steps queued in
           chunks of `--chunk` steps, each chunk preceded by a 512 MiB write
-          that flushes the 126 MB L2; max over ranks.
+          that flushes the 126 MB L2 (the system's positions alone are
+          192 MB); max over ranks.
 e2e    -- the same K steps driven through the public C API one step per call
-          (nepx_md_run: host draws H2D, graph launch, thermo row D2H,
-          synchronisation), host wall clock.
-roofline -- the dominant kernel (fused descriptor/ANN/angular-force kernel),
-          its FP32 work per launch (the operation count of the algorithm it
-          runs, see flops_per_atom) over its CUDA-event time, against the FP32
-          FMA peak of B200 (148 SMs x 128 lanes x 2 FLOP x max SM clock).
+          (nepx_md_run: graph launch, thermo row D2H, synchronisation), host
+          wall clock.
+roofline -- the four force kernels (k_filter_radial, k_nep_fused,
+          k_angular_f12, k_gather): the FP32 operations of the algorithm they
+          run (flops_per_atom + gather_flops_per_atom, per atom at the
+          system's mean neighbour counts) over their CUDA-event time, against
+          the FP32 FMA peak of B200 (148 SMs x 128 lanes x 2 FLOP x max SM
+          clock).  traffic: their DRAM bytes per force call from ncu.
 cpu_baseline -- the reference's own FP64 CPU NEP evaluator (NEP3_CPU,
-          oracle/_ref) over the full system on all host cores, force call,
-          on the final MD state (md_step: with a CPU velocity-Verlet update
-          around it); the same FP64 values give err_vs_fp64 (force RMSE and
-          energy error of the FP32 and mixed paths).
+          oracle/_ref) on all host cores, on a bounded sample of the same
+          workload (a periodic block of the same lattice, same displacement
+          statistics, every atom a center): force call, and md_step with a
+          CPU velocity-Verlet update around it.
+err_vs_fp64 -- force RMSE and energy error of the FP32 and mixed paths on the
+          final MD state against NEP3_CPU (FP64) on spherical clusters cut out
+          of it (core atoms whose 2 rc neighbourhood is inside the cluster:
+          their results equal the full system's).
 mixed_precision -- the same MD with the ANN on the tcgen05 tensor cores.
+other_workloads -- water (24,000 atoms, Bussi NVT) and copper (1.0 M atoms,
+          NEP-ZBL, Berendsen NPT): MD rate, force call, mixed precision and
+          FP64 errors.
 nve_drift -- NVE energy drift (eV/atom/ns) of 4096-atom diamond carbon,
           20,000 steps of 1 fs, both precisions.
-serving -- a bounded sample of the serving workload (--workload serving
-          runs the full stream): served structures/s, p50/p99 latency,
-          batched mixed-precision engine over the plain FP32 path.
+serving -- a 5,000-request sample of the serving stream (--workload serving
+          runs the full 20,000): served structures/s, p50/p99 latency at 30,
+          60 and 90% of saturation, batched engine over the plain FP32 path.
 
---impl reference times that same reference CPU evaluator alone (rank 0).
+--impl reference times that same reference CPU evaluator (force call plus a
+CPU velocity-Verlet update on the bounded sample, rank 0) on the same config
+dict, and the reference's own GPU kernels (src/gpumd_compat built for
+sm_100a) on the full system (reference_gpu).
 Multi-GPU: one independent replica per GPU (the reference's one-rank path
 does not shard; replicas only), no collective on the data path.
 """
@@ -60,44 +74,41 @@ import numpy as np  # noqa: E402
 import workloads  # noqa: E402
 
 K_B = 8.617343e-5
-# DRAM bytes per force call of the descriptor stage from the committed ncu
-# captures (profiles/descriptor_kernels_water24k.md): k_filter_radial +
-# k_nep_fused + k_angular_f12
-TRAFFIC = {"water": 18.78e6 + 6.94e6 + 17.97e6}
+# DRAM bytes per atom and force call of the four force kernels (k_filter_radial,
+# k_nep_fused, k_angular_f12, k_gather), dram__bytes_read.sum +
+# dram__bytes_write.sum of one ncu-captured launch each, divided by the atoms
+# of the captured system (traffic grows with the atoms processed)
+TRAFFIC_PER_ATOM = {}
 FP32_LANES = 148 * 128          # B200: SMs x FP32 lanes
 SM_MAX_MHZ = 1965.0
+L2_NOTE = "flushed by a 512 MiB write before every %d-step chunk"
 
 WORKLOADS = {
     # name: (builder, nep kwargs, ensemble kwargs, dt_fs)
     "water": dict(
-        nep=dict(version=4, symbols=("O", "H"), rc=(6.0, 4.0), mn=(250, 100), n_max=(4, 4),
-                 basis=(8, 8), l_max=(4, 2, 0), H=50, seed=2024, std=0.1, q_scaler=0.02),
+        nep=workloads.NEP_SPECS["water"],
         ens=dict(kind="nvt_bdp", T0=300.0, Tdamp=100.0), dt=0.5, T=300.0,
         desc="water_8000mol_24000atoms_nep4_O-H_rc6.0-4.0_H50_nvt_bdp_300K_dt0.5fs"),
     "carbon": dict(
-        nep=dict(version=4, symbols=("C",), rc=(4.2, 3.7), mn=(100, 60), n_max=(4, 4),
-                 basis=(8, 8), l_max=(4, 2, 1), H=30, seed=2025, std=0.1, q_scaler=0.02),
+        nep=workloads.NEP_SPECS["carbon"],
         ens=dict(kind="nve"), dt=1.0, T=300.0,
         desc="diamond_8x8x8_4096atoms_nep4_C_rc4.2-3.7_H30_nve_dt1fs"),
     "copper": dict(
-        nep=dict(version=4, symbols=("Cu",), zbl=(1.0, 2.0), rc=(5.0, 4.0), mn=(100, 60),
-                 n_max=(4, 4), basis=(8, 8), l_max=(4, 2, 1), H=40, seed=2026, std=0.1,
-                 q_scaler=0.02),
+        nep=workloads.NEP_SPECS["copper"],
         ens=dict(kind="npt_ber", T0=300.0, Tdamp=100.0, p_gpa=0.0, bulk_gpa=140.0,
                  tau_p=1000.0), dt=1.0, T=300.0,
         desc="cu_fcc_63x63x63_1pct_vacancies_nepzbl_rc5.0-4.0_H40_npt_ber_dt1fs"),
 }
 
 WORKLOADS["carbon8m"] = dict(
-    WORKLOADS["carbon"], steps=200,
-    desc="diamond_100x100x100_8000000atoms_10pct_displaced_nep4_C_rc4.2-3.7_H30_nve_dt1fs")
+    WORKLOADS["carbon"],
+    desc="diamond_100x100x100cells_8000000atoms_10pct_displaced_nep4_C_rc4.2-3.7_H30_"
+         "nve_300K_dt1fs")
 
 MASSES = {"O": 15.999, "H": 1.008, "C": 12.011, "Cu": 63.546}
 
 # serving stream: one shared synthetic four-type NEP5 (C, H, O, Cu)
-SERVING_NEP = dict(version=5, symbols=("C", "H", "O", "Cu"), rc=(5.0, 4.0), mn=(160, 80),
-                   n_max=(4, 4), basis=(8, 8), l_max=(4, 2, 1), H=64, seed=2027, std=0.1,
-                   q_scaler=0.02)
+SERVING_NEP = workloads.NEP_SPECS["serving"]
 
 
 def _percentile_ms(xs, q):
@@ -224,14 +235,27 @@ def build_system(name, seed):
     elif name == "carbon8m":
         # 8,000,000 atoms (100^3 cubic cells of 8); a random 10% of the atoms
         # displaced by N(0, 0.3 A) (amorphous regions)
-        t, h, p = workloads.diamond(a=3.567, ncell=100, jitter=0.05, seed=seed)
-        rng = np.random.default_rng(seed + 100)
-        pick = rng.random(len(t)) < 0.10
-        L = h[0]
-        p[:, pick] = (p[:, pick] + rng.normal(0.0, 0.3, (3, int(pick.sum())))) % L
+        t, h, p = workloads.displaced_diamond(ncell=100, seed=seed)
     else:
         t, h, p = workloads.fcc(a=3.615, ncell=63, vacancy=0.01, seed=seed)
     return t, h, p
+
+
+def cpu_sample_system(name, seed=1):
+    """The bounded sample of a workload that the CPU evaluator is timed on: the
+    whole system when it is small, else a periodic block of the same lattice
+    with the same vacancy / displacement statistics (the per-atom work of an
+    O(N) evaluator is that of the full system).  Returns (t, h, p, what)."""
+    if name == "carbon8m":
+        t, h, p = workloads.displaced_diamond(ncell=20, seed=seed)
+        return t, h, p, ("periodic 20x20x20-cell block (64,000 atoms) of the same displaced "
+                         "diamond, every atom a center")
+    if name == "copper":
+        t, h, p = workloads.fcc(a=3.615, ncell=20, vacancy=0.01, seed=seed)
+        return t, h, p, ("periodic 20x20x20-cell block (%d atoms) of the same FCC Cu with 1%% "
+                         "vacancies, every atom a center" % len(t))
+    t, h, p = build_system(name, seed)
+    return t, h, p, "the full system (%d atoms)" % len(t)
 
 
 def flops_per_atom(info, nr, na):
@@ -255,6 +279,18 @@ def flops_per_atom(info, nr, na):
     center = nA * (3 * nlm + 60) + 4 * dim * H + 12 * H + 4 * nA * nlm
     angular_force = na * (20 + 14 + 8 * kA + 4 * nA * kA + 4 * nA * nlm + 10 * nlm + 10)
     return radial + angular_desc + center + angular_force
+
+
+def gather_flops_per_atom(info, nr, na):
+    """FP32 operations per atom of k_gather: per radial edge geometry (~20),
+    cutoff (~12), basis values and derivatives (8 kR), the two alpha dot
+    products (4 kR) and the force / virial update (~30); per angular edge the
+    exchange F_i += f12(i,j) - f12(j,i) and the virial (~24), plus ZBL (~60)
+    for NEP-ZBL models."""
+    kR = info["basis_r"] + 1
+    radial = nr * (20 + 12 + 8 * kR + 4 * kR + 30)
+    angular = na * (24 + (60 if info.get("zbl") else 0))
+    return radial + angular
 
 
 class ClockSampler:
@@ -311,13 +347,16 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_reference_rate(nep_path, t, h, p, budget_s=8.0, max_reps=5, want_result=False):
-    """The reference's NEP3_CPU over all atoms on all host cores: atom-steps/s
-    (and, with want_result, its FP64 energies and forces of the last call)."""
+def cpu_reference_rate(nep_path, sample, budget_s=8.0, max_reps=5):
+    """The reference's NEP3_CPU on a bounded sample (t, h, p, what) of the
+    workload on all host cores: force-call atom-steps/s, and md_step with a
+    CPU velocity-Verlet update around it.  None when the reference library
+    is not built."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     if not oracle.ref_cpu_available():
         return None
+    t, h, p, what = sample
     threads = os.cpu_count() or 1
     ref = oracle.RefCpuModel(nep_path)
     ref.compute(t, h, p, threads=threads)           # warm (thread pool, pages)
@@ -329,16 +368,16 @@ def cpu_reference_rate(nep_path, t, h, p, budget_s=8.0, max_reps=5, want_result=
         result = ref.compute(t, h, p, threads=threads)
         times.append(time.perf_counter() - t0)
     sec = statistics.median(times)
-    line = {"value": len(t) / sec, "unit": "atom-steps/s", "cores": threads, "kind": "reference",
-            "sample": "NEP3_CPU (reference FP64 CPU evaluator) force call on all %d atoms, "
-                      "median of %d calls, %d threads" % (len(t), len(times), threads)}
+    n = len(t)
+    line = {"value": n / sec, "unit": "atom-steps/s", "cores": threads, "kind": "reference",
+            "sample": "NEP3_CPU (reference FP64 CPU evaluator) force call on %s, median of %d "
+                      "calls, %d threads" % (what, len(times), threads)}
     # with a CPU velocity-Verlet loop around it: both half kicks, the drift and
     # the wrap into the box (FP64, vectorised over atoms)
-    n = len(t)
     L = np.diag(np.asarray(h, dtype=np.float64).reshape(3, 3))[:, None]
     x = np.array(p, dtype=np.float64)
     v = np.zeros_like(x)
-    f = np.asarray(result[1]) if result is not None else np.zeros_like(x)
+    f = np.asarray(result[1])
     inv_m = np.ones(n)
     vv = []
     for _ in range(5):
@@ -352,7 +391,7 @@ def cpu_reference_rate(nep_path, t, h, p, budget_s=8.0, max_reps=5, want_result=
     line["md_step"] = {"value": n / (sec + vv_s), "unit": "atom-steps/s",
                        "what": "force call plus a CPU velocity-Verlet update (numpy, FP64)",
                        "vv_ms": vv_s * 1e3}
-    return (line, result) if want_result else line
+    return line
 
 
 def errors_vs(ref, pe, f):
@@ -364,6 +403,42 @@ def errors_vs(ref, pe, f):
             "force_rel_2norm": float(np.linalg.norm(f - f0) / np.linalg.norm(f0)),
             "energy_mae_eV_per_atom": float(np.abs(pe - pe0).mean()),
             "energy_total_eV_per_atom": float(abs(pe.sum() - pe0.sum()) / n)}
+
+
+def fp64_errors(nep_path, rc_max, t, h, p, outs, clusters=9, r_core=20.0, seed=5):
+    """Errors of GPU results outs = {label: (pe, f)} on the state (t, h, p)
+    against the reference's FP64 NEP3_CPU.  Systems up to 100k atoms are
+    evaluated whole; larger ones on `clusters` spherical cut-outs around
+    random atoms (core radius r_core, shell 2 rc: the cores' energies and
+    forces equal the full system's), the cores' atoms compared."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    if not oracle.ref_cpu_available():
+        return None
+    threads = os.cpu_count() or 1
+    ref = oracle.RefCpuModel(nep_path)
+    n = len(t)
+    if n <= 100000:
+        pe0, f0, _ = ref.compute(t, h, p, threads=threads)
+        idx = np.arange(n)
+        what = "NEP3_CPU (reference, FP64) on the whole final MD state (%d atoms)" % n
+    else:
+        rng = np.random.default_rng(seed)
+        pe_l, f_l, idx_l = [], [], []
+        for c in rng.choice(n, clusters, replace=False):
+            tc, hc, pc, core, orig = workloads.cutout(t, h, p, int(c), r_core, 2 * rc_max + 0.1)
+            pe_c, f_c, _ = ref.compute(tc, hc, pc, threads=threads)
+            pe_l.append(pe_c[core])
+            f_l.append(f_c[:, core])
+            idx_l.append(orig)
+        pe0, f0, idx = np.concatenate(pe_l), np.concatenate(f_l, axis=1), np.concatenate(idx_l)
+        what = ("NEP3_CPU (reference, FP64) on %d spherical cut-outs of the final MD state "
+                "(core radius %.0f A, shell 2 rc): %d core atoms compared"
+                % (clusters, r_core, len(idx)))
+    out = {"against": what}
+    for label, (pe, f) in outs.items():
+        out[label] = errors_vs((pe0, f0), pe[idx], f[:, idx])
+    return out
 
 
 def nve_drift(precision, steps=20000, every=100, equilibrate=10000):
@@ -420,7 +495,7 @@ def nve_drift(precision, steps=20000, every=100, equilibrate=10000):
     return out
 
 
-def gpu_reference_rate(nep_path, t, h, p, reps=50):
+def gpu_reference_rate(nep_path, t, h, p, reps=None):
     """The reference's own FP32 GPU NEP (its src/gpumd_compat kernels built for
     sm_100a, oracle/_ref) on this GPU: force calls on static positions (the
     Verlet list is built by the first call and kept), CUDA events on the
@@ -434,6 +509,8 @@ def gpu_reference_rate(nep_path, t, h, p, reps=50):
     if not (oracle.ref_gpu_available() and torch.cuda.is_available()):
         return None
     n = len(t)
+    if reps is None:
+        reps = max(5, min(50, 1200000 // n))
     d_type = torch.as_tensor(np.asarray(t, dtype=np.int32), device="cuda")
     d_pos = torch.as_tensor(np.ascontiguousarray(p, dtype=np.float64), device="cuda")
     ref = oracle.RefGpuModel(nep_path, n)
@@ -486,35 +563,86 @@ def mixed_sweep():
     return {"mixed_sweep": out, "workload": WORKLOADS["water"]["desc"]}
 
 
+def headline_config(name, n, world, chunk):
+    """The `config` of a bench line; both arms print the same dict."""
+    spec = WORKLOADS[name]
+    return {"workload": spec["desc"], "atoms_per_gpu": n, "ensemble": spec["ens"]["kind"],
+            "dt_fs": spec["dt"], "parallelism": "replicas x%d" % world,
+            "l2": L2_NOTE % chunk}
+
+
 def run_reference_arm(args, rank):
+    """The reference's own CPU implementation of the path: NEP3_CPU force call
+    plus a CPU velocity-Verlet update per step, on the bounded sample of the
+    workload (a periodic block of the same lattice for the large systems),
+    all host threads; rank 0 only.  reference_gpu: the reference's own GPU
+    kernels on the full system."""
     if rank != 0:
         return 0
     if args.workload == "serving":
         print(json.dumps({"impl": "reference", "unavailable": "the reference evaluates one "
                           "system per process: it has no batched or served path"}))
         return 0
-    spec = WORKLOADS[args.workload]
-    with tempfile.TemporaryDirectory() as tmp:
-        path = workloads.write_nep(os.path.join(tmp, "nep.txt"), **spec["nep"])
-        t, h, p = build_system(args.workload, seed=1)
-        base = cpu_reference_rate(path, t, h, p, budget_s=max(4.0, 0.5 * args.steps))
-        ref_gpu = gpu_reference_rate(path, t, h, p)
-    if base is None:
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    if not oracle.ref_cpu_available():
         print(json.dumps({"impl": "reference",
                           "unavailable": "reference NEP3_CPU library oracle/_ref not built"}))
         return 0
-    line = {"impl": "reference", "metric": "atom-steps/s", "value": base["value"],
+    spec = WORKLOADS[args.workload]
+    chunk = max(1, min(args.chunk, args.steps))
+    with tempfile.TemporaryDirectory() as tmp:
+        path = workloads.write_nep(os.path.join(tmp, "nep.txt"), **spec["nep"])
+        t, h, p = build_system(args.workload, seed=1)
+        n = len(t)
+        sample = cpu_sample_system(args.workload)
+        ts, hs, ps, what = sample
+        m = len(ts)
+        syms = spec["nep"]["symbols"]
+        inv_m = 1.0 / np.array([MASSES[syms[k]] for k in ts])
+        L = np.diag(np.asarray(hs, dtype=np.float64).reshape(3, 3))[:, None]
+        threads = os.cpu_count() or 1
+        ref = oracle.RefCpuModel(path)
+        x = np.array(ps, dtype=np.float64)
+        v = np.zeros_like(x)
+        dt = spec["dt"] / 10.18050571        # fs -> natural units (A, eV, amu)
+
+        # one step of velocity Verlet needs one new force call; the first
+        # half kick reuses the previous step's force
+        _, f, _ = ref.compute(ts, hs, x, threads=threads)
+        for _ in range(args.warmup):
+            v += 0.5 * dt * f * inv_m
+            x += dt * v
+            x -= np.floor(x / L) * L
+            _, f, _ = ref.compute(ts, hs, x, threads=threads)
+            v += 0.5 * dt * f * inv_m
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            v += 0.5 * dt * f * inv_m
+            x += dt * v
+            x -= np.floor(x / L) * L
+            _, f, _ = ref.compute(ts, hs, x, threads=threads)
+            v += 0.5 * dt * f * inv_m
+        sec = (time.perf_counter() - t0) / args.steps
+        value = m / sec
+        ref_gpu = gpu_reference_rate(path, t, h, p)
+    line = {"impl": "reference", "metric": "atom-steps/s", "value": value,
             "unit": "atom-steps/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * len(t) / base["value"],
+            "warmup": args.warmup, "ms_per_step": 1e3 * n / value,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
-            "data": "synthetic", "config": {"workload": spec["desc"], "atoms": len(t)},
-            "cpu_baseline": base,
-            "e2e": {"value": base["value"], "unit": "atom-steps/s", "h2d_bytes_per_step": 0,
+            "data": "synthetic (seeded structure, velocities and NEP weights)",
+            "config": headline_config(args.workload, n, args.gpus, chunk),
+            "cpu_baseline": {"value": value, "unit": "atom-steps/s", "cores": threads,
+                             "kind": "reference",
+                             "sample": "per step: NEP3_CPU (reference FP64 CPU evaluator) force "
+                                       "call and a velocity-Verlet update (numpy, FP64) on %s; "
+                                       "ms_per_step scales the sample's time to the %d atoms "
+                                       "of the config" % (what, n)},
+            "e2e": {"value": value, "unit": "atom-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
             "reference_gpu": ref_gpu}
     print(json.dumps(line))
     return 0
-
 
 
 class Ranks:
@@ -553,13 +681,150 @@ def replica_rate(units_per_rank, steps, ms_per_rank, ranks):
     ms = ranks.max(ms_per_rank)
     return total * steps / (ms / 1e3), ms
 
+def md_system(name, rank):
+    """Potential file, structure, masses and 300 K velocities of a workload."""
+    spec = WORKLOADS[name]
+    path = workloads.write_nep(os.path.join(tempfile.mkdtemp(), "nep.txt"), **spec["nep"])
+    t, h, p = build_system(name, seed=1 + rank)
+    syms = spec["nep"]["symbols"]
+    masses = np.array([MASSES[x] for x in syms])[t]
+    v = workloads.maxwell_boltzmann(masses, spec["T"], seed=7 + rank)
+    return dict(name=name, spec=spec, path=path, t=t, h=h, p=p, masses=masses, v=v)
+
+
+def new_md(pot, sysd, rank, warmup):
+    import nepx
+    spec = sysd["spec"]
+    md = nepx.MD(pot, sysd["t"], sysd["masses"], sysd["p"], sysd["v"], sysd["h"])
+    ens = dict(spec["ens"])
+    kind = ens.pop("kind")
+    md.set_ensemble(kind, seed=12345678 + rank, **ens)
+    md.run(warmup, spec["dt"])
+    return md
+
+
+def timed_md(pot, sysd, args, rank, ranks, flush, clocks=None):
+    """K MD steps in chunks, each after an L2 flush, timed by CUDA events on
+    the MD stream: (device ms, final state, clocks, number of chunks)."""
+    import torch
+    dt = sysd["spec"]["dt"]
+    md = new_md(pot, sysd, rank, args.warmup)
+    _, _, _, _, stream_ptr = md.device_state()
+    stream = torch.cuda.ExternalStream(stream_ptr)
+    K, chunk = args.steps, max(1, min(args.chunk, args.steps))
+    chunks = [chunk] * (K // chunk) + ([K % chunk] if K % chunk else [])
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in chunks]
+    ranks.barrier()
+    torch.cuda.synchronize()
+    if clocks:
+        clocks.start()
+        time.sleep(0.2)
+    for c, steps in enumerate(chunks):
+        with torch.cuda.stream(stream):
+            flush.fill_(c & 0xFF)
+        ev[c][0].record(stream)
+        md.run_async(steps, dt)
+        ev[c][1].record(stream)
+    md.sync()
+    torch.cuda.synchronize()
+    clock_info = clocks.stop() if clocks else None
+    ranks.barrier()
+    dev_ms = sum(a.elapsed_time(b) for a, b in ev)
+    st = md.state()
+    md.close()
+    return dev_ms, st, clock_info, len(chunks)
+
+
+def force_call_profile(pot, sysd, st, reps):
+    """Per-stage device time (nepx_profile) and the outputs (pe, f as numpy)
+    of one force call on the state st, at the handle's current precision."""
+    import torch
+    tt = torch.as_tensor(np.asarray(sysd["t"], dtype=np.int32), device="cuda")
+    pp = torch.as_tensor(np.ascontiguousarray(st["pos"]), device="cuda")
+    prof = pot.profile(tt, st["h"], pp, reps=reps)
+    pe, f, _ = pot.compute(tt, st["h"], pp, sync_check=True)
+    out = (pe.cpu().numpy(), f.cpu().numpy())
+    del tt, pp, pe, f
+    return prof, out
+
+
+def mean_neighbors(pot, n):
+    """Mean radial and angular row lengths of the last force call (the first
+    262,144 atoms of a larger system)."""
+    m = min(n, 262144)
+    return float(pot.neighbor_counts(0, m).mean()), float(pot.neighbor_counts(1, m).mean())
+
+
+def roofline_of(pot, name, n, prof):
+    """The four force kernels against the FP32 FMA peak (stage times of prof)."""
+    mean_r, mean_a = mean_neighbors(pot, n)
+    info = dict(pot.info)
+    fpa = flops_per_atom(info, mean_r, mean_a)
+    gfa = gather_flops_per_atom(info, mean_r, mean_a)
+    ms = prof["descriptor"] + prof["gather"]
+    achieved = (fpa + gfa) * n / (ms * 1e-3) / 1e12
+    peak = FP32_LANES * 2 * SM_MAX_MHZ * 1e6 / 1e12
+    per_atom = TRAFFIC_PER_ATOM.get(name)
+    return {"bound": "fp32",
+            "kernel": "k_filter_radial + k_nep_fused + k_angular_f12 + k_gather (force stage)",
+            "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "traffic": per_atom * n if per_atom else None,
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the four "
+                              "kernels, one launch each, per atom of the captured system "
+                              "times this system's atoms",
+            "peak_source": "B200 FP32 FMA peak: 148 SMs x 128 lanes x 2 FLOP x 1965 MHz "
+                           "(not in MEASURED_PEAKS.json, which holds HBM and bf16 only); "
+                           "fraction of that nominal peak",
+            "timing": "CUDA events around the stages of nepx_profile (force calls on the final "
+                      "MD state, L2 holding what fits)",
+            "ms_per_launch": ms, "flops_per_atom": fpa + gfa,
+            "flops_per_atom_descriptor_stage": fpa, "flops_per_atom_gather": gfa,
+            "mean_radial_neighbors": mean_r, "mean_angular_neighbors": mean_a}
+
+
+def profile_reps(n):
+    return max(5, min(50, 1200000 // n))
+
+
+def other_workload(name, args, rank, ranks, flush):
+    """MD rate (FP32 and mixed), force call and FP64 errors of a secondary
+    workload, for the extra keys of the headline line."""
+    import nepx
+    sysd = md_system(name, rank)
+    n = len(sysd["t"])
+    pot = nepx.Potential(sysd["path"], max_atoms=n)
+    dev_ms, st, _, _ = timed_md(pot, sysd, args, rank, ranks, flush)
+    prof, out32 = force_call_profile(pot, sysd, st, profile_reps(n))
+    pot.set_precision("mixed")
+    dev_ms_m, _, _, _ = timed_md(pot, sysd, args, rank, ranks, flush)
+    prof_m, outm = force_call_profile(pot, sysd, st, profile_reps(n))
+    pot.set_precision("fp32")
+    roof = roofline_of(pot, name, n, prof)
+    pot.close()
+    value = n * args.steps / (dev_ms * 1e-3)
+    line = {"workload": sysd["spec"]["desc"], "atoms": n, "ensemble": sysd["spec"]["ens"]["kind"],
+            "value": value, "unit": "atom-steps/s", "ms_per_step": dev_ms / args.steps,
+            "steps": args.steps,
+            "mixed_precision": {"value": n * args.steps / (dev_ms_m * 1e-3),
+                                "over_fp32": dev_ms / dev_ms_m, "stage_ms": prof_m},
+            "force_call": {"ms": prof["total"], "stage_ms": prof,
+                           "value": n / (prof["total"] * 1e-3)},
+            "roofline": roof}
+    if not args.no_cpu_baseline:
+        rc_max = max(sysd["spec"]["nep"]["rc"])
+        line["err_vs_fp64"] = fp64_errors(sysd["path"], rc_max, sysd["t"], st["h"], st["pos"],
+                                          {"fp32": out32, "mixed": outm})
+    return line
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
-    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="water", choices=sorted(WORKLOADS) + ["serving"])
+    ap.add_argument("--workload", default="carbon8m", choices=sorted(WORKLOADS) + ["serving"])
     ap.add_argument("--requests", type=int, default=20000)
     ap.add_argument("--arena", type=int, default=262144)
     ap.add_argument("--plain-sample", type=int, default=200)
@@ -568,8 +833,8 @@ def main():
     ap.add_argument("--mixed-sweep", action="store_true",
                     help="print FP32 vs mixed force-call times over NEP model sizes and exit")
     ap.add_argument("--no-extras", action="store_true",
-                    help="skip the NVE-drift and serving-sample measurements")
-    ap.add_argument("--serving-sample", type=int, default=600)
+                    help="skip the other workloads, the NVE drift and the serving sample")
+    ap.add_argument("--serving-sample", type=int, default=5000)
     ap.add_argument("--precision", default="mixed", choices=["fp32", "mixed"],
                     help="ANN precision of the serving workload")
     args = ap.parse_args()
@@ -600,67 +865,36 @@ def main():
     ranks = Ranks(dist, "cuda")
     import nepx
 
-    spec = WORKLOADS[args.workload]
-    tmp = tempfile.mkdtemp()
-    path = workloads.write_nep(os.path.join(tmp, "nep.txt"), **spec["nep"])
-    t, h, p = build_system(args.workload, seed=1 + rank)
+    sysd = md_system(args.workload, rank)
+    spec = sysd["spec"]
+    t, h, p = sysd["t"], sysd["h"], sysd["p"]
     n = len(t)
-    syms = spec["nep"]["symbols"]
-    masses = np.array([MASSES[syms[k]] for k in t])
-    v = workloads.maxwell_boltzmann(masses, spec["T"], seed=7 + rank)
-    pot = nepx.Potential(path, max_atoms=n)
-    md = nepx.MD(pot, t, masses, p, v, h)
-    ens = dict(spec["ens"])
-    kind = ens.pop("kind")
-    md.set_ensemble(kind, seed=12345678 + rank, **ens)
     dt = spec["dt"]
-    md.run(args.warmup, dt)
-
-    d_pos, d_vel, d_force, d_type, stream_ptr = md.device_state()
-    stream = torch.cuda.ExternalStream(stream_ptr)
+    kind = spec["ens"]["kind"]
+    K = args.steps
+    chunk = max(1, min(args.chunk, args.steps))
+    pot = nepx.Potential(sysd["path"], max_atoms=n)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
-    K, chunk = args.steps, max(1, min(args.chunk, args.steps))
-    chunks = [chunk] * (K // chunk) + ([K % chunk] if K % chunk else [])
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in chunks]
     props = torch.cuda.get_device_properties(local)
     gpu_id = getattr(props, "uuid", None)
     gpu_id = ("GPU-" + str(gpu_id)) if gpu_id is not None else local
     clocks = ClockSampler(gpu_id)
-    ranks.barrier()
-    torch.cuda.synchronize()
-    clocks.start()
-    time.sleep(0.2)
-    for c, steps in enumerate(chunks):
-        with torch.cuda.stream(stream):
-            flush.fill_(c & 0xFF)
-        ev[c][0].record(stream)
-        md.run_async(steps, dt)
-        ev[c][1].record(stream)
-    md.sync()
-    torch.cuda.synchronize()
-    clock_info = clocks.stop()
-    ranks.barrier()
-    value, dev_ms = replica_rate(n, K, sum(a.elapsed_time(b) for a, b in ev), ranks)
-    atoms_total = n * world
+
+    # 1. the headline: FP32 MD, device time
+    dev_ms, st, clock_info, nchunks = timed_md(pot, sysd, args, rank, ranks, flush, clocks)
+    value, dev_ms = replica_rate(n, K, dev_ms, ranks)
     # k_vv1 (with the skin check), five Verlet-rebuild kernels (each returns at
     # once unless a rebuild is due), k_filter_radial, k_nep_fused,
     # k_angular_f12, k_gather, k_vv2_thermo, k_ensemble, k_scale; NHC adds two
     kernels_per_step = 13 + (2 if kind == "nvt_nhc" else 0)
     # per call (chunk): k_mark_call before the step graphs and k_publish after
     # them; the L2-flush fills are torch's, not counted
-    launches = K * kernels_per_step + 2 * len(chunks)
+    launches = K * kernels_per_step + 2 * nchunks
 
-    st = md.state()     # the final state of the timed run
-    md.close()
-
-    # end to end through the public API: one nepx_md_run per step over the
-    # same steps as the timed run (a fresh MD from the same initial state:
-    # the synthetic liquid slowly clusters, so later steps cost more)
-    md = nepx.MD(pot, t, masses, p, v, h)
-    md.set_ensemble(kind, seed=12345678 + rank, **ens)
-    md.run(args.warmup, dt)
-    rows = np.zeros((1, len(nepx.THERMO_COLUMNS)))
+    # 2. end to end through the public API: one nepx_md_run per step over the
+    # same steps from the same initial state
+    md = new_md(pot, sysd, rank, args.warmup)
+    rows = None
     ranks.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -668,96 +902,54 @@ def main():
         rows = md.run(1, dt, thermo_every=1)
     e2e_value, _ = replica_rate(n, K, (time.perf_counter() - t0) * 1e3, ranks)
     e2e = {"value": e2e_value, "unit": "atom-steps/s",
-           "h2d_bytes_per_step": 8 * 8,           # the step's stochastic draws
+           "h2d_bytes_per_step": 8 * 8 if kind != "nve" else 0,   # stochastic draws
            # thermo row, status word, box, neighbour state
            "d2h_bytes_per_step": 20 * 8 + 4 + 232 + 128,
            "api": "nepx_md_run(steps=1, thermo_every=1) per step, the timed run's steps"}
     md.close()
 
-    # the same MD with the ANN on the tensor cores (mixed precision), from the
-    # same initial state
+    # 3. the same MD with the ANN on the tensor cores
     pot.set_precision("mixed")
-    md = nepx.MD(pot, t, masses, p, v, h)
-    md.set_ensemble(kind, seed=12345678 + rank, **ens)
-    md.run(args.warmup, dt)
-    d_pos, d_vel, d_force, d_type, stream_ptr = md.device_state()
-    stream = torch.cuda.ExternalStream(stream_ptr)
-    ev_m = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-            for _ in chunks]
-    ranks.barrier()
-    torch.cuda.synchronize()
-    for c, steps in enumerate(chunks):
-        with torch.cuda.stream(stream):
-            flush.fill_((c + 7) & 0xFF)
-        ev_m[c][0].record(stream)
-        md.run_async(steps, dt)
-        ev_m[c][1].record(stream)
-    md.sync()
-    torch.cuda.synchronize()
-    value_mixed, dev_ms_m = replica_rate(n, K, sum(a.elapsed_time(b) for a, b in ev_m), ranks)
-    # + four type-sort kernels, the tcgen05 ANN and k_acoef
-    launches += K * (kernels_per_step + 6) + 2 * len(chunks)
-
-    # per-kernel profile of the force path on the final state of the FP32
-    # run, both precisions
-    tt_ = torch.as_tensor(np.asarray(t, dtype=np.int32), device="cuda")
-    pp_ = torch.as_tensor(np.ascontiguousarray(st["pos"]), device="cuda")
-    prof_mixed = pot.profile(tt_, st["h"], pp_, reps=50)
-    out_mixed = [x.cpu().numpy() for x in pot.compute(tt_, st["h"], pp_, sync_check=True)]
+    dev_ms_m, _, _, _ = timed_md(pot, sysd, args, rank, ranks, flush)
+    value_mixed, dev_ms_m = replica_rate(n, K, dev_ms_m, ranks)
+    reps = profile_reps(n)
+    prof_mixed, out_mixed = force_call_profile(pot, sysd, st, reps)
     pot.set_precision("fp32")
-    prof = pot.profile(tt_, st["h"], pp_, reps=50)
-    out_fp32 = [x.cpu().numpy() for x in pot.compute(tt_, st["h"], pp_, sync_check=True)]
-    nr, na, nv = pot.neighbor_stats()
-    # mean neighbour counts of the final state
-    rr = pot.neighbors(0, n)
-    ra = pot.neighbors(1, n)
-    mean_r = float(np.mean([len(x) for x in rr]))
-    mean_a = float(np.mean([len(x) for x in ra]))
-    fpa = flops_per_atom(pot.info, mean_r, mean_a)
-    desc_flops = fpa * n
-    achieved = desc_flops / (prof["descriptor"] * 1e-3) / 1e12
-    peak = FP32_LANES * 2 * SM_MAX_MHZ * 1e6 / 1e12
-    roofline = {"bound": "fp32",
-                "kernel": "k_filter_radial + k_nep_fused + k_angular_f12 (descriptor stage)",
-                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "traffic": TRAFFIC.get(args.workload),
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the "
-                                  "three kernels, one launch each (profiles/)",
-                "peak_source": "B200 FP32 FMA peak: 148 SMs x 128 lanes x 2 FLOP x 1965 MHz "
-                               "(not in MEASURED_PEAKS.json, which holds HBM and bf16 only)",
-                "flops_per_atom": fpa, "mean_radial_neighbors": mean_r,
-                "mean_angular_neighbors": mean_a,
-                "stage_ms": prof}
+    prof, out_fp32 = force_call_profile(pot, sysd, st, reps)
+    roofline = roofline_of(pot, args.workload, n, prof)
     mixed = {"value": value_mixed, "unit": "atom-steps/s", "ms_per_step": dev_ms_m / K,
              "over_fp32": value_mixed / value,
-             "what": "the same MD with the ANN contractions on tcgen05 (3xTF32, FP32 "
-                     "accumulation in TMEM); descriptors and forces FP32",
+             "what": "the same MD with the ANN contractions on tcgen05 (FP32 accumulation in "
+                     "TMEM); descriptors and forces FP32",
              "stage_ms": prof_mixed}
-    drift = None
-    if rank == 0 and not args.no_extras:
-        drift = {"fp32": nve_drift("fp32"), "mixed": nve_drift("mixed")}
-    serving = None
-    if rank == 0 and not args.no_extras and args.serving_sample > 0:
-        sargs = argparse.Namespace(requests=args.serving_sample, arena=args.arena,
-                                   plain_sample=max(20, args.serving_sample // 10),
-                                   precision="mixed")
-        sv = run_serving(sargs)
-        serving = {k: sv[k] for k in ("value", "unit", "atom_steps_per_s", "latency_ms",
-                                      "plain_fp32_one_at_a_time", "batched_over_plain",
-                                      "config")}
+    pot.close()
+    del flush
+    torch.cuda.empty_cache()
 
     line = None
     if rank == 0:
-        cpu = None
-        err = None
+        cpu = err = None
         if world == 1 and not args.no_cpu_baseline:
-            # the reference FP64 CPU evaluator on the final state: the timed
-            # CPU baseline, and the FP64 values the GPU results are checked against
-            cpu, ref64 = cpu_reference_rate(path, t, st["h"], st["pos"], want_result=True)
-            if ref64 is not None:
-                err = {"against": "NEP3_CPU (reference, FP64) on the final MD state",
-                       "fp32": errors_vs(ref64, out_fp32[0], out_fp32[1]),
-                       "mixed": errors_vs(ref64, out_mixed[0], out_mixed[1])}
+            # the reference FP64 CPU evaluator: timed on a bounded sample, and
+            # the FP64 values the GPU results of the final state are checked against
+            cpu = cpu_reference_rate(sysd["path"], cpu_sample_system(args.workload))
+            err = fp64_errors(sysd["path"], max(spec["nep"]["rc"]), t, st["h"], st["pos"],
+                              {"fp32": out_fp32, "mixed": out_mixed})
+        others = drift = serving = None
+        if not args.no_extras:
+            flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+            others = {w: other_workload(w, args, rank, Ranks(None), flush)
+                      for w in ("water", "copper") if w != args.workload}
+            del flush
+            drift = {"fp32": nve_drift("fp32"), "mixed": nve_drift("mixed")}
+            if args.serving_sample > 0:
+                sargs = argparse.Namespace(requests=args.serving_sample, arena=args.arena,
+                                           plain_sample=max(20, args.serving_sample // 20),
+                                           precision="mixed")
+                sv = run_serving(sargs)
+                serving = {k: sv[k] for k in ("value", "unit", "atom_steps_per_s", "latency_ms",
+                                              "latency_sweep_ms", "plain_fp32_one_at_a_time",
+                                              "batched_over_plain", "config", "saturation")}
         T_last = float(rows[-1, 0]) if rows is not None else None
         line = {"metric": "atom-steps/s", "value": value, "unit": "atom-steps/s",
                 "n_gpus": world, "steps": K, "warmup": args.warmup,
@@ -765,21 +957,17 @@ def main():
                 "vs_baseline": None, "dtype": "fp32 (descriptors, ANN, forces) + fp64 "
                                               "(integration, thermo reductions)",
                 "data": "synthetic (seeded structure, velocities and NEP weights)",
-                "config": {"workload": spec["desc"], "atoms_per_gpu": n, "ensemble": kind,
-                           "dt_fs": dt, "parallelism": "replicas x%d" % world,
-                           "l2": "flushed by a 512 MiB write before every %d-step chunk" % chunk,
-                           "final_temperature_K": T_last},
+                "config": headline_config(args.workload, n, world, chunk),
+                "final_temperature_K": T_last,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "force_call": {"value": n / (prof["total"] * 1e-3), "unit": "atom-steps/s",
-                               "ms": prof["total"],
+                               "ms": prof["total"], "stage_ms": prof,
                                "what": "nepx_compute on the final state, static positions "
-                                       "(neighbour update + descriptor + gather), L2 warm"},
-                "mixed_precision": mixed, "err_vs_fp64": err, "nve_drift": drift,
-                "serving": serving,
+                                       "(neighbour update + descriptor + gather)"},
+                "mixed_precision": mixed, "err_vs_fp64": err, "other_workloads": others,
+                "nve_drift": drift, "serving": serving,
                 "gpu_launches": launches, "clocks": clock_info}
         print(json.dumps(line))
-    md.close()
-    pot.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

@@ -255,6 +255,17 @@ class Potential:
         nl = nl.cpu().numpy()
         return [nl[i, :nn[i]].copy() for i in range(n)]
 
+    def neighbor_counts(self, which, n, stream=None):
+        """Row lengths (numpy int32) of the first n atoms of the last compute."""
+        import torch
+        mn = self.info["MN_r"] if which == 0 else self.info["MN_a"]
+        nn = torch.empty(n, dtype=torch.int32, device="cuda")
+        nl = torch.empty(n, mn, dtype=torch.int32, device="cuda")
+        self._check(lib().nepx_neighbors(self._h, which, n, _ptr(nn), _ptr(nl), mn,
+                                         _stream_ptr(stream)))
+        torch.cuda.synchronize()
+        return nn.cpu().numpy()
+
     def neighbor_stats(self, stream=None):
         r, a, v = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         self._check(lib().nepx_neighbor_stats(self._h, ctypes.byref(r), ctypes.byref(a),

@@ -75,6 +75,27 @@ def write_nep(path, version=4, symbols=("C",), zbl=None, rc=(4.2, 3.7), mn=(100,
     return path
 
 
+# Synthetic models of the benchmark workloads (write_nep keyword arguments).
+# q_scaler 0.02 keeps the random-weight landscape gentle, so the systems keep
+# their density and neighbour counts through the runs.
+NEP_SPECS = {
+    # liquid water, O/H
+    "water": dict(version=4, symbols=("O", "H"), rc=(6.0, 4.0), mn=(250, 100), n_max=(4, 4),
+                  basis=(8, 8), l_max=(4, 2, 0), H=50, seed=2024, std=0.1, q_scaler=0.02),
+    # diamond / amorphous carbon (4,096 and 8,000,000 atoms)
+    "carbon": dict(version=4, symbols=("C",), rc=(4.2, 3.7), mn=(100, 60), n_max=(4, 4),
+                   basis=(8, 8), l_max=(4, 2, 1), H=30, seed=2025, std=0.1, q_scaler=0.02),
+    # FCC copper with the universal ZBL (inner 1.0 A, outer 2.0 A)
+    "copper": dict(version=4, symbols=("Cu",), zbl=(1.0, 2.0), rc=(5.0, 4.0), mn=(100, 60),
+                   n_max=(4, 4), basis=(8, 8), l_max=(4, 2, 1), H=40, seed=2026, std=0.1,
+                   q_scaler=0.02),
+    # the serving stream's shared four-type NEP5 (C, H, O, Cu)
+    "serving": dict(version=5, symbols=("C", "H", "O", "Cu"), rc=(5.0, 4.0), mn=(160, 80),
+                    n_max=(4, 4), basis=(8, 8), l_max=(4, 2, 1), H=64, seed=2027, std=0.1,
+                    q_scaler=0.02),
+}
+
+
 def _cubic_h(L):
     return np.array([L, 0, 0, 0, L, 0, 0, 0, L], dtype=np.float64)
 
@@ -89,6 +110,38 @@ def diamond(a=3.567, ncell=8, jitter=0.05, seed=0):
     rng = np.random.default_rng(seed)
     pos = frac * L + rng.normal(0.0, jitter, frac.shape)
     return np.zeros(len(pos), dtype=np.int32), _cubic_h(L), np.ascontiguousarray(pos.T % L)
+
+
+def displaced_diamond(ncell=100, fraction=0.10, sigma=0.3, seed=1):
+    """Diamond supercell (a = 3.567 A, jitter N(0, 0.05 A)) with a random
+    `fraction` of the atoms displaced by N(0, sigma) (amorphous regions).
+    ncell 100 gives the 8,000,000-atom large-carbon workload."""
+    t, h, p = diamond(a=3.567, ncell=ncell, jitter=0.05, seed=seed)
+    rng = np.random.default_rng(seed + 100)
+    pick = rng.random(len(t)) < fraction
+    L = h[0]
+    p[:, pick] = (p[:, pick] + rng.normal(0.0, sigma, (3, int(pick.sum())))) % L
+    return t, h, p
+
+
+def cutout(t, h, p, center, r_core, r_shell):
+    """Spherical cluster around atom `center` of an orthogonal periodic box.
+
+    Keeps every atom within r_core + r_shell (minimum image) and places the
+    cluster in a cubic box wide enough that its periodic images are more than
+    r_shell / 2 apart.  With r_shell >= 2 rc the energy, force and virial of
+    every atom within r_core are those of the full system (its descriptors
+    and its neighbours' descriptors see the same atoms).  Returns (types, h,
+    pos (3, m), core index into the cluster, original index of the core)."""
+    L = np.diag(np.asarray(h, dtype=np.float64).reshape(3, 3))
+    d = p - p[:, center][:, None]
+    d -= np.round(d / L[:, None]) * L[:, None]
+    r2 = (d * d).sum(axis=0)
+    keep = np.nonzero(r2 < (r_core + r_shell) ** 2)[0]
+    side = 2.0 * (r_core + r_shell) + r_shell / 2.0 + 1.0
+    pos = np.ascontiguousarray(d[:, keep] + side / 2.0)
+    core = np.nonzero(r2[keep] < r_core ** 2)[0]
+    return (np.ascontiguousarray(t[keep]), _cubic_h(side), pos, core, keep[core])
 
 
 def fcc(a=3.615, ncell=8, vacancy=0.0, jitter=0.0, seed=0):
