@@ -227,7 +227,7 @@ def run_serving(args):
     }
 
 
-def build_system(name, seed):
+def build_system(name, seed, ncell=100):
     if name == "water":
         t, h, p = workloads.water(n_mol=8000, seed=seed)
     elif name == "carbon":
@@ -235,7 +235,7 @@ def build_system(name, seed):
     elif name == "carbon8m":
         # 8,000,000 atoms (100^3 cubic cells of 8); a random 10% of the atoms
         # displaced by N(0, 0.3 A) (amorphous regions)
-        t, h, p = workloads.displaced_diamond(ncell=100, seed=seed)
+        t, h, p = workloads.displaced_diamond(ncell=ncell, seed=seed)
     else:
         t, h, p = workloads.fcc(a=3.615, ncell=63, vacancy=0.01, seed=seed)
     return t, h, p
@@ -563,9 +563,9 @@ def mixed_sweep():
     return {"mixed_sweep": out, "workload": WORKLOADS["water"]["desc"]}
 
 
-def headline_config(name, n, world, chunk):
+def headline_config(name, n, world, chunk, ncell=100):
     """The `config` of a bench line; both arms print the same dict."""
-    spec = WORKLOADS[name]
+    spec = workload_spec(name, ncell)
     return {"workload": spec["desc"], "atoms_per_gpu": n, "ensemble": spec["ens"]["kind"],
             "dt_fs": spec["dt"], "parallelism": "replicas x%d" % world,
             "l2": L2_NOTE % chunk}
@@ -589,11 +589,11 @@ def run_reference_arm(args, rank):
         print(json.dumps({"impl": "reference",
                           "unavailable": "reference NEP3_CPU library oracle/_ref not built"}))
         return 0
-    spec = WORKLOADS[args.workload]
+    spec = workload_spec(args.workload, args.ncell)
     chunk = max(1, min(args.chunk, args.steps))
     with tempfile.TemporaryDirectory() as tmp:
         path = workloads.write_nep(os.path.join(tmp, "nep.txt"), **spec["nep"])
-        t, h, p = build_system(args.workload, seed=1)
+        t, h, p = build_system(args.workload, seed=1, ncell=args.ncell)
         n = len(t)
         sample = cpu_sample_system(args.workload)
         ts, hs, ps, what = sample
@@ -631,7 +631,7 @@ def run_reference_arm(args, rank):
             "warmup": args.warmup, "ms_per_step": 1e3 * n / value,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64",
             "data": "synthetic (seeded structure, velocities and NEP weights)",
-            "config": headline_config(args.workload, n, args.gpus, chunk),
+            "config": headline_config(args.workload, n, args.gpus, chunk, args.ncell),
             "cpu_baseline": {"value": value, "unit": "atom-steps/s", "cores": threads,
                              "kind": "reference",
                              "sample": "per step: NEP3_CPU (reference FP64 CPU evaluator) force "
@@ -681,11 +681,22 @@ def replica_rate(units_per_rank, steps, ms_per_rank, ranks):
     ms = ranks.max(ms_per_rank)
     return total * steps / (ms / 1e3), ms
 
-def md_system(name, rank):
-    """Potential file, structure, masses and 300 K velocities of a workload."""
+def workload_spec(name, ncell=100):
+    """The workload's spec; the large carbon system at another size when
+    ncell (cubic cells per edge) is not 100."""
     spec = WORKLOADS[name]
+    if name == "carbon8m" and ncell != 100:
+        spec = dict(spec, desc=spec["desc"].replace(
+            "100x100x100cells_8000000atoms", "%dx%dx%dcells_%datoms" % (ncell, ncell, ncell,
+                                                                       8 * ncell ** 3)))
+    return spec
+
+
+def md_system(name, rank, ncell=100):
+    """Potential file, structure, masses and 300 K velocities of a workload."""
+    spec = workload_spec(name, ncell)
     path = workloads.write_nep(os.path.join(tempfile.mkdtemp(), "nep.txt"), **spec["nep"])
-    t, h, p = build_system(name, seed=1 + rank)
+    t, h, p = build_system(name, seed=1 + rank, ncell=ncell)
     syms = spec["nep"]["symbols"]
     masses = np.array([MASSES[x] for x in syms])[t]
     v = workloads.maxwell_boltzmann(masses, spec["T"], seed=7 + rank)
@@ -829,6 +840,8 @@ def main():
     ap.add_argument("--arena", type=int, default=262144)
     ap.add_argument("--plain-sample", type=int, default=200)
     ap.add_argument("--chunk", type=int, default=10)
+    ap.add_argument("--ncell", type=int, default=100,
+                    help="cubic cells per edge of the large carbon workload (8 atoms each)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mixed-sweep", action="store_true",
                     help="print FP32 vs mixed force-call times over NEP model sizes and exit")
@@ -865,7 +878,7 @@ def main():
     ranks = Ranks(dist, "cuda")
     import nepx
 
-    sysd = md_system(args.workload, rank)
+    sysd = md_system(args.workload, rank, args.ncell)
     spec = sysd["spec"]
     t, h, p = sysd["t"], sysd["h"], sysd["p"]
     n = len(t)
@@ -957,7 +970,7 @@ def main():
                 "vs_baseline": None, "dtype": "fp32 (descriptors, ANN, forces) + fp64 "
                                               "(integration, thermo reductions)",
                 "data": "synthetic (seeded structure, velocities and NEP weights)",
-                "config": headline_config(args.workload, n, world, chunk),
+                "config": headline_config(args.workload, n, world, chunk, args.ncell),
                 "final_temperature_K": T_last,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "force_call": {"value": n / (prof["total"] * 1e-3), "unit": "atom-steps/s",

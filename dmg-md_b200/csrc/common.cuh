@@ -55,7 +55,8 @@ struct NeighborState {
   int overflow;        // bit 0 Verlet row, bit 1 radial row, bit 2 angular row
   int nc[3];           // cells per direction
   int ncell;
-  int max_nn[3];       // largest Verlet / radial / angular row of the last build
+  int max_nn[3];       // largest Verlet / radial / angular row since the last stats read
+  int call_nn[2];      // largest radial / angular row of the latest force evaluation
   int nonfinite;       // a force or energy came out NaN/Inf
   int box_error;       // the device box became unsupported (small in one direction, >10 rc in another)
   int ann_error;       // a tensor-core ANN tile gave up waiting for its MMAs
@@ -164,6 +165,10 @@ __device__ __forceinline__ void skin_check_atom(int N, int i, const Box& b, doub
                                                 double rc_v, int force)
 {
   sites[i] = Site{xi, yi, zi, static_cast<long long>(type_i)};
+  if (i == 0) {   // the first kernel of a force evaluation: its row maxima start here
+    st->call_nn[0] = 0;
+    st->call_nn[1] = 0;
+  }
   if (force) {
     if (i == 0) st->rebuild = 1;
     return;

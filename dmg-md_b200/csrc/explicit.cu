@@ -41,10 +41,14 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 
 __global__ void k_pack_sites(int N, const double* __restrict__ pos, const int* __restrict__ type,
-                             Site* __restrict__ sites)
+                             Site* __restrict__ sites, NeighborState* st)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
+  if (i == 0) {   // the first kernel of a force evaluation: its row maxima start here
+    st->call_nn[0] = 0;
+    st->call_nn[1] = 0;
+  }
   sites[i] = Site{pos[i], pos[N + i], pos[2 * N + i], static_cast<long long>(type[i])};
 }
 
@@ -344,6 +348,8 @@ k_rows_explicit(const ModelParams p, int total, const StructInfo* __restrict__ s
       if (ca > mn_a) atomicOr(&st->overflow, 4);
       atomicMax(&st->max_nn[1], cr);
       atomicMax(&st->max_nn[2], ca);
+      atomicMax(&st->call_nn[0], cr);
+      atomicMax(&st->call_nn[1], ca);
     }
   }
 }
@@ -524,7 +530,7 @@ void launch_explicit_rows(Engine& e, int N, const double* pos, const int* type,
   ExplicitRows& x = e.xr;
   const int threads = 256;
   k_pack_sites<<<(N + threads - 1) / threads, threads, 0, stream>>>(N, pos, type,
-                                                                     e.scratch.sites);
+                                                                     e.scratch.sites, e.d_nstate);
   if (x.from_box) {
     k_struct_from_box<<<1, 1, 0, stream>>>(e.d_box, e.model.rc_radial_max, N, x.d_si, x.d_soff,
                                            e.d_nstate);

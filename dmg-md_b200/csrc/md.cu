@@ -109,6 +109,32 @@ __device__ __forceinline__ double target_temperature(const StepParams& p, long l
   return p.T0 + (p.T1 - p.T0) * fraction;
 }
 
+// Time step of the current step: the run's dt, or with an adaptive step
+// min(dt, max_dist / max|v|) over the velocities at the start of the step
+// (reference adaptive_time_step, runtime.cu:594-619).
+__device__ __forceinline__ double step_dt(const StepParams& p, const MdScalars* sc)
+{
+  if (p.max_dist <= 0.0) return p.dt;
+  const double v2 = __longlong_as_double(static_cast<long long>(sc->vmax2));
+  const double limited = v2 == 0.0 ? p.dt : p.max_dist / sqrt(v2);
+  return limited < p.dt ? limited : p.dt;
+}
+
+// max |v|^2 over the atoms (adaptive time step): a block maximum, then an
+// integer atomicMax on the bits (ordered like the values for doubles >= 0)
+__global__ void k_vmax(int N, const double* __restrict__ vel, MdScalars* sc)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v2 = 0.0;
+  if (i < N) {
+    const double vx = vel[i], vy = vel[N + i], vz = vel[2 * N + i];
+    v2 = vx * vx + vy * vy + vz * vz;
+  }
+  for (int off = 16; off > 0; off >>= 1) v2 = fmax(v2, __shfl_xor_sync(0xffffffffu, v2, off));
+  if ((threadIdx.x & 31) == 0 && v2 > 0.0)
+    atomicMax(&sc->vmax2, static_cast<unsigned long long>(__double_as_longlong(v2)));
+}
+
 __global__ void k_nhc_pre(StepParams p, MdScalars* sc, const double* __restrict__ partials,
                           int nblocks)
 {
@@ -118,7 +144,7 @@ __global__ void k_nhc_pre(StepParams p, MdScalars* sc, const double* __restrict_
   // before_force hands over the kinetic energy (ek2/2) and doubles it again
   // (ensemble_control.cpp:186-198)
   sc->vfactor_pre = nhc_half_step(sc->nhc_pos, sc->nhc_mom, sc->nhc_mass, ek2 * 0.5 * 2.0, kT,
-                                  3.0 * p.N, p.dt * 0.5);
+                                  3.0 * p.N, step_dt(p, sc) * 0.5);
 }
 
 // Skin check of the large-box neighbour path, done by k_vv1 on the new
@@ -135,21 +161,27 @@ struct SkinArgs {
 // v = v * f_pre + F/m dt/2 ; x += v dt ; wrap into the cell
 // (runtime.cu:392-421, runtime_internal.hpp:648-681); then the skin check
 // of the new position.
+// With unwrapped != nullptr the unwrapped positions gain this step's
+// displacement, new minus old position before the wrap (reference
+// update_unwrapped, runtime.cu:423-438).
 __global__ void k_vv1(StepParams p, const Box* __restrict__ box, const double* __restrict__ mass,
                       const double* __restrict__ force, double* pos, double* vel,
-                      const MdScalars* __restrict__ sc, SkinArgs sk)
+                      const MdScalars* __restrict__ sc, SkinArgs sk, double* unwrapped)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= p.N) return;
   const int N = p.N;
   const double f = sc->vfactor_pre;
-  const double half = p.dt * 0.5;
+  const double dt = step_dt(p, sc);
+  const double half = dt * 0.5;
   const double im = 1.0 / mass[i];
   double r[3];
   for (int d = 0; d < 3; ++d) {
     const double v = vel[d * N + i] * f + force[d * N + i] * im * half;
     vel[d * N + i] = v;
-    r[d] = pos[d * N + i] + v * p.dt;
+    const double x0 = pos[d * N + i];
+    r[d] = x0 + v * dt;
+    if (unwrapped) unwrapped[d * N + i] += r[d] - x0;
   }
   const Box& b = *box;
   double s[3];
@@ -174,13 +206,13 @@ __global__ void k_vv1(StepParams p, const Box* __restrict__ box, const double* _
 __global__ void k_vv2_thermo(StepParams p, const double* __restrict__ mass,
                              const double* __restrict__ force, double* vel,
                              const double* __restrict__ pe, const double* __restrict__ virial,
-                             double* partials)
+                             double* partials, const MdScalars* __restrict__ sc)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int N = p.N;
   double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   if (i < N) {
-    const double half = p.dt * 0.5;
+    const double half = step_dt(p, sc) * 0.5;
     const double m = mass[i];
     const double im = 1.0 / m;
     double vv[3];
@@ -313,6 +345,7 @@ k_ensemble(StepParams p, Box* box, MdScalars* sc, const double* __restrict__ par
   __syncthreads();
   if (threadIdx.x != 0) return;
   const long long step = sc->step;
+  const double dt = step_dt(p, sc);
   Box& b = *box;
   const double V = box_volume(b);
   double th[8];
@@ -334,7 +367,7 @@ k_ensemble(StepParams p, Box* box, MdScalars* sc, const double* __restrict__ par
     case kNvtNhc: {
       const double ek2 = th[0] * (3.0 * p.N * kBoltzmann);
       vf = nhc_half_step(sc->nhc_pos, sc->nhc_mom, sc->nhc_mass, ek2, kBoltzmann * Tt, 3.0 * p.N,
-                         p.dt * 0.5);
+                         dt * 0.5);
       break;
     }
     case kNvtBdp:
@@ -404,6 +437,8 @@ k_ensemble(StepParams p, Box* box, MdScalars* sc, const double* __restrict__ par
   }
   sc->step = step + 1;
   sc->vfactor_pre = 1.0;
+  sc->time += dt;
+  sc->vmax2 = 0ull;   // the next step's k_vmax starts from zero
 }
 
 // v *= velocity factor; under a box change x and the Verlet reference x0
@@ -438,6 +473,8 @@ __global__ void k_init_scalars(MdScalars* sc, StepParams p, double T0, double ta
 {
   sc->step = 0;
   sc->step0 = 0;
+  sc->time = 0.0;
+  sc->vmax2 = 0ull;
   sc->vfactor_pre = 1.0;
   sc->vfactor = 1.0;
   sc->bfactor = 1.0;
@@ -461,6 +498,7 @@ void md_enqueue_step(Md& md, const StepParams& p, int* d_status)
   const int N = md.N;
   const int blocks = (N + kThreads - 1) / kThreads;
   cudaStream_t s = md.stream;
+  if (p.max_dist > 0.0) k_vmax<<<blocks, kThreads, 0, s>>>(N, md.d_vel, md.d_sc);
   if (p.kind == kNvtNhc) {
     k_ke_partials<<<blocks, kThreads, 0, s>>>(N, md.d_mass, md.d_vel, md.d_partials);
     k_nhc_pre<<<1, 1, 0, s>>>(p, md.d_sc, md.d_partials, blocks);
@@ -468,11 +506,11 @@ void md_enqueue_step(Md& md, const StepParams& p, int* d_status)
   const SkinArgs sk{md.d_type, e.nbr.x0, e.d_nstate, e.scratch.sites, e.skin,
                     static_cast<double>(e.model.rc_max) + e.skin, e.use_xr ? 0 : 1};
   k_vv1<<<blocks, kThreads, 0, s>>>(p, e.d_box, md.d_mass, md.d_force, md.d_pos, md.d_vel, md.d_sc,
-                                    sk);
+                                    sk, p.unwrapped ? md.d_unwrapped : nullptr);
   launch_neighbor_update(e, N, md.d_pos, md.d_type, false, s, sk.enabled != 0);
   launch_force(e, N, md.d_pos, md.d_type, md.d_pe, md.d_force, md.d_virial, false, s);
   k_vv2_thermo<<<blocks, kThreads, 0, s>>>(p, md.d_mass, md.d_force, md.d_vel, md.d_pe,
-                                          md.d_virial, md.d_partials);
+                                          md.d_virial, md.d_partials, md.d_sc);
   k_ensemble<<<1, kEnsembleThreads, 0, s>>>(p, e.d_box, md.d_sc, md.d_partials, blocks,
                                             md.d_noise, md.d_rows, md.rows_cap, e.d_nstate,
                                             d_status);
@@ -664,8 +702,8 @@ int nepx_md_destroy(nepx_md_t* m)
   nepx::Md& md = m->md;
   if (md.stream) cudaStreamSynchronize(md.stream);
   drop_graphs(m);
-  void* ptrs[] = {md.d_type, md.d_mass, md.d_pos, md.d_vel, md.d_force, md.d_pe, md.d_virial,
-                  md.d_partials, md.d_sc, md.d_noise, md.d_rows};
+  void* ptrs[] = {md.d_type, md.d_mass,  md.d_pos,  md.d_vel,  md.d_force,    md.d_pe,
+                  md.d_virial, md.d_partials, md.d_sc, md.d_noise, md.d_rows, md.d_unwrapped};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (m->h_noise) cudaFreeHost(m->h_noise);
@@ -768,6 +806,11 @@ int md_enqueue_run(nepx_md* m, int steps, double dt_fs, int thermo_every, double
   p.Tdamp = c.Tdamp;
   p.rc_v = e.model.rc_max + e.skin;
   p.skin = e.skin;
+  p.max_dist = md.max_dist;
+  p.unwrapped = md.d_unwrapped ? 1 : 0;
+  if (p.max_dist > 0.0 && c.kind != nepx::kNVE && c.kind != nepx::kNvtBer)
+    return md_fail(m, NEPX_ERR_UNSUPPORTED,
+                   "the adaptive time step runs with nve and nvt_ber only, as in the reference");
   if (c.kind == nepx::kNptBer || c.kind == nepx::kNptScr) {
     p.p_target = c.p_gpa / nepx::kPressureUnit;
     // form pc in 1/GPa, then convert once (ensemble_control.cpp:84-95)
@@ -1018,6 +1061,119 @@ int nepx_md_get(nepx_md_t* m, double* h_pos, double* h_vel, double* h_force, dou
     for (int d = 0; d < 3; ++d) box->pbc[d] = md.box.pbc[d];
   }
   return ok ? NEPX_OK : md_cuda(m, "copy state");
+}
+
+int nepx_md_set_velocity(nepx_md_t* m, const double* h_vel)
+{
+  if (!m || !h_vel) return NEPX_ERR_ARG;
+  nepx::Md& md = m->md;
+  const size_t n = md.N;
+  std::vector<double> v(h_vel, h_vel + 3 * n);
+  for (double& x : v) {
+    if (!std::isfinite(x)) return md_fail(m, NEPX_ERR_ARG, "non-finite velocity");
+    x *= nepx::kTimeUnit;   // A/fs -> natural units
+  }
+  if (cudaStreamSynchronize(md.stream) != cudaSuccess ||
+      cudaMemcpy(md.d_vel, v.data(), sizeof(double) * 3 * n, cudaMemcpyHostToDevice) !=
+        cudaSuccess)
+    return md_cuda(m, "upload velocities");
+  return NEPX_OK;
+}
+
+int nepx_md_compute_forces(nepx_md_t* m)
+{
+  if (!m) return NEPX_ERR_ARG;
+  nepx::Md& md = m->md;
+  nepx::Engine& e = *md.engine;
+  const int N = md.N;
+  cudaStream_t s = md.stream;
+  e.use_xr = md.xr;
+  e.xr.from_box = true;
+  bool rebuild = !md.forces_valid;
+  if (e.box_owner != &md) {
+    nepx::launch_set_box(e, md.box, s);
+    e.box_owner = &md;
+    e.order_valid = false;
+    rebuild = true;
+  }
+  nepx::launch_neighbor_update(e, N, md.d_pos, md.d_type, rebuild, s);
+  if (!e.tuned) nepx::engine_autotune(e, N, md.d_pos, md.d_type, s);
+  nepx::launch_force(e, N, md.d_pos, md.d_type, md.d_pe, md.d_force, md.d_virial, false, s);
+  md.forces_valid = true;
+  e.force_rebuild = true;     // a later nepx_compute on this handle rebuilds
+  e.have_box = false;
+  if (cudaMemcpyAsync(&m->mirror->nstate, e.d_nstate, sizeof(nepx::NeighborState),
+                      cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return md_cuda(m, "force evaluation");
+  const nepx::NeighborState& st = m->mirror->nstate;
+  if (st.overflow) return md_fail(m, NEPX_ERR_OVERFLOW, "a neighbour row exceeded its capacity");
+  if (st.nonfinite) return md_fail(m, NEPX_ERR_NONFINITE, "non-finite energy or force");
+  if (st.box_error)
+    return md_fail(m, NEPX_ERR_BOX, "the box is small in one periodic direction and thicker "
+                                    "than 10 rc in another (unsupported, as in the reference)");
+  return NEPX_OK;
+}
+
+int nepx_md_neighbor_info(nepx_md_t* m, int* max_radial, int* max_angular)
+{
+  if (!m) return NEPX_ERR_ARG;
+  if (cudaStreamSynchronize(m->md.stream) != cudaSuccess) return md_cuda(m, "synchronise");
+  if (max_radial) *max_radial = m->mirror->nstate.call_nn[0];
+  if (max_angular) *max_angular = m->mirror->nstate.call_nn[1];
+  return NEPX_OK;
+}
+
+int nepx_md_set_max_distance(nepx_md_t* m, double max_distance)
+{
+  if (!m) return NEPX_ERR_ARG;
+  if (!(max_distance >= 0.0) || !std::isfinite(max_distance))
+    return md_fail(m, NEPX_ERR_ARG, "maximum distance per step should be >= 0");
+  m->md.max_dist = max_distance;
+  return NEPX_OK;
+}
+
+int nepx_md_time(nepx_md_t* m, double* time_fs)
+{
+  if (!m || !time_fs) return NEPX_ERR_ARG;
+  nepx::Md& md = m->md;
+  double t = 0.0;
+  if (cudaStreamSynchronize(md.stream) != cudaSuccess ||
+      cudaMemcpy(&t, &md.d_sc->time, sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return md_cuda(m, "read time");
+  *time_fs = t * nepx::kTimeUnit;
+  return NEPX_OK;
+}
+
+int nepx_md_enable_unwrapped(nepx_md_t* m)
+{
+  if (!m) return NEPX_ERR_ARG;
+  nepx::Md& md = m->md;
+  if (md.d_unwrapped) return NEPX_OK;
+  const size_t n = md.N;
+  if (cudaStreamSynchronize(md.stream) != cudaSuccess ||
+      cudaMalloc(reinterpret_cast<void**>(&md.d_unwrapped), sizeof(double) * 3 * n) !=
+        cudaSuccess) {
+    md.d_unwrapped = nullptr;
+    return md_cuda(m, "allocate unwrapped positions");
+  }
+  if (cudaMemcpy(md.d_unwrapped, md.d_pos, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice) !=
+      cudaSuccess)
+    return md_cuda(m, "copy unwrapped positions");
+  return NEPX_OK;
+}
+
+int nepx_md_get_unwrapped(nepx_md_t* m, double* h_unwrapped)
+{
+  if (!m || !h_unwrapped) return NEPX_ERR_ARG;
+  nepx::Md& md = m->md;
+  if (!md.d_unwrapped)
+    return md_fail(m, NEPX_ERR_ARG, "unwrapped positions are not enabled (nepx_md_enable_unwrapped)");
+  if (cudaStreamSynchronize(md.stream) != cudaSuccess ||
+      cudaMemcpy(h_unwrapped, md.d_unwrapped, sizeof(double) * 3 * md.N,
+                 cudaMemcpyDeviceToHost) != cudaSuccess)
+    return md_cuda(m, "copy unwrapped positions");
+  return NEPX_OK;
 }
 
 int nepx_md_device_state(nepx_md_t* m, double** d_pos, double** d_vel, double** d_force,

@@ -46,6 +46,8 @@ struct MdScalars {
   double mu[9];        // box deformation of this step, h' = mu h (component couplings)
   double thermo[8];    // T, PE, stresses xx yy zz xy xz yz (natural units, volume-normalised)
   double nhc_pos[kChain], nhc_mom[kChain], nhc_mass[kChain];
+  double time;         // simulated time since the segment's first step (natural units)
+  unsigned long long vmax2;   // bits of max |v|^2 this step (adaptive time step; >= 0)
 };
 
 // Per-run constants passed by value.
@@ -66,6 +68,8 @@ struct StepParams {
   double bdp_factor;   // exp(-1/Tdamp) (0 when Tdamp <= 0.1)
   double rc_v;         // rc + skin, for the NPT rebuild criterion
   double skin;
+  double max_dist;     // adaptive time step: largest displacement per step (A), 0 = off
+  int unwrapped;       // accumulate unwrapped positions in the first half kick
 };
 
 struct Md {
@@ -82,6 +86,8 @@ struct Md {
   double* d_rows = nullptr;       // [rows][kThermoCols]
   int rows_cap = 0;
   double* d_scale = nullptr;      // cumulative box scale since the last Verlet build
+  double* d_unwrapped = nullptr;  // [3][N] unwrapped positions (dump_xyz unwrapped_position)
+  double max_dist = 0.0;          // adaptive time step bound (A), 0 = fixed step
   Box box{};
   EnsembleConfig ens;
   SvrRng rng{12345678u};

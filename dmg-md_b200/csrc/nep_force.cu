@@ -445,6 +445,8 @@ k_filter_radial(const ModelParams p, int N, const Box* __restrict__ box,
     if (ca > mn_a) atomicOr(&st->overflow, 4);
     atomicMax(&st->max_nn[1], cr);
     atomicMax(&st->max_nn[2], ca);
+    atomicMax(&st->call_nn[0], cr);
+    atomicMax(&st->call_nn[1], ca);
 #pragma unroll
     for (int n = 0; n < NRM; ++n)
       if (n < nR) qrad[static_cast<size_t>(i) * nR + n] = qr[n];

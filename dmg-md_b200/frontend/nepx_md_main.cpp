@@ -15,6 +15,7 @@
 //
 // The ensemble RNG seed is DMGMD_ENSEMBLE_SEED when set (decimal), else
 // 12345678, restarted for every segment (reference runtime.cu:705-709).
+#include <algorithm>
 #include <chrono>
 #include <cinttypes>
 #include <cmath>
@@ -23,6 +24,7 @@
 #include <cstring>
 #include <iostream>
 #include <numeric>
+#include <optional>
 #include <string>
 #include <vector>
 
@@ -48,27 +50,29 @@ void check(int rc, const char* what, const char* message)
 
 // ---- velocities (reference runtime.cu:1002-1109) ---------------------------------
 
-// Removes the total linear momentum, then the rigid rotation about the
-// center of mass (angular momentum over the inertia tensor).
-void zero_momenta(const std::vector<double>& mass, const std::vector<double>& pos,
-                  std::vector<double>& vel)
+// Removes the linear momentum of the atoms `idx`, then their rigid rotation
+// about their center of mass (angular momentum over the inertia tensor):
+// the reference's correct_velocity_subset (runtime.cu:979-1063).
+void correct_subset(const std::vector<double>& mass, const std::vector<double>& pos,
+                    std::vector<double>& vel, const std::vector<size_t>& idx)
 {
+  if (idx.empty()) return;
   const size_t n = mass.size();
   double M = 0.0, p[3] = {0, 0, 0};
-  for (size_t a = 0; a < n; ++a) {
+  for (size_t a : idx) {
     M += mass[a];
     for (int d = 0; d < 3; ++d) p[d] += mass[a] * vel[d * n + a];
   }
   if (M == 0.0) return;
   for (int d = 0; d < 3; ++d) p[d] /= M;
-  for (size_t a = 0; a < n; ++a)
+  for (size_t a : idx)
     for (int d = 0; d < 3; ++d) vel[d * n + a] -= p[d];
   double c[3] = {0, 0, 0};
-  for (size_t a = 0; a < n; ++a)
+  for (size_t a : idx)
     for (int d = 0; d < 3; ++d) c[d] += pos[d * n + a] * mass[a];
   for (double& v : c) v /= M;
   double L[3] = {0, 0, 0}, I[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-  for (size_t a = 0; a < n; ++a) {
+  for (size_t a : idx) {
     const double x = pos[a] - c[0], y = pos[n + a] - c[1], z = pos[2 * n + a] - c[2];
     const double vx = vel[a], vy = vel[n + a], vz = vel[2 * n + a], m = mass[a];
     L[0] += m * (y * vz - z * vy);
@@ -99,11 +103,41 @@ void zero_momenta(const std::vector<double>& mass, const std::vector<double>& po
   double w[3] = {0, 0, 0};
   for (int r = 0; r < 3; ++r)
     for (int k = 0; k < 3; ++k) w[r] += A[r][k] / det * L[k];
-  for (size_t a = 0; a < n; ++a) {
+  for (size_t a : idx) {
     const double x = pos[a] - c[0], y = pos[n + a] - c[1], z = pos[2 * n + a] - c[2];
     vel[a] -= w[1] * z - w[2] * y;
     vel[n + a] -= w[2] * x - w[0] * z;
     vel[2 * n + a] -= w[0] * y - w[1] * x;
+  }
+}
+
+void zero_momenta(const std::vector<double>& mass, const std::vector<double>& pos,
+                  std::vector<double>& vel)
+{
+  std::vector<size_t> all(mass.size());
+  std::iota(all.begin(), all.end(), size_t(0));
+  correct_subset(mass, pos, vel, all);
+}
+
+// correct_velocity: every atom at once, or each group of one grouping method
+// of model.xyz in turn (reference correct_device_velocity, runtime.cu:620-655).
+void correct_velocity(const Model& m, const CorrectVelocityCmd& c, const std::vector<double>& pos,
+                      std::vector<double>& vel)
+{
+  if (!c.grouping) {
+    zero_momenta(m.mass, pos, vel);
+    return;
+  }
+  if (*c.grouping >= static_cast<int>(m.groups.size()))
+    throw std::runtime_error("correct_velocity grouping method is out of range");
+  const std::vector<int>& label = m.groups[*c.grouping];
+  int top = -1;
+  for (int g : label) top = std::max(top, g);
+  for (int g = 0; g <= top; ++g) {
+    std::vector<size_t> subset;
+    for (size_t a = 0; a < label.size(); ++a)
+      if (label[a] == g) subset.push_back(a);
+    correct_subset(m.mass, pos, vel, subset);
   }
 }
 
@@ -131,6 +165,7 @@ void random_velocities(const Model& m, double T, const int* seed, std::vector<do
 
 struct State {
   std::vector<double> pos, vel, force, pe, virial;
+  std::vector<double> unwrapped;   // when a dump_xyz asks for unwrapped_position
   nepx_box box;
 };
 
@@ -207,6 +242,7 @@ void write_xyz(const DumpXyzCmd& c, int step, double time_fs, const Model& m, co
   if (c.velocity) std::fprintf(f, ":vel:R:3");
   if (c.force) std::fprintf(f, ":forces:R:3");
   if (c.potential) std::fprintf(f, ":energy_atom:R:1");
+  if (c.unwrapped) std::fprintf(f, ":unwrapped_position:R:3");
   if (c.virial) std::fprintf(f, ":virial:R:9");
   if (c.group_labels) std::fprintf(f, ":group:I:%zu", m.groups.size());
   std::fprintf(f, "\n");
@@ -221,6 +257,8 @@ void write_xyz(const DumpXyzCmd& c, int step, double time_fs, const Model& m, co
     if (c.force)
       for (int d = 0; d < 3; ++d) std::fprintf(f, fmt, s.force[d * n + a]);
     if (c.potential) std::fprintf(f, fmt, s.pe[a]);
+    if (c.unwrapped)
+      for (int d = 0; d < 3; ++d) std::fprintf(f, fmt, s.unwrapped[d * n + a]);
     if (c.virial)
       for (int k : rowmajor) std::fprintf(f, fmt, s.virial[k * n + a]);
     if (c.group_labels)
@@ -266,8 +304,13 @@ struct Job {
   double dt_fs = 1.0;
   double time_fs = 0.0;
   std::uint32_t seed = 12345678u;
+  // per run (the reference clears them after every run, runtime.cu:950-952)
+  std::optional<CorrectVelocityCmd> correction;
+  double max_distance = 0.0;     // adaptive time step bound (A), 0 = fixed step
+  bool want_unwrapped = false;   // a dump_xyz asked for unwrapped positions
+  long long force_calls = 0;     // force evaluations so far (neighbor.out numbering)
 
-  State state()
+  State state(bool unwrapped = false)
   {
     State s;
     const size_t n = model.n;
@@ -279,6 +322,11 @@ struct Job {
     check(nepx_md_get(md, s.pos.data(), s.vel.data(), s.force.data(), s.pe.data(),
                       s.virial.data(), &s.box),
           "nepx_md_get", nepx_md_last_error(md));
+    if (unwrapped) {
+      s.unwrapped.resize(3 * n);
+      check(nepx_md_get_unwrapped(md, s.unwrapped.data()), "nepx_md_get_unwrapped",
+            nepx_md_last_error(md));
+    }
     return s;
   }
 
@@ -294,6 +342,32 @@ struct Job {
                           nepx_last_error(pot));
   }
 
+  // The reference appends a neighbor.out line at every 1000th force
+  // evaluation of the process, counted from 0 (nep.cu:1156-1176): the largest
+  // radial and angular row of that evaluation next to their capacities.
+  void neighbor_record(long long call)
+  {
+    if (call % 1000 != 0) return;
+    int info[16];
+    check(nepx_info(pot, info, nullptr), "nepx_info", nepx_last_error(pot));
+    int r = 0, a = 0;
+    check(nepx_md_neighbor_info(md, &r, &a), "nepx_md_neighbor_info", nepx_md_last_error(md));
+    FILE* f = std::fopen("neighbor.out", "a");
+    if (!f) throw Failure("cannot open neighbor.out");
+    std::fprintf(f, "Neighbor info at step %lld: radial(max=%d,actual=%d), angular(max=%d,actual=%d).\n",
+                 call, info[12], r, info[13], a);
+    std::fclose(f);
+  }
+
+  void correct_now()
+  {
+    std::vector<double> pos(3 * model.n), v(3 * model.n);
+    check(nepx_md_get(md, pos.data(), v.data(), nullptr, nullptr, nullptr, nullptr),
+          "nepx_md_get", nepx_md_last_error(md));
+    correct_velocity(model, *correction, pos, v);
+    check(nepx_md_set_velocity(md, v.data()), "nepx_md_set_velocity", nepx_md_last_error(md));
+  }
+
   void run(int steps, const EnsembleCmd& ens, const std::vector<int>& thermo,
            const std::vector<DumpXyzCmd>& xyz, const std::vector<int>& restart)
   {
@@ -304,36 +378,62 @@ struct Job {
     if (ens.baro)
       check(nepx_md_set_barostat(md, ens.baro, ens.p6_gpa, ens.c6_gpa), "nepx_md_set_barostat",
             nepx_md_last_error(md));
+    if (want_unwrapped)
+      check(nepx_md_enable_unwrapped(md), "nepx_md_enable_unwrapped", nepx_md_last_error(md));
+    check(nepx_md_set_max_distance(md, max_distance), "time_step", nepx_md_last_error(md));
+    // the reference evaluates the forces once before the steps of every run
+    // (runtime.cu:746); it is a force evaluation of the neighbor.out count
+    check(nepx_md_compute_forces(md), "force evaluation", nepx_md_last_error(md));
+    neighbor_record(force_calls++);
+    const long long call0 = force_calls;   // the force evaluation of step 0
     // stop at every multiple of the gcd of the output intervals
     int g = 0;
     for (int v : thermo) g = std::gcd(g, v);
     for (const auto& d : xyz) g = std::gcd(g, d.interval);
     for (int v : restart) g = std::gcd(g, v);
     if (g == 0) g = steps;
+    bool unwrapped_out = false;
+    for (const auto& d : xyz) unwrapped_out |= d.unwrapped;
     FILE* tf = nullptr;
     if (!thermo.empty()) {
       tf = std::fopen("thermo.out", "a");
       if (!tf) throw Failure("cannot open thermo.out");
       write_thermo_header(tf, thermo.back(), model.n, dt_fs);
     }
+    const double time0 = time_fs;
     double row[20];
     for (int done = 0; done < steps;) {
-      const int k = std::min(g, steps - done);
+      if (correction && done % correction->interval == 0) correct_now();
+      // the chunk ends at the next output step, the next velocity correction,
+      // or right after the step whose force evaluation neighbor.out records
+      int next = std::min(steps, (done / g + 1) * g);
+      if (correction) next = std::min(next, (done / correction->interval + 1) * correction->interval);
+      const long long to_record = (1000 - (call0 + done) % 1000) % 1000;
+      if (done + to_record < steps) next = std::min<long long>(next, done + to_record + 1);
+      const int k = next - done;
       check(nepx_md_run_segment(md, k, dt_fs, k, row, done, steps), "run",
             nepx_md_last_error(md));
-      done += k;
-      time_fs += k * dt_fs;
+      done = next;
+      if (max_distance > 0.0) {
+        double t = 0.0;
+        check(nepx_md_time(md, &t), "nepx_md_time", nepx_md_last_error(md));
+        time_fs = time0 + t;
+      } else {
+        time_fs += k * dt_fs;
+      }
+      neighbor_record(call0 + done - 1);
       if (tf && done % thermo.back() == 0) write_thermo_row(tf, row);
       bool need_state = false;
       for (const auto& d : xyz) need_state |= done % d.interval == 0;
       for (int v : restart) need_state |= done % v == 0;
       if (!need_state) continue;
-      const State s = state();
+      const State s = state(unwrapped_out);
       for (const auto& d : xyz)
         if (done % d.interval == 0) write_xyz(d, done - 1, time_fs, model, s, row);
       for (int v : restart)
         if (done % v == 0) write_restart(model, s);
     }
+    force_calls = call0 + steps;
     if (tf) std::fclose(tf);
   }
 };
@@ -372,11 +472,6 @@ int main(int argc, char** argv)
           throw InputError(c.source, "multiple potential commands are unsupported");
         potential = p->file;
       }
-      if (const auto* d = std::get_if<DumpXyzCmd>(&c.data))
-        if (d->unwrapped)
-          throw InputError(c.source, "dump_xyz unwrapped_position is not supported by nepx-md");
-      if (std::holds_alternative<CorrectVelocityCmd>(c.data))
-        throw InputError(c.source, "correct_velocity is not supported by nepx-md");
     }
     if (potential.empty())
       throw InputError(Source{"run.in", 0, {}}, "run.in does not contain a potential command");
@@ -421,6 +516,9 @@ int main(int argc, char** argv)
           }
         } else if (const auto* t = std::get_if<TimeStepCmd>(&c.data)) {
           job.dt_fs = t->fs;
+          job.max_distance = t->max_distance.value_or(0.0);
+        } else if (const auto* v = std::get_if<CorrectVelocityCmd>(&c.data)) {
+          job.correction = *v;
         } else if (const auto* e = std::get_if<EnsembleCmd>(&c.data)) {
           ensemble = *e;
           have_ensemble = true;
@@ -428,6 +526,7 @@ int main(int argc, char** argv)
           thermo.push_back(d->interval);
         } else if (const auto* d = std::get_if<DumpXyzCmd>(&c.data)) {
           xyz.push_back(*d);
+          job.want_unwrapped |= d->unwrapped;
         } else if (const auto* d = std::get_if<DumpRestartCmd>(&c.data)) {
           restart.push_back(d->interval);
         } else if (const auto* r = std::get_if<RunCmd>(&c.data)) {
@@ -437,6 +536,8 @@ int main(int argc, char** argv)
           thermo.clear();
           xyz.clear();
           restart.clear();
+          job.correction.reset();
+          job.max_distance = 0.0;
         }
       } catch (const Failure& f) {
         throw InputError(c.source, f.what());

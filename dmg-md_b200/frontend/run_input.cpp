@@ -291,9 +291,6 @@ void validate_program(const std::vector<Command>& program)
         if (!(std::isfinite(dt) && dt > 0.0))
           fail(c.source, "ensemble " + name + " requires a finite positive time_step");
       }
-      // this driver's own limits
-      if (adaptive)
-        fail(c.source, "adaptive time_step (maximum distance per step) is not supported by nepx-md");
       correction = false;
       adaptive = false;
     }

@@ -35,7 +35,9 @@ EXPORTED = ["nepx_create", "nepx_destroy", "nepx_last_error", "nepx_info", "nepx
             "nepx_server_create", "nepx_server_destroy", "nepx_server_last_error",
             "nepx_server_submit", "nepx_server_poll", "nepx_server_wait", "nepx_server_drain",
             "nepx_server_stats", "nepx_set_precision", "nepx_md_run_segment",
-            "nepx_md_set_barostat"]
+            "nepx_md_set_barostat", "nepx_md_set_velocity", "nepx_md_compute_forces",
+            "nepx_md_neighbor_info", "nepx_md_set_max_distance", "nepx_md_time",
+            "nepx_md_enable_unwrapped", "nepx_md_get_unwrapped"]
 
 ENSEMBLES = {"nve": 0, "nvt_ber": 1, "nvt_nhc": 2, "nvt_bdp": 3, "npt_ber": 4, "npt_scr": 5}
 BAROSTATS = {"isotropic": 0, "anisotropic": 1, "triclinic": 2}
@@ -130,6 +132,13 @@ def lib():
         L.nepx_server_wait.argtypes = [vp, ctypes.c_longlong, ip]
         L.nepx_server_drain.argtypes = [vp]
         L.nepx_server_stats.argtypes = [vp, dp]
+        L.nepx_md_set_velocity.argtypes = [vp, dp]
+        L.nepx_md_compute_forces.argtypes = [vp]
+        L.nepx_md_neighbor_info.argtypes = [vp, ip, ip]
+        L.nepx_md_set_max_distance.argtypes = [vp, ctypes.c_double]
+        L.nepx_md_time.argtypes = [vp, dp]
+        L.nepx_md_enable_unwrapped.argtypes = [vp]
+        L.nepx_md_get_unwrapped.argtypes = [vp, dp]
         for name in EXPORTED:
             if name not in ("nepx_last_error", "nepx_md_last_error", "nepx_server_last_error"):
                 getattr(L, name).restype = ctypes.c_int
@@ -377,6 +386,42 @@ class MD:
 
     def run_async(self, steps, dt_fs):
         self._check(lib().nepx_md_run_async(self._h, steps, dt_fs))
+
+    def set_velocity(self, vel):
+        """Replaces the velocities, (3, n) A/fs."""
+        import numpy as np
+        v = np.ascontiguousarray(vel, dtype=np.float64).reshape(-1)
+        self._check(lib().nepx_md_set_velocity(self._h, _dp(v)))
+
+    def compute_forces(self):
+        """Energy, forces and virials at the current positions."""
+        self._check(lib().nepx_md_compute_forces(self._h))
+
+    def neighbor_info(self):
+        """(largest radial row, largest angular row) of the latest force evaluation."""
+        r, a = ctypes.c_int(), ctypes.c_int()
+        self._check(lib().nepx_md_neighbor_info(self._h, ctypes.byref(r), ctypes.byref(a)))
+        return r.value, a.value
+
+    def set_max_distance(self, max_distance):
+        """Adaptive time step bound in A (0: fixed step)."""
+        self._check(lib().nepx_md_set_max_distance(self._h, float(max_distance)))
+
+    def time(self):
+        """Simulated time (fs) since the current segment's first step."""
+        t = ctypes.c_double()
+        self._check(lib().nepx_md_time(self._h, ctypes.byref(t)))
+        return t.value
+
+    def enable_unwrapped(self):
+        self._check(lib().nepx_md_enable_unwrapped(self._h))
+
+    def unwrapped(self):
+        """Unwrapped positions (3, n) in A."""
+        import numpy as np
+        out = np.zeros((3, self.n))
+        self._check(lib().nepx_md_get_unwrapped(self._h, _dp(out)))
+        return out
 
     def sync(self):
         self._check(lib().nepx_md_sync(self._h))

@@ -248,6 +248,46 @@ int nepx_md_sync(nepx_md_t* md);
 int nepx_md_get(nepx_md_t* md, double* h_pos, double* h_vel, double* h_force, double* h_pe,
                 double* h_virial, nepx_box* box);
 
+/* Replaces the velocities (host [3][n], A/fs), e.g. after a host-side
+ * momentum correction.  Replaces DeviceAtoms::upload_velocity as used by
+ * correct_device_velocity (src/runtime.cu:620-655). */
+int nepx_md_set_velocity(nepx_md_t* md, const double* h_vel);
+
+/* Evaluates energy, forces and virials at the current positions (what the
+ * reference does at the start of every run segment, force.compute before the
+ * step loop, src/runtime.cu:746); synchronous.  Recomputing at unchanged
+ * positions gives the same forces bit for bit. */
+int nepx_md_compute_forces(nepx_md_t* md);
+
+/* Largest radial and angular neighbour row of the md's latest force
+ * evaluation: the `actual` values of the reference's neighbor.out record
+ * (src/gpumd_compat/nep.cu:1156-1176).  Synchronises the md stream. */
+int nepx_md_neighbor_info(nepx_md_t* md, int* max_radial, int* max_angular);
+
+/* Adaptive time step: every later step takes dt = min(dt_fs, max_distance /
+ * max |v|) over the velocities at the start of the step, computed on the
+ * device (reference adaptive_time_step, src/runtime.cu:594-619, `time_step dt
+ * max_distance` in run.in).  max_distance in A; 0 turns it off.  Runs with
+ * NEPX_NVE and NEPX_NVT_BER only, as in the reference (other ensembles
+ * return NEPX_ERR_UNSUPPORTED at run time). */
+int nepx_md_set_max_distance(nepx_md_t* md, double max_distance);
+
+/* Simulated time (fs) since the first step of the current segment (the sum
+ * of the steps' time steps; with a fixed step, steps * dt).  Replaces the
+ * reference's global_time bookkeeping (src/runtime.cu:759-760). */
+int nepx_md_time(nepx_md_t* md, double* time_fs);
+
+/* Starts tracking unwrapped positions from the current positions (no-op when
+ * already on): each later first half kick adds the step's displacement
+ * before the wrap into the box.  Replaces DeviceAtoms::enable_unwrapped and
+ * update_unwrapped (src/runtime.cu:80-90, 423-438) behind dump_xyz
+ * unwrapped_position. */
+int nepx_md_enable_unwrapped(nepx_md_t* md);
+
+/* Copies the unwrapped positions (host [3][n], A); NEPX_ERR_ARG unless
+ * enabled. */
+int nepx_md_get_unwrapped(nepx_md_t* md, double* h_unwrapped);
+
 /* Device pointers of the state (positions, velocities in natural units,
  * forces, types) and the stream the md runs on. */
 int nepx_md_device_state(nepx_md_t* md, double** d_pos, double** d_vel, double** d_force,

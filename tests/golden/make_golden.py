@@ -11,6 +11,8 @@ It reads, as data only:
     energy, virial; NVE trajectory) of the reference's golden suite,
   * tests/baseline/inputs/*   -- the matching model.xyz / run.in inputs and
     the three NEP potential files,
+  * the programs' output files (thermo.out, dump_xyz, restart.xyz and the
+    neighbor.out occupancy records),
   * tests/thermostats/fixtures/{svr,nhc}.json -- bit-level thermostat KATs,
 and writes tests/golden/baseline_goldens.json, tests/golden/potentials/*.txt
 and tests/golden/thermostats/*.json.  The tests never read the reference
@@ -154,7 +156,7 @@ def main():
                    "model_from_stage": st.get("model_from_stage"),
                    "outputs": {}}
             for name, o in st["outputs"].items():
-                if o["kind"] in ("xyz", "thermo", "restart"):
+                if o["kind"] in ("xyz", "thermo", "restart", "text"):
                     rec["outputs"][name] = open(os.path.join(base, "goldens", case, st["name"],
                                                              name)).read()
             stages.append(rec)

@@ -71,6 +71,35 @@ def test_program_rules(tmp_path):
     assert r.returncode == 1 and "does not contain a potential command" in r.stderr
 
 
+@pytest.mark.parametrize("body", [
+    "time_step 1 0.05\nensemble nve\nrun 10\n",
+    "time_step 1 0.05\nensemble nvt_ber 300 300 100\nrun 10\n",
+    "ensemble nve\ncorrect_velocity 10\nrun 20\n",
+    "ensemble nvt_ber 300 300 100\ncorrect_velocity 10 0\nrun 20\n",
+    "ensemble nve\ndump_xyz 5 a.xyz unwrapped_position velocity\nrun 10\n",
+])
+def test_run_in_md_controls_accepted(tmp_path, body):
+    """correct_velocity, the adaptive time step and unwrapped positions run
+    with the ensembles the reference allows them with."""
+    _stage(tmp_path, run_in="potential nep.txt\n" + body)
+    r = _check(tmp_path)
+    assert r.returncode == 0, r.stderr
+
+
+@pytest.mark.parametrize("body,message", [
+    ("ensemble npt_ber 300 300 100 0 100 1000\ncorrect_velocity 10\nrun 10\n",
+     "ensemble npt_ber does not support correct_velocity"),
+    ("time_step 1 0.05\nensemble nvt_nhc 300 300 100\nrun 10\n",
+     "ensemble nvt_nhc does not support adaptive time_step"),
+    ("ensemble nve\ncorrect_velocity 5\nrun 10\n",
+     "velocity correction interval should be >= 10"),
+])
+def test_run_in_md_controls_rules(tmp_path, body, message):
+    _stage(tmp_path, run_in="potential nep.txt\n" + body)
+    r = _check(tmp_path)
+    assert r.returncode == 1 and message in r.stderr, r.stderr
+
+
 @pytest.mark.parametrize("edit,message", [
     (lambda m: m.replace("Lattice=\"24 0 0 0 24 0 0 0 24\"", "Lattice=\"24 0 0 0 24 0\""),
      "Lattice should contain nine values"),
