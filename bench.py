@@ -210,7 +210,8 @@ def run_serving(args):
         "metric": "served structures/s", "value": rate_sat, "unit": "structures/s",
         "n_gpus": 1, "higher_is_better": True,
         "dtype": "fp32 descriptors and forces, %s ANN, fp64 integration" %
-                 ("tcgen05 3xTF32" if args.precision == "mixed" else "fp32"),
+                 ({"mixed": "tcgen05 FP16 (per-layer power-of-two scaling, FP32 accumulation)",
+                   "mixed_bf16": "tcgen05 BF16 (FP32 accumulation)"}.get(args.precision, "fp32")),
         "data": "synthetic (seeded structures and NEP5 weights)",
         "config": {"workload": "serving_stream_%d_structs_16-8192_atoms_nep5_4type_rc5.0-4.0"
                                "_H64_20pct_nve100" % count,
@@ -848,7 +849,7 @@ def main():
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the other workloads, the NVE drift and the serving sample")
     ap.add_argument("--serving-sample", type=int, default=5000)
-    ap.add_argument("--precision", default="mixed", choices=["fp32", "mixed"],
+    ap.add_argument("--precision", default="mixed", choices=["fp32", "mixed", "mixed_bf16"],
                     help="ANN precision of the serving workload")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -932,8 +933,9 @@ def main():
     roofline = roofline_of(pot, args.workload, n, prof)
     mixed = {"value": value_mixed, "unit": "atom-steps/s", "ms_per_step": dev_ms_m / K,
              "over_fp32": value_mixed / value,
-             "what": "the same MD with the ANN contractions on tcgen05 (FP32 accumulation in "
-                     "TMEM); descriptors and forces FP32",
+             "what": "the same MD with the ANN's two contractions as tcgen05 MMAs inside the "
+                     "descriptor kernel: FP16 operands with per-layer power-of-two scaling, FP32 "
+                     "accumulation in TMEM; descriptors and forces FP32",
              "stage_ms": prof_mixed}
     pot.close()
     del flush

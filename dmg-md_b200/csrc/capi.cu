@@ -272,7 +272,8 @@ int nepx_neighbors(nepx_t* h, int which, int n, int* d_nn, int* d_nl, int mn, vo
 int nepx_set_precision(nepx_t* h, int mode)
 {
   if (!h) return NEPX_ERR_ARG;
-  if (mode != NEPX_PRECISION_FP32 && mode != NEPX_PRECISION_MIXED)
+  if (mode != NEPX_PRECISION_FP32 && mode != NEPX_PRECISION_MIXED &&
+      mode != NEPX_PRECISION_MIXED_BF16)
     return fail(h, NEPX_ERR_ARG, "unknown precision mode");
   const std::string err = nepx::engine_set_precision(h->engine, mode);
   if (!err.empty()) return fail(h, NEPX_ERR_UNSUPPORTED, err);

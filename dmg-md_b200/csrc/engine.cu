@@ -1,9 +1,13 @@
 // engine.cu -- handle construction, device uploads and box handling.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <vector>
 
 #include "engine.h"
 
@@ -225,9 +229,17 @@ void engine_autotune(Engine& e, int N, const double* pos, const int* type, cudaS
     }
     e.filter_group = pick;
   }
+  // the descriptor kernel's occupancy builds (CTAs per SM), when the shape has
+  // two (the FP32 build of the small shape; the tensor-core build comes at 3)
+  const int minbs[2] = {3, 4};
+  const int n_minb = (fused_occupancy_variants(e.params) && e.precision == 0) ? 2 : 1;
+  if (n_minb == 1) e.fused_minb = 3;
+  int pick_m = e.fused_minb;
   for (int gf : groups) {
+    for (int mi = 0; mi < n_minb; ++mi)
     for (int gg : groups) {
       e.group = gf;
+      e.fused_minb = minbs[mi];
       e.f12_group = gg;   // angular-force grouping varies together with the gather's
       e.gather_group = gg;
       float tf[3], tg[3];
@@ -248,6 +260,7 @@ void engine_autotune(Engine& e, int N, const double* pos, const int* type, cudaS
       if (tf[1] < best_f) {
         best_f = tf[1];
         pick_f = gf;
+        pick_m = e.fused_minb;
         pick_a = gg;
       }
       if (tg[1] < best_g) {
@@ -260,35 +273,93 @@ void engine_autotune(Engine& e, int N, const double* pos, const int* type, cudaS
   cudaEventDestroy(b);
   cudaEventDestroy(c);
   e.group = pick_f;
+  e.fused_minb = pick_m;
   e.f12_group = pick_a;
   e.gather_group = pick_g;
   e.tuned = true;
   if (std::getenv("NEPX_VERBOSE"))
     std::fprintf(stderr,
-                 "nepx autotune (N=%d): filter G=%d, fused G=%d, angular-force G=%d, gather G=%d\n",
-                 N, e.filter_group, e.group, e.f12_group, e.gather_group);
+                 "nepx autotune (N=%d): filter G=%d, fused G=%d at %d CTAs/SM, angular-force "
+                 "G=%d, gather G=%d\n",
+                 N, e.filter_group, e.group, e.fused_minb, e.f12_group, e.gather_group);
 }
+
+namespace {
+
+// Largest power of two p with max_abs * p <= 2^14 (1 when max_abs is 0): the
+// per-layer scale that keeps 16-bit operands inside FP16's range with room
+// for the products' accumulation.
+float pow2_scale(float max_abs)
+{
+  if (!(max_abs > 0.0f) || !std::isfinite(max_abs)) return 1.0f;
+  int ex = 0;
+  std::frexp(max_abs, &ex);   // max_abs < 2^ex
+  return std::ldexp(1.0f, std::max(-60, std::min(60, 14 - ex)));
+}
+
+unsigned short to16(float x, bool bf16)
+{
+  if (bf16) {
+    const __nv_bfloat16 h = __float2bfloat16_rn(x);
+    return *reinterpret_cast<const unsigned short*>(&h);
+  }
+  const __half h = __float2half_rn(x);
+  return *reinterpret_cast<const unsigned short*>(&h);
+}
+
+}  // namespace
 
 std::string engine_set_precision(Engine& e, int mode)
 {
-  if (mode != 0 && mode != 1) return "precision mode must be 0 (FP32) or 1 (mixed)";
-  if (mode == 1) {
-    std::string why;
-    if (!ann_tc_supported(e.params, why)) return why;
-    ForceScratch& sc = e.scratch;
-    const size_t N = e.capacity;
-    if (!sc.q) {
-      bool ok = dalloc(sc.q, N * e.params.dimK) == cudaSuccess;
-      ok &= dalloc(sc.fp, N * e.params.dimK) == cudaSuccess;
-      ok &= dalloc(sc.order, N) == cudaSuccess;
-      ok &= dalloc(sc.type_counts, 2 * kMaxTypes) == cudaSuccess;
-      if (!ok) return "cudaMalloc failed (mixed-precision buffers)";
+  if (mode < 0 || mode > 2) return "precision mode must be 0 (FP32), 1 (FP16) or 2 (BF16)";
+  ModelParams& p = e.params;
+  if (mode != 0) {
+    // the descriptor kernel's MMAs: M = 128 stacked hidden units per chunk
+    // (m = t H + h over all types) and M = 128 descriptor components
+    if (p.dim > 128 || p.T * p.H > 1024)
+      return "the tensor-core ANN takes dim <= 128 and at most 1024 hidden units over all types";
+    const NepModel& m = e.model;
+    const bool bf16 = mode == 2;
+    p.tc_dimk = (p.dim + 15) & ~15;
+    p.tc_kt = (p.T * p.H + 127) / 128 * 128;
+    float wmax = 0.0f, w1max = 0.0f;
+    for (float x : m.w0) wmax = std::max(wmax, std::fabs(x));
+    for (float x : m.w1) w1max = std::max(w1max, std::fabs(x));
+    p.tc_sw = pow2_scale(wmax);
+    p.tc_sg = pow2_scale(w1max);   // |w1 (1 - x^2)| <= |w1|
+    const size_t nw = static_cast<size_t>(p.T) * p.H * p.tc_dimk;
+    const size_t nwt = static_cast<size_t>(p.dim) * p.tc_kt;
+    std::vector<unsigned short> h16(nw + nwt, to16(0.0f, bf16));
+    for (int t = 0; t < p.T; ++t)
+      for (int h = 0; h < p.H; ++h)
+        for (int d = 0; d < p.dim; ++d) {
+          const size_t mrow = static_cast<size_t>(t) * p.H + h;
+          const float w = m.w0[mrow * p.dim + d] * p.tc_sw;
+          h16[mrow * p.tc_dimk + d] = to16(w, bf16);
+          h16[nw + static_cast<size_t>(d) * p.tc_kt + mrow] = to16(w, bf16);
+        }
+    // one buffer per handle (its size depends on the model only): captured MD
+    // graphs keep its address, so a later precision switch overwrites it in place
+    if (!e.d_w16 &&
+        cudaMalloc(reinterpret_cast<void**>(&e.d_w16), sizeof(unsigned short) * h16.size()) !=
+          cudaSuccess) {
+      e.d_w16 = nullptr;
+      return "cudaMalloc failed (16-bit ANN weights)";
     }
-    ann_tc_prepare(e.params);
+    if (cudaDeviceSynchronize() != cudaSuccess ||
+        cudaMemcpy(e.d_w16, h16.data(), sizeof(unsigned short) * h16.size(),
+                   cudaMemcpyHostToDevice) != cudaSuccess)
+      return "cudaMemcpy failed (16-bit ANN weights)";
+    p.w0h = e.d_w16;
+    p.w0th = e.d_w16 + nw;
+    p.tc_bf16 = bf16 ? 1 : 0;
+    if (fused_tc_smem_bytes(p) > 227 * 1024)
+      return "the tensor-core ANN tiles of this model do not fit one CTA's shared memory";
+    set_fused_smem_limits(p);
+    if (cudaGetLastError() != cudaSuccess) return "CUDA error setting up the tensor-core ANN";
   }
   if (e.precision != mode) e.tuned = false;
   e.precision = mode;
-  e.order_valid = false;
   return "";
 }
 
@@ -297,10 +368,9 @@ void engine_destroy(Engine& e)
   NeighborBuffers& nb = e.nbr;
   void* ptrs[] = {e.d_params, e.d_box, e.d_nstate, nb.nn_v, nb.nl_v, nb.nn_r, nb.nl_r,
                   nb.nn_a, nb.nl_a, nb.cell_count, nb.cell_start, nb.cell_atoms, nb.cell_of,
-                  nb.x0, e.scratch.alpha, e.scratch.f12, e.scratch.pe_ann, e.scratch.q,
+                  nb.x0, e.scratch.alpha, e.scratch.f12, e.scratch.pe_ann, e.d_w16,
                   e.scratch.tune_out, e.scratch.acoef, e.scratch.sites, e.scratch.qrad,
-                  e.scratch.fp,
-                  e.scratch.order, e.scratch.type_counts, e.xr.er, e.xr.ea, e.xr.large,
+                  e.xr.er, e.xr.ea, e.xr.large,
                   e.xr.d_si, e.xr.d_soff};
   for (void* q : ptrs)
     if (q) cudaFree(q);

@@ -34,10 +34,6 @@ struct ForceScratch {
   float4* f12 = nullptr;     // [N][mn_a] directed angular partial forces
   float* acoef = nullptr;    // [N][nA][24] dE/ds[n][lm] of each center
   double* pe_ann = nullptr;  // [N] site energy of the ANN
-  float* q = nullptr;        // [N][dimK] scaled descriptors (mixed-precision path)
-  float* fp = nullptr;       // [N][dimK] dE/dq (mixed-precision path)
-  int* order = nullptr;      // [N] centers sorted by type (mixed-precision path)
-  int* type_counts = nullptr;  // [2 kMaxTypes] type histogram and starts
   double* tune_out = nullptr;  // [13 N] throw-away outputs of the autotuning calls
 };
 
@@ -80,8 +76,8 @@ struct Engine {
   ForceScratch scratch;
   ExplicitRows xr;
   bool use_xr = false;       // neighbour rows with explicit displacements (small box, batch)
-  int precision = 0;         // 0: FP32 SIMT ANN; 1: mixed (ANN on the tensor cores, ann_tc.cu)
-  bool order_valid = false;  // scratch.order holds this system's type order
+  int precision = 0;         // 0: FP32 SIMT ANN; 1 / 2: ANN on the tensor cores, FP16 / BF16
+  unsigned short* d_w16 = nullptr;   // the 16-bit ANN weights of the mixed path
   // host-side bookkeeping
   Box last_box{};
   bool have_box = false;
@@ -89,6 +85,7 @@ struct Engine {
   const void* box_owner = nullptr;   // md whose box the device copy holds (nullptr: none)
   int last_n = -1;
   int group = 4;             // lanes per center in the fused kernel (autotuned)
+  int fused_minb = 3;        // CTAs per SM the small-shape fused kernel is built for (autotuned)
   int filter_group = 8;      // lanes per center in the typewise filter (autotuned)
   int f12_group = 4;         // lanes per center in the angular-force kernel (autotuned)
   int gather_group = 8;      // lanes per center in the gather (autotuned)
@@ -100,6 +97,11 @@ struct Engine {
 // of the shared-memory coefficient tables and of ForceScratch::alpha).
 int basis_stride(const ModelParams& p);
 size_t fused_smem_bytes(const ModelParams& p);
+// The same for the tensor-core (mixed-precision) build; needs the tc_* fields.
+size_t fused_tc_smem_bytes(const ModelParams& p);
+// True when the descriptor kernel comes in two occupancy builds (3 or 4 CTAs
+// per SM, Engine::fused_minb) for this model's shape.
+bool fused_occupancy_variants(const ModelParams& p);
 void set_fused_smem_limits(const ModelParams& p);
 
 // Times each kernel variant on the given system (a few calls each, stream
@@ -151,15 +153,8 @@ void launch_explicit_rows(Engine& e, int N, const double* pos, const int* type,
 void launch_explicit_row_indices(const Engine& e, int which, int n, int* nn, int* nl, int mn,
                                  cudaStream_t stream);
 
-// Mixed-precision path: the tensor-core ANN (ann_tc.cu).
-bool ann_tc_supported(const ModelParams& p, std::string& why);
-size_t ann_tc_smem_bytes(const ModelParams& p);
-void ann_tc_prepare(const ModelParams& p);
-void launch_ann_tc(Engine& e, int N, cudaStream_t stream);
-// Centers sorted by type for the tensor-core tiles; unless `always`, only
-// when the Verlet list is about to be consumed after a rebuild.
-void launch_type_order(Engine& e, int N, bool always, cudaStream_t stream);
-// Switches the ANN precision (0 FP32, 1 mixed); allocates the mixed buffers.
+// Switches the ANN precision (0 FP32, 1 FP16 / 2 BF16 tensor-core ANN inside
+// the descriptor kernel); uploads the 16-bit weights.
 std::string engine_set_precision(Engine& e, int mode);
 
 // Descriptor + ANN + angular partial forces, then the force/virial gather.

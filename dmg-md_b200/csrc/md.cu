@@ -879,10 +879,8 @@ int md_enqueue_run(nepx_md* m, int steps, double dt_fs, int thermo_every, double
   if (e.box_owner != &md) {
     nepx::launch_set_box(e, md.box, s);
     e.box_owner = &md;
-    // the engine served another caller: its Verlet rows and type order
-    // belong to that system
+    // the engine served another caller: its Verlet rows belong to that system
     if (md.forces_valid) nepx::launch_neighbor_update(e, N, md.d_pos, md.d_type, true, s);
-    e.order_valid = false;
   }
   const double tau = p.dt * c.Tdamp;
   if (!fold) {
@@ -894,12 +892,6 @@ int md_enqueue_run(nepx_md* m, int steps, double dt_fs, int thermo_every, double
     if (!e.tuned) nepx::engine_autotune(e, N, md.d_pos, md.d_type, s);
     nepx::launch_force(e, N, md.d_pos, md.d_type, md.d_pe, md.d_force, md.d_virial, false, s);
     md.forces_valid = true;
-  }
-  // a valid type order before the step graph is captured, whose sort then
-  // runs only on rebuild steps
-  if (e.precision == 1 && !md.xr && !e.order_valid) {
-    nepx::launch_type_order(e, N, true, s);
-    e.order_valid = true;
   }
   e.force_rebuild = true;     // a later nepx_compute on this handle rebuilds
   e.have_box = false;
@@ -1093,7 +1085,6 @@ int nepx_md_compute_forces(nepx_md_t* m)
   if (e.box_owner != &md) {
     nepx::launch_set_box(e, md.box, s);
     e.box_owner = &md;
-    e.order_valid = false;
     rebuild = true;
   }
   nepx::launch_neighbor_update(e, N, md.d_pos, md.d_type, rebuild, s);

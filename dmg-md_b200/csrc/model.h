@@ -56,6 +56,14 @@ struct ModelParams {
   const float* q_scaler;
   const float* zbl_para;
   int num_c_radial;
+  // mixed-precision ANN: 16-bit tensor-core operands (set by nepx_set_precision).
+  // The hidden units of all types are stacked, m = t H + h, in chunks of 128.
+  int tc_dimk;                // dim rounded up to 16 (GEMM1's K)
+  int tc_kt;                  // T H rounded up to 128 (GEMM2's K over all chunks)
+  int tc_bf16;                // operand format: 0 FP16, 1 BF16
+  float tc_sw, tc_sg;         // power-of-two scales of W0 and of w1 (1 - x^2)
+  const unsigned short* w0h;  // [T H][tc_dimk] W0 * tc_sw, row m = t H + h
+  const unsigned short* w0th; // [dim][tc_kt] W0^T * tc_sw, column m
 };
 
 }  // namespace nepx

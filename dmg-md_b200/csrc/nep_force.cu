@@ -2,7 +2,8 @@
 //
 // Four kernels per force call, each giving a group of G lanes (G = 4 or 8,
 // chosen by the autotuner in engine.cu) to one center; every phase is local
-// to the group, so no CTA-wide barrier follows the set-up.
+// to the group, so no CTA-wide barrier follows the set-up (except in the
+// tensor-core ANN, whose MMAs span the CTA's centers).
 //
 //  k_filter_radial  one sweep over the center's sorted Verlet row applies the
 //    reference's FP32 typewise predicate (nep.cu:503-561), writes the radial
@@ -19,8 +20,9 @@
 //       the one-hidden-layer ANN (site energy, dE/dq), the moment derivatives
 //       a[n][lm] = dE/ds[n][lm], and the radial force coefficients
 //       alpha[t][k] = sum_n dE/dq_n c(ti,t)[n][k] (stored for the gather).
-//    Mixed precision hands q and s to the tensor-core ANN (ann_tc.cu) and
-//    k_acoef forms a and alpha.  Reference: find_descriptor (nep.cu:569-748).
+//    Mixed precision runs the ANN of the CTA's centers as two tcgen05 MMAs
+//    (16-bit operands, FP32 accumulators in TMEM, tc_ann) in place of the
+//    per-center FP32 contraction.  Reference: find_descriptor (nep.cu:569-748).
 //  k_angular_f12  each directed partial force
 //       f12(i,j) = (sum_lm B_lm Y_lm) r^ + (1/d)(I - r^r^T) sum_lm A_lm dY_lm/dr^
 //    with A_lm = sum_n a[n][lm] g_n and B_lm = sum_n a[n][lm] g'_n: the
@@ -40,15 +42,20 @@
 #include <cstdio>
 #include <mutex>
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 #include "engine.h"
 #include "harmonic_tables.h"
+#include "tcgen05.cuh"
 
 namespace nepx {
 
 namespace {
 
 constexpr int kBlock = 128;      // threads per CTA
-constexpr int kChunkN = 5;       // radial functions per angular-moment sweep
+constexpr int kChunkN = 5;       // radial functions per angular-moment sweep (3 CTAs per SM)
+constexpr int kChunkN4 = 3;      // the same at 4 CTAs per SM (fewer live accumulators)
 constexpr unsigned kFull = 0xffffffffu;
 
 // Weights of the three-body invariants q_L and coefficients of the
@@ -125,7 +132,7 @@ __constant__ int c_inv_start[kMaxInv + 1];
 
 __host__ __device__ constexpr int round4(int x) { return (x + 3) & ~3; }
 
-// Shared-memory layout of k_nep_fused (in floats).
+// Shared-memory layout of k_nep_fused (in floats; the tensor-core region in bytes).
 struct FusedLayout {
   int kpr, kpa;        // basis sizes padded to float4
   int c_rad, c_ang;    // coefficient tables [T*T][n][kp]
@@ -134,22 +141,51 @@ struct FusedLayout {
   int s, a, q, fp, gh; // offsets inside one center's scratch
   int atoms_base;      // offset of the per-center scratch
   int total_bytes;
+  // tensor-core ANN (byte offsets from the start): 16-bit tiles of one chunk
+  // of 128 stacked hidden units, W0 [128][dimk] and W0^T [dim][128], the CTA's
+  // descriptors [APB][dimk] and hidden-layer derivatives [APB][128]; energy
+  // partials [4][APB]; per type, the bit mask of the CTA's centers of that
+  // type [kMaxTypes]; the mbarrier, the TMEM address and a flag
+  int tc_w, tc_wt, tc_q, tc_g, tc_e, tc_type, tc_bar, tc_misc;
 };
 
-// Shared memory one CTA may use with the ANN weights staged (three CTAs per SM).
-constexpr int kFusedSmemBudget = 72 * 1024;
+// Shared memory one CTA may use with the ANN weights staged, when `minb`
+// CTAs share an SM (228 KB per SM, 1 KB of it reserved per CTA).
+__host__ __device__ constexpr int fused_smem_budget(int minb) { return 228 * 1024 / minb - 1024; }
 
 // kp: row stride of the coefficient tables, the padded basis size of the
 // kernel instance (rows are zero-filled up to it, so float4 dot products of
 // the full compile-time width stay inside the row).
+// tc: the layout of the tensor-core ANN build (16-bit tiles first, no FP32
+// weights staged, no per-center hidden-unit scratch).  An MMA reads 128 rows
+// of its A tile: rows past the stacked hidden units (or dim) are read from
+// whatever follows in shared memory and only feed accumulator rows the
+// epilogue never reads, so total_bytes covers the 128-row span of both A tiles.
 __host__ __device__ inline FusedLayout fused_layout(const ModelParams& p, int atoms_per_block,
-                                                   int kp)
+                                                   int kp, int budget, bool tc = false)
 {
   FusedLayout L;
   L.kpr = kp;
   L.kpa = kp;
   const int tt = p.T * p.T;
-  L.c_rad = 0;
+  int base = 0;   // floats before the tables
+  if (tc) {
+    auto up128 = [](int x) { return (x + 127) & ~127; };
+    const int dimk = p.tc_dimk, th = p.T * p.H;
+    const int rows = ((th < 128 ? th : 128) + 7) & ~7;
+    L.tc_w = 0;
+    L.tc_wt = up128(L.tc_w + rows * dimk * 2);
+    L.tc_q = up128(L.tc_wt + ((p.dim + 7) & ~7) * 128 * 2);
+    L.tc_g = up128(L.tc_q + atoms_per_block * dimk * 2);
+    L.tc_e = up128(L.tc_g + atoms_per_block * 128 * 2);
+    L.tc_type = L.tc_e + 4 * atoms_per_block * 4;
+    L.tc_bar = (L.tc_type + kMaxTypes * 4 + 7) & ~7;
+    L.tc_misc = L.tc_bar + 8;
+    base = up128(L.tc_misc + 16) / 4;
+  } else {
+    L.tc_w = L.tc_wt = L.tc_q = L.tc_g = L.tc_e = L.tc_type = L.tc_bar = L.tc_misc = -1;
+  }
+  L.c_rad = base;
   L.c_ang = L.c_rad + tt * p.nR * L.kpr;
   L.s = 0;
   L.a = p.nA * p.nlm;
@@ -159,17 +195,23 @@ __host__ __device__ inline FusedLayout fused_layout(const ModelParams& p, int at
   // per-center stride: 16-byte aligned (float4 reads of the a[n][lm] rows)
   // and an odd number of 16-byte units, so float4 rows of neighbouring
   // centers start on different banks
-  L.per_atom = round4(L.gh + p.H);
+  L.per_atom = round4(L.gh + (tc ? 0 : p.H));
   if ((L.per_atom / 4) % 2 == 0) L.per_atom += 4;
   const int tables = round4(L.c_ang + tt * p.nA * L.kpa);
   const int wsize = p.T * p.dim * p.H4;
   L.wt = tables;
   L.atoms_base = tables + wsize;
   L.total_bytes = 4 * (L.atoms_base + atoms_per_block * L.per_atom);
-  if (L.total_bytes > kFusedSmemBudget) {   // weights stay in global memory
+  if (tc || L.total_bytes > budget) {   // weights stay in global memory
     L.wt = -1;
     L.atoms_base = tables;
     L.total_bytes = 4 * (L.atoms_base + atoms_per_block * L.per_atom);
+  }
+  if (tc) {
+    const int need_w = L.tc_w + 128 * p.tc_dimk * 2, need_wt = L.tc_wt + 128 * 128 * 2;
+    L.total_bytes = (L.total_bytes > need_w ? L.total_bytes : need_w);
+    L.total_bytes = (L.total_bytes > need_wt ? L.total_bytes : need_wt);
+    L.total_bytes = (L.total_bytes + 15) & ~15;
   }
   return L;
 }
@@ -305,6 +347,234 @@ __device__ __forceinline__ void center_acoef(const ModelParams& p, const float* 
         }
       }
     }
+  }
+}
+
+// tanh of the mixed-precision ANN: the hardware approximation (PTX
+// tanh.approx.f32, relative error about 2^-11, the size of an FP16 operand's
+// rounding).
+__device__ __forceinline__ float tanh_fast(float x)
+{
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// One FP32 value as a 16-bit MMA operand (FP16 or BF16, round to nearest).
+__device__ __forceinline__ void store16(unsigned char* at, float v, bool bf16)
+{
+  *reinterpret_cast<unsigned short*>(at) =
+    bf16 ? __bfloat16_as_ushort(__float2bfloat16_rn(v)) : __half_as_ushort(__float2half_rn(v));
+}
+
+// One chunk of the stacked weights into the tiles (16-byte rows of core
+// matrices): rows m = 128 k .. of W0 (stacked m = t H + h) and columns
+// 128 k .. of W0^T.
+__device__ __forceinline__ void tc_stage_chunk(const ModelParams& p, const FusedLayout& Lay,
+                                               unsigned char* smb, int k)
+{
+  const int dimk = p.tc_dimk, th = p.T * p.H, m0 = 128 * k;
+  const int rows = th - m0 < 128 ? th - m0 : 128;
+  const int cw = dimk / 8;
+  const uint4* w = reinterpret_cast<const uint4*>(p.w0h + static_cast<size_t>(m0) * dimk);
+  for (int e = threadIdx.x; e < rows * cw; e += kBlock)
+    *reinterpret_cast<uint4*>(smb + Lay.tc_w + tc::off16(e / cw, 8 * (e % cw), dimk)) =
+      __ldg(w + e);
+  for (int e = threadIdx.x; e < p.dim * 16; e += kBlock) {
+    const int d = e / 16, c = e % 16;
+    *reinterpret_cast<uint4*>(smb + Lay.tc_wt + tc::off16(d, 8 * c, 128)) =
+      __ldg(reinterpret_cast<const uint4*>(p.w0th + static_cast<size_t>(d) * p.tc_kt + m0 +
+                                           8 * c));
+  }
+}
+
+// Tensor-core set-up of a CTA of the mixed-precision descriptor kernel (before
+// its first barrier): TMEM for the two accumulators, the mbarrier, flags, and
+// with a single chunk of stacked hidden units the weight tiles.
+template <int APB>
+__device__ __forceinline__ void tc_ann_setup(const ModelParams& p, const FusedLayout& Lay,
+                                             unsigned char* smb)
+{
+  constexpr int kCols = 2 * APB < 32 ? 32 : 2 * APB;   // D1 | D2, APB columns each
+  uint32_t* misc = reinterpret_cast<uint32_t*>(smb + Lay.tc_misc);
+  if (threadIdx.x < 32) tc::tmem_alloc(misc + 2, kCols);
+  if (threadIdx.x == 0) {
+    tc::mbar_init(tc::smem_u32(smb + Lay.tc_bar));
+    misc[0] = 0u;   // largest |q| of the CTA (float bits)
+  }
+  unsigned* tmask = reinterpret_cast<unsigned*>(smb + Lay.tc_type);
+  if (threadIdx.x < kMaxTypes) tmask[threadIdx.x] = 0u;   // centers of each type
+  if (p.tc_kt == 128) {
+    tc_stage_chunk(p, Lay, smb, 0);
+    tc::fence_async_smem();
+  }
+}
+
+// The per-atom ANN of all APB centers of the CTA on the tensor cores (whole
+// CTA; s_q of every center holds its scaled descriptors).  The hidden units
+// of all types are stacked, m = t H + h, and run in chunks of 128:
+//   GEMM1 (M = 128 stacked units, N = APB centers, K = dim):
+//     Z = W0 Q^T, from the 16-bit tiles of W0 * sw and Q * sq;
+//   epilogue (thread = unit m = its TMEM lane, t = m / H): for the centers of
+//     type t, x = tanh(z / (sw sq) - b0) (hardware tanh), E += w1 x,
+//     G = w1 (1 - x^2) * sg (zero for the other centers);
+//   GEMM2 (M = dim, N = APB, K = the chunk's 128 units): dE/dq += W0^T G^T,
+//     accumulated over the chunks in TMEM.
+// sw, sg are the model's power-of-two scales (nepx_set_precision), sq the
+// CTA's (largest |q| to 2^14): in FP16 every operand keeps its 11-bit
+// significand; unscaling by powers of two is exact.  Then each center's
+// dE/dq (times q_scaler) lands in its s_fp and its site energy in pe_ann.
+// Every wait is bounded: a timeout sets ann_error, waits (bounded again) for
+// the MMAs in flight and lets the CTA finish with the error flagged.
+template <int APB, int G>
+__device__ void tc_ann(const ModelParams& p, const FusedLayout& Lay, float* sm, int slot,
+                       int gl, bool active, int t1, int i, const float* s_q,
+                       double* __restrict__ pe_ann, NeighborState* st)
+{
+  constexpr int kCols = 2 * APB < 32 ? 32 : 2 * APB;
+  unsigned char* smb = reinterpret_cast<unsigned char*>(sm);
+  unsigned char* Wt = smb + Lay.tc_w;
+  unsigned char* Vt = smb + Lay.tc_wt;
+  unsigned char* Qt = smb + Lay.tc_q;
+  unsigned char* Gt = smb + Lay.tc_g;
+  float* s_e = reinterpret_cast<float*>(smb + Lay.tc_e);
+  unsigned* s_tmask = reinterpret_cast<unsigned*>(smb + Lay.tc_type);
+  uint32_t* misc = reinterpret_cast<uint32_t*>(smb + Lay.tc_misc);
+  const uint32_t bar = tc::smem_u32(smb + Lay.tc_bar);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int H = p.H, dim = p.dim, dimk = p.tc_dimk, th = p.T * H;
+  const int chunks = p.tc_kt / 128;
+  const bool bf16 = p.tc_bf16 != 0;
+
+  // the CTA's largest |q| and the center types
+  float qm = 0.0f;
+  if (active)
+    for (int d = gl; d < dim; d += G) qm = fmaxf(qm, fabsf(s_q[d]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) qm = fmaxf(qm, __shfl_xor_sync(kFull, qm, o));
+  if (lane == 0) atomicMax(reinterpret_cast<int*>(misc), __float_as_int(qm));
+  if (gl == 0 && active) atomicOr(s_tmask + t1, 1u << slot);
+  __syncthreads();
+  const float qmax = __int_as_float(static_cast<int>(misc[0]));
+  int ex = 0;
+  frexpf(qmax, &ex);
+  const float sq = qmax > 0.0f ? ldexpf(1.0f, max(-60, min(60, 14 - ex))) : 1.0f;
+  // this center's row of the descriptor tile, zero past dim and for idle slots
+  for (int d = gl; d < dimk; d += G)
+    store16(Qt + tc::off16(slot, d, dimk), (active && d < dim) ? s_q[d] * sq : 0.0f, bf16);
+  tc::fence_async_smem();
+  const uint32_t tmem = misc[2];
+  const uint32_t lane_addr = tmem + (static_cast<uint32_t>(warp * 32) << 16);
+  const uint32_t id = tc::idesc_f16(128, APB, bf16);
+  const float unscale1 = 1.0f / (sq * p.tc_sw), unscale2 = 1.0f / (p.tc_sw * p.tc_sg);
+  float e_acc[APB];
+#pragma unroll
+  for (int c = 0; c < APB; ++c) e_acc[c] = 0.0f;
+  uint32_t phase = 0;
+  bool failed = false;
+  for (int k = 0; k < chunks; ++k) {
+    if (chunks > 1) {
+      // the previous chunk's MMAs are complete: its tiles may be overwritten
+      tc_stage_chunk(p, Lay, smb, k);
+      tc::fence_async_smem();
+    }
+    tc::before_sync();
+    __syncthreads();
+    tc::after_sync();
+    if (tid == 0) {
+      for (int s = 0; s < dimk / 16; ++s) {
+        const uint64_t a = tc::smem_desc(tc::smem_u32(Wt + tc::off16(0, 16 * s, dimk)), dimk);
+        const uint64_t b = tc::smem_desc(tc::smem_u32(Qt + tc::off16(0, 16 * s, dimk)), dimk);
+        tc::mma_f16(tmem, a, b, id, s > 0 ? 1u : 0u);
+      }
+      tc::mma_commit(bar);
+    }
+    bool ok = tc::mbar_wait(bar, phase);
+    phase ^= 1u;
+    if (__syncthreads_or(!ok)) {
+      failed = true;
+      break;
+    }
+    tc::after_sync();
+    const int m = 128 * k + tid;
+    const bool unit = m < th;
+    const unsigned mine = unit ? s_tmask[m / H] : 0u;   // the centers of this unit's type
+    const float b0m = unit ? __ldg(p.b0 + m) : 0.0f;   // b0 and w1 are [T][H]: index m
+    const float w1m = unit ? __ldg(p.w1 + m) : 0.0f;
+#pragma unroll
+    for (int c0 = 0; c0 < APB; c0 += 16) {
+      float z[16];
+      tc::tmem_ld16(lane_addr + c0, z);
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const int c = c0 + q;
+        float g = 0.0f;
+        if ((mine >> c) & 1u) {
+          const float x = tanh_fast(z[q] * unscale1 - b0m);
+          e_acc[c] += w1m * x;
+          g = w1m * (1.0f - x * x) * p.tc_sg;
+        }
+        store16(Gt + tc::off16(c, tid, 128), g, bf16);
+      }
+    }
+    tc::fence_async_smem();
+    tc::before_sync();
+    __syncthreads();   // G complete, D1 read
+    tc::after_sync();
+    if (tid == 0) {
+      for (int s = 0; s < 128 / 16; ++s) {
+        const uint64_t a = tc::smem_desc(tc::smem_u32(Vt + tc::off16(0, 16 * s, 128)), 128);
+        const uint64_t b = tc::smem_desc(tc::smem_u32(Gt + tc::off16(0, 16 * s, 128)), 128);
+        tc::mma_f16(tmem + APB, a, b, id, (k > 0 || s > 0) ? 1u : 0u);
+      }
+      tc::mma_commit(bar);
+    }
+    ok = tc::mbar_wait(bar, phase);
+    phase ^= 1u;
+    if (__syncthreads_or(!ok)) {
+      failed = true;
+      break;
+    }
+    tc::after_sync();
+  }
+  if (!failed) {
+    // dE/dq: descriptor component d = this thread's TMEM lane, every center
+    const int d = tid;
+    const float qs = d < dim ? __ldg(p.q_scaler + d) : 0.0f;
+#pragma unroll
+    for (int c0 = 0; c0 < APB; c0 += 16) {
+      float f[16];
+      tc::tmem_ld16(lane_addr + APB + c0, f);
+      if (d < dim)
+#pragma unroll
+        for (int q = 0; q < 16; ++q)
+          sm[Lay.atoms_base + (c0 + q) * Lay.per_atom + Lay.fp + d] = f[q] * unscale2 * qs;
+    }
+  }
+  // site energies: each warp's partial sums over its 32 hidden units, lane c
+  // ends with center c's (fixed order), then the four warps in order
+  if constexpr (APB == 16) {
+#pragma unroll
+    for (int c = 0; c < 16; ++c) e_acc[c] += __shfl_xor_sync(kFull, e_acc[c], 16);
+  }
+  int at = 0;
+  if constexpr (APB == 32) rs_step<32, 16>(e_acc, lane, at);
+  rs_step<16, 8>(e_acc, lane, at);
+  rs_step<8, 4>(e_acc, lane, at);
+  rs_step<4, 2>(e_acc, lane, at);
+  rs_step<2, 1>(e_acc, lane, at);
+  if (lane < APB) s_e[warp * APB + at] = e_acc[0];
+  if (failed) {
+    if (tid == 0) atomicOr(&st->ann_error, 1);
+    tc::mbar_wait(bar, phase ^ 1u);   // the MMAs of the phase that timed out
+  }
+  tc::before_sync();
+  __syncthreads();
+  tc::after_sync();
+  if (warp == 0) tc::tmem_dealloc(misc[2], kCols);
+  if (active && gl == 0) {
+    const float e = s_e[slot] + s_e[APB + slot] + s_e[2 * APB + slot] + s_e[3 * APB + slot];
+    pe_ann[i] = static_cast<double>(e - __ldg(p.out_bias + t1));
   }
 }
 
@@ -454,31 +724,36 @@ k_filter_radial(const ModelParams p, int N, const Box* __restrict__ box,
 }
 
 // NRM/KM/NAM: compile-time bounds of nR, basis size + 1, nA for this instance.
-// The small-shape instance is held to 168 registers (three CTAs per SM): the
-// kernel is latency bound and the extra warps outweigh a few spilled words.
+// MINB: CTAs per SM the instance is built for (register cap 65536 / (128
+// MINB)).  The small shape comes at 3 (168 registers, moments of five radial
+// functions per sweep) and at 4 (128 registers, three per sweep: the angular
+// row is swept twice but a third more warps hide the latency); the
+// autotuner picks one.
 // XR: explicit rows (small-box and batched paths) -- the radial and angular
 // rows hold the displacement and packed neighbour of every edge (er, ea),
 // built beforehand; phase 1 then only accumulates the radial descriptors.
 // LMAX: 4 (moments of 24 components per n, five n per sweep) or 8 (80
 // components, one n per sweep).
-template <int G, int NRM, int KM, int NAM, bool XR, int LMAX>
-__global__ void __launch_bounds__(kBlock, (KM <= 9 ? 3 : 2))
+// TC: the ANN of the CTA's centers runs on the tensor cores (tc_ann, the
+// mixed-precision path); otherwise in FP32 per center.
+template <int G, int NRM, int KM, int NAM, bool XR, int LMAX, int MINB, bool TC>
+__global__ void __launch_bounds__(kBlock, MINB)
 k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
             const Site* __restrict__ sites, NeighborState* st,
             const int* __restrict__ nn_v, const int* __restrict__ nl_v, int mn_v,
             int* __restrict__ nn_r, int* __restrict__ nl_r, int mn_r, int* __restrict__ nn_a,
             int* __restrict__ nl_a, int mn_a, const float4* __restrict__ er,
             const float4* __restrict__ ea, const float* __restrict__ qrad,
-            float* __restrict__ alpha, float* __restrict__ acoef, double* __restrict__ pe_ann,
-            float* __restrict__ qout)
+            float* __restrict__ alpha, float* __restrict__ acoef, double* __restrict__ pe_ann)
 {
   constexpr int APW = 32 / G;             // centers per warp
   constexpr int APB = kBlock / G;         // centers per block
   constexpr int KP = (KM + 3) & ~3;
   constexpr int NLM = num_lm<LMAX>();
-  constexpr int CN = LMAX <= 4 ? kChunkN : 1;   // radial functions per moment sweep
-  extern __shared__ float sm[];
-  const FusedLayout Lay = fused_layout(p, APB, KP);
+  // radial functions per moment sweep
+  constexpr int CN = LMAX <= 4 ? (MINB >= 4 ? kChunkN4 : kChunkN) : 1;
+  extern __shared__ __align__(128) float sm[];
+  const FusedLayout Lay = fused_layout(p, APB, KP, fused_smem_budget(MINB), TC);
   const int tid = threadIdx.x;
   const int T = p.T, nR = p.nR, nA = p.nA, kR = p.kR, kA = p.kA;
   const int dim = p.dim, H = p.H;
@@ -497,7 +772,12 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
     for (int k = tid; k < T * dim * p.H4 / 4; k += kBlock) dst[k] = __ldg(src + k);
   }
   if (blockIdx.x == 0 && tid == 0) st->rebuild = 0;   // the Verlet list is consumed
+  if constexpr (TC) {
+    tc_ann_setup<APB>(p, Lay, reinterpret_cast<unsigned char*>(sm));
+    tc::before_sync();
+  }
   __syncthreads();
+  if constexpr (TC) tc::after_sync();
 
   const int lane = tid & 31, warp = tid >> 5;
   const int group = lane / G, gl = lane % G;
@@ -650,101 +930,94 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
   // scaled descriptors; hidden-unit derivatives zero-padded to H4 for the
   // float4 dot products
   for (int d = gl; d < dim; d += G) s_q[d] *= __ldg(p.q_scaler + d);
-  for (int h = H + gl; h < p.H4; h += G) s_gh[h] = 0.0f;
-  const float* w0t = Lay.wt >= 0 ? sm + Lay.wt : p.w0t;
-  __syncwarp();
-  if (qout) {
-    // mixed-precision path: the ANN runs on the tensor cores (ann_tc.cu); hand
-    // over the scaled descriptors (zero-padded to dimK) and the moments
+  if constexpr (TC) {
+    __syncwarp();
+    tc_ann<APB, G>(p, Lay, sm, slot, gl, active, t1, i, s_q, pe_ann, st);
+  } else {
+    for (int h = H + gl; h < p.H4; h += G) s_gh[h] = 0.0f;
+    __syncwarp();
+    const float* w0t = Lay.wt >= 0 ? sm + Lay.wt : p.w0t;
+    float e_part = 0.0f;
     if (active) {
-      float* qrow = qout + static_cast<size_t>(i) * p.dimK;
-      for (int d = gl; d < p.dimK; d += G) qrow[d] = d < dim ? s_q[d] : 0.0f;
-      float4* dst = reinterpret_cast<float4*>(acoef + static_cast<size_t>(i) * nA * NLM);
-      const float4* src = reinterpret_cast<const float4*>(s_s);
-      for (int q = gl; q < nA * NLM / 4; q += G) dst[q] = src[q];
-    }
-    return;
-  }
-  float e_part = 0.0f;
-  if (active) {
-    // hidden layer: each lane owns two groups of four consecutive hidden units
-    // (float4 rows of the transposed w0; eight independent FMA chains in one
-    // pass, each sequential in d as in the reference)
-    const int hq = p.H4 / 4;
-    const float4* wt =
-      reinterpret_cast<const float4*>(w0t + static_cast<size_t>(t1) * dim * p.H4);
-    auto finish = [&](int h, float z) {
-      if (h < H) {
-        const float x1 = tanhf(z - __ldg(p.b0 + t1 * H + h));
-        const float w1 = __ldg(p.w1 + t1 * H + h);
-        e_part += w1 * x1;
-        s_gh[h] = w1 * (1.0f - x1 * x1);
-      }
-    };
-    for (int h4 = gl; h4 < hq; h4 += 2 * G) {
-      const bool has_b = h4 + G < hq;
-      const int h4b = has_b ? h4 + G : h4;   // past the end: computed, dropped
-      float z0 = 0.0f, z1 = 0.0f, z2 = 0.0f, z3 = 0.0f;
-      float z4 = 0.0f, z5 = 0.0f, z6 = 0.0f, z7 = 0.0f;
+      // hidden layer: each lane owns two groups of four consecutive hidden units
+      // (float4 rows of the transposed w0; eight independent FMA chains in one
+      // pass, each sequential in d as in the reference)
+      const int hq = p.H4 / 4;
+      const float4* wt =
+        reinterpret_cast<const float4*>(w0t + static_cast<size_t>(t1) * dim * p.H4);
+      auto finish = [&](int h, float z) {
+        if (h < H) {
+          const float x1 = tanhf(z - __ldg(p.b0 + t1 * H + h));
+          const float w1 = __ldg(p.w1 + t1 * H + h);
+          e_part += w1 * x1;
+          s_gh[h] = w1 * (1.0f - x1 * x1);
+        }
+      };
+      for (int h4 = gl; h4 < hq; h4 += 2 * G) {
+        const bool has_b = h4 + G < hq;
+        const int h4b = has_b ? h4 + G : h4;   // past the end: computed, dropped
+        float z0 = 0.0f, z1 = 0.0f, z2 = 0.0f, z3 = 0.0f;
+        float z4 = 0.0f, z5 = 0.0f, z6 = 0.0f, z7 = 0.0f;
 #pragma unroll 2
-      for (int d = 0; d < dim; ++d) {
-        const float q = s_q[d];
-        const float4 wa = wt[d * hq + h4];
-        const float4 wb = wt[d * hq + h4b];
-        z0 = fmaf(wa.x, q, z0);
-        z1 = fmaf(wa.y, q, z1);
-        z2 = fmaf(wa.z, q, z2);
-        z3 = fmaf(wa.w, q, z3);
-        z4 = fmaf(wb.x, q, z4);
-        z5 = fmaf(wb.y, q, z5);
-        z6 = fmaf(wb.z, q, z6);
-        z7 = fmaf(wb.w, q, z7);
-      }
-      finish(4 * h4, z0);
-      finish(4 * h4 + 1, z1);
-      finish(4 * h4 + 2, z2);
-      finish(4 * h4 + 3, z3);
-      if (has_b) {
-        finish(4 * h4b, z4);
-        finish(4 * h4b + 1, z5);
-        finish(4 * h4b + 2, z6);
-        finish(4 * h4b + 3, z7);
-      }
-    }
-  }
-  e_part = group_sum<G>(e_part);
-  if (active && gl == 0) pe_ann[i] = static_cast<double>(e_part - __ldg(p.out_bias + t1));
-  __syncwarp();
-  if (active) {
-    // dE/dq: four descriptor components per lane at once (d0, d0 + G,
-    // d0 + 2G, d0 + 3G), float4 over h, each sum in the same order as before
-    const int hq = p.H4 / 4;
-    const float4* g4 = reinterpret_cast<const float4*>(s_gh);
-    const float4* wt =
-      reinterpret_cast<const float4*>(w0t + static_cast<size_t>(t1) * dim * p.H4);
-    for (int d0 = gl; d0 < dim; d0 += 4 * G) {
-      int dd[4];
-#pragma unroll
-      for (int k = 0; k < 4; ++k) dd[k] = min(d0 + k * G, dim - 1);   // past dim: dropped
-      float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-#pragma unroll 2
-      for (int h = 0; h < hq; ++h) {
-        const float4 g = g4[h];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const float4 w = wt[dd[k] * hq + h];
-          acc[k] = fmaf(g.x, w.x, acc[k]);
-          acc[k] = fmaf(g.y, w.y, acc[k]);
-          acc[k] = fmaf(g.z, w.z, acc[k]);
-          acc[k] = fmaf(g.w, w.w, acc[k]);
+        for (int d = 0; d < dim; ++d) {
+          const float q = s_q[d];
+          const float4 wa = wt[d * hq + h4];
+          const float4 wb = wt[d * hq + h4b];
+          z0 = fmaf(wa.x, q, z0);
+          z1 = fmaf(wa.y, q, z1);
+          z2 = fmaf(wa.z, q, z2);
+          z3 = fmaf(wa.w, q, z3);
+          z4 = fmaf(wb.x, q, z4);
+          z5 = fmaf(wb.y, q, z5);
+          z6 = fmaf(wb.z, q, z6);
+          z7 = fmaf(wb.w, q, z7);
+        }
+        finish(4 * h4, z0);
+        finish(4 * h4 + 1, z1);
+        finish(4 * h4 + 2, z2);
+        finish(4 * h4 + 3, z3);
+        if (has_b) {
+          finish(4 * h4b, z4);
+          finish(4 * h4b + 1, z5);
+          finish(4 * h4b + 2, z6);
+          finish(4 * h4b + 3, z7);
         }
       }
-#pragma unroll
-      for (int k = 0; k < 4; ++k)
-        if (d0 + k * G < dim) s_fp[d0 + k * G] = acc[k] * __ldg(p.q_scaler + d0 + k * G);
     }
+    e_part = group_sum<G>(e_part);
+    if (active && gl == 0) pe_ann[i] = static_cast<double>(e_part - __ldg(p.out_bias + t1));
+    __syncwarp();
+    if (active) {
+      // dE/dq: four descriptor components per lane at once (d0, d0 + G,
+      // d0 + 2G, d0 + 3G), float4 over h, each sum in the same order as before
+      const int hq = p.H4 / 4;
+      const float4* g4 = reinterpret_cast<const float4*>(s_gh);
+      const float4* wt =
+        reinterpret_cast<const float4*>(w0t + static_cast<size_t>(t1) * dim * p.H4);
+      for (int d0 = gl; d0 < dim; d0 += 4 * G) {
+        int dd[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) dd[k] = min(d0 + k * G, dim - 1);   // past dim: dropped
+        float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll 2
+        for (int h = 0; h < hq; ++h) {
+          const float4 g = g4[h];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const float4 w = wt[dd[k] * hq + h];
+            acc[k] = fmaf(g.x, w.x, acc[k]);
+            acc[k] = fmaf(g.y, w.y, acc[k]);
+            acc[k] = fmaf(g.z, w.z, acc[k]);
+            acc[k] = fmaf(g.w, w.w, acc[k]);
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          if (d0 + k * G < dim) s_fp[d0 + k * G] = acc[k] * __ldg(p.q_scaler + d0 + k * G);
+      }
+    }
+    __syncwarp();
   }
-  __syncwarp();
   if (active) center_alpha<G>(p, t1, s_fp, sm + Lay.c_rad, Lay.kpr, gl,
                               alpha + static_cast<size_t>(i) * T * Lay.kpr);
   center_acoef<G, NLM>(p, s_s, s_a, s_fp, gl);
@@ -756,47 +1029,6 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
     const float4* src = reinterpret_cast<const float4*>(s_a);
     for (int q = gl; q < nA * NLM / 4; q += G) dst[q] = src[q];
   }
-}
-
-// Mixed-precision path: moment derivatives and radial force coefficients of
-// every center from its moments (left in acoef by k_nep_fused) and dE/dq of
-// the tensor-core ANN (fp, ann_tc.cu) -- the tail of k_nep_fused.
-template <int G, int KP, int LMAX>
-__global__ void __launch_bounds__(kBlock)
-k_acoef(const ModelParams p, int N, const Site* __restrict__ sites, const float* __restrict__ fp,
-        float* __restrict__ acoef, float* __restrict__ alpha)
-{
-  extern __shared__ float sm[];
-  const int T = p.T, nR = p.nR, kR = p.kR, nA = p.nA;
-  const int tab = round4(T * T * nR * KP);
-  for (int k = threadIdx.x; k < T * T * nR * KP; k += kBlock) {
-    const int kk = k % KP, row = k / KP;
-    sm[k] = kk < kR ? __ldg(p.c_pair + row * kR + kk) : 0.0f;
-  }
-  __syncthreads();
-  constexpr int APB = kBlock / G;
-  constexpr int NLM = num_lm<LMAX>();
-  const int per = round4(2 * nA * NLM + p.dimK);
-  const int gl = threadIdx.x % G, slot = threadIdx.x / G;
-  const int i = blockIdx.x * APB + slot;
-  const bool active = i < N;
-  float* s_s = sm + tab + slot * per;
-  float* s_a = s_s + nA * NLM;
-  float* s_fp = s_a + nA * NLM;
-  float4* arow = reinterpret_cast<float4*>(acoef + static_cast<size_t>(i) * nA * NLM);
-  if (active) {
-    for (int q = gl; q < nA * NLM / 4; q += G) reinterpret_cast<float4*>(s_s)[q] = arow[q];
-    for (int d = gl; d < p.dimK; d += G) s_fp[d] = fp[static_cast<size_t>(i) * p.dimK + d];
-  }
-  __syncwarp();
-  if (active) {
-    const int t1 = static_cast<int>(sites[i].type);
-    center_alpha<G>(p, t1, s_fp, sm, KP, gl, alpha + static_cast<size_t>(i) * T * KP);
-    center_acoef<G, NLM>(p, s_s, s_a, s_fp, gl);
-  }
-  __syncwarp();
-  if (active)
-    for (int q = gl; q < nA * NLM / 4; q += G) arow[q] = reinterpret_cast<const float4*>(s_a)[q];
 }
 
 // Directed angular partial force of a center on one neighbour at
@@ -1202,17 +1434,18 @@ bool small_shape(const ModelParams& p)
          p.kA <= kSmallK;
 }
 
-template <int G, int NRM, int KM, int NAM, bool XR, int LMAX>
+template <int G, int NRM, int KM, int NAM, bool XR, int LMAX, int MINB, bool TC>
 void launch_fused_t(Engine& e, int N, cudaStream_t s)
 {
   NeighborBuffers& nb = e.nbr;
   constexpr int APB = kBlock / G;
   const int blocks = (N + APB - 1) / APB;
-  const size_t smem = fused_layout(e.params, APB, (KM + 3) & ~3).total_bytes;
-  k_nep_fused<G, NRM, KM, NAM, XR, LMAX><<<blocks, kBlock, smem, s>>>(
+  const size_t smem =
+    fused_layout(e.params, APB, (KM + 3) & ~3, fused_smem_budget(MINB), TC).total_bytes;
+  k_nep_fused<G, NRM, KM, NAM, XR, LMAX, MINB, TC><<<blocks, kBlock, smem, s>>>(
     e.params, N, e.d_box, e.scratch.sites, e.d_nstate, nb.nn_v, nb.nl_v, nb.mn_v, nb.nn_r, nb.nl_r,
     nb.mn_r, nb.nn_a, nb.nl_a, nb.mn_a, e.xr.er, e.xr.ea, e.scratch.qrad, e.scratch.alpha,
-    e.scratch.acoef, e.scratch.pe_ann, e.precision == 1 ? e.scratch.q : nullptr);
+    e.scratch.acoef, e.scratch.pe_ann);
 }
 
 template <int G, int NRM, int KM>
@@ -1236,23 +1469,6 @@ void launch_filter_t(Engine& e, int N, cudaStream_t s)
   }
 }
 
-template <int G, int KP, int LMAX>
-size_t acoef_smem_bytes(const ModelParams& p)
-{
-  return sizeof(float) * (round4(p.T * p.T * p.nR * KP) +
-                          (kBlock / G) * round4(2 * p.nA * num_lm<LMAX>() + p.dimK));
-}
-
-template <int G, int KP, int LMAX>
-void launch_acoef_t(Engine& e, int N, cudaStream_t s)
-{
-  constexpr int APB = kBlock / G;
-  const ModelParams& p = e.params;
-  const size_t smem = acoef_smem_bytes<G, KP, LMAX>(p);
-  k_acoef<G, KP, LMAX><<<(N + APB - 1) / APB, kBlock, smem, s>>>(
-    p, N, e.scratch.sites, e.scratch.fp, e.scratch.acoef, e.scratch.alpha);
-}
-
 template <int G, int KM, int NAM, int LMAX>
 void launch_f12_t(Engine& e, int N, cudaStream_t s)
 {
@@ -1271,13 +1487,15 @@ void launch_f12_t(Engine& e, int N, cudaStream_t s)
       e.scratch.acoef, e.scratch.f12);
 }
 
-template <int G, int NRM, int KM, int NAM, int LMAX>
-void set_fused_smem_t(size_t bytes)
+template <int G, int NRM, int KM, int NAM, int LMAX, int MINB, bool TC>
+void set_fused_smem_t(const ModelParams& p)
 {
-  cudaFuncSetAttribute(k_nep_fused<G, NRM, KM, NAM, false, LMAX>,
-                       cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
-  cudaFuncSetAttribute(k_nep_fused<G, NRM, KM, NAM, true, LMAX>,
-                       cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+  const int bytes =
+    fused_layout(p, kBlock / G, (KM + 3) & ~3, fused_smem_budget(MINB), TC).total_bytes;
+  cudaFuncSetAttribute(k_nep_fused<G, NRM, KM, NAM, false, LMAX, MINB, TC>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(k_nep_fused<G, NRM, KM, NAM, true, LMAX, MINB, TC>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
 template <int G, int KM, int NAM, bool XR, int LMAX>
@@ -1296,11 +1514,31 @@ void launch_gather_t(Engine& e, int N, double* pe, double* force, double* virial
     force, virial, accumulate ? 1 : 0, e.d_nstate);
 }
 
-template <int G, int NRM, int KM, int NAM, int LMAX>
+// the FP32 build or, for the mixed precisions, the tensor-core one
+template <int G, int NRM, int KM, int NAM, int LMAX, int MINB>
 void launch_fused_g(Engine& e, int N, cudaStream_t s)
 {
-  if (e.use_xr) launch_fused_t<G, NRM, KM, NAM, true, LMAX>(e, N, s);
-  else launch_fused_t<G, NRM, KM, NAM, false, LMAX>(e, N, s);
+  const bool tc = e.precision != 0;
+  if (e.use_xr) {
+    if (tc) launch_fused_t<G, NRM, KM, NAM, true, LMAX, MINB, true>(e, N, s);
+    else launch_fused_t<G, NRM, KM, NAM, true, LMAX, MINB, false>(e, N, s);
+  } else {
+    if (tc) launch_fused_t<G, NRM, KM, NAM, false, LMAX, MINB, true>(e, N, s);
+    else launch_fused_t<G, NRM, KM, NAM, false, LMAX, MINB, false>(e, N, s);
+  }
+}
+
+// the small shape at 3 or 4 CTAs per SM (Engine::fused_minb, autotuned; the
+// tensor-core build comes at 3)
+template <int G>
+void launch_fused_small(Engine& e, int N, cudaStream_t s)
+{
+  if (e.fused_minb == 4 && e.precision == 0) {
+    if (e.use_xr) launch_fused_t<G, kSmallN, kSmallK, kSmallN, true, 4, 4, false>(e, N, s);
+    else launch_fused_t<G, kSmallN, kSmallK, kSmallN, false, 4, 4, false>(e, N, s);
+  } else {
+    launch_fused_g<G, kSmallN, kSmallK, kSmallN, 4, 3>(e, N, s);
+  }
 }
 
 template <int G, int KM, int NAM, int LMAX>
@@ -1318,36 +1556,55 @@ void launch_gather_g(Engine& e, int N, double* pe, double* force, double* virial
 // Padded basis width (row stride of the coefficient tables and of alpha).
 int basis_stride(const ModelParams& p) { return small_shape(p) ? round4(kSmallK) : round4(kMaxBasis); }
 
+bool fused_occupancy_variants(const ModelParams& p) { return small_shape(p); }
+
 // Largest dynamic shared memory a descriptor-kernel variant this model runs needs.
 size_t fused_smem_bytes(const ModelParams& p)
 {
-  if (high_degree(p)) return fused_layout(p, kBlock / kHighFusedGroup, basis_stride(p)).total_bytes;
-  return fused_layout(p, kBlock / 4, basis_stride(p)).total_bytes;
+  if (high_degree(p))
+    return fused_layout(p, kBlock / kHighFusedGroup, basis_stride(p), fused_smem_budget(2))
+      .total_bytes;
+  return fused_layout(p, kBlock / 4, basis_stride(p), fused_smem_budget(small_shape(p) ? 3 : 2))
+    .total_bytes;
 }
 
 void set_fused_smem_limits(const ModelParams& p)
 {
-  constexpr int KS = round4(kSmallK), KG = round4(kMaxBasis);
+  // the tensor-core builds' layout needs the 16-bit tile sizes of the current
+  // precision (set before this is called again by nepx_set_precision)
+  const bool tc = p.tc_dimk > 0;
   if (high_degree(p)) {
-    cudaFuncSetAttribute(k_acoef<kHighFusedGroup, KG, 8>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         static_cast<int>(acoef_smem_bytes<kHighFusedGroup, KG, 8>(p)));
-    set_fused_smem_t<kHighFusedGroup, kMaxN, kMaxBasis, kMaxN, 8>(fused_smem_bytes(p));
+    set_fused_smem_t<kHighFusedGroup, kMaxN, kMaxBasis, kMaxN, 8, 2, false>(p);
+    if (tc) set_fused_smem_t<kHighFusedGroup, kMaxN, kMaxBasis, kMaxN, 8, 2, true>(p);
     return;
   }
-  cudaFuncSetAttribute(k_acoef<4, KS, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       static_cast<int>(acoef_smem_bytes<4, KS, 4>(p)));
-  cudaFuncSetAttribute(k_acoef<4, KG, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       static_cast<int>(acoef_smem_bytes<4, KG, 4>(p)));
-  const size_t b4 = fused_layout(p, kBlock / 4, basis_stride(p)).total_bytes;
-  const size_t b8 = fused_layout(p, kBlock / 8, basis_stride(p)).total_bytes;
   if (small_shape(p)) {
-    set_fused_smem_t<4, kSmallN, kSmallK, kSmallN, 4>(b4);
-    set_fused_smem_t<8, kSmallN, kSmallK, kSmallN, 4>(b8);
+    set_fused_smem_t<4, kSmallN, kSmallK, kSmallN, 4, 3, false>(p);
+    set_fused_smem_t<8, kSmallN, kSmallK, kSmallN, 4, 3, false>(p);
+    set_fused_smem_t<4, kSmallN, kSmallK, kSmallN, 4, 4, false>(p);
+    set_fused_smem_t<8, kSmallN, kSmallK, kSmallN, 4, 4, false>(p);
+    if (tc) {
+      set_fused_smem_t<4, kSmallN, kSmallK, kSmallN, 4, 3, true>(p);
+      set_fused_smem_t<8, kSmallN, kSmallK, kSmallN, 4, 3, true>(p);
+    }
   } else {
-    set_fused_smem_t<4, kMaxN, kMaxBasis, kMaxN, 4>(b4);
-    set_fused_smem_t<8, kMaxN, kMaxBasis, kMaxN, 4>(b8);
+    set_fused_smem_t<4, kMaxN, kMaxBasis, kMaxN, 4, 2, false>(p);
+    set_fused_smem_t<8, kMaxN, kMaxBasis, kMaxN, 4, 2, false>(p);
+    if (tc) {
+      set_fused_smem_t<4, kMaxN, kMaxBasis, kMaxN, 4, 2, true>(p);
+      set_fused_smem_t<8, kMaxN, kMaxBasis, kMaxN, 4, 2, true>(p);
+    }
   }
+}
+
+size_t fused_tc_smem_bytes(const ModelParams& p)
+{
+  if (high_degree(p))
+    return fused_layout(p, kBlock / kHighFusedGroup, basis_stride(p), fused_smem_budget(2), true)
+      .total_bytes;
+  return fused_layout(p, kBlock / 4, basis_stride(p), fused_smem_budget(small_shape(p) ? 3 : 2),
+                      true)
+    .total_bytes;
 }
 
 void launch_filter(Engine& e, int N, cudaStream_t s)
@@ -1366,26 +1623,14 @@ void launch_descriptor(Engine& e, int N, const double*, const int*, cudaStream_t
 {
   const bool small = small_shape(e.params);
   const bool high = high_degree(e.params);
-  // the type order is taken while the rebuild flag is still up (k_nep_fused clears it)
-  if (e.precision == 1) {
-    launch_type_order(e, N, e.use_xr || !e.order_valid, stream);
-    e.order_valid = true;
-  }
   if (!e.use_xr) launch_filter(e, N, stream);
-  if (high) launch_fused_g<kHighFusedGroup, kMaxN, kMaxBasis, kMaxN, 8>(e, N, stream);
+  if (high) launch_fused_g<kHighFusedGroup, kMaxN, kMaxBasis, kMaxN, 8, 2>(e, N, stream);
   else if (e.group == 8) {
-    if (small) launch_fused_g<8, kSmallN, kSmallK, kSmallN, 4>(e, N, stream);
-    else launch_fused_g<8, kMaxN, kMaxBasis, kMaxN, 4>(e, N, stream);
+    if (small) launch_fused_small<8>(e, N, stream);
+    else launch_fused_g<8, kMaxN, kMaxBasis, kMaxN, 4, 2>(e, N, stream);
   } else {
-    if (small) launch_fused_g<4, kSmallN, kSmallK, kSmallN, 4>(e, N, stream);
-    else launch_fused_g<4, kMaxN, kMaxBasis, kMaxN, 4>(e, N, stream);
-  }
-  if (e.precision == 1) {
-    // mixed precision: the ANN on the tensor cores, then the fused kernel's tail
-    launch_ann_tc(e, N, stream);
-    if (high) launch_acoef_t<kHighFusedGroup, round4(kMaxBasis), 8>(e, N, stream);
-    else if (small) launch_acoef_t<4, round4(kSmallK), 4>(e, N, stream);
-    else launch_acoef_t<4, round4(kMaxBasis), 4>(e, N, stream);
+    if (small) launch_fused_small<4>(e, N, stream);
+    else launch_fused_g<4, kMaxN, kMaxBasis, kMaxN, 4, 2>(e, N, stream);
   }
   // a single explicit-row system: the gather evaluates both directed angular
   // forces itself; a batch's structures that are not small take f12 here

@@ -10,7 +10,7 @@
 // writes one file per output step) and restart.xyz (rewritten).
 //
 //   nepx-md                     run the job in the working directory
-//   nepx-md --precision mixed   the ANN on the tensor cores
+//   nepx-md --precision mixed   the ANN on the tensor cores (FP16; mixed_bf16: BF16)
 //   nepx-md --check             parse and validate the inputs only (no GPU)
 //
 // The ensemble RNG seed is DMGMD_ENSEMBLE_SEED when set (decimal), else
@@ -451,13 +451,14 @@ int main(int argc, char** argv)
     } else if (arg == "--precision" && a + 1 < argc) {
       const std::string v = argv[++a];
       if (v == "mixed") precision = NEPX_PRECISION_MIXED;
+      else if (v == "mixed_bf16") precision = NEPX_PRECISION_MIXED_BF16;
       else if (v != "fp32") {
-        std::cerr << "nepx-md: --precision takes fp32 or mixed\n";
+        std::cerr << "nepx-md: --precision takes fp32, mixed or mixed_bf16\n";
         return EXIT_FAILURE;
       }
     } else {
-      std::cerr << "usage: nepx-md [--precision fp32|mixed] [--check]   (run.in and model.xyz "
-                   "in the working directory)\n";
+      std::cerr << "usage: nepx-md [--precision fp32|mixed|mixed_bf16] [--check]   (run.in and "
+                   "model.xyz in the working directory)\n";
       return EXIT_FAILURE;
     }
   }

@@ -39,6 +39,7 @@ EXPORTED = ["nepx_create", "nepx_destroy", "nepx_last_error", "nepx_info", "nepx
             "nepx_md_neighbor_info", "nepx_md_set_max_distance", "nepx_md_time",
             "nepx_md_enable_unwrapped", "nepx_md_get_unwrapped"]
 
+PRECISIONS = {"fp32": 0, "mixed": 1, "mixed_bf16": 2}
 ENSEMBLES = {"nve": 0, "nvt_ber": 1, "nvt_nhc": 2, "nvt_bdp": 3, "npt_ber": 4, "npt_scr": 5}
 BAROSTATS = {"isotropic": 0, "anisotropic": 1, "triclinic": 2}
 THERMO_COLUMNS = ["T", "KE", "PE", "sxx", "syy", "szz", "syz", "sxz", "sxy", "ax", "ay", "az",
@@ -221,8 +222,9 @@ class Potential:
         return pe, force, virial
 
     def set_precision(self, mode):
-        """"fp32" (default) or "mixed" (the ANN on the tensor cores)."""
-        self._check(lib().nepx_set_precision(self._h, {"fp32": 0, "mixed": 1}[mode]))
+        """"fp32" (default), "mixed" (the ANN on the tensor cores, FP16 operands
+        with per-layer scaling) or "mixed_bf16" (BF16 operands)."""
+        self._check(lib().nepx_set_precision(self._h, PRECISIONS[mode]))
 
     def compute_batch(self, structs, types, pos, out=None, accumulate=False, sync_check=False,
                       stream=None):

@@ -31,8 +31,10 @@ extern "C" {
 #define NEPX_ERR_BOX 8          /* box too thin for the large-box path, or singular */
 
 /* ANN precision (nepx_set_precision) */
-#define NEPX_PRECISION_FP32 0   /* FP32 SIMT ANN: the reference's arithmetic */
-#define NEPX_PRECISION_MIXED 1  /* ANN on the tensor cores, 3xTF32 with FP32 accumulation */
+#define NEPX_PRECISION_FP32 0        /* FP32 SIMT ANN: the reference's arithmetic */
+#define NEPX_PRECISION_MIXED 1       /* ANN on the tensor cores: FP16 operands with per-layer
+                                        power-of-two scaling, FP32 accumulation */
+#define NEPX_PRECISION_MIXED_BF16 2  /* the same with BF16 operands */
 
 /* compute flags */
 #define NEPX_ACCUMULATE 1u      /* add into pe/force/virial (the reference's += contract) */
@@ -295,11 +297,16 @@ int nepx_md_device_state(nepx_md_t* md, double** d_pos, double** d_vel, double**
 
 /*
  * Chooses how the per-atom ANN runs for every later call on this handle
- * (compute, batch, MD, server): NEPX_PRECISION_FP32 (default) or
- * NEPX_PRECISION_MIXED, the two ANN contractions as tcgen05 tensor-core
- * GEMMs over tiles of 128 type-sorted atoms (descriptors and forces stay
- * FP32).  NEPX_ERR_UNSUPPORTED when the model's ANN does not fit the tiles.
- * No counterpart in the reference (its ANN is FP32 only).
+ * (compute, batch, MD, server): NEPX_PRECISION_FP32 (default), or the two
+ * ANN contractions as tcgen05 tensor-core MMAs inside the descriptor kernel,
+ * over the centers of each CTA (M = 128 hidden units or descriptor
+ * components, N = the CTA's 16 or 32 centers), with 16-bit operands and
+ * FP32 accumulation: NEPX_PRECISION_MIXED (FP16; W0, w1 (1 - x^2) and each
+ * CTA's descriptors scaled by powers of two to use FP16's range) or
+ * NEPX_PRECISION_MIXED_BF16.  Descriptors, forces and the rest of the ANN
+ * (tanh, energy sum) stay FP32.  NEPX_ERR_UNSUPPORTED for models with dim >
+ * 128 or more than 256 hidden units.  No counterpart in the reference (its
+ * ANN is FP32 only).
  */
 int nepx_set_precision(nepx_t* handle, int mode);
 

@@ -15,6 +15,7 @@ import pytest
 import oracle
 import workloads
 from test_gpu_force import assert_close, run_gpu
+from test_gpu_mixed import assert_mixed_close
 
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
@@ -65,8 +66,12 @@ def test_batch_and_mixed_precision(tmp_path):
         o = 0
         for k, (t, h, p) in enumerate(structs):
             n = len(t)
-            assert_close(orc.compute(t, h, p), (pe[o:o + n], f[:, o:o + n], w[:, o:o + n]),
-                         "%s struct %d" % (precision, k))
+            got = (pe[o:o + n], f[:, o:o + n], w[:, o:o + n])
+            label = "%s struct %d" % (precision, k)
+            if precision == "fp32":
+                assert_close(orc.compute(t, h, p), got, label)
+            else:
+                assert_mixed_close(orc.compute(t, h, p), got, label, precision)
             o += n
 
 

@@ -1,10 +1,10 @@
 """One handle, two users: an MD that shares its potential handle with direct
 force calls on another system between its runs continues as an MD that had
-the handle to itself: its Verlet rows, box and type order are rebuilt for it
-when it takes the handle back.  The agreement is to FP32 rounding, not
-bitwise: the typewise filter sums the radial descriptors over the Verlet
-candidates in lane order, and the candidate set depends on when the list was
-last built.  A stale list, box or type order would give errors of order one."""
+the handle to itself: its Verlet rows and box are rebuilt for it when it
+takes the handle back.  The agreement is to FP32 rounding, not bitwise: the
+typewise filter sums the radial descriptors over the Verlet candidates in
+lane order, and the candidate set depends on when the list was last built.
+A stale list or box would give errors of order one."""
 import numpy as np
 import pytest
 
@@ -41,7 +41,10 @@ def test_md_continues_after_another_caller(precision):
         md.close()
     pot.close()
     a, b = rows
-    # per column, against the column's scale (temperature, energies, stresses, box)
+    # per column, against the column's scale (temperature, energies, stresses, box).
+    # The rebuilt Verlet rows hand the radial edges to other lanes, which moves
+    # FP32 sums by an ulp; on the mixed path such an ulp can move a 16-bit ANN
+    # operand by one unit (2^-11 relative), hence the looser bound there
     scale = np.abs(a).max(axis=0) + 1e-12
     rel = (np.abs(a - b) / scale).max()
-    assert rel <= 1e-5, rel
+    assert rel <= (1e-5 if precision == "fp32" else 3e-4), rel
