@@ -76,9 +76,11 @@ import workloads  # noqa: E402
 K_B = 8.617343e-5
 # DRAM bytes per atom and force call of the four force kernels (k_filter_radial,
 # k_nep_fused, k_angular_f12, k_gather), dram__bytes_read.sum +
-# dram__bytes_write.sum of one ncu-captured launch each, divided by the atoms
-# of the captured system (traffic grows with the atoms processed)
-TRAFFIC_PER_ATOM = {}
+# dram__bytes_write.sum of one ncu-captured launch each on the large-carbon
+# system at 1,000,000 atoms (--ncell 50), divided by its atoms (traffic grows
+# with the atoms processed)
+TRAFFIC_PER_ATOM = {"carbon8m": (683.1 + 386.7 + 318.7 + 489.9 + 808.4 + 533.9 + 1352.8
+                                 + 103.9) * 1e6 / 1.0e6}
 FP32_LANES = 148 * 128          # B200: SMs x FP32 lanes
 SM_MAX_MHZ = 1965.0
 L2_NOTE = "flushed by a 512 MiB write before every %d-step chunk"
