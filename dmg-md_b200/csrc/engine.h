@@ -105,7 +105,12 @@ bool fused_occupancy_variants(const ModelParams& p);
 void set_fused_smem_limits(const ModelParams& p);
 
 // Times each kernel variant on the given system (a few calls each, stream
-// synchronised) and keeps the fastest.  Neighbour rows must be current.
+// synchronised) and keeps the fastest: the lane-group size of the filter,
+// descriptor, angular-force and gather kernels and the descriptor kernel's
+// CTAs per SM.  The picks are kept per (device, model shape, precision, row
+// path, size class log2 N) for every later handle of the process, and in the
+// file NEPX_TUNE_FILE names, when set, across runs.  Neighbour rows must be
+// current.
 void engine_autotune(Engine& e, int N, const double* pos, const int* type, cudaStream_t stream);
 
 // Loads the potential, uploads it and sizes every buffer for max_atoms.
@@ -129,6 +134,11 @@ void launch_set_box(Engine& e, const Box& b, cudaStream_t stream);
 void launch_neighbor_update(Engine& e, int N, const double* pos, const int* type, bool force,
                             cudaStream_t stream, bool skin_done = false);
 
+// Device bytes one atom and one structure slot of a served request occupy
+// (serve.cu): the server admits requests by these against its byte budget.
+size_t served_bytes_per_atom(const Engine& e);
+size_t served_bytes_per_struct();
+
 // Explicit rows: allocates them for the handle's capacity and max_struct
 // structures (once; later calls only check the size).
 std::string engine_enable_xr(Engine& e, int max_struct);
@@ -137,6 +147,9 @@ std::string engine_enable_xr(Engine& e, int max_struct);
 // rc thick (at most cell_cap in total, else it scans all its atoms); returns
 // the number of cells.  Structures are described by si[0..n).
 int assign_cells(const Engine& e, StructInfo* si, int n);
+// Cells of a structure's grid (0: small, or too few cells for the stencil,
+// so its rows scan all its atoms); nc_out (may be null) gets the grid.
+int structure_cells(const Engine& e, const StructInfo& s, int* nc_out);
 
 // Small-box test of the reference with its cutoff (largest radial cutoff)
 // and skin 1 A; returns 0 large, 1 small, -1 small in one direction and

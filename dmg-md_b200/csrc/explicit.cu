@@ -460,25 +460,35 @@ cudaError_t dalloc(T*& ptr, size_t count)
 
 }  // namespace
 
+int structure_cells(const Engine& e, const StructInfo& s, int* nc_out)
+{
+  if (s.small) return 0;
+  const double rc = e.model.rc_radial_max;
+  int nc[3], cells = 1;
+  for (int d = 0; d < 3; ++d) {
+    const double* r = s.box.hinv + 3 * d;
+    const double thick = 1.0 / std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    nc[d] = s.box.pbc[d] ? std::max(1, static_cast<int>(thick / (0.5 * rc))) : 1;
+    cells *= nc[d];
+  }
+  // a 5x5x5 stencil of cells at least rc/2 wide covers the cutoff; grids of
+  // fewer than 125 cells scan all the structure's atoms instead
+  if (cells < 125) return 0;
+  if (nc_out)
+    for (int d = 0; d < 3; ++d) nc_out[d] = nc[d];
+  return cells;
+}
+
 int assign_cells(const Engine& e, StructInfo* si, int n)
 {
-  const double rc = e.model.rc_radial_max;
   int used = 0;
   for (int k = 0; k < n; ++k) {
     StructInfo& s = si[k];
     s.nc[0] = s.nc[1] = s.nc[2] = 0;
     s.cell_base = 0;
-    if (s.small) continue;
-    int nc[3], cells = 1;
-    for (int d = 0; d < 3; ++d) {
-      const double* r = s.box.hinv + 3 * d;
-      const double thick = 1.0 / std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
-      nc[d] = s.box.pbc[d] ? std::max(1, static_cast<int>(thick / (0.5 * rc))) : 1;
-      cells *= nc[d];
-    }
-    // a 5x5x5 stencil of cells at least rc/2 wide covers the cutoff; grids
-    // of fewer than 125 cells scan all the structure's atoms instead
-    if (cells < 125 || used + cells > e.xr.cell_cap) continue;
+    int nc[3];
+    const int cells = structure_cells(e, s, nc);
+    if (cells == 0 || used + cells > e.xr.cell_cap) continue;
     for (int d = 0; d < 3; ++d) s.nc[d] = nc[d];
     s.cell_base = used;
     used += cells;

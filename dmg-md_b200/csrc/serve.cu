@@ -24,6 +24,7 @@
 // positions wrapped into each structure's own box.
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
@@ -190,6 +191,28 @@ int grid(int n) { return (n + kThreads - 1) / kThreads; }
 
 }  // namespace
 
+// Device bytes one served atom occupies: the handle's per-atom buffers of the
+// explicit-row path (radial and angular rows, angular partial forces, site
+// records, cell slots, descriptor scratch) and the server's two arena
+// buffers and I/O blocks.
+size_t served_bytes_per_atom(const Engine& e)
+{
+  const NeighborBuffers& nb = e.nbr;
+  const ModelParams& p = e.params;
+  size_t b = 16 * static_cast<size_t>(nb.mn_r + nb.mn_a);   // explicit rows (float4)
+  b += 16 * static_cast<size_t>(nb.mn_a);                    // angular partial forces
+  b += 2 * sizeof(int) + sizeof(Site) + 1 + 2 * sizeof(int); // counts, sites, flag, cell slots
+  b += sizeof(float) * (static_cast<size_t>(p.nA) * p.nlm + p.T * basis_stride(p) + p.nR);
+  b += sizeof(double);                                       // site energy
+  b += 2 * (2 * sizeof(int) + 10 * sizeof(double));          // arenas: type, sid, pos, vel, mass, force
+  b += sizeof(double) * (1 + 9 + kOutFields + 8);            // pe, virial, output and input blocks
+  return b;
+}
+
+// Device bytes of one structure slot: its table entry, offset, control words
+// and step size (its cell grid is counted per cell).
+size_t served_bytes_per_struct() { return sizeof(StructInfo) + 6 * sizeof(int) + sizeof(double); }
+
 // Explicit rows + force over structures already described in e.xr (d_si,
 // d_soff, n_struct uploaded).  Shared by the batch call and the server.
 void launch_batch_force(Engine& e, int T, const double* pos, const int* type, double* pe,
@@ -219,6 +242,8 @@ using Clock = std::chrono::steady_clock;
 struct Pending {
   long long ticket = 0;
   int n = 0, md_steps = 0;
+  int cells = 0;            // cells of its grid in the batch's cell lists
+  size_t bytes = 0;         // device bytes it occupies while resident
   double dt = 0.0;          // fs
   nepx_box box{};
   std::vector<int> type;
@@ -230,6 +255,8 @@ struct Pending {
 struct Resident {
   long long ticket = 0;
   int n = 0, md_steps = 0, steps_done = 0;
+  int cells = 0;
+  size_t bytes = 0;
   bool fresh = true;        // initial forces not evaluated yet
   double dt = 0.0;          // fs
   nepx::StructInfo si{};
@@ -250,6 +277,10 @@ struct Arena {
 struct nepx_server {
   nepx_t* h = nullptr;
   int max_atoms = 0, max_struct = 0;
+  // admission by device memory: a request is admitted while the resident
+  // requests' bytes plus its own stay within the budget (and the arena's atom,
+  // slot and cell capacities hold)
+  size_t bytes_per_atom = 0, bytes_per_struct = 0, budget = 0;
   cudaStream_t stream = nullptr;
   Arena arena[2];
   int cur = 0;
@@ -271,6 +302,7 @@ struct nepx_server {
   Clock::time_point t0;
   // statistics
   double done = 0, steps = 0, atom_steps = 0, busy = 0, resident_atoms = 0, resident_structs = 0;
+  double resident_bytes = 0;
 
   double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
   void run();
@@ -321,11 +353,21 @@ void nepx_server::run()
       if (queue.empty() && res.empty()) break;   // stopping with nothing left
       int atoms = T;
       int nst = static_cast<int>(res.size());
+      int cells = 0;
+      size_t bytes = 0;
+      for (const Resident& r : res) {
+        cells += r.cells;
+        bytes += r.bytes;
+      }
       while (!queue.empty()) {
         Pending& p = queue.front();
-        if (atoms + p.n > max_atoms || nst + 1 > MS) break;
+        if (atoms + p.n > max_atoms || nst + 1 > MS || bytes + p.bytes > budget ||
+            cells + p.cells > e.xr.cell_cap)
+          break;
         atoms += p.n;
         ++nst;
+        cells += p.cells;
+        bytes += p.bytes;
         adm.push_back(std::move(p));
         queue.pop_front();
       }
@@ -355,6 +397,8 @@ void nepx_server::run()
       Resident r;
       r.ticket = p.ticket;
       r.n = p.n;
+      r.cells = p.cells;
+      r.bytes = p.bytes;
       r.md_steps = p.md_steps;
       r.dt = p.dt;
       r.out = p.out;
@@ -497,6 +541,7 @@ void nepx_server::run()
       busy += t_end - t_tick;
       resident_atoms += T;
       resident_structs += S;
+      for (const Resident& r : res) resident_bytes += static_cast<double>(r.bytes);
     }
     if (nfin) done_cv.notify_all();
     std::vector<Resident> keep;
@@ -608,6 +653,11 @@ int nepx_server_create(nepx_t* h, int max_atoms, int max_struct, nepx_server_t**
   S->h = h;
   S->max_atoms = max_atoms;
   S->max_struct = max_struct;
+  S->bytes_per_atom = nepx::served_bytes_per_atom(e);
+  S->bytes_per_struct = nepx::served_bytes_per_struct();
+  S->budget = static_cast<size_t>(max_atoms) * S->bytes_per_atom +
+              static_cast<size_t>(max_struct) * S->bytes_per_struct +
+              sizeof(int) * 2 * static_cast<size_t>(e.xr.cell_cap);
   S->t0 = Clock::now();
   const size_t N = max_atoms, MS = max_struct;
   bool ok = cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking) == cudaSuccess;
@@ -677,6 +727,15 @@ int nepx_server_submit(nepx_server_t* S, const nepx_request* req, nepx_result* o
     if (req->type[a] < 0 || req->type[a] >= e.model.num_types) return NEPX_ERR_ARG;
   Pending p;
   p.n = req->n;
+  p.cells = nepx::structure_cells(e, si, nullptr);
+  p.bytes = static_cast<size_t>(req->n) * S->bytes_per_atom + S->bytes_per_struct +
+            sizeof(int) * 2 * static_cast<size_t>(p.cells);
+  if (p.bytes > S->budget || p.cells > e.xr.cell_cap) {
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->error = "request of " + std::to_string(req->n) + " atoms needs more device memory than "
+               "the server's budget";
+    return NEPX_ERR_CAPACITY;
+  }
   p.md_steps = req->md_steps;
   p.dt = req->dt_fs;
   p.box = req->box;
@@ -731,6 +790,38 @@ int nepx_server_drain(nepx_server_t* S)
       if (kv.second < 0) return false;
     return true;
   });
+  return NEPX_OK;
+}
+
+int nepx_server_create_budget(nepx_t* h, double hbm_bytes, int max_struct, nepx_server_t** out)
+{
+  if (!h || !out || max_struct < 1 || !(hbm_bytes > 0.0)) return NEPX_ERR_ARG;
+  *out = nullptr;
+  nepx::Engine& e = h->engine;
+  const double per_atom = static_cast<double>(nepx::served_bytes_per_atom(e)) + 2.0 * sizeof(int);
+  const double slots = static_cast<double>(max_struct) * nepx::served_bytes_per_struct();
+  const double atoms = std::floor((hbm_bytes - slots) / per_atom);
+  if (atoms < 1.0) {
+    h->error = "a device-memory budget of " + std::to_string(hbm_bytes) +
+               " bytes holds no atom of this model";
+    return NEPX_ERR_CAPACITY;
+  }
+  const int max_atoms = static_cast<int>(std::min<double>(atoms, e.capacity));
+  const int rc = nepx_server_create(h, max_atoms, max_struct, out);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk((*out)->mu);
+  (*out)->budget = static_cast<size_t>(hbm_bytes);
+  return NEPX_OK;
+}
+
+int nepx_server_memory(nepx_server_t* S, double* info)
+{
+  if (!S || !info) return NEPX_ERR_ARG;
+  std::lock_guard<std::mutex> lk(S->mu);
+  info[0] = static_cast<double>(S->budget);
+  info[1] = static_cast<double>(S->bytes_per_atom);
+  info[2] = static_cast<double>(S->bytes_per_struct);
+  info[3] = S->steps > 0 ? S->resident_bytes / S->steps : 0.0;
   return NEPX_OK;
 }
 

@@ -37,7 +37,8 @@ EXPORTED = ["nepx_create", "nepx_destroy", "nepx_last_error", "nepx_info", "nepx
             "nepx_server_stats", "nepx_set_precision", "nepx_md_run_segment",
             "nepx_md_set_barostat", "nepx_md_set_velocity", "nepx_md_compute_forces",
             "nepx_md_neighbor_info", "nepx_md_set_max_distance", "nepx_md_time",
-            "nepx_md_enable_unwrapped", "nepx_md_get_unwrapped"]
+            "nepx_md_enable_unwrapped", "nepx_md_get_unwrapped", "nepx_server_create_budget",
+            "nepx_server_memory"]
 
 PRECISIONS = {"fp32": 0, "mixed": 1, "mixed_bf16": 2}
 ENSEMBLES = {"nve": 0, "nvt_ber": 1, "nvt_nhc": 2, "nvt_bdp": 3, "npt_ber": 4, "npt_scr": 5}
@@ -133,6 +134,9 @@ def lib():
         L.nepx_server_wait.argtypes = [vp, ctypes.c_longlong, ip]
         L.nepx_server_drain.argtypes = [vp]
         L.nepx_server_stats.argtypes = [vp, dp]
+        L.nepx_server_create_budget.argtypes = [vp, ctypes.c_double, ctypes.c_int,
+                                                ctypes.POINTER(vp)]
+        L.nepx_server_memory.argtypes = [vp, dp]
         L.nepx_md_set_velocity.argtypes = [vp, dp]
         L.nepx_md_compute_forces.argtypes = [vp]
         L.nepx_md_neighbor_info.argtypes = [vp, ip, ip]
@@ -453,14 +457,27 @@ class Server:
     results land in numpy arrays owned by this object once wait()/poll()
     report the ticket done."""
 
-    def __init__(self, potential, max_atoms, max_struct):
+    def __init__(self, potential, max_atoms=None, max_struct=2048, hbm_bytes=None):
+        """An arena of max_atoms atoms, or one sized from a device-memory
+        budget (hbm_bytes) that admission then holds to."""
         self.pot = potential
         self._h = ctypes.c_void_p()
-        rc = lib().nepx_server_create(potential._h, int(max_atoms), int(max_struct),
-                                      ctypes.byref(self._h))
+        if hbm_bytes is not None:
+            rc = lib().nepx_server_create_budget(potential._h, float(hbm_bytes), int(max_struct),
+                                                 ctypes.byref(self._h))
+        else:
+            rc = lib().nepx_server_create(potential._h, int(max_atoms), int(max_struct),
+                                          ctypes.byref(self._h))
         if rc:
             raise NepxError(rc, lib().nepx_last_error(potential._h).decode())
         self._out = {}
+
+    def memory(self):
+        """budget_bytes, bytes_per_atom, bytes_per_struct, mean_resident_bytes."""
+        info = (ctypes.c_double * 4)()
+        self._check(lib().nepx_server_memory(self._h, info))
+        keys = ["budget_bytes", "bytes_per_atom", "bytes_per_struct", "mean_resident_bytes"]
+        return dict(zip(keys, list(info)))
 
     def close(self):
         if getattr(self, "_h", None) and self._h.value:

@@ -337,8 +337,11 @@ int nepx_compute_batch(nepx_t* handle, const nepx_struct_desc* descs, int nstruc
 /*
  * Serving loop: a worker thread owns the potential handle and a device
  * arena of max_atoms atoms and max_struct structure slots.  Requests are
- * admitted while they fit the arena (continuous batching: new requests join
- * between steps while others are mid-segment); every step evaluates all
+ * admitted while their device memory fits the server's budget (continuous
+ * batching: new requests join between steps while others are mid-segment):
+ * each request counts its atoms' bytes (explicit neighbour rows and partial
+ * forces at the model's row capacities, descriptor scratch, arena and I/O
+ * buffers), a structure slot and the cells of its grid; every step evaluates all
  * resident structures in one launch sequence, runs the NVE velocity-Verlet
  * half steps of the MD segments, and retires finished requests (results
  * copied to the caller's host buffers).  The handle must not be used by the
@@ -367,6 +370,14 @@ typedef struct nepx_result {
 } nepx_result;
 
 int nepx_server_create(nepx_t* handle, int max_atoms, int max_struct, nepx_server_t** out);
+/* The same with the arena sized from a device-memory budget in bytes (at most
+ * the handle's max_atoms atoms): requests are admitted while the resident
+ * requests' bytes stay within hbm_bytes.  No counterpart in the reference. */
+int nepx_server_create_budget(nepx_t* handle, double hbm_bytes, int max_struct,
+                              nepx_server_t** out);
+/* info[4]: the byte budget, bytes per served atom, bytes per structure slot,
+ * mean resident bytes per step. */
+int nepx_server_memory(nepx_server_t* server, double* info);
 /* Stops the worker after the queued requests are done, then frees the arena. */
 int nepx_server_destroy(nepx_server_t* server);
 const char* nepx_server_last_error(const nepx_server_t* server);

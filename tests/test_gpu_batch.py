@@ -8,7 +8,8 @@
   order);
 * the server returns, for every request of a randomly ordered stream that
   overflows its arena several times, exactly the batch-of-one result;
-* an MD segment run by the server follows nepx_md's NVE trajectory.
+* an MD segment run by the server follows nepx_md's NVE trajectory;
+* a server sized from a device-memory budget admits by bytes.
 """
 import numpy as np
 import pytest
@@ -133,4 +134,36 @@ def test_server_md_segment_follows_nepx_md():
     np.testing.assert_allclose(r["pos"], ref["pos"], rtol=0, atol=1e-9)
     np.testing.assert_allclose(r["vel"], ref["vel"], rtol=0, atol=1e-9)
     np.testing.assert_allclose(r["force"], ref["force"], rtol=0, atol=1e-7)
+    srv.close()
+
+
+def test_server_admits_by_device_memory():
+    """A server sized from a byte budget holds the resident requests' bytes
+    to it (a few structures at a time here), returns every request's
+    batch-of-one result, and rejects a request that alone exceeds it."""
+    import nepx
+    rng = np.random.default_rng(9)
+    base = _structures(seed=2)
+    stream = [base[k] for k in rng.integers(0, len(base), 16)]
+    pot = nepx.Potential(potential(WATER), max_atoms=2000)
+    expected = [_batch_one(pot, s) for s in stream]
+    probe = nepx.Server(pot, max_atoms=2000, max_struct=8)
+    per_atom = probe.memory()["bytes_per_atom"]
+    probe.close()
+    budget = 1400 * per_atom          # about two of the larger structures
+    srv = nepx.Server(pot, max_struct=8, hbm_bytes=budget)
+    mem = srv.memory()
+    assert mem["budget_bytes"] == pytest.approx(budget, rel=1e-9)
+    tickets = [srv.submit(t, p, h, pbc) for (t, h, p, pbc) in stream]
+    for tk, exp in zip(tickets, expected):
+        r = srv.wait(tk)
+        assert np.array_equal(r["pe"], exp[0])
+        assert np.array_equal(r["force"], exp[1])
+    st, mem = srv.stats(), srv.memory()
+    assert st["done"] == len(stream)
+    assert 0 < mem["mean_resident_bytes"] <= budget
+    t, h, p = workloads.water(n_mol=600, seed=8)            # 1800 atoms: over the budget
+    with pytest.raises(nepx.NepxError) as err:
+        srv.submit(t, p, h)
+    assert err.value.code == 5
     srv.close()
