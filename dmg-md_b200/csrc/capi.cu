@@ -43,6 +43,11 @@ int decode_state(nepx_handle* h, const NeighborState& s)
   if (s.box_error) return fail(h, NEPX_ERR_BOX, kUnsupportedBox);
   if (s.ann_error)
     return fail(h, NEPX_ERR_CUDA, "a tensor-core ANN tile timed out waiting for its MMAs");
+  if (s.sync_error) {
+    h->engine.nbr.gsync_dirty = true;
+    h->engine.force_rebuild = true;
+    return fail(h, NEPX_ERR_CUDA, "the neighbour-list rebuild timed out at a grid-wide barrier");
+  }
   return NEPX_OK;
 }
 

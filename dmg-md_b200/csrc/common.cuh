@@ -60,6 +60,7 @@ struct NeighborState {
   int nonfinite;       // a force or energy came out NaN/Inf
   int box_error;       // the device box became unsupported (small in one direction, >10 rc in another)
   int ann_error;       // a tensor-core ANN tile gave up waiting for its MMAs
+  int sync_error;      // the neighbour rebuild gave up waiting at a grid-wide barrier
   double box_scale;    // product of isotropic box factors since the last build (1 = none)
   double box_def[9];   // product of general box deformations since the last build (I = none)
 };

@@ -172,6 +172,10 @@ std::string engine_create(Engine& e, const std::string& nep_path, int max_atoms)
   ok &= dalloc(nb.nl_r, static_cast<size_t>(N) * nb.mn_r) == cudaSuccess;
   ok &= dalloc(nb.nn_a, N) == cudaSuccess;
   ok &= dalloc(nb.nl_a, static_cast<size_t>(N) * nb.mn_a) == cudaSuccess;
+  nb.rebuild_blocks = neighbor_rebuild_blocks(nb.pow2_v);
+  if (nb.rebuild_blocks < 1) return "the neighbour rebuild kernel cannot be resident on this device";
+  ok &= dalloc(nb.gsync, 2) == cudaSuccess;
+  ok &= dalloc(nb.scan_part, nb.rebuild_blocks) == cudaSuccess;
   ok &= dalloc(nb.cell_count, nb.cell_cap) == cudaSuccess;
   ok &= dalloc(nb.cell_start, nb.cell_cap) == cudaSuccess;
   ok &= dalloc(nb.cell_atoms, N) == cudaSuccess;
@@ -192,7 +196,9 @@ std::string engine_create(Engine& e, const std::string& nep_path, int max_atoms)
   for (int k = 0; k < 9; ++k) init.box_def[k] = (k % 4 == 0) ? 1.0 : 0.0;
   if (cudaMemcpy(e.d_nstate, &init, sizeof(init), cudaMemcpyHostToDevice) != cudaSuccess)
     return "cudaMemcpy failed (neighbour state)";
-  if (cudaMemset(nb.nn_a, 0, sizeof(int) * N) != cudaSuccess) return "cudaMemset failed";
+  if (cudaMemset(nb.nn_a, 0, sizeof(int) * N) != cudaSuccess ||
+      cudaMemset(nb.gsync, 0, 2 * sizeof(unsigned)) != cudaSuccess)
+    return "cudaMemset failed";
   if (fused_smem_bytes(p) > 227 * 1024)
     return "descriptor kernel needs more shared memory than a CTA has (not supported)";
   set_fused_smem_limits(p);
@@ -462,7 +468,7 @@ void engine_destroy(Engine& e)
 {
   NeighborBuffers& nb = e.nbr;
   void* ptrs[] = {e.d_params, e.d_box, e.d_nstate, nb.nn_v, nb.nl_v, nb.nn_r, nb.nl_r,
-                  nb.nn_a, nb.nl_a, nb.cell_count, nb.cell_start, nb.cell_atoms, nb.cell_of,
+                  nb.nn_a, nb.nl_a, nb.gsync, nb.scan_part, nb.cell_count, nb.cell_start, nb.cell_atoms, nb.cell_of,
                   nb.x0, e.scratch.alpha, e.scratch.f12, e.scratch.pe_ann, e.d_w16,
                   e.scratch.tune_out, e.scratch.acoef, e.scratch.sites, e.scratch.qrad,
                   e.xr.er, e.xr.ea, e.xr.large,

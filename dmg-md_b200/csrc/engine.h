@@ -19,6 +19,12 @@ struct NeighborBuffers {
   int* nl_r = nullptr;   // [N][mn_r]
   int* nn_a = nullptr;
   int* nl_a = nullptr;   // [N][mn_a]
+  // the cooperative rebuild kernel: its grid-barrier counters (arrivals,
+  // generation), per-block partial sums of the cell scan, its block count
+  unsigned* gsync = nullptr;         // [2]
+  int* scan_part = nullptr;          // [rebuild_blocks]
+  int rebuild_blocks = 0;
+  bool gsync_dirty = false;          // a barrier timed out: reset the counters first
   int* cell_count = nullptr;
   int* cell_start = nullptr;
   int* cell_atoms = nullptr;
@@ -131,6 +137,9 @@ void launch_set_box(Engine& e, const Box& b, cudaStream_t stream);
 // launch follows a neighbour update at the same positions.
 // skin_done: the caller has packed the site records and applied the skin
 // criterion itself (the MD step does it in its first half kick).
+// Blocks of the cooperative neighbour rebuild that fit on the current device
+// at once for Verlet rows padded to pow2_v (0 on failure).
+int neighbor_rebuild_blocks(int pow2_v);
 void launch_neighbor_update(Engine& e, int N, const double* pos, const int* type, bool force,
                             cudaStream_t stream, bool skin_done = false);
 

@@ -976,6 +976,21 @@ int md_enqueue_run(nepx_md* m, int steps, double dt_fs, int thermo_every, double
   return NEPX_OK;
 }
 
+// A bounded device wait that gave up: the tensor-core ANN's MMAs, or a grid
+// barrier of the neighbour rebuild (whose counters are then reset before the
+// next rebuild).
+int wait_errors(nepx_md* m, const nepx::NeighborState& st)
+{
+  if (st.ann_error)
+    return md_fail(m, NEPX_ERR_CUDA, "a tensor-core ANN tile timed out waiting for its MMAs");
+  if (st.sync_error) {
+    m->md.engine->nbr.gsync_dirty = true;
+    m->md.forces_valid = false;
+    return md_fail(m, NEPX_ERR_CUDA, "the neighbour-list rebuild timed out at a grid-wide barrier");
+  }
+  return NEPX_OK;
+}
+
 int md_finish(nepx_md* m)
 {
   nepx::Md& md = m->md;
@@ -998,7 +1013,7 @@ int md_finish(nepx_md* m)
   if (st.box_error)
     return md_fail(m, NEPX_ERR_BOX, "the box became small in one periodic direction and thicker "
                                     "than 10 rc in another (unsupported, as in the reference)");
-  return NEPX_OK;
+  return wait_errors(m, st);
 }
 
 }  // namespace
@@ -1103,7 +1118,7 @@ int nepx_md_compute_forces(nepx_md_t* m)
   if (st.box_error)
     return md_fail(m, NEPX_ERR_BOX, "the box is small in one periodic direction and thicker "
                                     "than 10 rc in another (unsupported, as in the reference)");
-  return NEPX_OK;
+  return wait_errors(m, st);
 }
 
 int nepx_md_neighbor_info(nepx_md_t* m, int* max_radial, int* max_angular)

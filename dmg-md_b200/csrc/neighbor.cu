@@ -8,13 +8,16 @@
 // filters it into typewise radial and angular lists with float
 // d^2 < ((rc_t1 + rc_t2)/2)^2.  Rows are ascending in atom index.
 //
-// B200 design: everything stays on the device.  The skin check sets a device
-// flag that the rebuild kernels read (they return at once when it is clear),
-// so a step never waits on the host.  Rows are row-major (atom i owns the
-// contiguous slots [i*MN, i*MN + count)) so the warp that owns a center reads
-// and writes coalesced.  The cell list is a counting sort on a grid of cells
-// at least (rc + skin)/2 wide with a 5x5x5 stencil; each Verlet row is sorted
-// in shared memory, which makes every later sum over neighbours ordered and
+// B200 design: everything stays on the device, in one cooperative launch.
+// Its phases -- skin check, cell grid, counting sort of the atoms into cells,
+// Verlet rows -- are separated by grid-wide barriers (every
+// block is resident, and every wait is bounded); a step whose skin check
+// finds nothing to rebuild costs that one launch, which returns at once, and
+// never waits on the host.  Rows are row-major (atom i owns the contiguous
+// slots [i*MN, i*MN + count)) so the warp that owns a center reads and writes
+// coalesced.  The cell list is a counting sort on a grid of cells at least
+// (rc + skin)/2 wide with a 5x5x5 stencil; each Verlet row is sorted in
+// shared memory, which makes every later sum over neighbours ordered and
 // bitwise reproducible.
 #include <algorithm>
 #include <climits>
@@ -25,6 +28,10 @@ namespace nepx {
 
 namespace {
 
+constexpr int kRebuildThreads = 128;                 // four warps: a center per warp in the row build
+constexpr int kRebuildWarps = kRebuildThreads / 32;
+constexpr long long kGridWaitCycles = 4000000000ll;  // ~2 s at the B200 clock
+
 __device__ __forceinline__ int wrapped_cell(double s, int nc, int pbc)
 {
   if (!pbc) return 0;
@@ -33,47 +40,142 @@ __device__ __forceinline__ int wrapped_cell(double s, int nc, int pbc)
   return c < 0 ? 0 : (c >= nc ? nc - 1 : c);
 }
 
-__device__ __forceinline__ void cell_coords(const Box& b, const NeighborState& st, double x,
-                                            double y, double z, int& cx, int& cy, int& cz)
-{
-  const double sx = b.hinv[0] * x + b.hinv[1] * y + b.hinv[2] * z;
-  const double sy = b.hinv[3] * x + b.hinv[4] * y + b.hinv[5] * z;
-  const double sz = b.hinv[6] * x + b.hinv[7] * y + b.hinv[8] * z;
-  cx = wrapped_cell(sx, st.nc[0], b.pbc[0]);
-  cy = wrapped_cell(sy, st.nc[1], b.pbc[1]);
-  cz = wrapped_cell(sz, st.nc[2], b.pbc[2]);
-}
-
 // Packs each atom into its Site record for the neighbour sweeps of this
 // step and applies the skin criterion (skin_check_atom, common.cuh).  The MD
 // step does the same inside its first half kick instead.
-__global__ void k_skin_check(int N, const Box* __restrict__ box, const double* __restrict__ pos,
-                             const int* __restrict__ type, const double* __restrict__ x0,
-                             NeighborState* st, Site* __restrict__ sites, double skin,
-                             double rc_v, int force)
+__device__ __forceinline__ void skin_phase(int N, const Box& b, const double* __restrict__ pos,
+                                           const int* __restrict__ type,
+                                           const double* __restrict__ x0, NeighborState* st,
+                                           Site* __restrict__ sites, double skin, double rc_v,
+                                           int force)
 {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= N) return;
-  skin_check_atom(N, i, *box, pos[i], pos[N + i], pos[2 * N + i], type[i], x0, st, sites, skin,
-                  rc_v, force);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+    skin_check_atom(N, i, b, pos[i], pos[N + i], pos[2 * N + i], type[i], x0, st, sites, skin,
+                    rc_v, force);
 }
 
-// Cell grid from the current box (cells at least rc_v/2 thick, at most
-// cell_cap of them), then clears the counts.  One block.
-__global__ void k_cell_setup(const Box* __restrict__ box, NeighborState* st, int* cell_count,
-                             double rc_v, int cell_cap)
+// Grid-wide barrier of the cooperative rebuild.  A generation counter: the
+// last block to arrive resets the arrival count and advances the generation,
+// the others wait for the advance -- at most kGridWaitCycles, after which they
+// record the timeout in sync_error and go on (the call then reports an error).
+__device__ void grid_sync(unsigned* gs, NeighborState* st)
 {
-  __shared__ int s_ncell;
-  if (!st->rebuild) return;
+  __syncthreads();
   if (threadIdx.x == 0) {
-    st->box_scale = 1.0;
-    for (int k = 0; k < 9; ++k) st->box_def[k] = (k % 4 == 0) ? 1.0 : 0.0;
-    const Box& b = *box;
-    double vol = fabs(b.h[0] * (b.h[4] * b.h[8] - b.h[5] * b.h[7]) +
-                      b.h[1] * (b.h[5] * b.h[6] - b.h[3] * b.h[8]) +
-                      b.h[2] * (b.h[3] * b.h[7] - b.h[4] * b.h[6]));
+    volatile unsigned* gen = gs + 1;
+    const unsigned g = *gen;
+    __threadfence();
+    if (atomicAdd(gs, 1u) == gridDim.x - 1) {
+      atomicExch(gs, 0u);
+      __threadfence();
+      atomicAdd(gs + 1, 1u);
+    } else {
+      const long long t0 = clock64();
+      while (*gen == g) {
+        if (clock64() - t0 > kGridWaitCycles) {
+          atomicOr(&st->sync_error, 1);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+// Sum over the block (kRebuildThreads threads).
+__device__ int block_sum(int v, int* s_tmp)
+{
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) s_tmp[warp] = v;
+  __syncthreads();
+  int t = 0;
+  for (int w = 0; w < kRebuildWarps; ++w) t += s_tmp[w];
+  return t;
+}
+
+// Inclusive prefix sum over the block; *total gets the block's sum.
+__device__ int block_scan(int v, int* s_tmp, int* total)
+{
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  __syncthreads();
+  if (lane == 31) s_tmp[warp] = x;
+  __syncthreads();
+  int before = 0, t = 0;
+  for (int w = 0; w < kRebuildWarps; ++w) {
+    if (w < warp) before += s_tmp[w];
+    t += s_tmp[w];
+  }
+  *total = t;
+  return x + before;
+}
+
+struct RebuildArgs {
+  int N;
+  const Box* box;
+  const double* pos;
+  const int* type;
+  NeighborState* st;
+  Site* sites;
+  int* cell_count;
+  int* cell_start;
+  int* cell_atoms;
+  int* cell_of;
+  int* nn_v;
+  int* nl_v;
+  double* x0;
+  unsigned* gsync;
+  int* part;           // [gridDim.x] per-block sums of the cell scan
+  int mn_v, pow2, cell_cap;
+  double skin, rc_v;
+  float cutoff_square;
+  int skin_check;      // 1: pack the sites and apply the skin criterion first
+  int force;           // with skin_check: rebuild whatever the displacements
+};
+
+// The whole neighbour update in one cooperative launch (grid-stride phases,
+// grid_sync between them):
+//   0. (skin_check) site records and the skin criterion;
+//   1. cell grid from the current box (cells at least rc_v/2 thick, at most
+//      cell_cap of them), counts cleared;
+//   2. cell of every atom, counts;
+//   3. exclusive scan of the counts (per-block chunks, then block offsets);
+//   4. atoms into their cells;
+//   5. Verlet rows: one warp per center gathers every candidate of the 5x5x5
+//      stencil with float d^2 < (rc + skin)^2, sorts the row in shared memory
+//      (bitonic) and writes it with the reference positions of the next skin
+//      check.
+// Phases 1-5 run only when the rebuild flag is set; the flag is the same for
+// every block, so all of them return together.
+__global__ void __launch_bounds__(kRebuildThreads, 12)
+k_neighbor_rebuild(const RebuildArgs a)
+{
+  extern __shared__ int s_rows[];
+  __shared__ int s_tmp[kRebuildWarps];
+  __shared__ int s_grid[4];
+  NeighborState* st = a.st;
+  const int N = a.N;
+  const int tid = threadIdx.x;
+  const int gtid = blockIdx.x * blockDim.x + tid, nthreads = gridDim.x * blockDim.x;
+  const Box b = *a.box;
+  if (a.skin_check) {
+    skin_phase(N, b, a.pos, a.type, a.x0, st, a.sites, a.skin, a.rc_v, a.force);
+    grid_sync(a.gsync, st);
+  }
+  if (!*reinterpret_cast<volatile int*>(&st->rebuild)) return;
+
+  // 1. cell grid (every block derives the same one; block 0 records it)
+  if (tid == 0) {
     int nc[3];
-    double width = 0.5 * rc_v;
+    double width = 0.5 * a.rc_v;
     for (int pass = 0; pass < 64; ++pass) {
       long long total = 1;
       for (int d = 0; d < 3; ++d) {
@@ -83,165 +185,178 @@ __global__ void k_cell_setup(const Box* __restrict__ box, NeighborState* st, int
         nc[d] = b.pbc[d] ? max(1, static_cast<int>(floor(thick / width))) : 1;
         total *= nc[d];
       }
-      if (total <= cell_cap) break;
+      if (total <= a.cell_cap) break;
       width *= 1.25;
     }
-    (void)vol;
-    st->nc[0] = nc[0];
-    st->nc[1] = nc[1];
-    st->nc[2] = nc[2];
-    st->ncell = nc[0] * nc[1] * nc[2];
-    s_ncell = st->ncell;
+    s_grid[0] = nc[0];
+    s_grid[1] = nc[1];
+    s_grid[2] = nc[2];
+    s_grid[3] = nc[0] * nc[1] * nc[2];
+    if (blockIdx.x == 0) {
+      st->box_scale = 1.0;
+      for (int k = 0; k < 9; ++k) st->box_def[k] = (k % 4 == 0) ? 1.0 : 0.0;
+      st->nc[0] = nc[0];
+      st->nc[1] = nc[1];
+      st->nc[2] = nc[2];
+      st->ncell = s_grid[3];
+    }
   }
   __syncthreads();
-  for (int c = threadIdx.x; c < s_ncell; c += blockDim.x) cell_count[c] = 0;
-}
+  const int nc0 = s_grid[0], nc1 = s_grid[1], nc2 = s_grid[2], ncell = s_grid[3];
+  for (int c = gtid; c < ncell; c += nthreads) a.cell_count[c] = 0;
+  grid_sync(a.gsync, st);
 
-__global__ void k_cell_count(int N, const Box* __restrict__ box, const double* __restrict__ pos,
-                             const NeighborState* __restrict__ st, int* cell_of, int* cell_count)
-{
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (!st->rebuild || i >= N) return;
-  int cx, cy, cz;
-  cell_coords(*box, *st, pos[i], pos[N + i], pos[2 * N + i], cx, cy, cz);
-  const int c = (cz * st->nc[1] + cy) * st->nc[0] + cx;
-  cell_of[i] = c;
-  atomicAdd(cell_count + c, 1);
-}
-
-// Exclusive scan of the cell counts (one block); resets the counts to serve
-// as fill cursors.
-__global__ void k_cell_scan(const NeighborState* __restrict__ st, int* cell_count, int* cell_start)
-{
-  __shared__ int s_part[1024];
-  if (!st->rebuild) return;
-  const int n = st->ncell;
-  const int per = (n + blockDim.x - 1) / blockDim.x;
-  const int lo = threadIdx.x * per;
-  const int hi = min(n, lo + per);
-  int sum = 0;
-  for (int c = lo; c < hi; ++c) sum += cell_count[c];
-  s_part[threadIdx.x] = sum;
-  __syncthreads();
-  for (int off = 1; off < blockDim.x; off <<= 1) {
-    int v = threadIdx.x >= off ? s_part[threadIdx.x - off] : 0;
-    __syncthreads();
-    s_part[threadIdx.x] += v;
-    __syncthreads();
+  // 2. cells and counts
+  for (int i = gtid; i < N; i += nthreads) {
+    const double x = a.pos[i], y = a.pos[N + i], z = a.pos[2 * N + i];
+    const double sx = b.hinv[0] * x + b.hinv[1] * y + b.hinv[2] * z;
+    const double sy = b.hinv[3] * x + b.hinv[4] * y + b.hinv[5] * z;
+    const double sz = b.hinv[6] * x + b.hinv[7] * y + b.hinv[8] * z;
+    const int c = (wrapped_cell(sz, nc2, b.pbc[2]) * nc1 + wrapped_cell(sy, nc1, b.pbc[1])) * nc0 +
+                  wrapped_cell(sx, nc0, b.pbc[0]);
+    a.cell_of[i] = c;
+    atomicAdd(a.cell_count + c, 1);
   }
-  int run = s_part[threadIdx.x] - sum;
-  for (int c = lo; c < hi; ++c) {
-    const int k = cell_count[c];
-    cell_start[c] = run;
-    run += k;
-    cell_count[c] = 0;
+  grid_sync(a.gsync, st);
+
+  // 3. exclusive scan: block sums of contiguous chunks, then each block
+  //    scans its chunk from the sum of the chunks before it; the counts
+  //    are reset to serve as fill cursors
+  const int chunk = (ncell + gridDim.x - 1) / gridDim.x;
+  const int c0 = min(ncell, static_cast<int>(blockIdx.x) * chunk), c1 = min(ncell, c0 + chunk);
+  {
+    int sum = 0;
+    for (int c = c0 + tid; c < c1; c += blockDim.x) sum += a.cell_count[c];
+    sum = block_sum(sum, s_tmp);
+    if (tid == 0) a.part[blockIdx.x] = sum;
   }
-}
+  grid_sync(a.gsync, st);
+  {
+    int off = 0;
+    for (int q = tid; q < static_cast<int>(blockIdx.x); q += blockDim.x) off += a.part[q];
+    off = block_sum(off, s_tmp);
+    for (int base = c0; base < c1; base += blockDim.x) {
+      const int c = base + tid;
+      const int v = c < c1 ? a.cell_count[c] : 0;
+      int tile = 0;
+      const int incl = block_scan(v, s_tmp, &tile);
+      if (c < c1) {
+        a.cell_start[c] = off + incl - v;
+        a.cell_count[c] = 0;
+      }
+      off += tile;
+    }
+  }
+  grid_sync(a.gsync, st);
 
-__global__ void k_cell_fill(int N, const NeighborState* __restrict__ st, const int* __restrict__ cell_of,
-                            int* cell_count, const int* __restrict__ cell_start, int* cell_atoms)
-{
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (!st->rebuild || i >= N) return;
-  const int c = cell_of[i];
-  const int slot = atomicAdd(cell_count + c, 1);
-  cell_atoms[cell_start[c] + slot] = i;
-}
+  // 4. fill (the counts are the cell totals again afterwards)
+  for (int i = gtid; i < N; i += nthreads) {
+    const int c = a.cell_of[i];
+    const int slot = atomicAdd(a.cell_count + c, 1);
+    a.cell_atoms[a.cell_start[c] + slot] = i;
+  }
+  grid_sync(a.gsync, st);
 
-// One warp per center: gathers every candidate of the 5x5x5 stencil with
-// float d^2 < (rc + skin)^2, sorts the row in shared memory (bitonic), and
-// writes it with the reference positions for the next skin check.
-__global__ void k_verlet_build(int N, const Box* __restrict__ box, const Site* __restrict__ sites,
-                               NeighborState* st, const int* __restrict__ cell_count,
-                               const int* __restrict__ cell_start, const int* __restrict__ cell_atoms,
-                               const int* __restrict__ cell_of, int* nn_v, int* nl_v, int mn_v,
-                               int pow2, float cutoff_square, double* x0)
-{
-  extern __shared__ int s_rows[];
-  if (!st->rebuild) return;
-  const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  const int wpb = blockDim.x >> 5;
+  // 5. Verlet rows, one warp per center
+  const int lane = tid & 31, warp = tid >> 5;
+  const int pow2 = a.pow2;
   int* buf = s_rows + warp * (pow2 + 1);
   int* count = buf + pow2;
-  const Box b = *box;
-  for (int i = blockIdx.x * wpb + warp; i < N; i += gridDim.x * wpb) {
-  if (lane == 0) *count = 0;
-  __syncwarp();
-  const double xi = sites[i].x, yi = sites[i].y, zi = sites[i].z;
-  const int nc0 = st->nc[0], nc1 = st->nc[1], nc2 = st->nc[2];
-  const int ci = cell_of[i];
-  const int cx = ci % nc0, cy = (ci / nc0) % nc1, cz = ci / (nc0 * nc1);
-  // per direction: 5 wrapped offsets when the grid is wide enough, else
-  // every cell of that direction exactly once
-  const int span0 = (b.pbc[0] && nc0 >= 5) ? 5 : nc0;
-  const int span1 = (b.pbc[1] && nc1 >= 5) ? 5 : nc1;
-  const int span2 = (b.pbc[2] && nc2 >= 5) ? 5 : nc2;
-  const int ncand = span0 * span1 * span2;
-  for (int s = lane; s < ncand; s += 32) {
-    const int s0 = s % span0, s1 = (s / span0) % span1, s2 = s / (span0 * span1);
-    int gx = span0 == 5 ? cx + s0 - 2 : s0;
-    int gy = span1 == 5 ? cy + s1 - 2 : s1;
-    int gz = span2 == 5 ? cz + s2 - 2 : s2;
-    if (gx < 0) gx += nc0; else if (gx >= nc0) gx -= nc0;
-    if (gy < 0) gy += nc1; else if (gy >= nc1) gy -= nc1;
-    if (gz < 0) gz += nc2; else if (gz >= nc2) gz -= nc2;
-    const int c = (gz * nc1 + gy) * nc0 + gx;
-    const int start = cell_start[c];
-    const int cnt = cell_count[c];
-    for (int m = 0; m < cnt; ++m) {
-      const int j = cell_atoms[start + m];
-      if (j == i) continue;
-      float dx, dy, dz;
-      int tj;
-      site_displacement(b, sites, xi, yi, zi, j, dx, dy, dz, tj);
-      const float d2 = dx * dx + dy * dy + dz * dz;
-      if (d2 < cutoff_square) {
-        const int slot = atomicAdd(count, 1);
-        if (slot < pow2) buf[slot] = j;
-      }
-    }
-  }
-  __syncwarp();
-  const int total = *count;
-  const int used = min(total, pow2);
-  // bitonic sort of the smallest power of two that holds the row (padding
-  // INT_MAX), one compare-exchange pair per lane and pass
-  int p2 = 1;
-  while (p2 < used) p2 <<= 1;
-  for (int k = used + lane; k < p2; k += 32) buf[k] = INT_MAX;
-  __syncwarp();
-  for (int k = 2; k <= p2; k <<= 1) {
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      for (int q = lane; q < (p2 >> 1); q += 32) {
-        const int t = ((q & ~(j - 1)) << 1) | (q & (j - 1));   // lower index of the pair
-        const int u = t | j;
-        const int a = buf[t], c = buf[u];
-        const bool up = (t & k) == 0;
-        if ((a > c) == up) {
-          buf[t] = c;
-          buf[u] = a;
+  for (int i = blockIdx.x * kRebuildWarps + warp; i < N; i += gridDim.x * kRebuildWarps) {
+    if (lane == 0) *count = 0;
+    __syncwarp();
+    const double xi = a.sites[i].x, yi = a.sites[i].y, zi = a.sites[i].z;
+    // the site records may have been written by this launch (phase 0): plain
+    // loads, which the barriers order, not the read-only path
+    const int ci = a.cell_of[i];
+    const int cx = ci % nc0, cy = (ci / nc0) % nc1, cz = ci / (nc0 * nc1);
+    // per direction: 5 wrapped offsets when the grid is wide enough, else
+    // every cell of that direction exactly once
+    const int span0 = (b.pbc[0] && nc0 >= 5) ? 5 : nc0;
+    const int span1 = (b.pbc[1] && nc1 >= 5) ? 5 : nc1;
+    const int span2 = (b.pbc[2] && nc2 >= 5) ? 5 : nc2;
+    const int ncand = span0 * span1 * span2;
+    for (int s = lane; s < ncand; s += 32) {
+      const int s0 = s % span0, s1 = (s / span0) % span1, s2 = s / (span0 * span1);
+      int gx = span0 == 5 ? cx + s0 - 2 : s0;
+      int gy = span1 == 5 ? cy + s1 - 2 : s1;
+      int gz = span2 == 5 ? cz + s2 - 2 : s2;
+      if (gx < 0) gx += nc0; else if (gx >= nc0) gx -= nc0;
+      if (gy < 0) gy += nc1; else if (gy >= nc1) gy -= nc1;
+      if (gz < 0) gz += nc2; else if (gz >= nc2) gz -= nc2;
+      const int c = (gz * nc1 + gy) * nc0 + gx;
+      const int start = a.cell_start[c];
+      const int cnt = a.cell_count[c];
+      for (int m = 0; m < cnt; ++m) {
+        const int j = a.cell_atoms[start + m];
+        if (j == i) continue;
+        const double2 sa = reinterpret_cast<const double2*>(a.sites + j)[0];
+        const double2 sc = reinterpret_cast<const double2*>(a.sites + j)[1];
+        float dx, dy, dz;
+        int tj;
+        site_delta(b, sa, sc, xi, yi, zi, dx, dy, dz, tj);
+        const float d2 = dx * dx + dy * dy + dz * dz;
+        if (d2 < a.cutoff_square) {
+          const int slot = atomicAdd(count, 1);
+          if (slot < pow2) buf[slot] = j;
         }
       }
-      __syncwarp();
     }
-  }
-  const int keep = min(total, mn_v);
-  int* row = nl_v + static_cast<size_t>(i) * mn_v;
-  for (int k = lane; k < keep; k += 32) row[k] = buf[k];
-  if (lane == 0) {
-    nn_v[i] = keep;
-    if (total > mn_v) atomicOr(&st->overflow, 1);
-    atomicMax(&st->max_nn[0], total);
-    x0[i] = xi;
-    x0[N + i] = yi;
-    x0[2 * N + i] = zi;
-  }
-  __syncwarp();   // the row buffer is reused by this warp's next center
+    __syncwarp();
+    const int total = *count;
+    const int used = min(total, pow2);
+    // bitonic sort of the smallest power of two that holds the row (padding
+    // INT_MAX), one compare-exchange pair per lane and pass
+    int p2 = 1;
+    while (p2 < used) p2 <<= 1;
+    for (int k = used + lane; k < p2; k += 32) buf[k] = INT_MAX;
+    __syncwarp();
+    for (int k = 2; k <= p2; k <<= 1) {
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        for (int q = lane; q < (p2 >> 1); q += 32) {
+          const int t = ((q & ~(j - 1)) << 1) | (q & (j - 1));   // lower index of the pair
+          const int u = t | j;
+          const int x = buf[t], y = buf[u];
+          const bool up = (t & k) == 0;
+          if ((x > y) == up) {
+            buf[t] = y;
+            buf[u] = x;
+          }
+        }
+        __syncwarp();
+      }
+    }
+    const int keep = min(total, a.mn_v);
+    int* row = a.nl_v + static_cast<size_t>(i) * a.mn_v;
+    for (int k = lane; k < keep; k += 32) row[k] = buf[k];
+    if (lane == 0) {
+      a.nn_v[i] = keep;
+      if (total > a.mn_v) atomicOr(&st->overflow, 1);
+      atomicMax(&st->max_nn[0], total);
+      a.x0[i] = xi;
+      a.x0[N + i] = yi;
+      a.x0[2 * N + i] = zi;
+    }
+    __syncwarp();   // the row buffer is reused by this warp's next center
   }
 }
 
+size_t rebuild_smem(int pow2) { return sizeof(int) * kRebuildWarps * (pow2 + 1); }
+
 }  // namespace
+
+// Blocks of the cooperative rebuild: as many as can be resident at once (the
+// launch fails rather than oversubscribe), at most 16 per SM.
+int neighbor_rebuild_blocks(int pow2_v)
+{
+  int dev = 0, sms = 0, per_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_neighbor_rebuild, kRebuildThreads,
+                                                    rebuild_smem(pow2_v)) != cudaSuccess)
+    return 0;
+  return sms * std::min(per_sm, 16);
+}
 
 void launch_neighbor_update(Engine& e, int N, const double* pos, const int* type, bool force,
                             cudaStream_t stream, bool skin_done)
@@ -251,28 +366,50 @@ void launch_neighbor_update(Engine& e, int N, const double* pos, const int* type
     return;
   }
   NeighborBuffers& nb = e.nbr;
-  const int threads = 256;
-  const int grid = (N + threads - 1) / threads;
-  const double rc_v_d = static_cast<double>(e.model.rc_max) + e.skin;
-  if (!skin_done)
-    k_skin_check<<<grid, threads, 0, stream>>>(N, e.d_box, pos, type, nb.x0, e.d_nstate,
-                                                e.scratch.sites, e.skin, rc_v_d, force ? 1 : 0);
-  k_cell_setup<<<1, 1024, 0, stream>>>(e.d_box, e.d_nstate, nb.cell_count, rc_v_d, nb.cell_cap);
-  k_cell_count<<<grid, threads, 0, stream>>>(N, e.d_box, pos, e.d_nstate, nb.cell_of,
-                                             nb.cell_count);
-  k_cell_scan<<<1, 1024, 0, stream>>>(e.d_nstate, nb.cell_count, nb.cell_start);
-  k_cell_fill<<<grid, threads, 0, stream>>>(N, e.d_nstate, nb.cell_of, nb.cell_count,
-                                            nb.cell_start, nb.cell_atoms);
-  // cell counts were consumed as cursors; they now hold the per-cell totals again
-  // a grid of at most 16 CTAs per SM walks all centers, so the launch is
-  // cheap on the (common) steps whose skin check found nothing to rebuild
-  const int warps = 4;
-  const size_t smem = static_cast<size_t>(warps) * (nb.pow2_v + 1) * sizeof(int);
-  const int vblocks = std::min((N + warps - 1) / warps, 148 * 16);
-  k_verlet_build<<<vblocks, warps * 32, smem, stream>>>(
-    N, e.d_box, e.scratch.sites, e.d_nstate, nb.cell_count, nb.cell_start, nb.cell_atoms, nb.cell_of,
-    nb.nn_v, nb.nl_v, nb.mn_v, nb.pow2_v, static_cast<float>(rc_v_d * rc_v_d), nb.x0);
-  // the typewise radial / angular filter follows in k_filter_radial
+  if (nb.gsync_dirty) {
+    // a barrier gave up waiting in an earlier launch: restart its counters
+    cudaMemsetAsync(nb.gsync, 0, 2 * sizeof(unsigned), stream);
+    nb.gsync_dirty = false;
+  }
+  RebuildArgs a;
+  a.N = N;
+  a.box = e.d_box;
+  a.pos = pos;
+  a.type = type;
+  a.st = e.d_nstate;
+  a.sites = e.scratch.sites;
+  a.cell_count = nb.cell_count;
+  a.cell_start = nb.cell_start;
+  a.cell_atoms = nb.cell_atoms;
+  a.cell_of = nb.cell_of;
+  a.nn_v = nb.nn_v;
+  a.nl_v = nb.nl_v;
+  a.x0 = nb.x0;
+  a.gsync = nb.gsync;
+  a.part = nb.scan_part;
+  a.mn_v = nb.mn_v;
+  a.pow2 = nb.pow2_v;
+  a.cell_cap = nb.cell_cap;
+  a.skin = e.skin;
+  a.rc_v = static_cast<double>(e.model.rc_max) + e.skin;
+  a.cutoff_square = static_cast<float>(a.rc_v * a.rc_v);
+  a.skin_check = skin_done ? 0 : 1;
+  a.force = force ? 1 : 0;
+  // small systems take fewer blocks: cheaper barriers, nothing to share out
+  const int want = std::max(1, (N + kRebuildWarps - 1) / kRebuildWarps);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(static_cast<unsigned>(std::min(nb.rebuild_blocks, want)));
+  cfg.blockDim = dim3(kRebuildThreads);
+  cfg.dynamicSmemBytes = rebuild_smem(nb.pow2_v);
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k_neighbor_rebuild, a);
+  // the typewise radial / angular filter follows in k_filter_radial (which
+  // clears the rebuild flag)
 }
 
 }  // namespace nepx

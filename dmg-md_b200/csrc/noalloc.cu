@@ -86,6 +86,8 @@ size_t bytes_needed(const nepx::Engine& e, int n)
   c.take<int>(N * nb.mn_r);     // nl_r
   c.take<int>(N);               // nn_a
   c.take<int>(N * nb.mn_a);     // nl_a
+  c.take<unsigned>(2);                   // grid-barrier counters
+  c.take<int>(nb.rebuild_blocks);        // cell-scan partial sums
   c.take<int>(cells);           // cell_count
   c.take<int>(cells);           // cell_start
   c.take<int>(N);               // cell_atoms
@@ -187,6 +189,9 @@ extern "C" int nepx_compute_noalloc(nepx_t* h, const nepx_box* box, int n, const
     nb.nl_r = c.take<int>(N * nb.mn_r);
     nb.nn_a = c.take<int>(N);
     nb.nl_a = c.take<int>(N * nb.mn_a);
+    nb.gsync = c.take<unsigned>(2);
+    nb.scan_part = c.take<int>(nb.rebuild_blocks);
+    nb.gsync_dirty = false;
     nb.cell_count = c.take<int>(cells);
     nb.cell_start = c.take<int>(cells);
     nb.cell_atoms = c.take<int>(N);
@@ -205,6 +210,7 @@ extern "C" int nepx_compute_noalloc(nepx_t* h, const nepx_box* box, int n, const
     e.use_xr = false;
     // the array keeps the previous call's contents: clear the flags, rebuild
     cudaMemsetAsync(e.d_nstate, 0, sizeof(nepx::NeighborState), s);
+    cudaMemsetAsync(nb.gsync, 0, 2 * sizeof(unsigned), s);
     nepx::launch_set_box(e, b, s);
     nepx::launch_neighbor_update(e, n, d_pos, d_type, true, s);
     nepx::launch_force(e, n, d_pos, d_type, d_pe, d_force, d_virial, false, s);

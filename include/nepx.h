@@ -103,8 +103,8 @@ int nepx_compute(nepx_t* handle, const nepx_box* box, int n, const int* d_type,
  * memory: all per-call scratch comes from one 16 MiB static device array
  * inside the library, held by every GPU that loads it until the process
  * exits.  n is limited by what fits in those 16 MiB for the handle's
- * neighbour capacities (about 5 KB per atom for MN_radial 250: some
- * 2,500-3,000 atoms); larger n returns NEPX_ERR_CAPACITY.  The handle
+ * neighbour capacities (about 6.4 KB per atom for MN_radial 250: some
+ * 2,600 atoms); larger n returns NEPX_ERR_CAPACITY.  The handle
  * (nepx_create, max_atoms may be 1) supplies only the model parameters; the
  * handle's device must be current (else NEPX_ERR_ARG).  The ANN always runs
  * in FP32, whatever nepx_set_precision chose for the handle, and only the
