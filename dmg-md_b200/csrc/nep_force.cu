@@ -45,8 +45,11 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <utility>
+
 #include "engine.h"
 #include "harmonic_tables.h"
+#include "invariants.h"
 #include "tcgen05.cuh"
 
 namespace nepx {
@@ -128,9 +131,143 @@ struct Monomial {
 __constant__ Monomial c_mono[128];
 __constant__ int c_inv_start[kMaxInv + 1];
 
+// The same invariants for degrees <= 4 in registers: the monomial list of
+// invariant ID (invariants.h) unrolled at compile time, so s and the
+// derivatives a are register arrays of the 24 moment components of one n.
+// Value: sum over monomials of c s[i0] s[i1] s[i2] (s[i3]), in list order.
+template <int ID, int M>
+__device__ __forceinline__ float inv_term(const float (&s)[kNumLM])
+{
+  constexpr InvMono mo = inv_mono(ID, M);
+  float t = mo.c * s[mo.a] * s[mo.b] * s[mo.cc];
+  if constexpr (mo.d >= 0) t *= s[mo.d];
+  return t;
+}
+
+template <int ID, int... M>
+__device__ __forceinline__ float inv_value(const float (&s)[kNumLM],
+                                           std::integer_sequence<int, M...>)
+{
+  float acc = 0.0f;
+  ((acc += inv_term<ID, M>(s)), ...);
+  return acc;
+}
+
+template <int I>
+__device__ __forceinline__ float inv_value_of(const float (&s)[kNumLM])
+{
+  return inv_value<I>(s, std::make_integer_sequence<int, inv_count(I)>{});
+}
+
+// Derivative terms: for every factor Q of monomial M, f c times the other
+// factors in list order, added to a[factor Q].
+template <int ID, int M, int Q, int R>
+__device__ __forceinline__ float inv_grad_prod(const float (&s)[kNumLM], float t)
+{
+  constexpr InvMono mo = inv_mono(ID, M);
+  constexpr int nf = mo.d >= 0 ? 4 : 3;
+  if constexpr (R >= nf) {
+    return t;
+  } else {
+    constexpr int i = R == 0 ? mo.a : R == 1 ? mo.b : R == 2 ? mo.cc : mo.d;
+    if constexpr (R != Q) t *= s[i];
+    return inv_grad_prod<ID, M, Q, R + 1>(s, t);
+  }
+}
+
+template <int ID, int M, int Q>
+__device__ __forceinline__ void inv_grad_factor(const float (&s)[kNumLM], float (&a)[kNumLM],
+                                                float f)
+{
+  constexpr InvMono mo = inv_mono(ID, M);
+  constexpr int nf = mo.d >= 0 ? 4 : 3;
+  if constexpr (Q < nf) {
+    constexpr int i = Q == 0 ? mo.a : Q == 1 ? mo.b : Q == 2 ? mo.cc : mo.d;
+    a[i] += inv_grad_prod<ID, M, Q, 0>(s, f * mo.c);
+    inv_grad_factor<ID, M, Q + 1>(s, a, f);
+  }
+}
+
+template <int ID, int... M>
+__device__ __forceinline__ void inv_grad(const float (&s)[kNumLM], float (&a)[kNumLM], float f,
+                                         std::integer_sequence<int, M...>)
+{
+  (inv_grad_factor<ID, M, 0>(s, a, f), ...);
+}
+
+template <int I>
+__device__ __forceinline__ void inv_grad_of(const float (&s)[kNumLM], float (&a)[kNumLM], float f)
+{
+  inv_grad<I>(s, a, f, std::make_integer_sequence<int, inv_count(I)>{});
+}
+
+// runtime invariant id -> its unrolled form
+__device__ __forceinline__ float inv_value_id(int id, const float (&s)[kNumLM])
+{
+  switch (id) {
+    case 0: return inv_value_of<0>(s);
+    case 1: return inv_value_of<1>(s);
+    case 2: return inv_value_of<2>(s);
+    case 3: return inv_value_of<3>(s);
+    case 4: return inv_value_of<4>(s);
+    default: return inv_value_of<5>(s);
+  }
+}
+
+__device__ __forceinline__ void inv_grad_id(int id, const float (&s)[kNumLM], float (&a)[kNumLM],
+                                            float f)
+{
+  switch (id) {
+    case 0: inv_grad_of<0>(s, a, f); break;
+    case 1: inv_grad_of<1>(s, a, f); break;
+    case 2: inv_grad_of<2>(s, a, f); break;
+    case 3: inv_grad_of<3>(s, a, f); break;
+    case 4: inv_grad_of<4>(s, a, f); break;
+    default: inv_grad_of<5>(s, a, f); break;
+  }
+}
+
+// The 24 moments of one n from shared memory (16-byte aligned) and back.
+__device__ __forceinline__ void load24(const float* src, float (&v)[kNumLM])
+{
+#pragma unroll
+  for (int q = 0; q < kNumLM / 4; ++q) {
+    const float4 x = reinterpret_cast<const float4*>(src)[q];
+    v[4 * q] = x.x;
+    v[4 * q + 1] = x.y;
+    v[4 * q + 2] = x.z;
+    v[4 * q + 3] = x.w;
+  }
+}
+
+__device__ __forceinline__ void store24(float* dst, const float (&v)[kNumLM])
+{
+#pragma unroll
+  for (int q = 0; q < kNumLM / 4; ++q)
+    reinterpret_cast<float4*>(dst)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2],
+                                                    v[4 * q + 3]);
+}
+
 #include "zbl.cuh"
 
 __host__ __device__ constexpr int round4(int x) { return (x + 3) & ~3; }
+
+// Asynchronous copy of one 32-byte Site record into shared memory (two 16-byte
+// cp.async, cached in L1 like the plain loads they replace): a lane fetches
+// the next neighbour's site while it works on the current one, without
+// holding the record in registers.  Sites are 32-byte aligned (cudaMalloc
+// base, 32-byte records), the destination 16-byte aligned.
+__device__ __forceinline__ void site_fetch_async(unsigned dst, const Site* src)
+{
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(dst + 16u),
+               "l"(reinterpret_cast<const char*>(src) + 16)
+               : "memory");
+}
+__device__ __forceinline__ void async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// all but the most recent group of this thread's copies have landed
+__device__ __forceinline__ void async_wait_prior() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // Shared-memory layout of k_nep_fused (in floats; the tensor-core region in bytes).
 struct FusedLayout {
@@ -147,7 +284,15 @@ struct FusedLayout {
   // partials [4][APB]; per type, the bit mask of the CTA's centers of that
   // type [kMaxTypes]; the mbarrier, the TMEM address and a flag
   int tc_w, tc_wt, tc_q, tc_g, tc_e, tc_type, tc_bar, tc_misc;
+  // site prefetch slots of the angular sweep, two 32-byte records per thread
+  // (offset in floats), or -1
+  int pf;
 };
+
+// The descriptor builds that prefetch neighbour sites through shared memory:
+// the Verlet-row path at three or fewer CTAs per SM (the four-CTA build has no
+// shared memory to spare; explicit rows carry their displacements already).
+__host__ __device__ constexpr bool fused_prefetch(bool xr, int minb) { return !xr && minb <= 3; }
 
 // Shared memory one CTA may use with the ANN weights staged, when `minb`
 // CTAs share an SM (228 KB per SM, 1 KB of it reserved per CTA).
@@ -161,8 +306,10 @@ __host__ __device__ constexpr int fused_smem_budget(int minb) { return 228 * 102
 // of its A tile: rows past the stacked hidden units (or dim) are read from
 // whatever follows in shared memory and only feed accumulator rows the
 // epilogue never reads, so total_bytes covers the 128-row span of both A tiles.
+// prefetch: room for the site prefetch slots at the end (fused_prefetch).
 __host__ __device__ inline FusedLayout fused_layout(const ModelParams& p, int atoms_per_block,
-                                                   int kp, int budget, bool tc = false)
+                                                   int kp, int budget, bool tc = false,
+                                                   bool prefetch = false)
 {
   FusedLayout L;
   L.kpr = kp;
@@ -202,7 +349,8 @@ __host__ __device__ inline FusedLayout fused_layout(const ModelParams& p, int at
   L.wt = tables;
   L.atoms_base = tables + wsize;
   L.total_bytes = 4 * (L.atoms_base + atoms_per_block * L.per_atom);
-  if (tc || L.total_bytes > budget) {   // weights stay in global memory
+  const int pf_bytes = prefetch ? 2 * 32 * kBlock : 0;
+  if (tc || L.total_bytes + pf_bytes > budget) {   // weights stay in global memory
     L.wt = -1;
     L.atoms_base = tables;
     L.total_bytes = 4 * (L.atoms_base + atoms_per_block * L.per_atom);
@@ -212,6 +360,11 @@ __host__ __device__ inline FusedLayout fused_layout(const ModelParams& p, int at
     L.total_bytes = (L.total_bytes > need_w ? L.total_bytes : need_w);
     L.total_bytes = (L.total_bytes > need_wt ? L.total_bytes : need_wt);
     L.total_bytes = (L.total_bytes + 15) & ~15;
+  }
+  L.pf = -1;
+  if (prefetch) {
+    L.pf = (L.total_bytes + 15) / 16 * 4;
+    L.total_bytes = 4 * L.pf + pf_bytes;
   }
   return L;
 }
@@ -321,29 +474,52 @@ __device__ __forceinline__ void center_acoef(const ModelParams& p, const float* 
                                              const float* s_fp, int gl)
 {
   const int nR = p.nR, nA = p.nA;
-  for (int n = gl; n < nA; n += G) {
-    const float* sv = s_s + n * NLM;
-    float* av = s_a + n * NLM;
+  if constexpr (NLM == kNumLM) {
+    // degrees <= 4: moments and derivatives of one n in registers
     const float* fp = s_fp + nR;
-    int col = 0;
-    for (int Lq = 1; Lq <= p.L_max; ++Lq, ++col) {
-      const int st0 = Lq * Lq - 1;
-      const float f = fp[col * nA + n];
-      av[st0] = 2.0f * f * c_C3B[st0] * sv[st0];
-      for (int k = 1; k < 2 * Lq + 1; ++k) av[st0 + k] = 4.0f * f * c_C3B[st0 + k] * sv[st0 + k];
+    for (int n = gl; n < nA; n += G) {
+      float sv[kNumLM], av[kNumLM];
+      load24(s_s + n * NLM, sv);
+#pragma unroll
+      for (int Lq = 1; Lq <= 4; ++Lq) {
+        const int st0 = Lq * Lq - 1;
+        const bool on = Lq <= p.L_max;
+        const float f = on ? fp[(Lq - 1) * nA + n] : 0.0f;
+        av[st0] = on ? 2.0f * f * c_C3B[st0] * sv[st0] : 0.0f;
+#pragma unroll
+        for (int k = 1; k < 2 * Lq + 1; ++k)
+          av[st0 + k] = on ? 4.0f * f * c_C3B[st0 + k] * sv[st0 + k] : 0.0f;
+      }
+      int col = p.L_max;
+      for (int w = 0; w < p.num_inv; ++w, ++col)
+        inv_grad_id(p.inv_id[w], sv, av, fp[col * nA + n]);
+      store24(s_a + n * NLM, av);
     }
-    for (int lm = (p.L_max + 1) * (p.L_max + 1) - 1; lm < NLM; ++lm) av[lm] = 0.0f;
-    for (int w = 0; w < p.num_inv; ++w, ++col) {
-      const int id = p.inv_id[w];
-      const float f = fp[col * nA + n];
-      for (int m = c_inv_start[id]; m < c_inv_start[id + 1]; ++m) {
-        const Monomial mo = c_mono[m];
-        const int nf = mo.i[3] >= 0 ? 4 : 3;
-        for (int a = 0; a < nf; ++a) {
-          float t = f * mo.c;
-          for (int r = 0; r < nf; ++r)
-            if (r != a) t *= sv[mo.i[r]];
-          av[mo.i[a]] += t;
+  } else {
+    for (int n = gl; n < nA; n += G) {
+      const float* sv = s_s + n * NLM;
+      float* av = s_a + n * NLM;
+      const float* fp = s_fp + nR;
+      int col = 0;
+      for (int Lq = 1; Lq <= p.L_max; ++Lq, ++col) {
+        const int st0 = Lq * Lq - 1;
+        const float f = fp[col * nA + n];
+        av[st0] = 2.0f * f * c_C3B[st0] * sv[st0];
+        for (int k = 1; k < 2 * Lq + 1; ++k) av[st0 + k] = 4.0f * f * c_C3B[st0 + k] * sv[st0 + k];
+      }
+      for (int lm = (p.L_max + 1) * (p.L_max + 1) - 1; lm < NLM; ++lm) av[lm] = 0.0f;
+      for (int w = 0; w < p.num_inv; ++w, ++col) {
+        const int id = p.inv_id[w];
+        const float f = fp[col * nA + n];
+        for (int m = c_inv_start[id]; m < c_inv_start[id + 1]; ++m) {
+          const Monomial mo = c_mono[m];
+          const int nf = mo.i[3] >= 0 ? 4 : 3;
+          for (int a = 0; a < nf; ++a) {
+            float t = f * mo.c;
+            for (int r = 0; r < nf; ++r)
+              if (r != a) t *= sv[mo.i[r]];
+            av[mo.i[a]] += t;
+          }
         }
       }
     }
@@ -634,20 +810,24 @@ k_filter_radial(const ModelParams p, int N, const Box* __restrict__ box,
   int* rrow = nl_r + static_cast<size_t>(i) * mn_r;
   int* arow = nl_a + static_cast<size_t>(i) * mn_a;
   int cr = 0, ca = 0;
-  int j_next = 0;
+  // the next candidate's site and the index of the one after it in flight:
+  // no load inside the loop waits on another
+  int j_next = 0, j_after = 0;
   double2 sa_next = make_double2(0.0, 0.0), sc_next = make_double2(0.0, 0.0);
   if (gl < nv) {
     j_next = vrow[gl];
     site_load(sites, j_next, sa_next, sc_next);
   }
+  if (gl + G < nv) j_after = vrow[gl + G];
   for (int base = 0; base < nv_max; base += G) {
     const int k = base + gl;
     const int j = j_next;
     const double2 sa = sa_next, sc = sc_next;
     if (k + G < nv) {
-      j_next = vrow[k + G];
+      j_next = j_after;
       site_load(sites, j_next, sa_next, sc_next);
     }
+    if (k + 2 * G < nv) j_after = vrow[k + 2 * G];
     bool in_r = false, in_a = false;
     int t2 = 0;
     float x12 = 0.0f, y12 = 0.0f, z12 = 0.0f, d12_square = 0.0f, rc_radial = 1.0f;
@@ -753,7 +933,8 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
   // radial functions per moment sweep
   constexpr int CN = LMAX <= 4 ? (MINB >= 4 ? kChunkN4 : kChunkN) : 1;
   extern __shared__ __align__(128) float sm[];
-  const FusedLayout Lay = fused_layout(p, APB, KP, fused_smem_budget(MINB), TC);
+  constexpr bool PF = fused_prefetch(XR, MINB);
+  const FusedLayout Lay = fused_layout(p, APB, KP, fused_smem_budget(MINB), TC, PF);
   const int tid = threadIdx.x;
   const int T = p.T, nR = p.nR, nA = p.nA, kR = p.kR, kA = p.kA;
   const int dim = p.dim, H = p.H;
@@ -857,8 +1038,27 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
     float v[CN * NLM];
 #pragma unroll
     for (int q = 0; q < CN * NLM; ++q) v[q] = 0.0f;
+    // PF: the site of the lane's next edge is copied into the lane's other
+    // shared-memory slot while the current one is worked on; the index of the
+    // edge after that is loaded one iteration early, so no load waits on
+    // another inside the loop
+    const unsigned slots =
+      PF ? static_cast<unsigned>(__cvta_generic_to_shared(sm + Lay.pf)) + 64u * tid : 0u;
+    int j_next = 0;
+    if constexpr (PF) {
+      if (gl < na) site_fetch_async(slots, sites + arow[gl]);
+      async_commit();
+      if (gl + G < na) j_next = arow[gl + G];
+    }
     for (int base = 0; base < na_max; base += G) {
       const int k = base + gl;
+      const int par = (base / G) & 1;
+      if constexpr (PF) {
+        if (k + G < na) site_fetch_async(slots + 32u * (par ^ 1), sites + j_next);
+        async_commit();
+        if (k + 2 * G < na) j_next = arow[k + 2 * G];
+        async_wait_prior();
+      }
       if (k < na) {
         int t2;
         float dx, dy, dz;
@@ -868,6 +1068,9 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
           dy = e.y;
           dz = e.z;
           t2 = static_cast<int>(static_cast<unsigned>(__float_as_int(e.w)) >> kRowTypeShift);
+        } else if constexpr (PF) {
+          const double2* sl = reinterpret_cast<const double2*>(sm + Lay.pf + 16 * tid + 8 * par);
+          site_delta(b, sl[0], sl[1], xi, yi, zi, dx, dy, dz, t2);
         } else {
           site_displacement(b, sites, xi, yi, zi, arow[k], dx, dy, dz, t2);
         }
@@ -892,6 +1095,7 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
         });
       }
     }
+    if constexpr (PF) async_wait_all();
     const int at = reduce_scatter<G, CN * NLM>(v, gl);
     constexpr int share = CN * NLM / G;
     const int lim = (nA - nc < CN ? nA - nc : CN) * NLM;
@@ -902,28 +1106,51 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
   __syncwarp();
 
   // ---- 3. invariants, ANN, derivatives ---------------------------------------
-  for (int n = gl; n < nA; n += G) {
-    const float* s = s_s + n * NLM;
-    float* q = s_q + nR;
-    int col = 0;
-    for (int Lq = 1; Lq <= p.L_max; ++Lq, ++col) {
-      const int st0 = Lq * Lq - 1;
-      float val = 0.0f;
-      for (int k = 1; k < 2 * Lq + 1; ++k) val += c_C3B[st0 + k] * s[st0 + k] * s[st0 + k];
-      val *= 2.0f;
-      val += c_C3B[st0] * s[st0] * s[st0];
-      q[col * nA + n] = val;
-    }
-    for (int w = 0; w < p.num_inv; ++w, ++col) {
-      const int id = p.inv_id[w];
-      float acc = 0.0f;
-      for (int m = c_inv_start[id]; m < c_inv_start[id + 1]; ++m) {
-        const Monomial mo = c_mono[m];
-        float t = mo.c * s[mo.i[0]] * s[mo.i[1]] * s[mo.i[2]];
-        if (mo.i[3] >= 0) t *= s[mo.i[3]];
-        acc += t;
+  if constexpr (NLM == kNumLM) {
+    // degrees <= 4: the n's 24 moments in registers, monomials unrolled
+    for (int n = gl; n < nA; n += G) {
+      float sv[kNumLM];
+      load24(s_s + n * NLM, sv);
+      float* q = s_q + nR;
+#pragma unroll
+      for (int Lq = 1; Lq <= 4; ++Lq) {
+        if (Lq <= p.L_max) {
+          const int st0 = Lq * Lq - 1;
+          float val = 0.0f;
+#pragma unroll
+          for (int k = 1; k < 2 * Lq + 1; ++k) val += c_C3B[st0 + k] * sv[st0 + k] * sv[st0 + k];
+          val *= 2.0f;
+          val += c_C3B[st0] * sv[st0] * sv[st0];
+          q[(Lq - 1) * nA + n] = val;
+        }
       }
-      q[col * nA + n] = acc;
+      int col = p.L_max;
+      for (int w = 0; w < p.num_inv; ++w, ++col) q[col * nA + n] = inv_value_id(p.inv_id[w], sv);
+    }
+  } else {
+    for (int n = gl; n < nA; n += G) {
+      const float* s = s_s + n * NLM;
+      float* q = s_q + nR;
+      int col = 0;
+      for (int Lq = 1; Lq <= p.L_max; ++Lq, ++col) {
+        const int st0 = Lq * Lq - 1;
+        float val = 0.0f;
+        for (int k = 1; k < 2 * Lq + 1; ++k) val += c_C3B[st0 + k] * s[st0 + k] * s[st0 + k];
+        val *= 2.0f;
+        val += c_C3B[st0] * s[st0] * s[st0];
+        q[col * nA + n] = val;
+      }
+      for (int w = 0; w < p.num_inv; ++w, ++col) {
+        const int id = p.inv_id[w];
+        float acc = 0.0f;
+        for (int m = c_inv_start[id]; m < c_inv_start[id + 1]; ++m) {
+          const Monomial mo = c_mono[m];
+          float t = mo.c * s[mo.i[0]] * s[mo.i[1]] * s[mo.i[2]];
+          if (mo.i[3] >= 0) t *= s[mo.i[3]];
+          acc += t;
+        }
+        q[col * nA + n] = acc;
+      }
     }
   }
   __syncwarp();
@@ -1231,9 +1458,16 @@ k_gather(const ModelParams p, int N, const Box* __restrict__ box,
     // radial pairs: both site energies through the alpha coefficients
     const int nr = nn_r[i];
     const int* rrow = nl_r + static_cast<size_t>(i) * mn_r;
+    // the next edge's index is loaded one iteration early: the site and alpha
+    // loads of an edge then issue together at the top of its iteration
+    int jr_next = (!XR && gl < nr) ? rrow[gl] : 0;
     for (int k = gl; k < nr; k += G) {
       int j, t2;
       float dx, dy, dz;
+      const int jr = jr_next;
+      if constexpr (!XR) {
+        if (k + G < nr) jr_next = rrow[k + G];
+      }
       if constexpr (XR) {
         const float4 e = er[static_cast<size_t>(i) * mn_r + k];
         const unsigned bits = static_cast<unsigned>(__float_as_int(e.w));
@@ -1243,7 +1477,7 @@ k_gather(const ModelParams p, int N, const Box* __restrict__ box,
         dy = e.y;
         dz = e.z;
       } else {
-        j = rrow[k];
+        j = jr;
         site_displacement(b, sites, xi, yi, zi, j, dx, dy, dz, t2);
       }
       const float d = sqrtf(dx * dx + dy * dy + dz * dz);
@@ -1283,10 +1517,15 @@ k_gather(const ModelParams p, int N, const Box* __restrict__ box,
     const bool large_i = XR && large[i];
     const int zi_ = p.Z[t1];
     const float pow_zi = p.zbl ? powf(static_cast<float>(zi_), 0.23f) : 0.0f;
+    int ja_next = (!XR && gl < na) ? arow[gl] : 0;
     for (int k = gl; k < na; k += G) {
       int t2;
       float dx, dy, dz;
       float4 a12, a21;
+      const int ja = ja_next;
+      if constexpr (!XR) {
+        if (k + G < na) ja_next = arow[k + G];
+      }
       if constexpr (XR) {
         const float4 e = ea[static_cast<size_t>(i) * mn_a + k];
         const unsigned bits = static_cast<unsigned>(__float_as_int(e.w));
@@ -1326,7 +1565,7 @@ k_gather(const ModelParams p, int N, const Box* __restrict__ box,
           a21 = make_float4(fji.x, fji.y, fji.z, 0.0f);
         }
       } else {
-        const int j = arow[k];
+        const int j = ja;
         site_displacement(b, sites, xi, yi, zi, j, dx, dy, dz, t2);
         a12 = f12[static_cast<size_t>(i) * mn_a + k];
         // reverse slot: i inside j's ascending row
@@ -1440,8 +1679,9 @@ void launch_fused_t(Engine& e, int N, cudaStream_t s)
   NeighborBuffers& nb = e.nbr;
   constexpr int APB = kBlock / G;
   const int blocks = (N + APB - 1) / APB;
-  const size_t smem =
-    fused_layout(e.params, APB, (KM + 3) & ~3, fused_smem_budget(MINB), TC).total_bytes;
+  const size_t smem = fused_layout(e.params, APB, (KM + 3) & ~3, fused_smem_budget(MINB), TC,
+                                   fused_prefetch(XR, MINB))
+                        .total_bytes;
   k_nep_fused<G, NRM, KM, NAM, XR, LMAX, MINB, TC><<<blocks, kBlock, smem, s>>>(
     e.params, N, e.d_box, e.scratch.sites, e.d_nstate, nb.nn_v, nb.nl_v, nb.mn_v, nb.nn_r, nb.nl_r,
     nb.mn_r, nb.nn_a, nb.nl_a, nb.mn_a, e.xr.er, e.xr.ea, e.scratch.qrad, e.scratch.alpha,
@@ -1490,12 +1730,15 @@ void launch_f12_t(Engine& e, int N, cudaStream_t s)
 template <int G, int NRM, int KM, int NAM, int LMAX, int MINB, bool TC>
 void set_fused_smem_t(const ModelParams& p)
 {
-  const int bytes =
-    fused_layout(p, kBlock / G, (KM + 3) & ~3, fused_smem_budget(MINB), TC).total_bytes;
+  auto bytes = [&](bool xr) {
+    return fused_layout(p, kBlock / G, (KM + 3) & ~3, fused_smem_budget(MINB), TC,
+                        fused_prefetch(xr, MINB))
+      .total_bytes;
+  };
   cudaFuncSetAttribute(k_nep_fused<G, NRM, KM, NAM, false, LMAX, MINB, TC>,
-                       cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, bytes(false));
   cudaFuncSetAttribute(k_nep_fused<G, NRM, KM, NAM, true, LMAX, MINB, TC>,
-                       cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, bytes(true));
 }
 
 template <int G, int KM, int NAM, bool XR, int LMAX>
@@ -1562,9 +1805,11 @@ bool fused_occupancy_variants(const ModelParams& p) { return small_shape(p); }
 size_t fused_smem_bytes(const ModelParams& p)
 {
   if (high_degree(p))
-    return fused_layout(p, kBlock / kHighFusedGroup, basis_stride(p), fused_smem_budget(2))
+    return fused_layout(p, kBlock / kHighFusedGroup, basis_stride(p), fused_smem_budget(2), false,
+                        true)
       .total_bytes;
-  return fused_layout(p, kBlock / 4, basis_stride(p), fused_smem_budget(small_shape(p) ? 3 : 2))
+  return fused_layout(p, kBlock / 4, basis_stride(p), fused_smem_budget(small_shape(p) ? 3 : 2),
+                      false, true)
     .total_bytes;
 }
 
@@ -1600,10 +1845,11 @@ void set_fused_smem_limits(const ModelParams& p)
 size_t fused_tc_smem_bytes(const ModelParams& p)
 {
   if (high_degree(p))
-    return fused_layout(p, kBlock / kHighFusedGroup, basis_stride(p), fused_smem_budget(2), true)
+    return fused_layout(p, kBlock / kHighFusedGroup, basis_stride(p), fused_smem_budget(2), true,
+                        true)
       .total_bytes;
   return fused_layout(p, kBlock / 4, basis_stride(p), fused_smem_budget(small_shape(p) ? 3 : 2),
-                      true)
+                      true, true)
     .total_bytes;
 }
 
