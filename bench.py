@@ -146,14 +146,20 @@ def run_serving(args):
     for r in stream[:8]:
         srv.wait(submit(srv, dict(r, md_steps=0, mass=None, vel=None)))
     srv.close()
+    def new_server():
+        srv = nepx.Server(pot, max_atoms=arena, max_struct=slots)
+        srv.set_row_reuse(args.row_reuse == "on")
+        return srv
+
     # 1. saturation: every request queued at t = 0
-    srv = nepx.Server(pot, max_atoms=arena, max_struct=slots)
+    srv = new_server()
     t0 = time.perf_counter()
     tickets = [submit(srv, r) for r in stream]
     srv.drain()
     wall = time.perf_counter() - t0
     sat = [srv.wait(tk) for tk in tickets]
     st = srv.stats()
+    rows = srv.rows()
     srv.close()
     rate_sat = count / wall
     # 2. Poisson arrivals at 30%, 60% and 90% of the saturation rate: latency
@@ -161,7 +167,7 @@ def run_serving(args):
         rate = fraction * rate_sat
         rng = np.random.default_rng(seed)
         arrivals = np.cumsum(rng.exponential(1.0 / rate, count))
-        srv = nepx.Server(pot, max_atoms=arena, max_struct=slots)
+        srv = new_server()
         t0 = time.perf_counter()
         tickets = []
         for r, ta in zip(stream, arrivals):
@@ -222,6 +228,10 @@ def run_serving(args):
         "atom_steps_per_s": served_rate,
         "saturation": {"wall_s": wall, "steps": st["steps"], "mean_resident_atoms":
                        st["mean_atoms"], "mean_resident_structs": st["mean_structs"]},
+        "row_reuse": {"on": args.row_reuse == "on", "candidate_builds": rows["builds"],
+                      "kept_center_steps": rows["kept"],
+                      "reused_fraction": (1.0 - rows["builds"] / rows["kept"])
+                      if rows["kept"] else None},
         "latency_ms": sweep[1],   # Poisson arrivals at 60% of saturation
         "latency_sweep_ms": sweep,
         "plain_fp32_one_at_a_time": {"atom_steps_per_s": plain_rate, "requests": len(sample),
@@ -851,6 +861,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the other workloads, the NVE drift and the serving sample")
     ap.add_argument("--serving-sample", type=int, default=5000)
+    ap.add_argument("--row-reuse", default="on", choices=["on", "off"],
+                    help="serving: MD segments keep Verlet candidates between steps")
     ap.add_argument("--precision", default="mixed", choices=["fp32", "mixed", "mixed_bf16"],
                     help="ANN precision of the serving workload")
     args = ap.parse_args()
@@ -962,11 +974,12 @@ def main():
             if args.serving_sample > 0:
                 sargs = argparse.Namespace(requests=args.serving_sample, arena=args.arena,
                                            plain_sample=max(20, args.serving_sample // 20),
-                                           precision="mixed")
+                                           precision="mixed", row_reuse=args.row_reuse)
                 sv = run_serving(sargs)
                 serving = {k: sv[k] for k in ("value", "unit", "atom_steps_per_s", "latency_ms",
                                               "latency_sweep_ms", "plain_fp32_one_at_a_time",
-                                              "batched_over_plain", "config", "saturation")}
+                                              "batched_over_plain", "config", "saturation",
+                                              "row_reuse")}
         T_last = float(rows[-1, 0]) if rows is not None else None
         line = {"metric": "atom-steps/s", "value": value, "unit": "atom-steps/s",
                 "n_gpus": world, "steps": K, "warmup": args.warmup,

@@ -43,6 +43,7 @@ struct StructInfo {
   int off, n;
   int nc[3];      // cell grid of a large structure's candidate search (nc[0] = 0: scan all atoms)
   int cell_base;  // first cell of this structure in the batch's cell arrays
+  int keep;       // 1: keeps Verlet candidates across steps (cells sized for rc + skin)
 };
 
 // Packed neighbour of an explicit row: index j (low 28 bits) and type (high 4).
@@ -61,6 +62,7 @@ struct NeighborState {
   int box_error;       // the device box became unsupported (small in one direction, >10 rc in another)
   int ann_error;       // a tensor-core ANN tile gave up waiting for its MMAs
   int sync_error;      // the neighbour rebuild gave up waiting at a grid-wide barrier
+  unsigned xr_builds;  // centers whose batch Verlet candidates were built (wraps)
   double box_scale;    // product of isotropic box factors since the last build (1 = none)
   double box_def[9];   // product of general box deformations since the last build (I = none)
 };

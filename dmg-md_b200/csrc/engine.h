@@ -43,6 +43,28 @@ struct ForceScratch {
   double* tune_out = nullptr;  // [13 N] throw-away outputs of the autotuning calls
 };
 
+// Verlet candidates of the explicit rows of a batch (the server's MD
+// segments): per center, the structure-local neighbours (small boxes: with
+// their image) within the cutoff plus the skin at the last build, in the
+// order of the rows.  Each step filters them into the rows; a structure
+// rebuilds them when it is new or one of its atoms has moved more than
+// skin / 2 since the build.  sflag == nullptr: off (every row built afresh).
+struct BatchVerlet {
+  const int* sflag = nullptr;      // per structure: bit 1 keeps candidates, bit 2 new (build)
+  const double* dmax2 = nullptr;   // per structure: largest squared displacement since the build
+  double half_skin2 = 0.0;         // (skin / 2)^2
+  float skin = 0.0f;
+  int mn = 0;                      // candidates per center
+  int* vcnt = nullptr;             // [N] candidates of each center
+  int* vrow = nullptr;             // [N][mn]
+  double* x0 = nullptr;            // [3][N] positions at the build
+};
+
+// Candidate code of a small-box structure: local index (20 bits) and the
+// image (4 bits per direction).
+constexpr int kCandIndexBits = 20;
+constexpr int kCandMaxImages = 16;
+
 // Explicit-row state: the small-box path (one structure, rebuilt from the
 // device box at every call) and the batched path (many structures).
 struct ExplicitRows {
@@ -64,6 +86,7 @@ struct ExplicitRows {
   // hold each neighbour once, ascending, and its angular forces take the
   // directed-f12 scheme of the large-box path
   unsigned char* large = nullptr;
+  BatchVerlet bv;
 };
 
 struct Engine {
@@ -153,8 +176,9 @@ size_t served_bytes_per_struct();
 std::string engine_enable_xr(Engine& e, int max_struct);
 
 // Cell grids of the large structures of a batch: each gets cells at least
-// rc thick (at most cell_cap in total, else it scans all its atoms); returns
-// the number of cells.  Structures are described by si[0..n).
+// rc / 2 thick, (rc + skin) / 2 where it keeps Verlet candidates (at most
+// cell_cap in total, else it scans all its atoms); returns the number of
+// cells.  Structures are described by si[0..n).
 int assign_cells(const Engine& e, StructInfo* si, int n);
 // Cells of a structure's grid (0: small, or too few cells for the stencil,
 // so its rows scan all its atoms); nc_out (may be null) gets the grid.
@@ -169,6 +193,11 @@ int box_kind(const Engine& e, const Box& b);
 // from_box mode first the single StructInfo from the device box.
 void launch_explicit_rows(Engine& e, int N, const double* pos, const int* type,
                           cudaStream_t stream);
+// True when a structure can keep Verlet candidates: every periodic width at
+// least 4 skins (its skin check takes minimum-image displacements) and, for
+// a small box, candidates that fit the code (local index below 2^20, at most
+// 16 images per direction).
+bool verlet_encodable(const StructInfo& s, double skin);
 
 // Neighbour indices of the explicit rows (which = 0 radial, 1 angular) into
 // caller arrays nn[n], nl[n][mn] (row-major), as for the Verlet-path rows.

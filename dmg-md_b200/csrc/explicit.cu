@@ -81,6 +81,25 @@ __device__ __forceinline__ void mic_small_box(const StructInfo& s, float& x12, f
   z12 = e[6] * sx12 + e[7] * sy12 + e[8] * sz12;
 }
 
+// Displacement from a center (float position) to atom j (double position) at
+// image (ia, ib, ic) of the expanded box: the reference's small-box
+// arithmetic (nep_small_box.cuh:134-143).  Shared by the row builder and the
+// Verlet-candidate filter, so both produce the same float values.
+__device__ __forceinline__ void small_box_delta(const StructInfo& s, float x1, float y1,
+                                                float z1, double xj, double yj, double zj,
+                                                int ia, int ib, int ic, float& x12, float& y12,
+                                                float& z12)
+{
+  const float* fh = s.box.fh;
+  const float d0 = fh[0] * ia + fh[1] * ib + fh[2] * ic;
+  const float d1 = fh[3] * ia + fh[4] * ib + fh[5] * ic;
+  const float d2 = fh[6] * ia + fh[7] * ib + fh[8] * ic;
+  x12 = xj + d0 - x1;
+  y12 = yj + d1 - y1;
+  z12 = zj + d2 - z1;
+  mic_small_box(s, x12, y12, z12);
+}
+
 __device__ __forceinline__ float4 row_entry(float x, float y, float z, int j, int t)
 {
   return make_float4(x, y, z, __int_as_float(j | (t << kRowTypeShift)));
@@ -94,7 +113,7 @@ k_rows_explicit(const ModelParams p, int total, const StructInfo* __restrict__ s
                 const int* __restrict__ cell_count, const int* __restrict__ cell_start,
                 const int* __restrict__ cell_atoms, const int* __restrict__ cell_of, int p2r,
                 const Site* __restrict__ sites, unsigned char* __restrict__ large, int mark_large,
-                NeighborState* st)
+                const BatchVerlet bv, NeighborState* st)
 {
   extern __shared__ int s_rows[];   // per warp: p2r row slots + a counter
   const int lane = threadIdx.x & 31;
@@ -111,6 +130,15 @@ k_rows_explicit(const ModelParams p, int total, const StructInfo* __restrict__ s
     const int off = s.off, n = s.n;
     const int t1 = type[i];
     const float rr1 = p.rc_r[t1], ra1 = p.rc_a[t1];
+    // a structure that keeps Verlet candidates: (re)build them here when it is
+    // new or has moved more than skin / 2 since the build; its rows come from
+    // them in k_rows_verlet
+    const int sf = bv.sflag ? bv.sflag[lo] : 0;
+    const bool keep = (sf & 2) != 0;
+    if (keep && !(sf & 4) && bv.dmax2[lo] <= bv.half_skin2) continue;
+    auto cand_cut = [&](int tj) {
+      return fmaxf((rr1 + p.rc_r[tj]) * 0.5f, (ra1 + p.rc_a[tj]) * 0.5f) + bv.skin;
+    };
     float4* rrow = er + static_cast<size_t>(i) * mn_r;
     float4* arow = ea + static_cast<size_t>(i) * mn_a;
     int cr = 0, ca = 0;
@@ -127,8 +155,8 @@ k_rows_explicit(const ModelParams p, int total, const StructInfo* __restrict__ s
         int tj;
         site_displacement(b, sites, xi, yi, zi, j, x12, y12, z12, tj);
         const float d12_square = x12 * x12 + y12 * y12 + z12 * z12;
-        const float rc_radial = (rr1 + p.rc_r[tj]) * 0.5f;
-        if (d12_square < rc_radial * rc_radial) {
+        const float rcut = keep ? cand_cut(tj) : (rr1 + p.rc_r[tj]) * 0.5f;
+        if (d12_square < rcut * rcut) {
           const int slot = atomicAdd(count, 1);
           if (slot < p2r) buf[slot] = j;
         }
@@ -255,6 +283,21 @@ k_rows_explicit(const ModelParams p, int total, const StructInfo* __restrict__ s
           }
         }
       }
+      if (keep) {
+        // ascending candidates, structure-local
+        int* vr = bv.vrow + static_cast<size_t>(i) * bv.mn;
+        for (int k = lane; k < used && k < bv.mn; k += 32) vr[k] = buf[k] - off;
+        if (lane == 0) {
+          bv.vcnt[i] = min(found, bv.mn);
+          if (found > bv.mn || found > p2r) atomicOr(&st->overflow, 1);
+          bv.x0[i] = xi;
+          bv.x0[total + i] = yi;
+          bv.x0[2 * total + i] = zi;
+          atomicAdd(&st->xr_builds, 1u);
+        }
+        __syncwarp();   // the buffer is reused by this warp's next center
+        continue;
+      }
       // ascending radial row; the angular row is its subset inside the angular cutoff
       for (int k0 = 0; k0 < used; k0 += 32) {
         const int k = k0 + lane;
@@ -280,10 +323,63 @@ k_rows_explicit(const ModelParams p, int total, const StructInfo* __restrict__ s
       }
       cr = found;
       __syncwarp();   // the buffer is reused by this warp's next center
+    } else if (keep) {
+      // candidates (j, image) within the cutoff plus the skin, in row order:
+      // j ascending, then the images; count per lane, scan, then write
+      const float x1 = pos[i], y1 = pos[total + i], z1 = pos[2 * total + i];
+      int* vr = bv.vrow + static_cast<size_t>(i) * bv.mn;
+      int cv = 0;
+      for (int base = 0; base < n; base += 32) {
+        const int j = off + base + lane;
+        const bool valid = base + lane < n;
+        const float rcut = cand_cut(valid ? type[j] : 0);
+        const double xj = valid ? pos[j] : 0.0, yj = valid ? pos[total + j] : 0.0,
+                     zj = valid ? pos[2 * total + j] : 0.0;
+        const unsigned jl = static_cast<unsigned>(j - off);
+        int wv = 0;
+        for (int pass = 0; pass < 2; ++pass) {
+          int kv = 0;
+          if (valid) {
+            for (int ia = 0; ia < s.ncell[0]; ++ia)
+              for (int ib = 0; ib < s.ncell[1]; ++ib)
+                for (int ic = 0; ic < s.ncell[2]; ++ic) {
+                  if (ia == 0 && ib == 0 && ic == 0 && j == i) continue;   // self
+                  float x12, y12, z12;
+                  small_box_delta(s, x1, y1, z1, xj, yj, zj, ia, ib, ic, x12, y12, z12);
+                  if (x12 * x12 + y12 * y12 + z12 * z12 < rcut * rcut) {
+                    if (pass == 1 && wv + kv < bv.mn)
+                      vr[wv + kv] = static_cast<int>(
+                        jl | (static_cast<unsigned>(ia) << kCandIndexBits) |
+                        (static_cast<unsigned>(ib) << (kCandIndexBits + 4)) |
+                        (static_cast<unsigned>(ic) << (kCandIndexBits + 8)));
+                    ++kv;
+                  }
+                }
+          }
+          if (pass == 0) {
+            int sv = kv;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+              const int u = __shfl_up_sync(kFull, sv, o);
+              if (lane >= o) sv += u;
+            }
+            wv = cv + sv - kv;
+            cv += __shfl_sync(kFull, sv, 31);
+          }
+        }
+      }
+      if (lane == 0) {
+        bv.vcnt[i] = min(cv, bv.mn);
+        if (cv > bv.mn) atomicOr(&st->overflow, 1);
+        bv.x0[i] = pos[i];
+        bv.x0[total + i] = pos[total + i];
+        bv.x0[2 * total + i] = pos[2 * total + i];
+        atomicAdd(&st->xr_builds, 1u);
+      }
+      continue;
     } else {
       // the small-box arithmetic: float center, double image position
       const float x1 = pos[i], y1 = pos[total + i], z1 = pos[2 * total + i];
-      const float* fh = s.box.fh;
       for (int base = 0; base < n; base += 32) {
         const int j = off + base + lane;
         const bool valid = base + lane < n;
@@ -301,13 +397,8 @@ k_rows_explicit(const ModelParams p, int total, const StructInfo* __restrict__ s
               for (int ib = 0; ib < s.ncell[1]; ++ib)
                 for (int ic = 0; ic < s.ncell[2]; ++ic) {
                   if (ia == 0 && ib == 0 && ic == 0 && j == i) continue;   // self
-                  const float d0 = fh[0] * ia + fh[1] * ib + fh[2] * ic;
-                  const float d1 = fh[3] * ia + fh[4] * ib + fh[5] * ic;
-                  const float d2 = fh[6] * ia + fh[7] * ib + fh[8] * ic;
-                  float x12 = xj + d0 - x1;
-                  float y12 = yj + d1 - y1;
-                  float z12 = zj + d2 - z1;
-                  mic_small_box(s, x12, y12, z12);
+                  float x12, y12, z12;
+                  small_box_delta(s, x1, y1, z1, xj, yj, zj, ia, ib, ic, x12, y12, z12);
                   const float d12_square = x12 * x12 + y12 * y12 + z12 * z12;
                   if (d12_square < rc_radial * rc_radial) {
                     if (pass == 1 && wr + kr < mn_r)
@@ -344,6 +435,98 @@ k_rows_explicit(const ModelParams p, int total, const StructInfo* __restrict__ s
       nn_r[i] = min(cr, mn_r);
       nn_a[i] = min(ca, mn_a);
       large[i] = mark_large && !s.small ? 1 : 0;
+      if (cr > mn_r) atomicOr(&st->overflow, 2);
+      if (ca > mn_a) atomicOr(&st->overflow, 4);
+      atomicMax(&st->max_nn[1], cr);
+      atomicMax(&st->max_nn[2], ca);
+      atomicMax(&st->call_nn[0], cr);
+      atomicMax(&st->call_nn[1], ca);
+    }
+  }
+}
+
+// Rows of the centers whose structure keeps Verlet candidates: one warp per
+// center filters its candidates (in row order) with the predicates and the
+// arithmetic of k_rows_explicit, so the rows equal a fresh build's bit for
+// bit while no atom of the structure has moved more than skin / 2 since the
+// candidates were built.  Radial and angular rows are written in order by
+// warp ballot + popcount.
+__global__ void __launch_bounds__(256)
+k_rows_verlet(const ModelParams p, int total, const StructInfo* __restrict__ si,
+              const int* __restrict__ soff, int S, const double* __restrict__ pos,
+              const int* __restrict__ type, int* __restrict__ nn_r, float4* __restrict__ er,
+              int mn_r, int* __restrict__ nn_a, float4* __restrict__ ea, int mn_a,
+              const Site* __restrict__ sites, unsigned char* __restrict__ large,
+              const BatchVerlet bv, NeighborState* st)
+{
+  const int lane = threadIdx.x & 31;
+  const int wpb = blockDim.x >> 5;
+  const unsigned below = (1u << lane) - 1u;
+  for (int i = blockIdx.x * wpb + (threadIdx.x >> 5); i < total; i += gridDim.x * wpb) {
+    int lo = 0, hi = S - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (soff[mid] <= i) lo = mid; else hi = mid - 1;
+    }
+    if (!(bv.sflag[lo] & 2)) continue;
+    const StructInfo& s = si[lo];
+    const int off = s.off;
+    const int t1 = type[i];
+    const float rr1 = p.rc_r[t1], ra1 = p.rc_a[t1];
+    float4* rrow = er + static_cast<size_t>(i) * mn_r;
+    float4* arow = ea + static_cast<size_t>(i) * mn_a;
+    const int* vr = bv.vrow + static_cast<size_t>(i) * bv.mn;
+    const int nv = bv.vcnt[i];
+    int cr = 0, ca = 0;
+    const double xi = pos[i], yi = pos[total + i], zi = pos[2 * total + i];
+    const float x1 = static_cast<float>(xi), y1 = static_cast<float>(yi),
+                z1 = static_cast<float>(zi);
+    for (int k0 = 0; k0 < nv; k0 += 32) {
+      const int k = k0 + lane;
+      bool in_r = false, in_a = false;
+      float4 entry = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      if (k < nv) {
+        const unsigned code = static_cast<unsigned>(vr[k]);
+        int j, t2;
+        float x12, y12, z12;
+        if (!s.small) {
+          j = off + static_cast<int>(code);
+          site_displacement(s.box, sites, xi, yi, zi, j, x12, y12, z12, t2);
+        } else {
+          j = off + static_cast<int>(code & ((1u << kCandIndexBits) - 1u));
+          const int ia = static_cast<int>((code >> kCandIndexBits) & 15u);
+          const int ib = static_cast<int>((code >> (kCandIndexBits + 4)) & 15u);
+          const int ic = static_cast<int>(code >> (kCandIndexBits + 8));
+          t2 = type[j];
+          small_box_delta(s, x1, y1, z1, pos[j], pos[total + j], pos[2 * total + j], ia, ib,
+                          ic, x12, y12, z12);
+        }
+        const float d12_square = x12 * x12 + y12 * y12 + z12 * z12;
+        const float rc_radial = (rr1 + p.rc_r[t2]) * 0.5f;
+        const float rc_angular = (ra1 + p.rc_a[t2]) * 0.5f;
+        in_r = d12_square < rc_radial * rc_radial;
+        // large structures: the angular row is the radial row's subset (as
+        // k_rows_explicit builds it); small boxes test both cutoffs apart
+        in_a = (s.small || in_r) && d12_square < rc_angular * rc_angular;
+        entry = row_entry(x12, y12, z12, j, t2);
+      }
+      const unsigned mr = __ballot_sync(kFull, in_r);
+      const unsigned ma = __ballot_sync(kFull, in_a);
+      if (in_r) {
+        const int at = cr + __popc(mr & below);
+        if (at < mn_r) rrow[at] = entry;
+      }
+      if (in_a) {
+        const int at = ca + __popc(ma & below);
+        if (at < mn_a) arow[at] = entry;
+      }
+      cr += __popc(mr);
+      ca += __popc(ma);
+    }
+    if (lane == 0) {
+      nn_r[i] = min(cr, mn_r);
+      nn_a[i] = min(ca, mn_a);
+      large[i] = s.small ? 0 : 1;
       if (cr > mn_r) atomicOr(&st->overflow, 2);
       if (ca > mn_a) atomicOr(&st->overflow, 4);
       atomicMax(&st->max_nn[1], cr);
@@ -463,7 +646,9 @@ cudaError_t dalloc(T*& ptr, size_t count)
 int structure_cells(const Engine& e, const StructInfo& s, int* nc_out)
 {
   if (s.small) return 0;
-  const double rc = e.model.rc_radial_max;
+  // cells at least half the candidate radius: the cutoff, plus the skin for
+  // a structure that keeps Verlet candidates
+  const double rc = s.keep ? e.model.rc_max + e.skin : e.model.rc_radial_max;
   int nc[3], cells = 1;
   for (int d = 0; d < 3; ++d) {
     const double* r = s.box.hinv + 3 * d;
@@ -554,15 +739,37 @@ void launch_explicit_rows(Engine& e, int N, const double* pos, const int* type,
     k_xcell_fill<<<(N + threads - 1) / threads, threads, 0, stream>>>(
       N, x.cell_of, x.cell_count, x.cell_start, x.cell_atoms);
   }
+  const bool verlet = !x.from_box && x.bv.sflag != nullptr;
   int p2r = 1;
-  while (p2r < e.nbr.mn_r) p2r <<= 1;
+  while (p2r < std::max(e.nbr.mn_r, verlet ? x.bv.mn : 0)) p2r <<= 1;
   const int warps = threads / 32;
   const int blocks = std::min((N + warps - 1) / warps, 148 * 8);
   const size_t smem = sizeof(int) * warps * (p2r + 1);
+  BatchVerlet bv = x.bv;
+  if (!verlet) bv.sflag = nullptr;
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(k_rows_explicit, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(smem));
   k_rows_explicit<<<blocks, threads, smem, stream>>>(
     e.params, N, x.d_si, x.d_soff, x.n_struct, pos, type, e.nbr.nn_r, x.er, e.nbr.mn_r,
     e.nbr.nn_a, x.ea, e.nbr.mn_a, x.cell_count, x.cell_start, x.cell_atoms, x.cell_of, p2r,
-    e.scratch.sites, x.large, x.from_box ? 0 : 1, e.d_nstate);
+    e.scratch.sites, x.large, x.from_box ? 0 : 1, bv, e.d_nstate);
+  if (verlet)
+    k_rows_verlet<<<blocks, threads, 0, stream>>>(
+      e.params, N, x.d_si, x.d_soff, x.n_struct, pos, type, e.nbr.nn_r, x.er, e.nbr.mn_r,
+      e.nbr.nn_a, x.ea, e.nbr.mn_a, e.scratch.sites, x.large, bv, e.d_nstate);
+}
+
+bool verlet_encodable(const StructInfo& s, double skin)
+{
+  for (int d = 0; d < 3; ++d) {
+    const double* r = s.box.hinv + 3 * d;
+    const double thick = 1.0 / std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    if (s.box.pbc[d] && thick < 4.0 * skin) return false;
+  }
+  if (!s.small) return true;
+  return s.n <= (1 << kCandIndexBits) && s.ncell[0] <= kCandMaxImages &&
+         s.ncell[1] <= kCandMaxImages && s.ncell[2] <= kCandMaxImages;
 }
 
 void launch_explicit_row_indices(const Engine& e, int which, int n, int* nn, int* nl, int mn,

@@ -65,7 +65,8 @@ __global__ void k_arena_build(int T, int S, const int* __restrict__ soff,
                               const double* __restrict__ o_force, int t_in,
                               const double* __restrict__ in_d, const int* __restrict__ in_type,
                               int* n_type, int* n_sid, double* n_pos, double* n_vel,
-                              double* n_mass, double* n_force)
+                              double* n_mass, double* n_force, const int* __restrict__ o_vcnt,
+                              const double* __restrict__ o_x0, int* n_vcnt, double* n_x0)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= T) return;
@@ -77,29 +78,60 @@ __global__ void k_arena_build(int T, int S, const int* __restrict__ soff,
     const int j = sr.x + local;
     n_type[i] = o_type[j];
     n_mass[i] = o_mass[j];
+    n_vcnt[i] = o_vcnt[j];
     for (int d = 0; d < 3; ++d) {
       n_pos[d * T + i] = o_pos[d * t_old + j];
       n_vel[d * T + i] = o_vel[d * t_old + j];
       n_force[d * T + i] = o_force[d * t_old + j];
+      n_x0[d * T + i] = o_x0[d * t_old + j];
     }
   } else {
     const int j = sr.y + local;
     n_type[i] = in_type[j];
     n_mass[i] = in_d[6 * t_in + j];
+    n_vcnt[i] = 0;
     for (int d = 0; d < 3; ++d) {
       n_pos[d * T + i] = in_d[d * t_in + j];
       n_vel[d * T + i] = in_d[(3 + d) * t_in + j];
       n_force[d * T + i] = 0.0;
+      n_x0[d * T + i] = 0.0;
     }
   }
 }
 
+// Verlet candidates of the surviving structures that keep them (flag bit 1)
+// into the new arena: one warp per atom, coalesced over the row.
+__global__ void k_arena_rows(int T, int S, const int* __restrict__ soff,
+                             const int2* __restrict__ src, const int* __restrict__ sflag,
+                             const int* __restrict__ n_vcnt, const int* __restrict__ o_vrow,
+                             int* __restrict__ n_vrow, int mn)
+{
+  const int lane = threadIdx.x & 31;
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (i >= T) return;
+  const int s = find_struct(soff, S, i);
+  const int2 sr = src[s];
+  if (sr.x < 0 || !(sflag[s] & 2)) return;
+  const int j = sr.x + (i - soff[s]);
+  const int n = n_vcnt[i];
+  const int* from = o_vrow + static_cast<size_t>(j) * mn;
+  int* to = n_vrow + static_cast<size_t>(i) * mn;
+  for (int k = lane; k < n; k += 32) to[k] = from[k];
+}
+
 // First half kick and drift of the atoms whose structure steps (flag bit 0),
 // wrapped into the structure's box: the arithmetic of md.cu k_vv1 (NVE).
+// Structures that keep Verlet candidates (bit 1) record the largest squared
+// displacement of their atoms since the build (dmax2, as the ordered bits of
+// a non-negative double); in a large box by minimum image, exact while an
+// atom has moved less than half the box's thinnest periodic width, which
+// holds for the boxes that keep candidates (at least 4 skins thick: an atom
+// is caught at skin / 2).
 __global__ void k_vv1_batch(int T, const int* __restrict__ sid, const int* __restrict__ sflag,
                             const double* __restrict__ sdt, const StructInfo* __restrict__ si,
                             const double* __restrict__ mass, const double* __restrict__ force,
-                            double* pos, double* vel)
+                            double* pos, double* vel, const double* __restrict__ x0,
+                            double* dmax2)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= T) return;
@@ -123,8 +155,32 @@ __global__ void k_vv1_batch(int T, const int* __restrict__ sid, const int* __res
       else if (f[d] > 1.0) f[d] -= 1.0;
     }
   }
-  for (int d = 0; d < 3; ++d)
-    pos[d * T + i] = b.h[3 * d] * f[0] + b.h[3 * d + 1] * f[1] + b.h[3 * d + 2] * f[2];
+  double x[3];
+  for (int d = 0; d < 3; ++d) {
+    x[d] = b.h[3 * d] * f[0] + b.h[3 * d + 1] * f[1] + b.h[3 * d + 2] * f[2];
+    pos[d * T + i] = x[d];
+  }
+  if (sflag[s] & 2) {
+    // displacement since the build.  A large box's candidates are plain
+    // indices, whose displacement is taken by minimum image: an atom that
+    // crossed a periodic face has not moved a box length.  A small box's
+    // candidates name images relative to the wrapped positions, so there a
+    // wrap counts as the box-length jump it is and forces a rebuild.
+    const bool mic = !si[s].small;
+    double u[3], g[3];
+    for (int d = 0; d < 3; ++d) u[d] = x[d] - x0[d * T + i];
+    for (int d = 0; d < 3; ++d) {
+      g[d] = b.hinv[3 * d] * u[0] + b.hinv[3 * d + 1] * u[1] + b.hinv[3 * d + 2] * u[2];
+      if (mic && b.pbc[d] == 1) g[d] -= rint(g[d]);
+    }
+    double d2 = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      const double w = b.h[3 * d] * g[0] + b.h[3 * d + 1] * g[1] + b.h[3 * d + 2] * g[2];
+      d2 += w * w;
+    }
+    atomicMax(reinterpret_cast<unsigned long long*>(dmax2 + s),
+              static_cast<unsigned long long>(__double_as_longlong(d2)));
+  }
 }
 
 // Second half kick (md.cu k_vv2_thermo without the thermo sums).
@@ -205,6 +261,7 @@ size_t served_bytes_per_atom(const Engine& e)
   b += sizeof(float) * (static_cast<size_t>(p.nA) * p.nlm + p.T * basis_stride(p) + p.nR);
   b += sizeof(double);                                       // site energy
   b += 2 * (2 * sizeof(int) + 10 * sizeof(double));          // arenas: type, sid, pos, vel, mass, force
+  b += 2 * (sizeof(int) * (1 + static_cast<size_t>(nb.mn_v)) + 3 * sizeof(double));   // candidates
   b += sizeof(double) * (1 + 9 + kOutFields + 8);            // pe, virial, output and input blocks
   return b;
 }
@@ -270,6 +327,9 @@ struct Arena {
   int* type = nullptr;
   int* sid = nullptr;
   double *pos = nullptr, *vel = nullptr, *mass = nullptr, *force = nullptr;
+  // Verlet candidates of the MD segments' centers (explicit.cu BatchVerlet)
+  int *vcnt = nullptr, *vrow = nullptr;
+  double* x0 = nullptr;
 };
 
 }  // namespace
@@ -287,6 +347,9 @@ struct nepx_server {
   double *d_pe = nullptr, *d_virial = nullptr, *d_out = nullptr, *d_in = nullptr;
   int* d_ctl = nullptr;       // per-structure src (int2), flags, finishing lists
   double* d_sdt = nullptr;
+  double* d_dmax2 = nullptr;  // per structure: largest squared displacement since its candidates' build
+  int mn_cand = 0;            // Verlet candidates per served atom
+  bool row_reuse = true;      // MD segments admitted from now on keep Verlet candidates
   // pinned host staging, two copies (the worker stages one step while the
   // previous one runs)
   double *h_in[2] = {}, *h_out[2] = {}, *h_sdt[2] = {};
@@ -305,6 +368,8 @@ struct nepx_server {
   // statistics
   double done = 0, steps = 0, atom_steps = 0, busy = 0, resident_atoms = 0, resident_structs = 0;
   double resident_bytes = 0;
+  double cand_builds = 0, kept_center_steps = 0;
+  unsigned last_builds = 0;
 
   double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
   void run();
@@ -315,11 +380,11 @@ namespace {
 void free_server(nepx_server* S)
 {
   for (auto& a : S->arena) {
-    void* ptrs[] = {a.type, a.sid, a.pos, a.vel, a.mass, a.force};
+    void* ptrs[] = {a.type, a.sid, a.pos, a.vel, a.mass, a.force, a.vcnt, a.vrow, a.x0};
     for (void* p : ptrs)
       if (p) cudaFree(p);
   }
-  void* dptrs[] = {S->d_pe, S->d_virial, S->d_out, S->d_in, S->d_ctl, S->d_sdt};
+  void* dptrs[] = {S->d_pe, S->d_virial, S->d_out, S->d_in, S->d_ctl, S->d_sdt, S->d_dmax2};
   for (void* p : dptrs)
     if (p) cudaFree(p);
   for (int c = 0; c < 2; ++c) {
@@ -362,6 +427,7 @@ void nepx_server::run()
   struct Step {
     int par = 0, T = 0, S = 0, t_in = 0, t_out = 0, n_cells = 0;
     double t_tick = 0.0, bytes = 0.0;
+    double kept = 0.0;           // atoms of structures that keep Verlet candidates
     std::vector<Finishing> fin;
   };
   Step fly;                    // the step on the GPU
@@ -372,6 +438,7 @@ void nepx_server::run()
     int code = NEPX_OK;
     std::string msg;
     double t_end = 0.0;
+    double fly_builds = 0.0;
     if (flying) {
       const cudaError_t cerr = cudaStreamSynchronize(s);
       t_end = now();
@@ -380,6 +447,8 @@ void nepx_server::run()
         msg = std::string("server step: ") + cudaGetErrorString(cerr);
       } else {
         const NeighborState& st = *h->h_state;
+        fly_builds = static_cast<double>(st.xr_builds - last_builds);   // wraps
+        last_builds = st.xr_builds;
         if (st.overflow) {
           code = NEPX_ERR_OVERFLOW;
           msg = "a neighbour row exceeded its capacity; raise MN_radial/MN_angular in nep.txt";
@@ -397,10 +466,12 @@ void nepx_server::run()
     }
     // ---- 2. admission --------------------------------------------------------
     std::vector<Pending> adm;
+    bool keep_new = true;
     {
       std::unique_lock<std::mutex> lk(mu);
       if (!flying) cv.wait(lk, [&] { return !queue.empty() || !res.empty() || stopping; });
       if (!flying && queue.empty() && res.empty()) break;   // stopping with nothing left
+      keep_new = row_reuse;
       int atoms = 0;
       int nst = static_cast<int>(res.size());
       int cells = 0;
@@ -466,6 +537,8 @@ void nepx_server::run()
         r.t_admit = nx.t_tick;
         r.off = Tn;
         struct_info(e, p.box, 0, p.n, r.si);   // validated at submit
+        r.si.n = p.n;
+        r.si.keep = (keep_new && p.md_steps > 0 && verlet_encodable(r.si, e.skin)) ? 1 : 0;
         const int idx = static_cast<int>(res.size());
         c_src[2 * idx] = -1;
         c_src[2 * idx + 1] = in_off[k];
@@ -495,7 +568,9 @@ void nepx_server::run()
         r.si.n = r.n;
         h_si[par][k] = r.si;
         h_soff[par][k] = r.off;
-        c_flag[k] = r.fresh ? 0 : 1;
+        // bit 0 steps, bit 1 keeps Verlet candidates, bit 2 builds them (new)
+        c_flag[k] = (r.fresh ? 0 : 1) | (r.si.keep ? 2 : 0) | (r.fresh && r.si.keep ? 4 : 0);
+        if (r.si.keep) nx.kept += r.n;
         h_sdt[par][k] = r.dt / kTimeUnit;
         nx.bytes += static_cast<double>(r.bytes);
         const bool finishes = r.fresh ? r.md_steps == 0 : r.steps_done + 1 == r.md_steps;
@@ -546,12 +621,29 @@ void nepx_server::run()
         nx.T, nx.S, e.xr.d_soff, reinterpret_cast<const int2*>(d_src), fly_T, A.type, A.pos,
         A.vel, A.mass, A.force, nx.t_in, d_in,
         reinterpret_cast<const int*>(d_in + static_cast<size_t>(7) * nx.t_in), B.type, B.sid,
-        B.pos, B.vel, B.mass, B.force);
+        B.pos, B.vel, B.mass, B.force, A.vcnt, A.x0, B.vcnt, B.x0);
+      if (nx.kept > 0)
+        k_arena_rows<<<(nx.T + 7) / 8, kThreads, 0, s>>>(
+          nx.T, nx.S, e.xr.d_soff, reinterpret_cast<const int2*>(d_src), d_flag, B.vcnt, A.vrow,
+          B.vrow, mn_cand);
       cur = 1 - cur;
       Arena& R = arena[cur];
+      cudaMemsetAsync(d_dmax2, 0, sizeof(double) * nx.S, s);
       k_vv1_batch<<<grid(nx.T), kThreads, 0, s>>>(nx.T, R.sid, d_flag, d_sdt, e.xr.d_si, R.mass,
-                                                  R.force, R.pos, R.vel);
+                                                  R.force, R.pos, R.vel, R.x0, d_dmax2);
+      if (nx.kept > 0) {
+        BatchVerlet& bv = e.xr.bv;
+        bv.sflag = d_flag;
+        bv.dmax2 = d_dmax2;
+        bv.skin = static_cast<float>(e.skin);
+        bv.half_skin2 = 0.25 * e.skin * e.skin;
+        bv.mn = mn_cand;
+        bv.vcnt = R.vcnt;
+        bv.vrow = R.vrow;
+        bv.x0 = R.x0;
+      }
       launch_batch_force(e, nx.T, R.pos, R.type, d_pe, R.force, d_virial, false, s);
+      e.xr.bv = BatchVerlet{};
       k_vv2_batch<<<grid(nx.T), kThreads, 0, s>>>(nx.T, R.sid, d_flag, d_sdt, R.mass, R.force,
                                                   R.vel);
       const int nfin = static_cast<int>(nx.fin.size());
@@ -599,6 +691,8 @@ void nepx_server::run()
         resident_atoms += fly.T;
         resident_structs += fly.S;
         resident_bytes += fly.bytes;
+        cand_builds += fly_builds;
+        kept_center_steps += fly.kept;
       }
       if (!fly.fin.empty()) done_cv.notify_all();
     }
@@ -709,13 +803,16 @@ int nepx_server_create(nepx_t* h, int max_atoms, int max_struct, nepx_server_t**
   S->t0 = Clock::now();
   const size_t N = max_atoms, MS = max_struct;
   bool ok = cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking) == cudaSuccess;
+  S->mn_cand = e.nbr.mn_v;
   for (auto& a : S->arena)
     ok = ok && nepx::dalloc(a.type, N) && nepx::dalloc(a.sid, N) &&
          nepx::dalloc(a.pos, 3 * N) && nepx::dalloc(a.vel, 3 * N) && nepx::dalloc(a.mass, N) &&
-         nepx::dalloc(a.force, 3 * N);
+         nepx::dalloc(a.force, 3 * N) && nepx::dalloc(a.vcnt, N) &&
+         nepx::dalloc(a.vrow, N * static_cast<size_t>(S->mn_cand)) && nepx::dalloc(a.x0, 3 * N);
   ok = ok && nepx::dalloc(S->d_pe, N) && nepx::dalloc(S->d_virial, 9 * N) &&
        nepx::dalloc(S->d_out, size_t(nepx::kOutFields) * N) && nepx::dalloc(S->d_in, 8 * N) &&
-       nepx::dalloc(S->d_ctl, 5 * MS + 1) && nepx::dalloc(S->d_sdt, MS);
+       nepx::dalloc(S->d_ctl, 5 * MS + 1) && nepx::dalloc(S->d_sdt, MS) &&
+       nepx::dalloc(S->d_dmax2, MS);
   for (int c = 0; c < 2; ++c)
     ok = ok && nepx::halloc(S->h_in[c], 8 * N) &&
          nepx::halloc(S->h_out[c], nepx::kOutFields * N) && nepx::halloc(S->h_sdt[c], MS) &&
@@ -723,6 +820,14 @@ int nepx_server_create(nepx_t* h, int max_atoms, int max_struct, nepx_server_t**
          nepx::halloc(S->h_soff[c], MS + 1);
   if (ok) ok = cudaMemsetAsync(S->arena[0].force, 0, sizeof(double) * 3 * N, S->stream) ==
                cudaSuccess;
+  if (ok) ok = cudaMemsetAsync(S->arena[0].x0, 0, sizeof(double) * 3 * N, S->stream) ==
+               cudaSuccess;
+  if (ok) {
+    // candidate builds are counted from the handle's running device counter
+    nepx::NeighborState now{};
+    ok = cudaMemcpy(&now, e.d_nstate, sizeof(now), cudaMemcpyDeviceToHost) == cudaSuccess;
+    S->last_builds = now.xr_builds;
+  }
   if (!ok) {
     free_server(S);
     delete S;
@@ -872,6 +977,23 @@ int nepx_server_memory(nepx_server_t* S, double* info)
   info[1] = static_cast<double>(S->bytes_per_atom);
   info[2] = static_cast<double>(S->bytes_per_struct);
   info[3] = S->steps > 0 ? S->resident_bytes / S->steps : 0.0;
+  return NEPX_OK;
+}
+
+int nepx_server_set_row_reuse(nepx_server_t* S, int on)
+{
+  if (!S) return NEPX_ERR_ARG;
+  std::lock_guard<std::mutex> lk(S->mu);
+  S->row_reuse = on != 0;
+  return NEPX_OK;
+}
+
+int nepx_server_rows(nepx_server_t* S, double* info)
+{
+  if (!S || !info) return NEPX_ERR_ARG;
+  std::lock_guard<std::mutex> lk(S->mu);
+  info[0] = S->cand_builds;
+  info[1] = S->kept_center_steps;
   return NEPX_OK;
 }
 

@@ -61,6 +61,7 @@ __host__ __device__ inline int expanded_box(const Box& b, double rc, StructInfo&
   si.small = 0;
   si.nc[0] = si.nc[1] = si.nc[2] = 0;
   si.cell_base = 0;
+  si.keep = 0;
   for (int d = 0; d < 3; ++d) {
     si.ncell[d] = b.pbc[d] ? static_cast<int>(ceil(2.0 * rc / thick[d])) : 1;
     if (b.pbc[d] && thick[d] <= 2.5 * (rc + 1.0)) si.small = 1;

@@ -38,7 +38,7 @@ EXPORTED = ["nepx_create", "nepx_destroy", "nepx_last_error", "nepx_info", "nepx
             "nepx_md_set_barostat", "nepx_md_set_velocity", "nepx_md_compute_forces",
             "nepx_md_neighbor_info", "nepx_md_set_max_distance", "nepx_md_time",
             "nepx_md_enable_unwrapped", "nepx_md_get_unwrapped", "nepx_server_create_budget",
-            "nepx_server_memory"]
+            "nepx_server_memory", "nepx_server_set_row_reuse", "nepx_server_rows"]
 
 PRECISIONS = {"fp32": 0, "mixed": 1, "mixed_bf16": 2}
 ENSEMBLES = {"nve": 0, "nvt_ber": 1, "nvt_nhc": 2, "nvt_bdp": 3, "npt_ber": 4, "npt_scr": 5}
@@ -137,6 +137,8 @@ def lib():
         L.nepx_server_create_budget.argtypes = [vp, ctypes.c_double, ctypes.c_int,
                                                 ctypes.POINTER(vp)]
         L.nepx_server_memory.argtypes = [vp, dp]
+        L.nepx_server_set_row_reuse.argtypes = [vp, ctypes.c_int]
+        L.nepx_server_rows.argtypes = [vp, dp]
         L.nepx_md_set_velocity.argtypes = [vp, dp]
         L.nepx_md_compute_forces.argtypes = [vp]
         L.nepx_md_neighbor_info.argtypes = [vp, ip, ip]
@@ -552,6 +554,17 @@ class Server:
 
     def drain(self):
         self._check(lib().nepx_server_drain(self._h))
+
+    def set_row_reuse(self, on):
+        """Row reuse (Verlet candidates) for MD segments admitted from now on."""
+        self._check(lib().nepx_server_set_row_reuse(self._h, 1 if on else 0))
+
+    def rows(self):
+        """{'builds': centers whose candidates were built, 'kept': centers of
+        candidate-keeping structures summed over the steps}."""
+        s = (ctypes.c_double * 2)()
+        self._check(lib().nepx_server_rows(self._h, s))
+        return {"builds": s[0], "kept": s[1]}
 
     def stats(self):
         s = (ctypes.c_double * 8)()

@@ -394,6 +394,18 @@ int nepx_server_drain(nepx_server_t* server);
  * mean resident atoms per step, mean resident structures per step, current
  * queue length, seconds since creation. */
 int nepx_server_stats(nepx_server_t* server, double* stats);
+/* Row reuse of MD segments (on by default): a segment admitted while it is on
+ * keeps, per atom, the neighbours within the cutoff plus the handle's Verlet
+ * skin (small boxes: with their image) and filters them into its rows at each
+ * step, rebuilding them when one of its atoms has moved more than skin / 2
+ * since the build; the rows are those a fresh build gives.  Off: every step
+ * builds every row afresh.  Applies to requests admitted afterwards.  The
+ * Verlet idea of Neighbor::find_neighbor_global (neighbor.cu:537-582) for the
+ * batched rows; no counterpart in the reference. */
+int nepx_server_set_row_reuse(nepx_server_t* server, int on);
+/* info[2]: centers whose candidates were (re)built, centers of candidate-
+ * keeping structures summed over the steps (reuse = 1 - info[0] / info[1]). */
+int nepx_server_rows(nepx_server_t* server, double* info);
 
 #ifdef __cplusplus
 }

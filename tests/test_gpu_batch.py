@@ -167,3 +167,51 @@ def test_server_admits_by_device_memory():
         srv.submit(t, p, h)
     assert err.value.code == 5
     srv.close()
+
+
+def _md_stream(seed):
+    """MD segments of water in small, large and slab boxes (300 K, 1 fs:
+    the hydrogens pass skin / 2 within a few tens of steps) mixed with single
+    points, in a random order."""
+    rng = np.random.default_rng(seed)
+    mass_of = np.array([15.999, 1.008])
+    out = []
+    for k, s in enumerate(_structures(seed=seed)):
+        t, h, p, pbc = s
+        m = mass_of[np.asarray(t)]
+        v = workloads.maxwell_boltzmann(m, 300.0, seed=40 + k)
+        out.append((t, h, p, pbc, 60, m, v))
+        out.append((t, h, p, pbc, 0, None, None))
+    return [out[k] for k in rng.permutation(len(out))]
+
+
+def test_server_row_reuse_equals_fresh_rows():
+    """MD segments that keep Verlet candidates and filter them into their
+    rows at each step (rebuilding them when an atom has moved more than
+    skin / 2) give bit for bit the results of segments whose rows are built
+    afresh at every step; the candidates were rebuilt inside the segments and
+    reused on most steps."""
+    import nepx
+    stream = _md_stream(3)
+    pot = nepx.Potential(potential(WATER), max_atoms=4000)
+    outs = []
+    for reuse in (True, False):
+        srv = nepx.Server(pot, max_atoms=4000, max_struct=8)
+        srv.set_row_reuse(reuse)
+        tickets = [srv.submit(t, p, h, pbc, md_steps=ms, dt_fs=1.0, masses=m, vel=v,
+                              want_state=True)
+                   for (t, h, p, pbc, ms, m, v) in stream]
+        outs.append([srv.wait(tk) for tk in tickets])
+        rows = srv.rows()
+        if reuse:
+            md_atoms = sum(len(s[0]) for s in stream if s[4])
+            # every segment built its candidates once on admission; more builds
+            # mean skin-triggered rebuilds, fewer than the kept centers reuse
+            assert rows["builds"] > md_atoms, rows
+            assert rows["builds"] < 0.5 * rows["kept"], rows
+        else:
+            assert rows["builds"] == 0 and rows["kept"] == 0, rows
+        srv.close()
+    for a, b in zip(*outs):
+        for key in ("pe", "force", "virial", "pos", "vel"):
+            assert np.array_equal(a[key], b[key]), key
