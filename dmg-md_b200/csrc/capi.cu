@@ -285,6 +285,38 @@ int nepx_set_precision(nepx_t* h, int mode)
   return NEPX_OK;
 }
 
+int nepx_get_tuning(nepx_t* h, int* v, int* tuned)
+{
+  if (!h || !v) return NEPX_ERR_ARG;
+  const nepx::Engine& e = h->engine;
+  v[0] = e.filter_group;
+  v[1] = e.group;
+  v[2] = e.fused_minb;
+  v[3] = e.f12_group;
+  v[4] = e.gather_group;
+  v[5] = e.fuse_f12 ? 1 : 0;
+  if (tuned) *tuned = e.tuned ? 1 : 0;
+  return NEPX_OK;
+}
+
+int nepx_set_tuning(nepx_t* h, const int* v)
+{
+  if (!h || !v) return NEPX_ERR_ARG;
+  auto lanes = [](int g) { return g == 4 || g == 8; };
+  if (!lanes(v[0]) || !lanes(v[1]) || !(v[2] == 3 || v[2] == 4) || !lanes(v[3]) ||
+      !lanes(v[4]) || !(v[5] == 0 || v[5] == 1))
+    return fail(h, NEPX_ERR_ARG, "launch choice outside the built variants");
+  nepx::Engine& e = h->engine;
+  e.filter_group = v[0];
+  e.group = v[1];
+  e.fused_minb = v[2];
+  e.f12_group = v[3];
+  e.gather_group = v[4];
+  e.fuse_f12 = v[5] == 1;
+  e.tuned = true;
+  return NEPX_OK;
+}
+
 int nepx_neighbor_stats(nepx_t* h, int* max_radial, int* max_angular, int* max_verlet,
                         void* stream)
 {

@@ -217,7 +217,7 @@ struct TuneKey {
   bool operator==(const TuneKey& o) const { return std::memcmp(v, o.v, sizeof(v)) == 0; }
 };
 struct TuneVal {
-  int filter_group, group, fused_minb, f12_group, gather_group;
+  int filter_group, group, fused_minb, f12_group, gather_group, fuse_f12;
 };
 
 std::mutex g_tune_mu;
@@ -230,7 +230,7 @@ TuneKey tune_key(const Engine& e, int N)
   int size_class = 0;
   while ((1 << (size_class + 1)) <= N) ++size_class;   // floor(log2 N)
   TuneKey k{{e.device, e.use_xr ? 1 : 0, e.precision, p.T, p.nR, p.nA, p.kR, p.kA, p.L_max,
-             p.dim, p.H, p.num_inv, size_class, 1}};
+             p.dim, p.H, p.num_inv, size_class, 2}};
   return k;
 }
 
@@ -249,11 +249,12 @@ void tune_load_file()
     bool ok = true;
     for (int& x : k.v) ok = ok && static_cast<bool>(ls >> x);
     ok = ok && static_cast<bool>(ls >> v.filter_group >> v.group >> v.fused_minb >> v.f12_group >>
-                                 v.gather_group);
+                                 v.gather_group >> v.fuse_f12);
     // only the shapes the launchers instantiate; anything else is ignored
     auto lanes = [](int g) { return g == 4 || g == 8; };
     ok = ok && lanes(v.filter_group) && lanes(v.group) && lanes(v.f12_group) &&
-         lanes(v.gather_group) && (v.fused_minb == 3 || v.fused_minb == 4);
+         lanes(v.gather_group) && (v.fused_minb == 3 || v.fused_minb == 4) &&
+         (v.fuse_f12 == 0 || v.fuse_f12 == 1);
     if (ok) g_tune.emplace_back(k, v);
   }
 }
@@ -280,7 +281,7 @@ void tune_store(const TuneKey& k, const TuneVal& v)
     std::ofstream out(path, std::ios::app);
     for (int x : k.v) out << x << ' ';
     out << v.filter_group << ' ' << v.group << ' ' << v.fused_minb << ' ' << v.f12_group << ' '
-        << v.gather_group << '\n';
+        << v.gather_group << ' ' << v.fuse_f12 << '\n';
   }
 }
 
@@ -296,6 +297,7 @@ void engine_autotune(Engine& e, int N, const double* pos, const int* type, cudaS
     e.fused_minb = known.fused_minb;
     e.f12_group = known.f12_group;
     e.gather_group = known.gather_group;
+    e.fuse_f12 = known.fuse_f12 != 0;
     e.tuned = true;
     return;
   }
@@ -335,13 +337,24 @@ void engine_autotune(Engine& e, int N, const double* pos, const int* type, cudaS
   const int n_minb = (fused_occupancy_variants(e.params) && e.precision == 0) ? 2 : 1;
   if (n_minb == 1) e.fused_minb = 3;
   int pick_m = e.fused_minb;
+  // the descriptor kernel with and without the angular partial forces (the
+  // fused form exists for the small shape on Verlet rows)
+  e.fuse_f12 = true;
+  const int n_ff = fused_angular_force(e) ? 2 : 1;
+  e.fuse_f12 = false;
+  bool pick_ff = false;
+  for (int ff = 0; ff < n_ff; ++ff)
   for (int gf : groups) {
     for (int mi = 0; mi < n_minb; ++mi)
     for (int gg : groups) {
+      e.fuse_f12 = ff == 1;
       e.group = gf;
       e.fused_minb = minbs[mi];
       e.f12_group = gg;   // angular-force grouping varies together with the gather's
       e.gather_group = gg;
+      // with the fused form the angular-force grouping plays no part (the
+      // gather's groupings are timed with the separate form)
+      if (e.fuse_f12 && gg != groups[0]) continue;
       float tf[3], tg[3];
       for (int r = 0; r < 3; ++r) {
         cudaEventRecord(a, stream);
@@ -362,6 +375,7 @@ void engine_autotune(Engine& e, int N, const double* pos, const int* type, cudaS
         pick_f = gf;
         pick_m = e.fused_minb;
         pick_a = gg;
+        pick_ff = e.fuse_f12;
       }
       if (tg[1] < best_g) {
         best_g = tg[1];
@@ -376,13 +390,17 @@ void engine_autotune(Engine& e, int N, const double* pos, const int* type, cudaS
   e.fused_minb = pick_m;
   e.f12_group = pick_a;
   e.gather_group = pick_g;
+  e.fuse_f12 = pick_ff;
   e.tuned = true;
-  tune_store(key, TuneVal{e.filter_group, e.group, e.fused_minb, e.f12_group, e.gather_group});
+  tune_store(key, TuneVal{e.filter_group, e.group, e.fused_minb, e.f12_group, e.gather_group,
+                          e.fuse_f12 ? 1 : 0});
   if (std::getenv("NEPX_VERBOSE"))
     std::fprintf(stderr,
-                 "nepx autotune (N=%d): filter G=%d, fused G=%d at %d CTAs/SM, angular-force "
-                 "G=%d, gather G=%d\n",
-                 N, e.filter_group, e.group, e.fused_minb, e.f12_group, e.gather_group);
+                 "nepx autotune (N=%d): filter G=%d, fused G=%d at %d CTAs/SM, angular force "
+                 "%s, G=%d, gather G=%d\n",
+                 N, e.filter_group, e.group, e.fused_minb,
+                 e.fuse_f12 ? "in the descriptor kernel" : "own kernel", e.f12_group,
+                 e.gather_group);
 }
 
 namespace {

@@ -118,6 +118,7 @@ struct Engine {
   int filter_group = 8;      // lanes per center in the typewise filter (autotuned)
   int f12_group = 4;         // lanes per center in the angular-force kernel (autotuned)
   int gather_group = 8;      // lanes per center in the gather (autotuned)
+  bool fuse_f12 = false;     // the descriptor kernel evaluates f12 itself (autotuned)
   bool tuned = false;
   std::string error;
 };
@@ -131,12 +132,16 @@ size_t fused_tc_smem_bytes(const ModelParams& p);
 // True when the descriptor kernel comes in two occupancy builds (3 or 4 CTAs
 // per SM, Engine::fused_minb) for this model's shape.
 bool fused_occupancy_variants(const ModelParams& p);
+// True when the descriptor kernel writes the angular partial forces itself
+// (Engine::fuse_f12 on a small-shape model and Verlet rows): no k_angular_f12.
+bool fused_angular_force(const Engine& e);
 void set_fused_smem_limits(const ModelParams& p);
 
 // Times each kernel variant on the given system (a few calls each, stream
 // synchronised) and keeps the fastest: the lane-group size of the filter,
-// descriptor, angular-force and gather kernels and the descriptor kernel's
-// CTAs per SM.  The picks are kept per (device, model shape, precision, row
+// descriptor, angular-force and gather kernels, the descriptor kernel's
+// CTAs per SM, and whether the descriptor kernel evaluates the angular
+// partial forces itself.  The picks are kept per (device, model shape, precision, row
 // path, size class log2 N) for every later handle of the process, and in the
 // file NEPX_TUNE_FILE names, when set, across runs.  Neighbour rows must be
 // current.

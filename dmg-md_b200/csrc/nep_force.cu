@@ -903,6 +903,103 @@ k_filter_radial(const ModelParams p, int N, const Box* __restrict__ box,
   }
 }
 
+// Directed angular partial force of a center on one neighbour at
+// r = (dx, dy, dz) = r_j - r_i:
+//   f12 = (sum_lm B_lm Y_lm) r^ + (1/d)(I - r^r^T) sum_lm A_lm dY_lm/dr^,
+//   A_lm = sum_n a[n][lm] g_n(d), B_lm = sum_n a[n][lm] g'_n(d),
+// with a[n][lm] = dE/ds[n][lm] of the center (av: global memory, or with AG
+// false the center's shared-memory scratch) and c its angular coefficient
+// table for the pair (nA rows of the padded basis, shared memory).
+// Reference find_partial_force_angular (nep.cu:890-991) with the
+// accumulate_f12 ladder (nep_utilities.cuh:1240-1491) evaluated once per edge
+// instead of once per (edge, n).
+template <int KM, int NAM, int LMAX, bool AG = true>
+__device__ __forceinline__ float3 angular_edge_force(const ModelParams& p, const float* c,
+                                                    const float* __restrict__ av, float rc,
+                                                    float dx, float dy, float dz)
+{
+  constexpr int KP = (KM + 3) & ~3;
+  constexpr int NLM = num_lm<LMAX>();
+  const int nA = p.nA;
+  const float d = sqrtf(dx * dx + dy * dy + dz * dz);
+  const float dinv = 1.0f / d;
+  const float ux = dx * dinv, uy = dy * dinv, uz = dz * dinv;
+  const float rcinv = 1.0f / rc;
+  float fc, fcp;
+  cutoff_fc(rc, rcinv, d, fc, fcp);
+  float fn[KP], fnp[KP];
+#pragma unroll
+  for (int kk = 0; kk < KP; ++kk) {
+    fn[kk] = 0.0f;
+    fnp[kk] = 0.0f;
+  }
+  radial_basis_d<KM>(p.kA, rcinv, d, fc, fcp, fn, fnp);
+  float A[NLM], B[NLM];
+#pragma unroll
+  for (int lm = 0; lm < NLM; ++lm) {
+    A[lm] = 0.0f;
+    B[lm] = 0.0f;
+  }
+#pragma unroll
+  for (int n = 0; n < NAM; ++n) {
+    if (n < nA) {
+      const float g = dot_basis<KM>(c + n * KP, fn);
+      const float gp = dot_basis<KM>(c + n * KP, fnp);
+      const float* an = av + n * NLM;
+#pragma unroll
+      for (int q = 0; q < NLM / 4; ++q) {
+        const float4 a4 = AG ? __ldg(reinterpret_cast<const float4*>(an) + q)
+                             : reinterpret_cast<const float4*>(an)[q];
+        A[4 * q] += a4.x * g;
+        A[4 * q + 1] += a4.y * g;
+        A[4 * q + 2] += a4.z * g;
+        A[4 * q + 3] += a4.w * g;
+        B[4 * q] += a4.x * gp;
+        B[4 * q + 1] += a4.y * gp;
+        B[4 * q + 2] += a4.z * gp;
+        B[4 * q + 3] += a4.w * gp;
+      }
+    }
+  }
+  // SB = sum B Y, V = sum A dY/du (u components independent)
+  float zp[LMAX + 1];
+  zp[0] = 1.0f;
+#pragma unroll
+  for (int q = 1; q <= LMAX; ++q) zp[q] = zp[q - 1] * uz;
+  float SB = 0.0f, vx = 0.0f, vy = 0.0f, vz = 0.0f;
+  int idx = 0;
+#pragma unroll
+  for (int Lq = 1; Lq <= LMAX; ++Lq) {
+    if (Lq > p.L_max) break;
+    float re0 = 1.0f, im0 = 0.0f;   // (ux + i uy)^(m-1)
+#pragma unroll
+    for (int m = 0; m <= Lq; ++m) {
+      float dzf;
+      const float zf = zpoly_any(Lq, m, zp, &dzf);
+      if (m == 0) {
+        SB += B[idx] * zf;
+        vz += A[idx] * dzf;
+        ++idx;
+      } else {
+        const float re = ux * re0 - uy * im0;
+        const float im = ux * im0 + uy * re0;
+        const float Ar = A[idx], Ai = A[idx + 1];
+        SB += (B[idx] * re + B[idx + 1] * im) * zf;
+        const float mzf = m * zf;
+        vx += mzf * (Ar * re0 + Ai * im0);
+        vy += mzf * (Ai * re0 - Ar * im0);
+        vz += dzf * (Ar * re + Ai * im);
+        idx += 2;
+        re0 = re;
+        im0 = im;
+      }
+    }
+  }
+  const float uv = ux * vx + uy * vy + uz * vz;
+  return make_float3(SB * ux + (vx - uv * ux) * dinv, SB * uy + (vy - uv * uy) * dinv,
+                     SB * uz + (vz - uv * uz) * dinv);
+}
+
 // NRM/KM/NAM: compile-time bounds of nR, basis size + 1, nA for this instance.
 // MINB: CTAs per SM the instance is built for (register cap 65536 / (128
 // MINB)).  The small shape comes at 3 (168 registers, moments of five radial
@@ -916,7 +1013,11 @@ k_filter_radial(const ModelParams p, int N, const Box* __restrict__ box,
 // components, one n per sweep).
 // TC: the ANN of the CTA's centers runs on the tensor cores (tc_ann, the
 // mixed-precision path); otherwise in FP32 per center.
-template <int G, int NRM, int KM, int NAM, bool XR, int LMAX, int MINB, bool TC>
+// FF (Verlet-row path only): the kernel ends with the directed angular partial
+// forces f12 of the center's edges, from a[n][lm] in its shared-memory
+// scratch, in place of handing a[n][lm] to k_angular_f12 through memory (the
+// autotuner times both forms).
+template <int G, int NRM, int KM, int NAM, bool XR, int LMAX, int MINB, bool TC, bool FF>
 __global__ void __launch_bounds__(kBlock, MINB)
 k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
             const Site* __restrict__ sites, NeighborState* st,
@@ -924,8 +1025,10 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
             int* __restrict__ nn_r, int* __restrict__ nl_r, int mn_r, int* __restrict__ nn_a,
             int* __restrict__ nl_a, int mn_a, const float4* __restrict__ er,
             const float4* __restrict__ ea, const float* __restrict__ qrad,
-            float* __restrict__ alpha, float* __restrict__ acoef, double* __restrict__ pe_ann)
+            float* __restrict__ alpha, float* __restrict__ acoef, float4* __restrict__ f12,
+            double* __restrict__ pe_ann)
 {
+  static_assert(!(FF && XR), "the fused angular force is built for Verlet rows only");
   constexpr int APW = 32 / G;             // centers per warp
   constexpr int APB = kBlock / G;         // centers per block
   constexpr int KP = (KM + 3) & ~3;
@@ -1251,106 +1354,57 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
   __syncwarp();
 
   // ---- 4. hand a[n][lm] to the angular-force kernel -------------------------
-  if (active) {
-    float4* dst = reinterpret_cast<float4*>(acoef + static_cast<size_t>(i) * nA * NLM);
-    const float4* src = reinterpret_cast<const float4*>(s_a);
-    for (int q = gl; q < nA * NLM / 4; q += G) dst[q] = src[q];
-  }
-}
-
-// Directed angular partial force of a center on one neighbour at
-// r = (dx, dy, dz) = r_j - r_i:
-//   f12 = (sum_lm B_lm Y_lm) r^ + (1/d)(I - r^r^T) sum_lm A_lm dY_lm/dr^,
-//   A_lm = sum_n a[n][lm] g_n(d), B_lm = sum_n a[n][lm] g'_n(d),
-// with a[n][lm] = dE/ds[n][lm] of the center (av, global) and c its angular
-// coefficient table for the pair (nA rows of the padded basis, shared memory).
-// Reference find_partial_force_angular (nep.cu:890-991) with the
-// accumulate_f12 ladder (nep_utilities.cuh:1240-1491) evaluated once per edge
-// instead of once per (edge, n).
-template <int KM, int NAM, int LMAX>
-__device__ __forceinline__ float3 angular_edge_force(const ModelParams& p, const float* c,
-                                                    const float* __restrict__ av, float rc,
-                                                    float dx, float dy, float dz)
-{
-  constexpr int KP = (KM + 3) & ~3;
-  constexpr int NLM = num_lm<LMAX>();
-  const int nA = p.nA;
-  const float d = sqrtf(dx * dx + dy * dy + dz * dz);
-  const float dinv = 1.0f / d;
-  const float ux = dx * dinv, uy = dy * dinv, uz = dz * dinv;
-  const float rcinv = 1.0f / rc;
-  float fc, fcp;
-  cutoff_fc(rc, rcinv, d, fc, fcp);
-  float fn[KP], fnp[KP];
-#pragma unroll
-  for (int kk = 0; kk < KP; ++kk) {
-    fn[kk] = 0.0f;
-    fnp[kk] = 0.0f;
-  }
-  radial_basis_d<KM>(p.kA, rcinv, d, fc, fcp, fn, fnp);
-  float A[NLM], B[NLM];
-#pragma unroll
-  for (int lm = 0; lm < NLM; ++lm) {
-    A[lm] = 0.0f;
-    B[lm] = 0.0f;
-  }
-#pragma unroll
-  for (int n = 0; n < NAM; ++n) {
-    if (n < nA) {
-      const float g = dot_basis<KM>(c + n * KP, fn);
-      const float gp = dot_basis<KM>(c + n * KP, fnp);
-      const float* an = av + n * NLM;
-#pragma unroll
-      for (int q = 0; q < NLM / 4; ++q) {
-        const float4 a4 = __ldg(reinterpret_cast<const float4*>(an) + q);
-        A[4 * q] += a4.x * g;
-        A[4 * q + 1] += a4.y * g;
-        A[4 * q + 2] += a4.z * g;
-        A[4 * q + 3] += a4.w * g;
-        B[4 * q] += a4.x * gp;
-        B[4 * q + 1] += a4.y * gp;
-        B[4 * q + 2] += a4.z * gp;
-        B[4 * q + 3] += a4.w * gp;
-      }
+  if constexpr (!FF) {
+    if (active) {
+      float4* dst = reinterpret_cast<float4*>(acoef + static_cast<size_t>(i) * nA * NLM);
+      const float4* src = reinterpret_cast<const float4*>(s_a);
+      for (int q = gl; q < nA * NLM / 4; q += G) dst[q] = src[q];
     }
-  }
-  // SB = sum B Y, V = sum A dY/du (u components independent)
-  float zp[LMAX + 1];
-  zp[0] = 1.0f;
-#pragma unroll
-  for (int q = 1; q <= LMAX; ++q) zp[q] = zp[q - 1] * uz;
-  float SB = 0.0f, vx = 0.0f, vy = 0.0f, vz = 0.0f;
-  int idx = 0;
-#pragma unroll
-  for (int Lq = 1; Lq <= LMAX; ++Lq) {
-    if (Lq > p.L_max) break;
-    float re0 = 1.0f, im0 = 0.0f;   // (ux + i uy)^(m-1)
-#pragma unroll
-    for (int m = 0; m <= Lq; ++m) {
-      float dzf;
-      const float zf = zpoly_any(Lq, m, zp, &dzf);
-      if (m == 0) {
-        SB += B[idx] * zf;
-        vz += A[idx] * dzf;
-        ++idx;
+  } else {
+    // ---- 4'. or evaluate the angular partial forces here (k_angular_f12's
+    // arithmetic, the moments read from shared memory); the sites come again
+    // through the lane's two prefetch slots (PF) or with the next index in
+    // flight
+    const float* ctab = sm + Lay.c_ang + t1 * T * nA * Lay.kpa;
+    float4* frow = f12 + static_cast<size_t>(i) * mn_a;
+    const unsigned slots =
+      PF ? static_cast<unsigned>(__cvta_generic_to_shared(sm + Lay.pf)) + 64u * tid : 0u;
+    int j_next = (gl < na) ? arow[gl] : 0;
+    if constexpr (PF) {
+      if (gl < na) site_fetch_async(slots, sites + j_next);
+      async_commit();
+      j_next = (gl + G < na) ? arow[gl + G] : 0;
+    }
+    for (int base = 0; base < na_max; base += G) {
+      const int k = base + gl;
+      const int par = (base / G) & 1;
+      int j = 0;
+      if constexpr (PF) {
+        if (k + G < na) site_fetch_async(slots + 32u * (par ^ 1), sites + j_next);
+        async_commit();
+        if (k + 2 * G < na) j_next = arow[k + 2 * G];
+        async_wait_prior();
       } else {
-        const float re = ux * re0 - uy * im0;
-        const float im = ux * im0 + uy * re0;
-        const float Ar = A[idx], Ai = A[idx + 1];
-        SB += (B[idx] * re + B[idx + 1] * im) * zf;
-        const float mzf = m * zf;
-        vx += mzf * (Ar * re0 + Ai * im0);
-        vy += mzf * (Ai * re0 - Ar * im0);
-        vz += dzf * (Ar * re + Ai * im);
-        idx += 2;
-        re0 = re;
-        im0 = im;
+        j = j_next;
+        if (k + G < na) j_next = arow[k + G];
+      }
+      if (k < na) {
+        int t2;
+        float dx, dy, dz;
+        if constexpr (PF) {
+          const double2* sl = reinterpret_cast<const double2*>(sm + Lay.pf + 16 * tid + 8 * par);
+          site_delta(b, sl[0], sl[1], xi, yi, zi, dx, dy, dz, t2);
+        } else {
+          site_displacement(b, sites, xi, yi, zi, j, dx, dy, dz, t2);
+        }
+        const float rc = (ra1 + p.rc_a[t2]) * 0.5f;
+        const float3 f = angular_edge_force<KM, NAM, LMAX, false>(p, ctab + t2 * nA * Lay.kpa,
+                                                                  s_a, rc, dx, dy, dz);
+        frow[k] = make_float4(f.x, f.y, f.z, 0.0f);
       }
     }
+    if constexpr (PF) async_wait_all();
   }
-  const float uv = ux * vx + uy * vy + uz * vz;
-  return make_float3(SB * ux + (vx - uv * ux) * dinv, SB * uy + (vy - uv * uy) * dinv,
-                     SB * uz + (vz - uv * uz) * dinv);
 }
 
 // Angular coefficient tables [T*T][nA][KP] into shared memory (zero-padded rows).
@@ -1673,7 +1727,7 @@ bool small_shape(const ModelParams& p)
          p.kA <= kSmallK;
 }
 
-template <int G, int NRM, int KM, int NAM, bool XR, int LMAX, int MINB, bool TC>
+template <int G, int NRM, int KM, int NAM, bool XR, int LMAX, int MINB, bool TC, bool FF = false>
 void launch_fused_t(Engine& e, int N, cudaStream_t s)
 {
   NeighborBuffers& nb = e.nbr;
@@ -1682,10 +1736,10 @@ void launch_fused_t(Engine& e, int N, cudaStream_t s)
   const size_t smem = fused_layout(e.params, APB, (KM + 3) & ~3, fused_smem_budget(MINB), TC,
                                    fused_prefetch(XR, MINB))
                         .total_bytes;
-  k_nep_fused<G, NRM, KM, NAM, XR, LMAX, MINB, TC><<<blocks, kBlock, smem, s>>>(
+  k_nep_fused<G, NRM, KM, NAM, XR, LMAX, MINB, TC, FF><<<blocks, kBlock, smem, s>>>(
     e.params, N, e.d_box, e.scratch.sites, e.d_nstate, nb.nn_v, nb.nl_v, nb.mn_v, nb.nn_r, nb.nl_r,
     nb.mn_r, nb.nn_a, nb.nl_a, nb.mn_a, e.xr.er, e.xr.ea, e.scratch.qrad, e.scratch.alpha,
-    e.scratch.acoef, e.scratch.pe_ann);
+    e.scratch.acoef, e.scratch.f12, e.scratch.pe_ann);
 }
 
 template <int G, int NRM, int KM>
@@ -1727,7 +1781,8 @@ void launch_f12_t(Engine& e, int N, cudaStream_t s)
       e.scratch.acoef, e.scratch.f12);
 }
 
-template <int G, int NRM, int KM, int NAM, int LMAX, int MINB, bool TC>
+// FFI: the build also comes with the fused angular force (small shape)
+template <int G, int NRM, int KM, int NAM, int LMAX, int MINB, bool TC, bool FFI = false>
 void set_fused_smem_t(const ModelParams& p)
 {
   auto bytes = [&](bool xr) {
@@ -1735,10 +1790,13 @@ void set_fused_smem_t(const ModelParams& p)
                         fused_prefetch(xr, MINB))
       .total_bytes;
   };
-  cudaFuncSetAttribute(k_nep_fused<G, NRM, KM, NAM, false, LMAX, MINB, TC>,
+  cudaFuncSetAttribute(k_nep_fused<G, NRM, KM, NAM, false, LMAX, MINB, TC, false>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, bytes(false));
-  cudaFuncSetAttribute(k_nep_fused<G, NRM, KM, NAM, true, LMAX, MINB, TC>,
+  cudaFuncSetAttribute(k_nep_fused<G, NRM, KM, NAM, true, LMAX, MINB, TC, false>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, bytes(true));
+  if constexpr (FFI)
+    cudaFuncSetAttribute(k_nep_fused<G, NRM, KM, NAM, false, LMAX, MINB, TC, true>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, bytes(false));
 }
 
 template <int G, int KM, int NAM, bool XR, int LMAX>
@@ -1776,6 +1834,13 @@ void launch_fused_g(Engine& e, int N, cudaStream_t s)
 template <int G>
 void launch_fused_small(Engine& e, int N, cudaStream_t s)
 {
+  if (!e.use_xr && e.fuse_f12) {
+    constexpr int n = kSmallN, k = kSmallK;
+    if (e.precision != 0) launch_fused_t<G, n, k, n, false, 4, 3, true, true>(e, N, s);
+    else if (e.fused_minb == 4) launch_fused_t<G, n, k, n, false, 4, 4, false, true>(e, N, s);
+    else launch_fused_t<G, n, k, n, false, 4, 3, false, true>(e, N, s);
+    return;
+  }
   if (e.fused_minb == 4 && e.precision == 0) {
     if (e.use_xr) launch_fused_t<G, kSmallN, kSmallK, kSmallN, true, 4, 4, false>(e, N, s);
     else launch_fused_t<G, kSmallN, kSmallK, kSmallN, false, 4, 4, false>(e, N, s);
@@ -1824,13 +1889,13 @@ void set_fused_smem_limits(const ModelParams& p)
     return;
   }
   if (small_shape(p)) {
-    set_fused_smem_t<4, kSmallN, kSmallK, kSmallN, 4, 3, false>(p);
-    set_fused_smem_t<8, kSmallN, kSmallK, kSmallN, 4, 3, false>(p);
-    set_fused_smem_t<4, kSmallN, kSmallK, kSmallN, 4, 4, false>(p);
-    set_fused_smem_t<8, kSmallN, kSmallK, kSmallN, 4, 4, false>(p);
+    set_fused_smem_t<4, kSmallN, kSmallK, kSmallN, 4, 3, false, true>(p);
+    set_fused_smem_t<8, kSmallN, kSmallK, kSmallN, 4, 3, false, true>(p);
+    set_fused_smem_t<4, kSmallN, kSmallK, kSmallN, 4, 4, false, true>(p);
+    set_fused_smem_t<8, kSmallN, kSmallK, kSmallN, 4, 4, false, true>(p);
     if (tc) {
-      set_fused_smem_t<4, kSmallN, kSmallK, kSmallN, 4, 3, true>(p);
-      set_fused_smem_t<8, kSmallN, kSmallK, kSmallN, 4, 3, true>(p);
+      set_fused_smem_t<4, kSmallN, kSmallK, kSmallN, 4, 3, true, true>(p);
+      set_fused_smem_t<8, kSmallN, kSmallK, kSmallN, 4, 3, true, true>(p);
     }
   } else {
     set_fused_smem_t<4, kMaxN, kMaxBasis, kMaxN, 4, 2, false>(p);
@@ -1865,6 +1930,13 @@ void launch_filter(Engine& e, int N, cudaStream_t s)
   }
 }
 
+// The descriptor kernel evaluates the angular partial forces itself (small
+// shape, Verlet rows, when the autotuner picked it).
+bool fused_angular_force(const Engine& e)
+{
+  return e.fuse_f12 && !e.use_xr && small_shape(e.params);
+}
+
 void launch_descriptor(Engine& e, int N, const double*, const int*, cudaStream_t stream)
 {
   const bool small = small_shape(e.params);
@@ -1881,6 +1953,7 @@ void launch_descriptor(Engine& e, int N, const double*, const int*, cudaStream_t
   // a single explicit-row system: the gather evaluates both directed angular
   // forces itself; a batch's structures that are not small take f12 here
   if (e.use_xr && e.xr.from_box) return;
+  if (fused_angular_force(e)) return;   // the descriptor kernel wrote f12
   if (high) launch_f12_t<kHighGroup, kMaxBasis, kMaxN, 8>(e, N, stream);
   else if (e.f12_group == 8) {
     if (small) launch_f12_t<8, kSmallK, kSmallN, 4>(e, N, stream);

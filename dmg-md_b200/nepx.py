@@ -38,7 +38,10 @@ EXPORTED = ["nepx_create", "nepx_destroy", "nepx_last_error", "nepx_info", "nepx
             "nepx_md_set_barostat", "nepx_md_set_velocity", "nepx_md_compute_forces",
             "nepx_md_neighbor_info", "nepx_md_set_max_distance", "nepx_md_time",
             "nepx_md_enable_unwrapped", "nepx_md_get_unwrapped", "nepx_server_create_budget",
-            "nepx_server_memory", "nepx_server_set_row_reuse", "nepx_server_rows"]
+            "nepx_server_memory", "nepx_server_set_row_reuse", "nepx_server_rows",
+            "nepx_get_tuning", "nepx_set_tuning"]
+TUNING_FIELDS = ("filter_group", "fused_group", "fused_ctas_per_sm", "f12_group",
+                 "gather_group", "fused_f12")
 
 PRECISIONS = {"fp32": 0, "mixed": 1, "mixed_bf16": 2}
 ENSEMBLES = {"nve": 0, "nvt_ber": 1, "nvt_nhc": 2, "nvt_bdp": 3, "npt_ber": 4, "npt_scr": 5}
@@ -120,6 +123,8 @@ def lib():
                                            ctypes.POINTER(vp), ctypes.POINTER(vp),
                                            ctypes.POINTER(vp)]
         L.nepx_set_precision.argtypes = [vp, ctypes.c_int]
+        L.nepx_get_tuning.argtypes = [vp, ip, ip]
+        L.nepx_set_tuning.argtypes = [vp, ip]
         L.nepx_md_run_segment.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, vp,
                                           ctypes.c_int, ctypes.c_int]
         L.nepx_compute_batch.argtypes = [vp, ctypes.POINTER(StructDesc), ctypes.c_int, vp, vp, vp,
@@ -231,6 +236,25 @@ class Potential:
         """"fp32" (default), "mixed" (the ANN on the tensor cores, FP16 operands
         with per-layer scaling) or "mixed_bf16" (BF16 operands)."""
         self._check(lib().nepx_set_precision(self._h, PRECISIONS[mode]))
+
+    def tuning(self):
+        """The force kernels' launch choices (dict of TUNING_FIELDS) and whether
+        they are fixed yet (the autotuner runs at the first compute)."""
+        v = (ctypes.c_int * len(TUNING_FIELDS))()
+        tuned = ctypes.c_int(0)
+        self._check(lib().nepx_get_tuning(self._h, v, ctypes.byref(tuned)))
+        return dict(zip(TUNING_FIELDS, list(v))), bool(tuned.value)
+
+    def set_tuning(self, **choices):
+        """Fixes the launch choices (the current ones, updated by `choices`)
+        for every later call: no autotuning runs."""
+        cur, _ = self.tuning()
+        for k in choices:
+            if k not in cur:
+                raise KeyError(k)
+        cur.update(choices)
+        v = (ctypes.c_int * len(TUNING_FIELDS))(*[int(cur[k]) for k in TUNING_FIELDS])
+        self._check(lib().nepx_set_tuning(self._h, v))
 
     def compute_batch(self, structs, types, pos, out=None, accumulate=False, sync_check=False,
                       stream=None):

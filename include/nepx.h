@@ -310,6 +310,31 @@ int nepx_md_device_state(nepx_md_t* md, double** d_pos, double** d_vel, double**
  */
 int nepx_set_precision(nepx_t* handle, int mode);
 
+/*
+ * Launch choices of the force kernels, as NEPX_TUNING_FIELDS ints:
+ *   [0] lanes per center of the typewise filter (4 or 8)
+ *   [1] lanes per center of the descriptor kernel (4 or 8)
+ *   [2] CTAs per SM the descriptor kernel is built for (3 or 4; the
+ *       tensor-core build runs at 3 whatever is set)
+ *   [3] lanes per center of the angular-force kernel (4 or 8)
+ *   [4] lanes per center of the gather (4 or 8)
+ *   [5] 1: the descriptor kernel evaluates the angular partial forces itself
+ *       (models with n_max <= 4, basis <= 8, l_max <= 4, on the Verlet-row
+ *       path), 0: k_angular_f12 does
+ * The first compute of a handle times the variants and keeps the fastest
+ * (the autotuner; its picks are shared by the handles of the process and,
+ * with NEPX_TUNE_FILE set, kept in that file).  nepx_get_tuning reports the
+ * current choices and *tuned = 1 once they are fixed.  nepx_set_tuning fixes
+ * them for every later call on the handle (no timing runs), for example to
+ * repeat a run's summation order bit for bit; values outside the lists
+ * above return NEPX_ERR_ARG.  nepx_set_precision with a new mode lets the
+ * autotuner choose again.  No counterpart in the reference (fixed launch
+ * shapes).
+ */
+#define NEPX_TUNING_FIELDS 6
+int nepx_get_tuning(nepx_t* handle, int* values, int* tuned);
+int nepx_set_tuning(nepx_t* handle, const int* values);
+
 /* ---- many independent structures --------------------------------------- */
 
 /* One structure of a batch: n atoms, consecutive in the batch arrays. */

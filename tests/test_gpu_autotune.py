@@ -48,6 +48,78 @@ def test_tune_file_reused_across_processes(tmp_path):
     # second process found it in the file
     assert len(lines[0]) == 1 and lines[1] == lines[0]
     fields = lines[0][0].split()
-    assert len(fields) == 19
+    assert len(fields) == 20   # 14 key fields, 6 launch choices
     import numpy as np
     assert np.array_equal(np.load(forces[0]), np.load(forces[1]))
+
+
+# ---- pinned launch choices ------------------------------------------------
+
+def _systems(tmp_path):
+    """Models of the shape the fused angular force serves (n_max <= 4, basis
+    <= 8, l_max <= 4): the water potential and the benchmark's synthetic
+    carbon NEP4, on large boxes."""
+    import workloads
+    from conftest import potential
+    t, h, p = workloads.water(n_mol=700, seed=5)
+    yield "water", potential("nep_water.txt"), t, h, p
+    path = workloads.write_nep(str(tmp_path / "c.txt"), version=4, symbols=("C",),
+                               rc=(4.2, 3.7), mn=(100, 60), n_max=(4, 4), basis=(8, 8),
+                               l_max=(4, 2, 1), H=30, seed=2025, q_scaler=0.02)
+    t, h, p = workloads.diamond(ncell=5, jitter=0.08, seed=6)
+    yield "carbon", path, t, h, p
+
+
+def test_every_launch_choice_matches_oracle(tmp_path):
+    """Each lane grouping, occupancy build and both forms of the angular
+    force (own kernel, or inside the descriptor kernel), pinned with
+    nepx_set_tuning, against the FP64 oracle at the FP32 tolerances; the
+    mixed-precision build with the fused angular force at its own."""
+    import numpy as np
+    import torch
+    import nepx
+    import oracle
+    from test_gpu_force import assert_close
+    from test_gpu_mixed import assert_mixed_close
+    for name, path, t, h, p in _systems(tmp_path):
+        ref = oracle.OracleModel(path).compute(t, h, p)
+        tt = torch.as_tensor(np.asarray(t, dtype=np.int32), device="cuda")
+        pp = torch.as_tensor(np.ascontiguousarray(p), device="cuda")
+        pot = nepx.Potential(path, max_atoms=len(t))
+        for ff in (0, 1):
+            for g in (4, 8):
+                for ctas in (3, 4):
+                    pot.set_tuning(filter_group=g, fused_group=g, fused_ctas_per_sm=ctas,
+                                   f12_group=12 - g, gather_group=g, fused_f12=ff)
+                    got = [x.cpu().numpy() for x in pot.compute(tt, h, pp, sync_check=True)]
+                    assert pot.tuning() == ({"filter_group": g, "fused_group": g,
+                                             "fused_ctas_per_sm": ctas, "f12_group": 12 - g,
+                                             "gather_group": g, "fused_f12": ff}, True)
+                    assert_close(ref, got, "%s ff=%d G=%d ctas=%d" % (name, ff, g, ctas))
+        pot.set_precision("mixed")
+        pot.set_tuning(fused_f12=1, fused_group=4)
+        got = [x.cpu().numpy() for x in pot.compute(tt, h, pp, sync_check=True)]
+        assert_mixed_close(ref, got, name + " fused f12", "mixed")
+        with pytest.raises(nepx.NepxError):
+            pot.set_tuning(fused_group=5)
+        pot.close()
+
+
+def test_autotuner_times_the_fused_angular_force(tmp_path):
+    """With nothing pinned the first compute fixes every choice, and the
+    chosen form gives the oracle's forces."""
+    import numpy as np
+    import torch
+    import nepx
+    import oracle
+    from test_gpu_force import assert_close
+    name, path, t, h, p = next(_systems(tmp_path))
+    pot = nepx.Potential(path, max_atoms=len(t))
+    assert pot.tuning()[1] is False
+    tt = torch.as_tensor(np.asarray(t, dtype=np.int32), device="cuda")
+    pp = torch.as_tensor(np.ascontiguousarray(p), device="cuda")
+    got = [x.cpu().numpy() for x in pot.compute(tt, h, pp, sync_check=True)]
+    choice, tuned = pot.tuning()
+    assert tuned and choice["fused_f12"] in (0, 1)
+    assert_close(oracle.OracleModel(path).compute(t, h, p), got, name)
+    pot.close()
