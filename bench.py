@@ -22,12 +22,13 @@ value  -- device time (CUDA events on the MD stream) of K steps queued in
 e2e    -- the same K steps driven through the public C API one step per call
           (nepx_md_run: graph launch, thermo row D2H, synchronisation), host
           wall clock.
-roofline -- the four force kernels (k_filter_radial, k_nep_fused,
-          k_angular_f12, k_gather): the FP32 operations of the algorithm they
-          run (flops_per_atom + gather_flops_per_atom, per atom at the
-          system's mean neighbour counts) over their CUDA-event time, against
-          the FP32 FMA peak of B200 (148 SMs x 128 lanes x 2 FLOP x max SM
-          clock).  traffic: their DRAM bytes per force call from ncu.
+roofline -- the force kernels (k_filter_radial, k_nep_fused, k_gather, and
+          k_angular_f12 unless the autotuner moved the angular partial forces
+          into k_nep_fused): the FP32 operations of the algorithm they run
+          (flops_per_atom + gather_flops_per_atom, per atom at the system's
+          mean neighbour counts) over their CUDA-event time, against the FP32
+          FMA peak of B200 (148 SMs x 128 lanes x 2 FLOP x max SM clock).
+          traffic: their DRAM bytes per force call from ncu.
 cpu_baseline -- the reference's own FP64 CPU NEP evaluator (NEP3_CPU,
           oracle/_ref) on all host cores, on a bounded sample of the same
           workload (a periodic block of the same lattice, same displacement
@@ -42,7 +43,8 @@ other_workloads -- water (24,000 atoms, Bussi NVT) and copper (1.0 M atoms,
           NEP-ZBL, Berendsen NPT): MD rate, force call, mixed precision and
           FP64 errors.
 nve_drift -- NVE energy drift (eV/atom/ns) of 4096-atom diamond carbon,
-          20,000 steps of 1 fs, both precisions.
+          both precisions: 20 ps from the lattice, and 200 ps after 10 ps of
+          Berendsen NVT (slope, its block standard error, 20 ps sub-windows).
 serving -- a 5,000-request sample of the serving stream (--workload serving
           runs the full 20,000): served structures/s, p50/p99 latency at 30,
           60 and 90% of saturation, batched engine over the plain FP32 path.
@@ -74,13 +76,16 @@ import numpy as np  # noqa: E402
 import workloads  # noqa: E402
 
 K_B = 8.617343e-5
-# DRAM bytes per atom and force call of the four force kernels (k_filter_radial,
-# k_nep_fused, k_angular_f12, k_gather), dram__bytes_read.sum +
+# DRAM bytes per atom and force call of the force kernels (k_filter_radial,
+# k_nep_fused with the angular partial forces inside, k_gather: the form the
+# autotuner picks for this model), dram__bytes_read.sum +
 # dram__bytes_write.sum of one ncu-captured launch each on the large-carbon
 # system at 1,000,000 atoms (--ncell 50), divided by its atoms (traffic grows
-# with the atoms processed)
-TRAFFIC_PER_ATOM = {"carbon8m": (683.1 + 386.7 + 318.7 + 489.9 + 808.4 + 533.9 + 1352.8
-                                 + 103.9) * 1e6 / 1.0e6}
+# with the atoms processed).  Keyed by workload and the kernel list; another
+# form reports no traffic.
+TRAFFIC_PER_ATOM = {
+    ("carbon8m", ("k_filter_radial", "k_nep_fused", "k_gather")):
+        (694.4 + 402.8 + 349.1 + 567.1 + 1349.8 + 99.0) * 1e6 / 1.0e6}
 FP32_LANES = 148 * 128          # B200: SMs x FP32 lanes
 SM_MAX_MHZ = 1965.0
 L2_NOTE = "flushed by a 512 MiB write before every %d-step chunk"
@@ -454,20 +459,27 @@ def fp64_errors(nep_path, rc_max, t, h, p, outs, clusters=9, r_core=20.0, seed=5
     return out
 
 
-def nve_drift(precision, steps=20000, every=100, equilibrate=10000):
+def nve_drift(precision, steps=20000, long_steps=200000, every=100, equilibrate=10000):
     """NVE energy drift of the diamond-carbon workload (8x8x8 cells, 4096
-    atoms, synthetic NEP4, 300 K, dt 1 fs, 20 ps): least-squares slope of the total
+    atoms, synthetic NEP4, 300 K, dt 1 fs): least-squares slope of the total
     energy per atom against time, the reference's definition
     (tests/long_nve/long_nve_common.py nve_metrics), in eV/atom/ns.
 
-    Two windows: from the lattice with Maxwell-Boltzmann velocities (the
-    reference's long NVE run), where kinetic energy flows into the lattice
-    over the first picoseconds and velocity Verlet's O(dt^2) energy offset
-    moves with it; and after `equilibrate` steps of Berendsen NVT at 300 K,
-    where what is left is the integrator's and the arithmetic's drift.  The
-    model's neighbour-row capacities are raised to MN 200/150: over tens of
-    picoseconds the random-weight model densifies parts of the crystal, and
-    its largest angular row (about 74) would reach the workload's 75."""
+    Two windows: 20 ps from the lattice with Maxwell-Boltzmann velocities
+    (the reference's long NVE run), where kinetic energy flows into the
+    lattice over the first picoseconds and velocity Verlet's O(dt^2) energy
+    offset moves with it; and 200 ps after `equilibrate` steps of Berendsen
+    NVT at 300 K, where what is left is the integrator's and the arithmetic's
+    drift.  The total energy of a 4096-atom NVE system fluctuates by ~1e-7
+    eV/atom over picoseconds (the shadow-energy offset follows the kinetic /
+    potential split), so the slope of one 20 ps window scatters by about
+    2e-5 eV/atom/ns whatever the precision; over 200 ps it resolves a few
+    1e-6.  The long window reports its slope, the slope's standard error from
+    ten block means, and the mean and spread of the slopes of its ten 20 ps
+    sub-windows.  The model's neighbour-row capacities are raised to MN
+    200/150: over tens of picoseconds the random-weight model densifies parts
+    of the crystal, and its largest angular row (about 74) would reach the
+    workload's 75."""
     import nepx
     spec = WORKLOADS["carbon"]
     tmp = tempfile.mkdtemp()
@@ -478,27 +490,42 @@ def nve_drift(precision, steps=20000, every=100, equilibrate=10000):
     pot = nepx.Potential(path, max_atoms=len(t))
     pot.set_precision(precision)
 
-    def window(md):
+    def window(md, nsteps, blocks=0):
         try:
-            rows = md.run(steps, 1.0, thermo_every=every)
+            rows = md.run(nsteps, 1.0, thermo_every=every)
         except nepx.NepxError as exc:   # reported in the line instead of ending the bench
             return {"error": str(exc)}
         e = (rows[:, 1] + rows[:, 2]) / len(t)
         time_ns = np.arange(1, len(e) + 1) * every * 1.0e-6
-        return {"drift_eV_per_atom_per_ns": float(np.polyfit(time_ns, e, 1)[0]),
-                "max_excursion_eV_per_atom": float(np.abs(e - e[0]).max())}
+        out = {"drift_eV_per_atom_per_ns": float(np.polyfit(time_ns, e, 1)[0]),
+               "max_excursion_eV_per_atom": float(np.abs(e - e[0]).max()),
+               "ps": nsteps * 1.0e-3}
+        if blocks:
+            m = len(e) // blocks
+            sub = [float(np.polyfit(time_ns[k * m:(k + 1) * m], e[k * m:(k + 1) * m], 1)[0])
+                   for k in range(blocks)]
+            bt = np.array([time_ns[k * m:(k + 1) * m].mean() for k in range(blocks)])
+            be = np.array([e[k * m:(k + 1) * m].mean() for k in range(blocks)])
+            c = np.polyfit(bt, be, 1)
+            r = be - np.polyval(c, bt)
+            out["slope_stderr_blocks"] = float(
+                np.sqrt((r ** 2).sum() / (blocks - 2) / ((bt - bt.mean()) ** 2).sum()))
+            out["sub_windows_ps"] = nsteps * 1.0e-3 / blocks
+            out["sub_window_drift_mean"] = float(np.mean(sub))
+            out["sub_window_drift_std"] = float(np.std(sub))
+        return out
 
     md = nepx.MD(pot, t, masses, p, v, h)
     md.set_ensemble("nve")
     md.run(1, 1.0)
-    out = window(md)
+    out = window(md, steps)
     md.close()
     md = nepx.MD(pot, t, masses, p, v, h)
     md.set_ensemble("nvt_ber", T0=300.0, Tdamp=100.0)
     try:
         md.run(equilibrate, 1.0)
         md.set_ensemble("nve")
-        out["equilibrated"] = window(md)
+        out["equilibrated"] = window(md, long_steps, blocks=10)
     except nepx.NepxError as exc:
         out["equilibrated"] = {"error": str(exc)}
     out["equilibrated"]["nvt_ber_steps_before"] = equilibrate
@@ -780,8 +807,16 @@ def mean_neighbors(pot, n):
     return float(pot.neighbor_counts(0, m).mean()), float(pot.neighbor_counts(1, m).mean())
 
 
+def force_kernels(pot):
+    """The force kernels of a Verlet-row force call with the handle's launch
+    choices: the angular partial forces come from the descriptor kernel
+    itself or from k_angular_f12."""
+    fused = pot.tuning()[0]["fused_f12"] == 1
+    return ["k_filter_radial", "k_nep_fused"] + ([] if fused else ["k_angular_f12"]) + ["k_gather"]
+
+
 def roofline_of(pot, name, n, prof):
-    """The four force kernels against the FP32 FMA peak (stage times of prof)."""
+    """The force kernels against the FP32 FMA peak (stage times of prof)."""
     mean_r, mean_a = mean_neighbors(pot, n)
     info = dict(pot.info)
     fpa = flops_per_atom(info, mean_r, mean_a)
@@ -789,12 +824,12 @@ def roofline_of(pot, name, n, prof):
     ms = prof["descriptor"] + prof["gather"]
     achieved = (fpa + gfa) * n / (ms * 1e-3) / 1e12
     peak = FP32_LANES * 2 * SM_MAX_MHZ * 1e6 / 1e12
-    per_atom = TRAFFIC_PER_ATOM.get(name)
+    per_atom = TRAFFIC_PER_ATOM.get((name, tuple(force_kernels(pot))))
     return {"bound": "fp32",
-            "kernel": "k_filter_radial + k_nep_fused + k_angular_f12 + k_gather (force stage)",
+            "kernel": " + ".join(force_kernels(pot)) + " (force stage)",
             "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
             "traffic": per_atom * n if per_atom else None,
-            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the four "
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the force "
                               "kernels, one launch each, per atom of the captured system "
                               "times this system's atoms",
             "peak_source": "B200 FP32 FMA peak: 148 SMs x 128 lanes x 2 FLOP x 1965 MHz "
@@ -911,10 +946,10 @@ def main():
     # 1. the headline: FP32 MD, device time
     dev_ms, st, clock_info, nchunks = timed_md(pot, sysd, args, rank, ranks, flush, clocks)
     value, dev_ms = replica_rate(n, K, dev_ms, ranks)
-    # k_vv1 (with the skin check), five Verlet-rebuild kernels (each returns at
-    # once unless a rebuild is due), k_filter_radial, k_nep_fused,
-    # k_angular_f12, k_gather, k_vv2_thermo, k_ensemble, k_scale; NHC adds two
-    kernels_per_step = 13 + (2 if kind == "nvt_nhc" else 0)
+    # k_vv1 (with the skin check), k_neighbor_rebuild (returns at once unless
+    # a rebuild is due), the force kernels, k_vv2_thermo, k_ensemble, k_scale;
+    # NHC adds two
+    kernels_per_step = 5 + len(force_kernels(pot)) + (2 if kind == "nvt_nhc" else 0)
     # per call (chunk): k_mark_call before the step graphs and k_publish after
     # them; the L2-flush fills are torch's, not counted
     launches = K * kernels_per_step + 2 * nchunks
