@@ -180,6 +180,7 @@ std::string engine_create(Engine& e, const std::string& nep_path, int max_atoms)
   ok &= dalloc(nb.cell_start, nb.cell_cap) == cudaSuccess;
   ok &= dalloc(nb.cell_atoms, N) == cudaSuccess;
   ok &= dalloc(nb.cell_of, N) == cudaSuccess;
+  ok &= dalloc(nb.cell_sites, N) == cudaSuccess;
   ok &= dalloc(nb.x0, 3 * static_cast<size_t>(N)) == cudaSuccess;
   ok &= dalloc(e.scratch.sites, N) == cudaSuccess;
   ok &= dalloc(e.scratch.qrad, static_cast<size_t>(N) * p.nR) == cudaSuccess;
@@ -487,7 +488,7 @@ void engine_destroy(Engine& e)
   NeighborBuffers& nb = e.nbr;
   void* ptrs[] = {e.d_params, e.d_box, e.d_nstate, nb.nn_v, nb.nl_v, nb.nn_r, nb.nl_r,
                   nb.nn_a, nb.nl_a, nb.gsync, nb.scan_part, nb.cell_count, nb.cell_start, nb.cell_atoms, nb.cell_of,
-                  nb.x0, e.scratch.alpha, e.scratch.f12, e.scratch.pe_ann, e.d_w16,
+                  nb.cell_sites, nb.x0, e.scratch.alpha, e.scratch.f12, e.scratch.pe_ann, e.d_w16,
                   e.scratch.tune_out, e.scratch.acoef, e.scratch.sites, e.scratch.qrad,
                   e.xr.er, e.xr.ea, e.xr.large,
                   e.xr.d_si, e.xr.d_soff};

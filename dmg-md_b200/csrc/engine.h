@@ -29,6 +29,7 @@ struct NeighborBuffers {
   int* cell_start = nullptr;
   int* cell_atoms = nullptr;
   int* cell_of = nullptr;
+  Site* cell_sites = nullptr;   // [N] site records in cell order (beside cell_atoms)
   int cell_cap = 0;
   double* x0 = nullptr;  // positions at the last Verlet build (3N SoA)
 };

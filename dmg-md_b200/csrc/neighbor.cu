@@ -118,6 +118,43 @@ __device__ int block_scan(int v, int* s_tmp, int* total)
   return x + before;
 }
 
+// Compare-exchange of two values held by one lane: the pair's lower element
+// keeps the smaller value when its block sorts ascending.
+__device__ __forceinline__ void cx_pair(int& lo, int& hi, bool ascending)
+{
+  const int a = min(lo, hi), c = max(lo, hi);
+  lo = ascending ? a : c;
+  hi = ascending ? c : a;
+}
+
+// Ascending bitonic sort of the first p2 (a power of two, at most 128)
+// values of a warp, four per lane: element e = lane + 32 r is v[r] (padding
+// INT_MAX).  Partners e ^ jj exchange by shuffle (jj < 32) or inside the
+// lane (jj = 32, 64); e keeps the smaller value when (e < partner) matches the
+// ascending direction (e & k) == 0 of its block.
+__device__ __forceinline__ void warp_sort128(int (&v)[4], int p2, int lane)
+{
+  for (int k = 2; k <= p2; k <<= 1) {
+    for (int jj = k >> 1; jj > 0; jj >>= 1) {
+      if (jj == 64) {
+        cx_pair(v[0], v[2], (lane & k) == 0);
+        cx_pair(v[1], v[3], ((lane + 32) & k) == 0);
+      } else if (jj == 32) {
+        cx_pair(v[0], v[1], (lane & k) == 0);
+        cx_pair(v[2], v[3], ((lane + 64) & k) == 0);
+      } else {
+        const bool lower = (lane & jj) == 0;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const int pv = __shfl_xor_sync(0xffffffffu, v[r], jj);
+          const bool asc = ((lane + 32 * r) & k) == 0;
+          v[r] = (lower == asc) ? min(v[r], pv) : max(v[r], pv);
+        }
+      }
+    }
+  }
+}
+
 struct RebuildArgs {
   int N;
   const Box* box;
@@ -129,6 +166,7 @@ struct RebuildArgs {
   int* cell_start;
   int* cell_atoms;
   int* cell_of;
+  Site* cell_sites;    // the site records in cell order (beside cell_atoms)
   int* nn_v;
   int* nl_v;
   double* x0;
@@ -148,11 +186,11 @@ struct RebuildArgs {
 //      cell_cap of them), counts cleared;
 //   2. cell of every atom, counts;
 //   3. exclusive scan of the counts (per-block chunks, then block offsets);
-//   4. atoms into their cells;
+//   4. atoms into their cells (index and site record, in cell order);
 //   5. Verlet rows: one warp per center gathers every candidate of the 5x5x5
-//      stencil with float d^2 < (rc + skin)^2, sorts the row in shared memory
-//      (bitonic) and writes it with the reference positions of the next skin
-//      check.
+//      stencil with float d^2 < (rc + skin)^2, sorts the row (bitonic, in
+//      registers up to 128 entries) and writes it with the reference
+//      positions of the next skin check.
 // Phases 1-5 run only when the rebuild flag is set; the flag is the same for
 // every block, so all of them return together.
 __global__ void __launch_bounds__(kRebuildThreads, 12)
@@ -249,86 +287,141 @@ k_neighbor_rebuild(const RebuildArgs a)
   }
   grid_sync(a.gsync, st);
 
-  // 4. fill (the counts are the cell totals again afterwards)
+  // 4. fill (the counts are the cell totals again afterwards); each atom's
+  //    site record goes beside its index, so a cell's candidates are one
+  //    contiguous run of records
   for (int i = gtid; i < N; i += nthreads) {
     const int c = a.cell_of[i];
     const int slot = atomicAdd(a.cell_count + c, 1);
-    a.cell_atoms[a.cell_start[c] + slot] = i;
+    const int at = a.cell_start[c] + slot;
+    a.cell_atoms[at] = i;
+    a.cell_sites[at] = a.sites[i];
   }
   grid_sync(a.gsync, st);
 
-  // 5. Verlet rows, one warp per center
+  // 5. Verlet rows, one warp per center.  The 5x5x5 stencil cells go in
+  //    rounds of 32: lane q takes a cell, a warp prefix sum of their counts
+  //    flattens their atoms into one range, and the warp sweeps it 32
+  //    candidates at a time, reading the cell-ordered index and site record
+  //    side by side (no load waits on another).  Hits are compacted in order
+  //    of discovery (ballot + popcount) and the row is sorted: in registers,
+  //    four values per lane, up to 128 entries; in shared memory above.
   const int lane = tid & 31, warp = tid >> 5;
+  const unsigned below = (1u << lane) - 1u;
   const int pow2 = a.pow2;
   int* buf = s_rows + warp * (pow2 + 1);
-  int* count = buf + pow2;
+  const int span0 = (b.pbc[0] && nc0 >= 5) ? 5 : nc0;
+  const int span1 = (b.pbc[1] && nc1 >= 5) ? 5 : nc1;
+  const int span2 = (b.pbc[2] && nc2 >= 5) ? 5 : nc2;
+  const int ncand = span0 * span1 * span2;   // at most 125
+  const bool full = span0 == 5 && span1 == 5 && span2 == 5;
   for (int i = blockIdx.x * kRebuildWarps + warp; i < N; i += gridDim.x * kRebuildWarps) {
-    if (lane == 0) *count = 0;
-    __syncwarp();
-    const double xi = a.sites[i].x, yi = a.sites[i].y, zi = a.sites[i].z;
     // the site records may have been written by this launch (phase 0): plain
     // loads, which the barriers order, not the read-only path
+    const double xi = a.sites[i].x, yi = a.sites[i].y, zi = a.sites[i].z;
     const int ci = a.cell_of[i];
     const int cx = ci % nc0, cy = (ci / nc0) % nc1, cz = ci / (nc0 * nc1);
-    // per direction: 5 wrapped offsets when the grid is wide enough, else
-    // every cell of that direction exactly once
-    const int span0 = (b.pbc[0] && nc0 >= 5) ? 5 : nc0;
-    const int span1 = (b.pbc[1] && nc1 >= 5) ? 5 : nc1;
-    const int span2 = (b.pbc[2] && nc2 >= 5) ? 5 : nc2;
-    const int ncand = span0 * span1 * span2;
-    for (int s = lane; s < ncand; s += 32) {
-      const int s0 = s % span0, s1 = (s / span0) % span1, s2 = s / (span0 * span1);
-      int gx = span0 == 5 ? cx + s0 - 2 : s0;
-      int gy = span1 == 5 ? cy + s1 - 2 : s1;
-      int gz = span2 == 5 ? cz + s2 - 2 : s2;
-      if (gx < 0) gx += nc0; else if (gx >= nc0) gx -= nc0;
-      if (gy < 0) gy += nc1; else if (gy >= nc1) gy -= nc1;
-      if (gz < 0) gz += nc2; else if (gz >= nc2) gz -= nc2;
-      const int c = (gz * nc1 + gy) * nc0 + gx;
-      const int start = a.cell_start[c];
-      const int cnt = a.cell_count[c];
-      for (int m = 0; m < cnt; ++m) {
-        const int j = a.cell_atoms[start + m];
-        if (j == i) continue;
-        const double2 sa = reinterpret_cast<const double2*>(a.sites + j)[0];
-        const double2 sc = reinterpret_cast<const double2*>(a.sites + j)[1];
-        float dx, dy, dz;
-        int tj;
-        site_delta(b, sa, sc, xi, yi, zi, dx, dy, dz, tj);
-        const float d2 = dx * dx + dy * dy + dz * dz;
-        if (d2 < a.cutoff_square) {
-          const int slot = atomicAdd(count, 1);
+    int total = 0;
+    for (int r0 = 0; r0 < ncand; r0 += 32) {
+      int my_start = 0, my_cnt = 0;
+      if (r0 + lane < ncand) {
+        const int q = r0 + lane;
+        int q0, q1, q2;
+        if (full) {   // constant divisors
+          q0 = q % 5;
+          q1 = (q / 5) % 5;
+          q2 = q / 25;
+        } else {
+          q0 = q % span0;
+          q1 = (q / span0) % span1;
+          q2 = q / (span0 * span1);
+        }
+        int gx = span0 == 5 ? cx + q0 - 2 : q0;
+        int gy = span1 == 5 ? cy + q1 - 2 : q1;
+        int gz = span2 == 5 ? cz + q2 - 2 : q2;
+        if (gx < 0) gx += nc0; else if (gx >= nc0) gx -= nc0;
+        if (gy < 0) gy += nc1; else if (gy >= nc1) gy -= nc1;
+        if (gz < 0) gz += nc2; else if (gz >= nc2) gz -= nc2;
+        const int c = (gz * nc1 + gy) * nc0 + gx;
+        my_start = a.cell_start[c];
+        my_cnt = a.cell_count[c];
+      }
+      int incl = my_cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+      }
+      const int total_c = __shfl_sync(0xffffffffu, incl, 31);
+      for (int base = 0; base < total_c; base += 32) {
+        const int k = base + lane;
+        // stencil cell of candidate k: the first lane whose inclusive count exceeds k
+        int lo = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+          const int v = __shfl_sync(0xffffffffu, incl, lo + step - 1);
+          if (v <= k) lo += step;
+        }
+        const int cstart = __shfl_sync(0xffffffffu, my_start, lo);
+        const int cincl = __shfl_sync(0xffffffffu, incl, lo);
+        const int ccnt = __shfl_sync(0xffffffffu, my_cnt, lo);
+        bool hit = false;
+        int j = 0;
+        if (k < total_c) {
+          const int at = cstart + (k - (cincl - ccnt));
+          j = a.cell_atoms[at];
+          const double2 sa = reinterpret_cast<const double2*>(a.cell_sites + at)[0];
+          const double2 sc = reinterpret_cast<const double2*>(a.cell_sites + at)[1];
+          float dx, dy, dz;
+          int tj;
+          site_delta(b, sa, sc, xi, yi, zi, dx, dy, dz, tj);
+          const float d2 = dx * dx + dy * dy + dz * dz;
+          hit = j != i && d2 < a.cutoff_square;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, hit);
+        if (hit) {
+          const int slot = total + __popc(m & below);
           if (slot < pow2) buf[slot] = j;
         }
+        total += __popc(m);
       }
     }
     __syncwarp();
-    const int total = *count;
     const int used = min(total, pow2);
-    // bitonic sort of the smallest power of two that holds the row (padding
-    // INT_MAX), one compare-exchange pair per lane and pass
     int p2 = 1;
     while (p2 < used) p2 <<= 1;
-    for (int k = used + lane; k < p2; k += 32) buf[k] = INT_MAX;
-    __syncwarp();
-    for (int k = 2; k <= p2; k <<= 1) {
-      for (int j = k >> 1; j > 0; j >>= 1) {
-        for (int q = lane; q < (p2 >> 1); q += 32) {
-          const int t = ((q & ~(j - 1)) << 1) | (q & (j - 1));   // lower index of the pair
-          const int u = t | j;
-          const int x = buf[t], y = buf[u];
-          const bool up = (t & k) == 0;
-          if ((x > y) == up) {
-            buf[t] = y;
-            buf[u] = x;
-          }
-        }
-        __syncwarp();
-      }
-    }
     const int keep = min(total, a.mn_v);
     int* row = a.nl_v + static_cast<size_t>(i) * a.mn_v;
-    for (int k = lane; k < keep; k += 32) row[k] = buf[k];
+    if (p2 <= 128) {
+      int v[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) v[r] = lane + 32 * r < used ? buf[lane + 32 * r] : INT_MAX;
+      warp_sort128(v, p2, lane);
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+        if (lane + 32 * r < keep) row[lane + 32 * r] = v[r];
+    } else {
+      // bitonic sort of the smallest power of two that holds the row (padding
+      // INT_MAX), one compare-exchange pair per lane and pass
+      for (int k = used + lane; k < p2; k += 32) buf[k] = INT_MAX;
+      __syncwarp();
+      for (int k = 2; k <= p2; k <<= 1) {
+        for (int jj = k >> 1; jj > 0; jj >>= 1) {
+          for (int q = lane; q < (p2 >> 1); q += 32) {
+            const int t = ((q & ~(jj - 1)) << 1) | (q & (jj - 1));   // lower index of the pair
+            const int u = t | jj;
+            const int x = buf[t], y = buf[u];
+            const bool up = (t & k) == 0;
+            if ((x > y) == up) {
+              buf[t] = y;
+              buf[u] = x;
+            }
+          }
+          __syncwarp();
+        }
+      }
+      for (int k = lane; k < keep; k += 32) row[k] = buf[k];
+    }
     if (lane == 0) {
       a.nn_v[i] = keep;
       if (total > a.mn_v) atomicOr(&st->overflow, 1);
@@ -382,6 +475,7 @@ void launch_neighbor_update(Engine& e, int N, const double* pos, const int* type
   a.cell_start = nb.cell_start;
   a.cell_atoms = nb.cell_atoms;
   a.cell_of = nb.cell_of;
+  a.cell_sites = nb.cell_sites;
   a.nn_v = nb.nn_v;
   a.nl_v = nb.nl_v;
   a.x0 = nb.x0;

@@ -92,6 +92,7 @@ size_t bytes_needed(const nepx::Engine& e, int n)
   c.take<int>(cells);           // cell_start
   c.take<int>(N);               // cell_atoms
   c.take<int>(N);               // cell_of
+  c.take<nepx::Site>(N);        // cell_sites
   c.take<double>(3 * N);        // x0
   c.take<nepx::Site>(N);
   c.take<float>(N * e.params.nR);
@@ -196,6 +197,7 @@ extern "C" int nepx_compute_noalloc(nepx_t* h, const nepx_box* box, int n, const
     nb.cell_start = c.take<int>(cells);
     nb.cell_atoms = c.take<int>(N);
     nb.cell_of = c.take<int>(N);
+    nb.cell_sites = c.take<nepx::Site>(N);
     nb.x0 = c.take<double>(3 * N);
     nb.cell_cap = static_cast<int>(cells);
     e.scratch.sites = c.take<nepx::Site>(N);
