@@ -295,6 +295,7 @@ int nepx_get_tuning(nepx_t* h, int* v, int* tuned)
   v[3] = e.f12_group;
   v[4] = e.gather_group;
   v[5] = e.fuse_f12 ? 1 : 0;
+  v[6] = e.gather_minb;
   if (tuned) *tuned = e.tuned ? 1 : 0;
   return NEPX_OK;
 }
@@ -304,7 +305,7 @@ int nepx_set_tuning(nepx_t* h, const int* v)
   if (!h || !v) return NEPX_ERR_ARG;
   auto lanes = [](int g) { return g == 4 || g == 8; };
   if (!lanes(v[0]) || !lanes(v[1]) || !(v[2] == 3 || v[2] == 4) || !lanes(v[3]) ||
-      !lanes(v[4]) || !(v[5] == 0 || v[5] == 1))
+      !lanes(v[4]) || !(v[5] == 0 || v[5] == 1) || !(v[6] == 3 || v[6] == 4))
     return fail(h, NEPX_ERR_ARG, "launch choice outside the built variants");
   nepx::Engine& e = h->engine;
   e.filter_group = v[0];
@@ -313,6 +314,7 @@ int nepx_set_tuning(nepx_t* h, const int* v)
   e.f12_group = v[3];
   e.gather_group = v[4];
   e.fuse_f12 = v[5] == 1;
+  e.gather_minb = v[6];
   e.tuned = true;
   return NEPX_OK;
 }

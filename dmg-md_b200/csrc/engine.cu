@@ -218,7 +218,7 @@ struct TuneKey {
   bool operator==(const TuneKey& o) const { return std::memcmp(v, o.v, sizeof(v)) == 0; }
 };
 struct TuneVal {
-  int filter_group, group, fused_minb, f12_group, gather_group, fuse_f12;
+  int filter_group, group, fused_minb, f12_group, gather_group, fuse_f12, gather_minb;
 };
 
 std::mutex g_tune_mu;
@@ -231,7 +231,7 @@ TuneKey tune_key(const Engine& e, int N)
   int size_class = 0;
   while ((1 << (size_class + 1)) <= N) ++size_class;   // floor(log2 N)
   TuneKey k{{e.device, e.use_xr ? 1 : 0, e.precision, p.T, p.nR, p.nA, p.kR, p.kA, p.L_max,
-             p.dim, p.H, p.num_inv, size_class, 2}};
+             p.dim, p.H, p.num_inv, size_class, 3}};
   return k;
 }
 
@@ -250,12 +250,12 @@ void tune_load_file()
     bool ok = true;
     for (int& x : k.v) ok = ok && static_cast<bool>(ls >> x);
     ok = ok && static_cast<bool>(ls >> v.filter_group >> v.group >> v.fused_minb >> v.f12_group >>
-                                 v.gather_group >> v.fuse_f12);
+                                 v.gather_group >> v.fuse_f12 >> v.gather_minb);
     // only the shapes the launchers instantiate; anything else is ignored
     auto lanes = [](int g) { return g == 4 || g == 8; };
     ok = ok && lanes(v.filter_group) && lanes(v.group) && lanes(v.f12_group) &&
          lanes(v.gather_group) && (v.fused_minb == 3 || v.fused_minb == 4) &&
-         (v.fuse_f12 == 0 || v.fuse_f12 == 1);
+         (v.fuse_f12 == 0 || v.fuse_f12 == 1) && (v.gather_minb == 3 || v.gather_minb == 4);
     if (ok) g_tune.emplace_back(k, v);
   }
 }
@@ -282,7 +282,7 @@ void tune_store(const TuneKey& k, const TuneVal& v)
     std::ofstream out(path, std::ios::app);
     for (int x : k.v) out << x << ' ';
     out << v.filter_group << ' ' << v.group << ' ' << v.fused_minb << ' ' << v.f12_group << ' '
-        << v.gather_group << ' ' << v.fuse_f12 << '\n';
+        << v.gather_group << ' ' << v.fuse_f12 << ' ' << v.gather_minb << '\n';
   }
 }
 
@@ -299,6 +299,7 @@ void engine_autotune(Engine& e, int N, const double* pos, const int* type, cudaS
     e.f12_group = known.f12_group;
     e.gather_group = known.gather_group;
     e.fuse_f12 = known.fuse_f12 != 0;
+    e.gather_minb = known.gather_minb;
     e.tuned = true;
     return;
   }
@@ -384,9 +385,37 @@ void engine_autotune(Engine& e, int N, const double* pos, const int* type, cudaS
       }
     }
   }
+  // the Verlet-row gather's two occupancy builds, with each grouping (the
+  // rows, alpha and f12 of the last descriptor call serve every variant)
+  int pick_gm = 3;
+  if (!e.use_xr && e.params.L_max <= 4) {
+    best_g = 1e30f;
+    for (int gm = 3; gm <= 4; ++gm)
+      for (int gg : groups) {
+        e.gather_minb = gm;
+        e.gather_group = gg;
+        float tg[3];
+        for (int r = 0; r < 3; ++r) {
+          cudaEventRecord(a, stream);
+          double* out = e.scratch.tune_out;
+          launch_gather(e, N, pos, type, out, out + N, out + 4 * static_cast<size_t>(N), false,
+                        stream);
+          cudaEventRecord(b, stream);
+          cudaEventSynchronize(b);
+          cudaEventElapsedTime(&tg[r], a, b);
+        }
+        std::sort(tg, tg + 3);
+        if (tg[1] < best_g) {
+          best_g = tg[1];
+          pick_g = gg;
+          pick_gm = gm;
+        }
+      }
+  }
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   cudaEventDestroy(c);
+  e.gather_minb = pick_gm;
   e.group = pick_f;
   e.fused_minb = pick_m;
   e.f12_group = pick_a;
@@ -394,14 +423,14 @@ void engine_autotune(Engine& e, int N, const double* pos, const int* type, cudaS
   e.fuse_f12 = pick_ff;
   e.tuned = true;
   tune_store(key, TuneVal{e.filter_group, e.group, e.fused_minb, e.f12_group, e.gather_group,
-                          e.fuse_f12 ? 1 : 0});
+                          e.fuse_f12 ? 1 : 0, e.gather_minb});
   if (std::getenv("NEPX_VERBOSE"))
     std::fprintf(stderr,
                  "nepx autotune (N=%d): filter G=%d, fused G=%d at %d CTAs/SM, angular force "
-                 "%s, G=%d, gather G=%d\n",
+                 "%s, G=%d, gather G=%d at %d CTAs/SM\n",
                  N, e.filter_group, e.group, e.fused_minb,
                  e.fuse_f12 ? "in the descriptor kernel" : "own kernel", e.f12_group,
-                 e.gather_group);
+                 e.gather_group, e.gather_minb);
 }
 
 namespace {

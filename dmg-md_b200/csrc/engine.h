@@ -119,6 +119,7 @@ struct Engine {
   int filter_group = 8;      // lanes per center in the typewise filter (autotuned)
   int f12_group = 4;         // lanes per center in the angular-force kernel (autotuned)
   int gather_group = 8;      // lanes per center in the gather (autotuned)
+  int gather_minb = 3;       // CTAs per SM the Verlet-row gather is built for (autotuned)
   bool fuse_f12 = false;     // the descriptor kernel evaluates f12 itself (autotuned)
   bool tuned = false;
   std::string error;
@@ -140,9 +141,9 @@ void set_fused_smem_limits(const ModelParams& p);
 
 // Times each kernel variant on the given system (a few calls each, stream
 // synchronised) and keeps the fastest: the lane-group size of the filter,
-// descriptor, angular-force and gather kernels, the descriptor kernel's
-// CTAs per SM, and whether the descriptor kernel evaluates the angular
-// partial forces itself.  The picks are kept per (device, model shape, precision, row
+// descriptor, angular-force and gather kernels, the CTAs per SM of the
+// descriptor kernel and of the gather, and whether the descriptor kernel
+// evaluates the angular partial forces itself.  The picks are kept per (device, model shape, precision, row
 // path, size class log2 N) for every later handle of the process, and in the
 // file NEPX_TUNE_FILE names, when set, across runs.  Neighbour rows must be
 // current.

@@ -1477,8 +1477,11 @@ k_angular_f12(const ModelParams p, int N, const Box* __restrict__ box,
 // (periodic images), so the reverse partial force f12(j,i) is not looked up
 // but evaluated here from j's moment derivatives at -r: the angular force
 // work doubles and the f12 buffer and its kernel drop out.
-template <int G, int KM, int NAM, bool XR, int LMAX>
-__global__ void __launch_bounds__(256)
+// GMINB: CTAs of 256 per SM the instance is built for (register cap), 0: no
+// cap.  The Verlet-row gather comes at 3 (its natural 78 registers) and at 4
+// (64 registers, a few spills, a third more warps); the autotuner picks one.
+template <int G, int KM, int NAM, bool XR, int LMAX, int GMINB = 0>
+__global__ void __launch_bounds__(256, (GMINB > 0 ? GMINB : 1))
 k_gather(const ModelParams p, int N, const Box* __restrict__ box,
          const Site* __restrict__ sites, const int* __restrict__ nn_r, const int* __restrict__ nl_r,
          int mn_r, const int* __restrict__ nn_a, const int* __restrict__ nl_a, int mn_a,
@@ -1799,7 +1802,7 @@ void set_fused_smem_t(const ModelParams& p)
                          cudaFuncAttributeMaxDynamicSharedMemorySize, bytes(false));
 }
 
-template <int G, int KM, int NAM, bool XR, int LMAX>
+template <int G, int KM, int NAM, bool XR, int LMAX, int GMINB = 0>
 void launch_gather_t(Engine& e, int N, double* pe, double* force, double* virial,
                      bool accumulate, cudaStream_t s)
 {
@@ -1808,7 +1811,7 @@ void launch_gather_t(Engine& e, int N, double* pe, double* force, double* virial
   const int blocks = static_cast<int>((static_cast<long long>(N) * G + threads - 1) / threads);
   const size_t smem =
     XR ? sizeof(float) * e.params.T * e.params.T * e.params.nA * ((KM + 3) & ~3) : 0;
-  k_gather<G, KM, NAM, XR, LMAX><<<blocks, threads, smem, s>>>(
+  k_gather<G, KM, NAM, XR, LMAX, GMINB><<<blocks, threads, smem, s>>>(
     e.params, N, e.d_box, e.scratch.sites, nb.nn_r, nb.nl_r, nb.mn_r, nb.nn_a, nb.nl_a, nb.mn_a,
     e.xr.er, e.xr.ea, e.scratch.acoef, e.scratch.alpha, e.scratch.f12, e.xr.large,
     e.scratch.pe_ann, pe,
@@ -1854,7 +1857,9 @@ void launch_gather_g(Engine& e, int N, double* pe, double* force, double* virial
                      bool accumulate, cudaStream_t s)
 {
   if (e.use_xr) launch_gather_t<G, KM, NAM, true, LMAX>(e, N, pe, force, virial, accumulate, s);
-  else launch_gather_t<G, KM, NAM, false, LMAX>(e, N, pe, force, virial, accumulate, s);
+  else if (LMAX == 4 && e.gather_minb == 4)
+    launch_gather_t<G, KM, NAM, false, LMAX, 4>(e, N, pe, force, virial, accumulate, s);
+  else launch_gather_t<G, KM, NAM, false, LMAX, 3>(e, N, pe, force, virial, accumulate, s);
 }
 
 }  // namespace

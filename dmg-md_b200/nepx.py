@@ -41,7 +41,7 @@ EXPORTED = ["nepx_create", "nepx_destroy", "nepx_last_error", "nepx_info", "nepx
             "nepx_server_memory", "nepx_server_set_row_reuse", "nepx_server_rows",
             "nepx_get_tuning", "nepx_set_tuning"]
 TUNING_FIELDS = ("filter_group", "fused_group", "fused_ctas_per_sm", "f12_group",
-                 "gather_group", "fused_f12")
+                 "gather_group", "fused_f12", "gather_ctas_per_sm")
 
 PRECISIONS = {"fp32": 0, "mixed": 1, "mixed_bf16": 2}
 ENSEMBLES = {"nve": 0, "nvt_ber": 1, "nvt_nhc": 2, "nvt_bdp": 3, "npt_ber": 4, "npt_scr": 5}

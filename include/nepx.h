@@ -321,6 +321,8 @@ int nepx_set_precision(nepx_t* handle, int mode);
  *   [5] 1: the descriptor kernel evaluates the angular partial forces itself
  *       (models with n_max <= 4, basis <= 8, l_max <= 4, on the Verlet-row
  *       path), 0: k_angular_f12 does
+ *   [6] CTAs of 256 per SM the Verlet-row gather is built for (3 or 4; models
+ *       with l_max <= 4)
  * The first compute of a handle times the variants and keeps the fastest
  * (the autotuner; its picks are shared by the handles of the process and,
  * with NEPX_TUNE_FILE set, kept in that file).  nepx_get_tuning reports the
@@ -331,7 +333,7 @@ int nepx_set_precision(nepx_t* handle, int mode);
  * autotuner choose again.  No counterpart in the reference (fixed launch
  * shapes).
  */
-#define NEPX_TUNING_FIELDS 6
+#define NEPX_TUNING_FIELDS 7
 int nepx_get_tuning(nepx_t* handle, int* values, int* tuned);
 int nepx_set_tuning(nepx_t* handle, const int* values);
 

@@ -48,7 +48,7 @@ def test_tune_file_reused_across_processes(tmp_path):
     # second process found it in the file
     assert len(lines[0]) == 1 and lines[1] == lines[0]
     fields = lines[0][0].split()
-    assert len(fields) == 20   # 14 key fields, 6 launch choices
+    assert len(fields) == 21   # 14 key fields, 7 launch choices
     import numpy as np
     assert np.array_equal(np.load(forces[0]), np.load(forces[1]))
 
@@ -71,8 +71,9 @@ def _systems(tmp_path):
 
 
 def test_every_launch_choice_matches_oracle(tmp_path):
-    """Each lane grouping, occupancy build and both forms of the angular
-    force (own kernel, or inside the descriptor kernel), pinned with
+    """Each lane grouping, occupancy build (descriptor kernel and gather) and
+    both forms of the angular force (own kernel, or inside the descriptor
+    kernel), pinned with
     nepx_set_tuning, against the FP64 oracle at the FP32 tolerances; the
     mixed-precision build with the fused angular force at its own."""
     import numpy as np
@@ -90,11 +91,13 @@ def test_every_launch_choice_matches_oracle(tmp_path):
             for g in (4, 8):
                 for ctas in (3, 4):
                     pot.set_tuning(filter_group=g, fused_group=g, fused_ctas_per_sm=ctas,
-                                   f12_group=12 - g, gather_group=g, fused_f12=ff)
+                                   f12_group=12 - g, gather_group=g, fused_f12=ff,
+                                   gather_ctas_per_sm=7 - ctas)
                     got = [x.cpu().numpy() for x in pot.compute(tt, h, pp, sync_check=True)]
                     assert pot.tuning() == ({"filter_group": g, "fused_group": g,
                                              "fused_ctas_per_sm": ctas, "f12_group": 12 - g,
-                                             "gather_group": g, "fused_f12": ff}, True)
+                                             "gather_group": g, "fused_f12": ff,
+                                             "gather_ctas_per_sm": 7 - ctas}, True)
                     assert_close(ref, got, "%s ff=%d G=%d ctas=%d" % (name, ff, g, ctas))
         pot.set_precision("mixed")
         pot.set_tuning(fused_f12=1, fused_group=4)
