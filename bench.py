@@ -807,6 +807,35 @@ def mean_neighbors(pot, n):
     return float(pot.neighbor_counts(0, m).mean()), float(pot.neighbor_counts(1, m).mean())
 
 
+# ncu on the tensor-core build of the descriptor kernel (one launch, 1,000,000
+# atoms of the large-carbon system, --set full): sm__pipe_tensor_cycles_active
+# and sm__pipe_tc_cycles_active, percent of the launch's cycles
+TENSOR_PIPE_ACTIVE_PCT = {"tensor": 0.63, "tc": 2.27}
+
+
+def ann_tensor_fraction(sysd, atom_steps_per_s):
+    """The ANN's algorithmic work on the tensor cores: 4 dim H FLOP per atom
+    (forward and backward contraction, FMA = 2) at the mixed MD's rate, as a
+    fraction of the measured dense bf16 peak (the FP16 MMAs run at the same
+    rate), with the tensor-pipe activity ncu measured."""
+    nep = sysd["spec"]["nep"]
+    n_r, n_a = nep["n_max"][0] + 1, nep["n_max"][1] + 1
+    l3 = nep["l_max"]
+    dim = n_r + n_a * (l3[0] + (1 if l3[1] else 0) + (1 if l3[2] else 0))
+    flops = 4 * dim * nep["H"]
+    peak = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            peak = json.load(fh).get("bf16_tflops")
+    except (OSError, ValueError):
+        pass
+    achieved = atom_steps_per_s * flops / 1e12
+    return {"flops_per_atom": flops, "dim": dim, "H": nep["H"], "achieved_tflops": achieved,
+            "peak_tflops": peak, "peak_source": "MEASURED_PEAKS.json bf16_tflops (measured)",
+            "frac": achieved / peak if peak else None,
+            "pipe_active_pct_ncu": TENSOR_PIPE_ACTIVE_PCT}
+
+
 def force_kernels(pot):
     """The force kernels of a Verlet-row force call with the handle's launch
     choices: the angular partial forces come from the descriptor kernel
@@ -866,7 +895,9 @@ def other_workload(name, args, rank, ranks, flush):
             "value": value, "unit": "atom-steps/s", "ms_per_step": dev_ms / args.steps,
             "steps": args.steps,
             "mixed_precision": {"value": n * args.steps / (dev_ms_m * 1e-3),
-                                "over_fp32": dev_ms / dev_ms_m, "stage_ms": prof_m},
+                                "over_fp32": dev_ms / dev_ms_m, "stage_ms": prof_m,
+                                "ann_tensor": ann_tensor_fraction(
+                                    sysd, n * args.steps / (dev_ms_m * 1e-3))},
             "force_call": {"ms": prof["total"], "stage_ms": prof,
                            "value": n / (prof["total"] * 1e-3)},
             "roofline": roof}
@@ -985,7 +1016,8 @@ def main():
              "what": "the same MD with the ANN's two contractions as tcgen05 MMAs inside the "
                      "descriptor kernel: FP16 operands with per-layer power-of-two scaling, FP32 "
                      "accumulation in TMEM; descriptors and forces FP32",
-             "stage_ms": prof_mixed}
+             "stage_ms": prof_mixed,
+             "ann_tensor": ann_tensor_fraction(sysd, value_mixed)}
     pot.close()
     del flush
     torch.cuda.empty_cache()
