@@ -202,16 +202,43 @@ __device__ __forceinline__ void skin_check_atom(int N, int i, const Box& b, doub
 }
 
 // Cutoff function fc = (1 + cos(pi d / rc)) / 2 and its d-derivative.
+// FAST (the mixed-precision kernels): sine and cosine from the hardware
+// approximations (absolute error about 4e-7 on [0, pi)) in place of the
+// correctly rounded sinpi/cospi.
+template <bool FAST = false>
 __device__ __forceinline__ void cutoff_fc(float rc, float rcinv, float d, float& fc, float& fcp)
 {
   if (d < rc) {
     float s, c;
-    sincospif(d * rcinv, &s, &c);
+    if constexpr (FAST) __sincosf(3.14159265f * (d * rcinv), &s, &c);
+    else sincospif(d * rcinv, &s, &c);
     fc = 0.5f * c + 0.5f;
     fcp = -1.5707963f * s * rcinv;
   } else {
     fc = 0.0f;
     fcp = 0.0f;
+  }
+}
+
+// 1 / x: IEEE rounded, or with FAST the hardware approximation (2 ulp).
+template <bool FAST>
+__device__ __forceinline__ float recip(float x)
+{
+  if constexpr (FAST) return __fdividef(1.0f, x);
+  else return 1.0f / x;
+}
+
+// Edge length d and 1 / d from d^2: correctly rounded square root and
+// division, or with FAST one hardware reciprocal square root (2 ulp).
+template <bool FAST>
+__device__ __forceinline__ void edge_length(float d2, float& d, float& dinv)
+{
+  if constexpr (FAST) {
+    dinv = rsqrtf(d2);
+    d = d2 * dinv;
+  } else {
+    d = sqrtf(d2);
+    dinv = 1.0f / d;
   }
 }
 

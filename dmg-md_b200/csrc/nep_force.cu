@@ -766,7 +766,9 @@ __device__ void tc_ann(const ModelParams& p, const FusedLayout& Lay, float* sm, 
 // (q_n = sum_t sum_k c(ti,t)[n][k] B[t][k]): a few float4 updates per edge
 // instead of the nR x kR contraction.  Kept apart from k_nep_fused so this
 // latency-bound sweep runs at the occupancy of its own register count.
-template <int G, int NRM, int KM, bool BIN>
+// FAST: the mixed-precision build (hardware sqrt / reciprocal / sine-cosine
+// approximations, see cutoff_fc).
+template <int G, int NRM, int KM, bool BIN, bool FAST>
 __global__ void __launch_bounds__(kBlock)
 k_filter_radial(const ModelParams p, int N, const Box* __restrict__ box,
                 const Site* __restrict__ sites, NeighborState* st,
@@ -844,10 +846,11 @@ k_filter_radial(const ModelParams p, int N, const Box* __restrict__ box,
     if (in_r) {
       const int at = cr + __popc(mr & below);
       if (at < mn_r) rrow[at] = j;
-      const float d = sqrtf(d12_square);
-      const float rcinv = 1.0f / rc_radial;
+      float d, dinv;
+      edge_length<FAST>(d12_square, d, dinv);
+      const float rcinv = recip<FAST>(rc_radial);
       float fc, fcp;
-      cutoff_fc(rc_radial, rcinv, d, fc, fcp);
+      cutoff_fc<FAST>(rc_radial, rcinv, d, fc, fcp);
       float fn[KP];
 #pragma unroll
       for (int kk = 0; kk < KP; ++kk) fn[kk] = 0.0f;
@@ -913,7 +916,7 @@ k_filter_radial(const ModelParams p, int N, const Box* __restrict__ box,
 // Reference find_partial_force_angular (nep.cu:890-991) with the
 // accumulate_f12 ladder (nep_utilities.cuh:1240-1491) evaluated once per edge
 // instead of once per (edge, n).
-template <int KM, int NAM, int LMAX, bool AG = true>
+template <int KM, int NAM, int LMAX, bool AG = true, bool FAST = false>
 __device__ __forceinline__ float3 angular_edge_force(const ModelParams& p, const float* c,
                                                     const float* __restrict__ av, float rc,
                                                     float dx, float dy, float dz)
@@ -921,12 +924,12 @@ __device__ __forceinline__ float3 angular_edge_force(const ModelParams& p, const
   constexpr int KP = (KM + 3) & ~3;
   constexpr int NLM = num_lm<LMAX>();
   const int nA = p.nA;
-  const float d = sqrtf(dx * dx + dy * dy + dz * dz);
-  const float dinv = 1.0f / d;
+  float d, dinv;
+  edge_length<FAST>(dx * dx + dy * dy + dz * dz, d, dinv);
   const float ux = dx * dinv, uy = dy * dinv, uz = dz * dinv;
-  const float rcinv = 1.0f / rc;
+  const float rcinv = recip<FAST>(rc);
   float fc, fcp;
-  cutoff_fc(rc, rcinv, d, fc, fcp);
+  cutoff_fc<FAST>(rc, rcinv, d, fc, fcp);
   float fn[KP], fnp[KP];
 #pragma unroll
   for (int kk = 0; kk < KP; ++kk) {
@@ -1029,6 +1032,9 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
             double* __restrict__ pe_ann)
 {
   static_assert(!(FF && XR), "the fused angular force is built for Verlet rows only");
+  // the mixed-precision build also takes the hardware approximations of
+  // sqrt, reciprocal, sine and cosine (cutoff_fc)
+  constexpr bool FAST = TC;
   constexpr int APW = 32 / G;             // centers per warp
   constexpr int APB = kBlock / G;         // centers per block
   constexpr int KP = (KM + 3) & ~3;
@@ -1086,10 +1092,11 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
   for (int n = 0; n < NRM; ++n) qr[n] = 0.0f;
   // q_n += sum_k c(t1,t2)[n][k] f_k(d) for one radial edge
   auto add_radial = [&](int t2, float d12_square, float rc_radial) {
-    const float d = sqrtf(d12_square);
-    const float rcinv = 1.0f / rc_radial;
+    float d, dinv;
+    edge_length<FAST>(d12_square, d, dinv);
+    const float rcinv = recip<FAST>(rc_radial);
     float fc, fcp;
-    cutoff_fc(rc_radial, rcinv, d, fc, fcp);
+    cutoff_fc<FAST>(rc_radial, rcinv, d, fc, fcp);
     float fn[KP];
 #pragma unroll
     for (int kk = 0; kk < KP; ++kk) fn[kk] = 0.0f;
@@ -1177,11 +1184,12 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
         } else {
           site_displacement(b, sites, xi, yi, zi, arow[k], dx, dy, dz, t2);
         }
-        const float d = sqrtf(dx * dx + dy * dy + dz * dz);
+        float d, dinv;
+        edge_length<FAST>(dx * dx + dy * dy + dz * dz, d, dinv);
         const float rc = (ra1 + p.rc_a[t2]) * 0.5f;
-        const float rcinv = 1.0f / rc;
+        const float rcinv = recip<FAST>(rc);
         float fc, fcp;
-        cutoff_fc(rc, rcinv, d, fc, fcp);
+        cutoff_fc<FAST>(rc, rcinv, d, fc, fcp);
         float fn[KP];
 #pragma unroll
         for (int kk = 0; kk < KP; ++kk) fn[kk] = 0.0f;
@@ -1191,7 +1199,6 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
 #pragma unroll
         for (int n = 0; n < CN; ++n)
           g[n] = (nc + n < nA) ? dot_basis<KM>(c + n * Lay.kpa, fn) : 0.0f;
-        const float dinv = 1.0f / d;
         for_each_harmonic<LMAX>(p.L_max, dx * dinv, dy * dinv, dz * dinv, [&](int lm, float y) {
 #pragma unroll
           for (int n = 0; n < CN; ++n) v[n * NLM + lm] += g[n] * y;
@@ -1398,8 +1405,8 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
           site_displacement(b, sites, xi, yi, zi, j, dx, dy, dz, t2);
         }
         const float rc = (ra1 + p.rc_a[t2]) * 0.5f;
-        const float3 f = angular_edge_force<KM, NAM, LMAX, false>(p, ctab + t2 * nA * Lay.kpa,
-                                                                  s_a, rc, dx, dy, dz);
+        const float3 f = angular_edge_force<KM, NAM, LMAX, false, FAST>(
+          p, ctab + t2 * nA * Lay.kpa, s_a, rc, dx, dy, dz);
         frow[k] = make_float4(f.x, f.y, f.z, 0.0f);
       }
     }
@@ -1422,7 +1429,7 @@ __device__ __forceinline__ void load_angular_tables(const ModelParams& p, float*
 // every edge of the center's angular row, f12[i][k] (float4, w unused).
 // XR: explicit rows of a batch; only the centers of structures that are not
 // small (each neighbour once in their rows) take this scheme.
-template <int G, int KM, int NAM, bool XR, int LMAX>
+template <int G, int KM, int NAM, bool XR, int LMAX, bool FAST>
 __global__ void __launch_bounds__(kBlock)
 k_angular_f12(const ModelParams p, int N, const Box* __restrict__ box,
               const Site* __restrict__ sites,
@@ -1463,8 +1470,8 @@ k_angular_f12(const ModelParams p, int N, const Box* __restrict__ box,
       site_displacement(b, sites, xi, yi, zi, arow[k], dx, dy, dz, t2);
     }
     const float rc = (ra1 + p.rc_a[t2]) * 0.5f;
-    const float3 f = angular_edge_force<KM, NAM, LMAX>(p, sm + (t1 * T + t2) * nA * KP, ai, rc,
-                                                       dx, dy, dz);
+    const float3 f = angular_edge_force<KM, NAM, LMAX, true, FAST>(
+      p, sm + (t1 * T + t2) * nA * KP, ai, rc, dx, dy, dz);
     f12[static_cast<size_t>(i) * mn_a + k] = make_float4(f.x, f.y, f.z, 0.0f);
   }
 }
@@ -1480,7 +1487,7 @@ k_angular_f12(const ModelParams p, int N, const Box* __restrict__ box,
 // GMINB: CTAs of 256 per SM the instance is built for (register cap), 0: no
 // cap.  The Verlet-row gather comes at 3 (its natural 78 registers) and at 4
 // (64 registers, a few spills, a third more warps); the autotuner picks one.
-template <int G, int KM, int NAM, bool XR, int LMAX, int GMINB = 0>
+template <int G, int KM, int NAM, bool XR, int LMAX, int GMINB, bool FAST>
 __global__ void __launch_bounds__(256, (GMINB > 0 ? GMINB : 1))
 k_gather(const ModelParams p, int N, const Box* __restrict__ box,
          const Site* __restrict__ sites, const int* __restrict__ nn_r, const int* __restrict__ nl_r,
@@ -1537,12 +1544,12 @@ k_gather(const ModelParams p, int N, const Box* __restrict__ box,
         j = jr;
         site_displacement(b, sites, xi, yi, zi, j, dx, dy, dz, t2);
       }
-      const float d = sqrtf(dx * dx + dy * dy + dz * dz);
-      const float dinv = 1.0f / d;
+      float d, dinv;
+      edge_length<FAST>(dx * dx + dy * dy + dz * dz, d, dinv);
       const float rc = (rr1 + p.rc_r[t2]) * 0.5f;
-      const float rcinv = 1.0f / rc;
+      const float rcinv = recip<FAST>(rc);
       float fc, fcp;
-      cutoff_fc(rc, rcinv, d, fc, fcp);
+      cutoff_fc<FAST>(rc, rcinv, d, fc, fcp);
       float fn[KP], fnp[KP];
 #pragma unroll
       for (int kk = 0; kk < KP; ++kk) {
@@ -1612,10 +1619,10 @@ k_gather(const ModelParams p, int N, const Box* __restrict__ box,
           const float rc = (p.rc_a[t1] + p.rc_a[t2]) * 0.5f;
           const int nA = p.nA;
           constexpr int NLM = num_lm<LMAX>();
-          const float3 fij = angular_edge_force<KM, NAM, LMAX>(
+          const float3 fij = angular_edge_force<KM, NAM, LMAX, true, FAST>(
             p, sm + (t1 * T + t2) * nA * KP, acoef + static_cast<size_t>(i) * nA * NLM, rc, dx,
             dy, dz);
-          const float3 fji = angular_edge_force<KM, NAM, LMAX>(
+          const float3 fji = angular_edge_force<KM, NAM, LMAX, true, FAST>(
             p, sm + (t2 * T + t1) * nA * KP, acoef + static_cast<size_t>(j) * nA * NLM, rc, -dx,
             -dy, -dz);
           a12 = make_float4(fij.x, fij.y, fij.z, 0.0f);
@@ -1745,8 +1752,13 @@ void launch_fused_t(Engine& e, int N, cudaStream_t s)
     e.scratch.acoef, e.scratch.f12, e.scratch.pe_ann);
 }
 
-template <int G, int NRM, int KM>
-void launch_filter_t(Engine& e, int N, cudaStream_t s)
+// The mixed precisions take the FAST builds of the filter, angular-force and
+// gather kernels (and of the descriptor kernel, whose tensor-core build is
+// FAST); they exist for the small shape, the others run the exact build.
+inline bool fast_math(const Engine& e) { return e.precision != 0; }
+
+template <int G, int NRM, int KM, bool FAST>
+void launch_filter_tf(Engine& e, int N, cudaStream_t s)
 {
   NeighborBuffers& nb = e.nbr;
   constexpr int APB = kBlock / G, KP = (KM + 3) & ~3;
@@ -1755,19 +1767,31 @@ void launch_filter_t(Engine& e, int N, cudaStream_t s)
   if (filter_bins(p, KP)) {
     const size_t smem =
       sizeof(float) * (filter_table_floats(p, KP) + 4 * kBlock * filter_bin_float4(p, KP));
-    k_filter_radial<G, NRM, KM, true><<<blocks, kBlock, smem, s>>>(
+    k_filter_radial<G, NRM, KM, true, FAST><<<blocks, kBlock, smem, s>>>(
       p, N, e.d_box, e.scratch.sites, e.d_nstate, nb.nn_v, nb.nl_v, nb.mn_v, nb.nn_r, nb.nl_r,
       nb.mn_r, nb.nn_a, nb.nl_a, nb.mn_a, e.scratch.qrad);
   } else {
     const size_t smem = sizeof(float) * filter_table_floats(p, KP);
-    k_filter_radial<G, NRM, KM, false><<<blocks, kBlock, smem, s>>>(
+    k_filter_radial<G, NRM, KM, false, FAST><<<blocks, kBlock, smem, s>>>(
       p, N, e.d_box, e.scratch.sites, e.d_nstate, nb.nn_v, nb.nl_v, nb.mn_v, nb.nn_r, nb.nl_r,
       nb.mn_r, nb.nn_a, nb.nl_a, nb.mn_a, e.scratch.qrad);
   }
 }
 
-template <int G, int KM, int NAM, int LMAX>
-void launch_f12_t(Engine& e, int N, cudaStream_t s)
+template <int G, int NRM, int KM>
+void launch_filter_t(Engine& e, int N, cudaStream_t s)
+{
+  if constexpr (KM == kSmallK) {
+    if (fast_math(e)) {
+      launch_filter_tf<G, NRM, KM, true>(e, N, s);
+      return;
+    }
+  }
+  launch_filter_tf<G, NRM, KM, false>(e, N, s);
+}
+
+template <int G, int KM, int NAM, int LMAX, bool FAST>
+void launch_f12_tf(Engine& e, int N, cudaStream_t s)
 {
   NeighborBuffers& nb = e.nbr;
   constexpr int APB = kBlock / G;
@@ -1775,13 +1799,25 @@ void launch_f12_t(Engine& e, int N, cudaStream_t s)
   const size_t smem =
     sizeof(float) * e.params.T * e.params.T * e.params.nA * ((KM + 3) & ~3);
   if (e.use_xr)
-    k_angular_f12<G, KM, NAM, true, LMAX><<<blocks, kBlock, smem, s>>>(
+    k_angular_f12<G, KM, NAM, true, LMAX, FAST><<<blocks, kBlock, smem, s>>>(
       e.params, N, e.d_box, e.scratch.sites, nb.nn_a, nb.nl_a, nb.mn_a, e.xr.ea, e.xr.large,
       e.scratch.acoef, e.scratch.f12);
   else
-    k_angular_f12<G, KM, NAM, false, LMAX><<<blocks, kBlock, smem, s>>>(
+    k_angular_f12<G, KM, NAM, false, LMAX, FAST><<<blocks, kBlock, smem, s>>>(
       e.params, N, e.d_box, e.scratch.sites, nb.nn_a, nb.nl_a, nb.mn_a, e.xr.ea, e.xr.large,
       e.scratch.acoef, e.scratch.f12);
+}
+
+template <int G, int KM, int NAM, int LMAX>
+void launch_f12_t(Engine& e, int N, cudaStream_t s)
+{
+  if constexpr (KM == kSmallK && LMAX == 4) {
+    if (fast_math(e)) {
+      launch_f12_tf<G, KM, NAM, LMAX, true>(e, N, s);
+      return;
+    }
+  }
+  launch_f12_tf<G, KM, NAM, LMAX, false>(e, N, s);
 }
 
 // FFI: the build also comes with the fused angular force (small shape)
@@ -1802,20 +1838,33 @@ void set_fused_smem_t(const ModelParams& p)
                          cudaFuncAttributeMaxDynamicSharedMemorySize, bytes(false));
 }
 
-template <int G, int KM, int NAM, bool XR, int LMAX, int GMINB = 0>
-void launch_gather_t(Engine& e, int N, double* pe, double* force, double* virial,
-                     bool accumulate, cudaStream_t s)
+template <int G, int KM, int NAM, bool XR, int LMAX, int GMINB, bool FAST>
+void launch_gather_tf(Engine& e, int N, double* pe, double* force, double* virial,
+                      bool accumulate, cudaStream_t s)
 {
   NeighborBuffers& nb = e.nbr;
   const int threads = 256;
   const int blocks = static_cast<int>((static_cast<long long>(N) * G + threads - 1) / threads);
   const size_t smem =
     XR ? sizeof(float) * e.params.T * e.params.T * e.params.nA * ((KM + 3) & ~3) : 0;
-  k_gather<G, KM, NAM, XR, LMAX, GMINB><<<blocks, threads, smem, s>>>(
+  k_gather<G, KM, NAM, XR, LMAX, GMINB, FAST><<<blocks, threads, smem, s>>>(
     e.params, N, e.d_box, e.scratch.sites, nb.nn_r, nb.nl_r, nb.mn_r, nb.nn_a, nb.nl_a, nb.mn_a,
     e.xr.er, e.xr.ea, e.scratch.acoef, e.scratch.alpha, e.scratch.f12, e.xr.large,
     e.scratch.pe_ann, pe,
     force, virial, accumulate ? 1 : 0, e.d_nstate);
+}
+
+template <int G, int KM, int NAM, bool XR, int LMAX, int GMINB = 0>
+void launch_gather_t(Engine& e, int N, double* pe, double* force, double* virial,
+                     bool accumulate, cudaStream_t s)
+{
+  if constexpr (KM == kSmallK && LMAX == 4) {
+    if (fast_math(e)) {
+      launch_gather_tf<G, KM, NAM, XR, LMAX, GMINB, true>(e, N, pe, force, virial, accumulate, s);
+      return;
+    }
+  }
+  launch_gather_tf<G, KM, NAM, XR, LMAX, GMINB, false>(e, N, pe, force, virial, accumulate, s);
 }
 
 // the FP32 build or, for the mixed precisions, the tensor-core one

@@ -33,7 +33,9 @@ extern "C" {
 /* ANN precision (nepx_set_precision) */
 #define NEPX_PRECISION_FP32 0        /* FP32 SIMT ANN: the reference's arithmetic */
 #define NEPX_PRECISION_MIXED 1       /* ANN on the tensor cores: FP16 operands with per-layer
-                                        power-of-two scaling, FP32 accumulation */
+                                        power-of-two scaling, FP32 accumulation; descriptor and
+                                        force kernels with the hardware square root, reciprocal
+                                        and sine/cosine approximations */
 #define NEPX_PRECISION_MIXED_BF16 2  /* the same with BF16 operands */
 
 /* compute flags */
@@ -304,7 +306,12 @@ int nepx_md_device_state(nepx_md_t* md, double** d_pos, double** d_vel, double**
  * FP32 accumulation: NEPX_PRECISION_MIXED (FP16; W0, w1 (1 - x^2) and each
  * CTA's descriptors scaled by powers of two to use FP16's range) or
  * NEPX_PRECISION_MIXED_BF16.  Descriptors, forces and the rest of the ANN
- * (tanh, energy sum) stay FP32.  NEPX_ERR_UNSUPPORTED for models with dim >
+ * (tanh, energy sum) stay FP32 arithmetic; in the mixed modes the descriptor
+ * and force kernels (models with n_max <= 4, basis <= 8, l_max <= 4) take
+ * the hardware approximations of 1/sqrt (edge lengths), 1/x and sine/cosine
+ * (the cutoff function), 2 ulp or about 4e-7 absolute, in place of the
+ * correctly rounded functions the FP32 mode keeps for parity with the
+ * reference.  NEPX_ERR_UNSUPPORTED for models with dim >
  * 128 or more than 256 hidden units.  No counterpart in the reference (its
  * ANN is FP32 only).
  */
