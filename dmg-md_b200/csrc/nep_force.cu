@@ -1484,11 +1484,14 @@ k_angular_f12(const ModelParams p, int N, const Box* __restrict__ box,
 // (periodic images), so the reverse partial force f12(j,i) is not looked up
 // but evaluated here from j's moment derivatives at -r: the angular force
 // work doubles and the f12 buffer and its kernel drop out.
-// GMINB: CTAs of 256 per SM the instance is built for (register cap), 0: no
-// cap.  The Verlet-row gather comes at 3 (its natural 78 registers) and at 4
-// (64 registers, a few spills, a third more warps); the autotuner picks one.
+// GMINB: CTAs of 256 per SM the instance is built for (register cap), 0 for
+// none.  The Verlet-row gather comes uncapped (about 80 registers for the
+// small shape, three CTAs) and at 4 (64 registers, a few spills, a third
+// more warps); the autotuner picks one.  The small shape's explicit-row
+// FAST build is held to two CTAs (128 registers: uncapped it would take 144,
+// and one CTA per SM).
 template <int G, int KM, int NAM, bool XR, int LMAX, int GMINB, bool FAST>
-__global__ void __launch_bounds__(256, (GMINB > 0 ? GMINB : 1))
+__global__ void __launch_bounds__(256, GMINB)
 k_gather(const ModelParams p, int N, const Box* __restrict__ box,
          const Site* __restrict__ sites, const int* __restrict__ nn_r, const int* __restrict__ nl_r,
          int mn_r, const int* __restrict__ nn_a, const int* __restrict__ nl_a, int mn_a,
@@ -1860,7 +1863,9 @@ void launch_gather_t(Engine& e, int N, double* pe, double* force, double* virial
 {
   if constexpr (KM == kSmallK && LMAX == 4) {
     if (fast_math(e)) {
-      launch_gather_tf<G, KM, NAM, XR, LMAX, GMINB, true>(e, N, pe, force, virial, accumulate, s);
+      // the explicit-row FAST build is held to two CTAs per SM
+      launch_gather_tf<G, KM, NAM, XR, LMAX, (XR ? 2 : GMINB), true>(e, N, pe, force, virial,
+                                                                      accumulate, s);
       return;
     }
   }
@@ -1905,10 +1910,10 @@ template <int G, int KM, int NAM, int LMAX>
 void launch_gather_g(Engine& e, int N, double* pe, double* force, double* virial,
                      bool accumulate, cudaStream_t s)
 {
-  if (e.use_xr) launch_gather_t<G, KM, NAM, true, LMAX>(e, N, pe, force, virial, accumulate, s);
+  if (e.use_xr) launch_gather_t<G, KM, NAM, true, LMAX, 0>(e, N, pe, force, virial, accumulate, s);
   else if (LMAX == 4 && e.gather_minb == 4)
     launch_gather_t<G, KM, NAM, false, LMAX, 4>(e, N, pe, force, virial, accumulate, s);
-  else launch_gather_t<G, KM, NAM, false, LMAX, 3>(e, N, pe, force, virial, accumulate, s);
+  else launch_gather_t<G, KM, NAM, false, LMAX, 0>(e, N, pe, force, virial, accumulate, s);
 }
 
 }  // namespace
