@@ -175,6 +175,7 @@ struct RebuildArgs {
   int mn_v, pow2, cell_cap;
   double skin, rc_v;
   float cutoff_square;
+  double prune_square; // (rc_v (1 + 1e-5) + 1e-5)^2: the stencil rows' trimming bound
   int skin_check;      // 1: pack the sites and apply the skin criterion first
   int force;           // with skin_check: rebuild whatever the displacements
 };
@@ -188,9 +189,10 @@ struct RebuildArgs {
 //   3. exclusive scan of the counts (per-block chunks, then block offsets);
 //   4. atoms into their cells (index and site record, in cell order);
 //   5. Verlet rows: one warp per center gathers every candidate of the 5x5x5
-//      stencil with float d^2 < (rc + skin)^2, sorts the row (bitonic, in
-//      registers up to 128 entries) and writes it with the reference
-//      positions of the next skin check.
+//      stencil (its rows along x, trimmed to the cells in reach) with float
+//      d^2 < (rc + skin)^2, sorts the row (bitonic, in registers up to 128
+//      entries) and writes it with the reference positions of the next skin
+//      check.
 // Phases 1-5 run only when the rebuild flag is set; the flag is the same for
 // every block, so all of them return together.
 __global__ void __launch_bounds__(kRebuildThreads, 12)
@@ -299,13 +301,22 @@ k_neighbor_rebuild(const RebuildArgs a)
   }
   grid_sync(a.gsync, st);
 
-  // 5. Verlet rows, one warp per center.  The 5x5x5 stencil cells go in
-  //    rounds of 32: lane q takes a cell, a warp prefix sum of their counts
-  //    flattens their atoms into one range, and the warp sweeps it 32
-  //    candidates at a time, reading the cell-ordered index and site record
-  //    side by side (no load waits on another).  Hits are compacted in order
-  //    of discovery (ballot + popcount) and the row is sorted: in registers,
-  //    four values per lane, up to 128 entries; in shared memory above.
+  // 5. Verlet rows, one warp per center.  The 5x5x5 stencil is taken as its
+  //    25 rows of cells along x (span1 x span2 of them on narrow grids); a
+  //    row's cells are consecutive in the cell order, so its atoms are one
+  //    contiguous run of the cell-ordered arrays (two where the row wraps
+  //    around the box).  In an orthogonal box each row is trimmed to the
+  //    cells that can hold a neighbour: a row whose y-z distance from the
+  //    center exceeds rc + skin is dropped, and the x extent keeps the
+  //    offsets whose distance along x fits in what is left (the bound is the
+  //    exact geometric distance to the cell, widened by 1e-5 relative so
+  //    that no pair the float predicate accepts is ever cut).  Lane r takes
+  //    row r, a warp prefix sum of the runs flattens them into one range,
+  //    and the warp sweeps it 32 candidates at a time, reading the
+  //    cell-ordered index and site record side by side.  Hits are compacted
+  //    in order of discovery (ballot + popcount) and the row is sorted: in
+  //    registers, four values per lane, up to 128 entries; in shared memory
+  //    above.
   const int lane = tid & 31, warp = tid >> 5;
   const unsigned below = (1u << lane) - 1u;
   const int pow2 = a.pow2;
@@ -313,78 +324,123 @@ k_neighbor_rebuild(const RebuildArgs a)
   const int span0 = (b.pbc[0] && nc0 >= 5) ? 5 : nc0;
   const int span1 = (b.pbc[1] && nc1 >= 5) ? 5 : nc1;
   const int span2 = (b.pbc[2] && nc2 >= 5) ? 5 : nc2;
-  const int ncand = span0 * span1 * span2;   // at most 125
-  const bool full = span0 == 5 && span1 == 5 && span2 == 5;
+  const int nrows = span1 * span2;   // at most 25
+  const bool prune = b.ortho != 0;
+  const double w0 = b.h[0] / nc0, w1 = b.h[4] / nc1, w2 = b.h[8] / nc2;
+  const double r2 = a.prune_square;
   for (int i = blockIdx.x * kRebuildWarps + warp; i < N; i += gridDim.x * kRebuildWarps) {
     // the site records may have been written by this launch (phase 0): plain
     // loads, which the barriers order, not the read-only path
     const double xi = a.sites[i].x, yi = a.sites[i].y, zi = a.sites[i].z;
     const int ci = a.cell_of[i];
     const int cx = ci % nc0, cy = (ci / nc0) % nc1, cz = ci / (nc0 * nc1);
-    int total = 0;
-    for (int r0 = 0; r0 < ncand; r0 += 32) {
-      int my_start = 0, my_cnt = 0;
-      if (r0 + lane < ncand) {
-        const int q = r0 + lane;
-        int q0, q1, q2;
-        if (full) {   // constant divisors
-          q0 = q % 5;
-          q1 = (q / 5) % 5;
-          q2 = q / 25;
-        } else {
-          q0 = q % span0;
-          q1 = (q / span0) % span1;
-          q2 = q / (span0 * span1);
+    int st1 = 0, n1 = 0, st2 = 0, n2 = 0;
+    if (lane < nrows) {
+      const int q1 = lane % span1, q2 = lane / span1;
+      // the center's position inside its cell, in cell widths (phase 2's
+      // fractional coordinates)
+      auto frac = [&](int d, int c, int nc) {
+        double sd = b.hinv[3 * d] * xi + b.hinv[3 * d + 1] * yi + b.hinv[3 * d + 2] * zi;
+        sd -= floor(sd);
+        return fmin(fmax(sd * nc - c, 0.0), 1.0);
+      };
+      // distance from the center to the cells k rows away along a direction
+      auto gap = [](int k, double u, double w) {
+        return k > 0 ? (k - u) * w : (k < 0 ? (u - k - 1) * w : 0.0);
+      };
+      double dyz2 = 0.0;
+      double ux = 0.0;
+      if (prune) {
+        if (span1 == 5) {
+          const double g = gap(q1 - 2, frac(1, cy, nc1), w1);
+          dyz2 += g * g;
         }
-        int gx = span0 == 5 ? cx + q0 - 2 : q0;
+        if (span2 == 5) {
+          const double g = gap(q2 - 2, frac(2, cz, nc2), w2);
+          dyz2 += g * g;
+        }
+        if (span0 == 5) ux = frac(0, cx, nc0);
+      }
+      if (dyz2 < r2) {
         int gy = span1 == 5 ? cy + q1 - 2 : q1;
         int gz = span2 == 5 ? cz + q2 - 2 : q2;
-        if (gx < 0) gx += nc0; else if (gx >= nc0) gx -= nc0;
         if (gy < 0) gy += nc1; else if (gy >= nc1) gy -= nc1;
         if (gz < 0) gz += nc2; else if (gz >= nc2) gz -= nc2;
-        const int c = (gz * nc1 + gy) * nc0 + gx;
-        my_start = a.cell_start[c];
-        my_cnt = a.cell_count[c];
+        const int row = (gz * nc1 + gy) * nc0;
+        // atoms of the row's cells c0..c1 (consecutive)
+        auto run = [&](int c0, int c1, int& st, int& n) {
+          st = a.cell_start[row + c0];
+          n = a.cell_start[row + c1] + a.cell_count[row + c1] - st;
+        };
+        if (span0 < 5) {
+          run(0, nc0 - 1, st1, n1);
+        } else {
+          int klo = -2, khi = 2;
+          if (prune) {
+            const double rx2 = r2 - dyz2;
+            auto within = [&](int k) {
+              const double g = gap(k, ux, w0);
+              return g * g < rx2;
+            };
+            klo = within(-1) ? (within(-2) ? -2 : -1) : 0;
+            khi = within(1) ? (within(2) ? 2 : 1) : 0;
+          }
+          const int g0 = cx + klo, g1 = cx + khi;
+          if (g0 < 0) {
+            run(g0 + nc0, nc0 - 1, st1, n1);
+            run(0, g1, st2, n2);
+          } else if (g1 >= nc0) {
+            run(g0, nc0 - 1, st1, n1);
+            run(0, g1 - nc0, st2, n2);
+          } else {
+            run(g0, g1, st1, n1);
+          }
+        }
       }
-      int incl = my_cnt;
+    }
+    const int my_cnt = n1 + n2;
+    int incl = my_cnt;
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
-      }
-      const int total_c = __shfl_sync(0xffffffffu, incl, 31);
-      for (int base = 0; base < total_c; base += 32) {
-        const int k = base + lane;
-        // stencil cell of candidate k: the first lane whose inclusive count exceeds k
-        int lo = 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const int total_c = __shfl_sync(0xffffffffu, incl, 31);
+    int total = 0;
+    for (int base = 0; base < total_c; base += 32) {
+      const int k = base + lane;
+      // stencil row of candidate k: the first lane whose inclusive count exceeds k
+      int lo = 0;
 #pragma unroll
-        for (int step = 16; step > 0; step >>= 1) {
-          const int v = __shfl_sync(0xffffffffu, incl, lo + step - 1);
-          if (v <= k) lo += step;
-        }
-        const int cstart = __shfl_sync(0xffffffffu, my_start, lo);
-        const int cincl = __shfl_sync(0xffffffffu, incl, lo);
-        const int ccnt = __shfl_sync(0xffffffffu, my_cnt, lo);
-        bool hit = false;
-        int j = 0;
-        if (k < total_c) {
-          const int at = cstart + (k - (cincl - ccnt));
-          j = a.cell_atoms[at];
-          const double2 sa = reinterpret_cast<const double2*>(a.cell_sites + at)[0];
-          const double2 sc = reinterpret_cast<const double2*>(a.cell_sites + at)[1];
-          float dx, dy, dz;
-          int tj;
-          site_delta(b, sa, sc, xi, yi, zi, dx, dy, dz, tj);
-          const float d2 = dx * dx + dy * dy + dz * dz;
-          hit = j != i && d2 < a.cutoff_square;
-        }
-        const unsigned m = __ballot_sync(0xffffffffu, hit);
-        if (hit) {
-          const int slot = total + __popc(m & below);
-          if (slot < pow2) buf[slot] = j;
-        }
-        total += __popc(m);
+      for (int step = 16; step > 0; step >>= 1) {
+        const int v = __shfl_sync(0xffffffffu, incl, lo + step - 1);
+        if (v <= k) lo += step;
       }
+      const int r_incl = __shfl_sync(0xffffffffu, incl, lo);
+      const int r_cnt = __shfl_sync(0xffffffffu, my_cnt, lo);
+      const int r_st1 = __shfl_sync(0xffffffffu, st1, lo);
+      const int r_n1 = __shfl_sync(0xffffffffu, n1, lo);
+      const int r_st2 = __shfl_sync(0xffffffffu, st2, lo);
+      bool hit = false;
+      int j = 0;
+      if (k < total_c) {
+        const int local = k - (r_incl - r_cnt);
+        const int at = local < r_n1 ? r_st1 + local : r_st2 + (local - r_n1);
+        j = a.cell_atoms[at];
+        const double2 sa = reinterpret_cast<const double2*>(a.cell_sites + at)[0];
+        const double2 sc = reinterpret_cast<const double2*>(a.cell_sites + at)[1];
+        float dx, dy, dz;
+        int tj;
+        site_delta(b, sa, sc, xi, yi, zi, dx, dy, dz, tj);
+        const float d2 = dx * dx + dy * dy + dz * dz;
+        hit = j != i && d2 < a.cutoff_square;
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, hit);
+      if (hit) {
+        const int slot = total + __popc(m & below);
+        if (slot < pow2) buf[slot] = j;
+      }
+      total += __popc(m);
     }
     __syncwarp();
     const int used = min(total, pow2);
@@ -487,6 +543,8 @@ void launch_neighbor_update(Engine& e, int N, const double* pos, const int* type
   a.skin = e.skin;
   a.rc_v = static_cast<double>(e.model.rc_max) + e.skin;
   a.cutoff_square = static_cast<float>(a.rc_v * a.rc_v);
+  const double rp = a.rc_v * (1.0 + 1e-5) + 1e-5;
+  a.prune_square = rp * rp;
   a.skin_check = skin_done ? 0 : 1;
   a.force = force ? 1 : 0;
   // small systems take fewer blocks: cheaper barriers, nothing to share out
