@@ -220,14 +220,6 @@ __device__ __forceinline__ void cutoff_fc(float rc, float rcinv, float d, float&
   }
 }
 
-// 1 / x: IEEE rounded, or with FAST the hardware approximation (2 ulp).
-template <bool FAST>
-__device__ __forceinline__ float recip(float x)
-{
-  if constexpr (FAST) return __fdividef(1.0f, x);
-  else return 1.0f / x;
-}
-
 // Edge length d and 1 / d from d^2: correctly rounded square root and
 // division, or with FAST one hardware reciprocal square root (2 ulp).
 template <bool FAST>

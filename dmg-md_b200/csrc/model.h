@@ -43,6 +43,11 @@ struct ModelParams {
   int dimK;           // dim rounded up to 8: row stride of the descriptor and dE/dq buffers
   int num_inv, inv_id[kMaxInv];
   float rc_r[kMaxTypes], rc_a[kMaxTypes];
+  // per type pair t1 * T + t2: [0] radial cutoff (rc_r[t1] + rc_r[t2]) / 2,
+  // [1] its reciprocal, [2] angular cutoff, [3] its reciprocal, T * T floats
+  // each (computed on the host with the same float operations: the kernels'
+  // results are unchanged, each edge saves a division)
+  const float* pair_cut;
   int zbl, zbl_flexible, typewise_zbl;
   float zbl_rc_inner, zbl_rc_outer, typewise_factor;
   int Z[kMaxTypes];

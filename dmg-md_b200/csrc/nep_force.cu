@@ -369,6 +369,25 @@ __host__ __device__ inline FusedLayout fused_layout(const ModelParams& p, int at
   return L;
 }
 
+// Cutoff of a type pair and its reciprocal: which 0 radial, 1 angular.  The
+// exact builds read both from ModelParams::pair_cut (the correctly rounded
+// reciprocal without a division per edge); the FAST builds form them from
+// the per-type cutoffs with the hardware reciprocal, which costs less than
+// the two loads.
+template <bool FAST>
+__device__ __forceinline__ void pair_cutoff(const ModelParams& p, int which, int t1, int t2,
+                                            float& rc, float& rcinv)
+{
+  if constexpr (FAST) {
+    rc = which == 0 ? (p.rc_r[t1] + p.rc_r[t2]) * 0.5f : (p.rc_a[t1] + p.rc_a[t2]) * 0.5f;
+    rcinv = __fdividef(1.0f, rc);
+  } else {
+    const int tt = p.T * p.T, k = t1 * p.T + t2;
+    rc = __ldg(p.pair_cut + 2 * which * tt + k);
+    rcinv = __ldg(p.pair_cut + (2 * which + 1) * tt + k);
+  }
+}
+
 // f[k] . c[k] over KM basis values with float4 loads of a padded row.
 template <int KM>
 __device__ __forceinline__ float dot_basis(const float* __restrict__ c, const float* f)
@@ -802,7 +821,6 @@ k_filter_radial(const ModelParams p, int N, const Box* __restrict__ box,
   const double xi = me.x, yi = me.y, zi = me.z;
   const int t1 = static_cast<int>(me.type);
   const unsigned below = (1u << gl) - 1u;
-  const float rr1 = p.rc_r[t1], ra1 = p.rc_a[t1];
   float qr[NRM];
 #pragma unroll
   for (int n = 0; n < NRM; ++n) qr[n] = 0.0f;
@@ -833,11 +851,13 @@ k_filter_radial(const ModelParams p, int N, const Box* __restrict__ box,
     bool in_r = false, in_a = false;
     int t2 = 0;
     float x12 = 0.0f, y12 = 0.0f, z12 = 0.0f, d12_square = 0.0f, rc_radial = 1.0f;
+    float rcinv_r = 1.0f;
     if (k < nv) {
       site_delta(b, sa, sc, xi, yi, zi, x12, y12, z12, t2);
       d12_square = x12 * x12 + y12 * y12 + z12 * z12;
-      rc_radial = (rr1 + p.rc_r[t2]) * 0.5f;
-      const float rc_angular = (ra1 + p.rc_a[t2]) * 0.5f;
+      float rc_angular, rcinv_a;
+      pair_cutoff<FAST>(p, 0, t1, t2, rc_radial, rcinv_r);
+      pair_cutoff<FAST>(p, 1, t1, t2, rc_angular, rcinv_a);
       in_r = d12_square < rc_radial * rc_radial;
       in_a = in_r && d12_square < rc_angular * rc_angular;
     }
@@ -848,7 +868,7 @@ k_filter_radial(const ModelParams p, int N, const Box* __restrict__ box,
       if (at < mn_r) rrow[at] = j;
       float d, dinv;
       edge_length<FAST>(d12_square, d, dinv);
-      const float rcinv = recip<FAST>(rc_radial);
+      const float rcinv = rcinv_r;
       float fc, fcp;
       cutoff_fc<FAST>(rc_radial, rcinv, d, fc, fcp);
       float fn[KP];
@@ -919,7 +939,7 @@ k_filter_radial(const ModelParams p, int N, const Box* __restrict__ box,
 template <int KM, int NAM, int LMAX, bool AG = true, bool FAST = false>
 __device__ __forceinline__ float3 angular_edge_force(const ModelParams& p, const float* c,
                                                     const float* __restrict__ av, float rc,
-                                                    float dx, float dy, float dz)
+                                                    float rcinv, float dx, float dy, float dz)
 {
   constexpr int KP = (KM + 3) & ~3;
   constexpr int NLM = num_lm<LMAX>();
@@ -927,7 +947,6 @@ __device__ __forceinline__ float3 angular_edge_force(const ModelParams& p, const
   float d, dinv;
   edge_length<FAST>(dx * dx + dy * dy + dz * dz, d, dinv);
   const float ux = dx * dinv, uy = dy * dinv, uz = dz * dinv;
-  const float rcinv = recip<FAST>(rc);
   float fc, fcp;
   cutoff_fc<FAST>(rc, rcinv, d, fc, fcp);
   float fn[KP], fnp[KP];
@@ -1086,15 +1105,15 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
   const int t1 = static_cast<int>(me.type);
 
   // ---- 1. filter the Verlet row, radial descriptors -------------------------
-  const float rr1 = p.rc_r[t1], ra1 = p.rc_a[t1];
   float qr[NRM];
 #pragma unroll
   for (int n = 0; n < NRM; ++n) qr[n] = 0.0f;
   // q_n += sum_k c(t1,t2)[n][k] f_k(d) for one radial edge
-  auto add_radial = [&](int t2, float d12_square, float rc_radial) {
+  auto add_radial = [&](int t2, float d12_square) {
+    float rc_radial, rcinv;
+    pair_cutoff<FAST>(p, 0, t1, t2, rc_radial, rcinv);
     float d, dinv;
     edge_length<FAST>(d12_square, d, dinv);
-    const float rcinv = recip<FAST>(rc_radial);
     float fc, fcp;
     cutoff_fc<FAST>(rc_radial, rcinv, d, fc, fcp);
     float fn[KP];
@@ -1118,7 +1137,7 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
       if (k < cr) {
         const float4 e = erow[k];
         const int t2 = static_cast<int>(static_cast<unsigned>(__float_as_int(e.w)) >> kRowTypeShift);
-        add_radial(t2, e.x * e.x + e.y * e.y + e.z * e.z, (rr1 + p.rc_r[t2]) * 0.5f);
+        add_radial(t2, e.x * e.x + e.y * e.y + e.z * e.z);
       }
     }
   } else {
@@ -1186,8 +1205,8 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
         }
         float d, dinv;
         edge_length<FAST>(dx * dx + dy * dy + dz * dz, d, dinv);
-        const float rc = (ra1 + p.rc_a[t2]) * 0.5f;
-        const float rcinv = recip<FAST>(rc);
+        float rc, rcinv;
+        pair_cutoff<FAST>(p, 1, t1, t2, rc, rcinv);
         float fc, fcp;
         cutoff_fc<FAST>(rc, rcinv, d, fc, fcp);
         float fn[KP];
@@ -1404,9 +1423,10 @@ k_nep_fused(const ModelParams p, int N, const Box* __restrict__ box,
         } else {
           site_displacement(b, sites, xi, yi, zi, j, dx, dy, dz, t2);
         }
-        const float rc = (ra1 + p.rc_a[t2]) * 0.5f;
+        float rc, rcinv;
+        pair_cutoff<FAST>(p, 1, t1, t2, rc, rcinv);
         const float3 f = angular_edge_force<KM, NAM, LMAX, false, FAST>(
-          p, ctab + t2 * nA * Lay.kpa, s_a, rc, dx, dy, dz);
+          p, ctab + t2 * nA * Lay.kpa, s_a, rc, rcinv, dx, dy, dz);
         frow[k] = make_float4(f.x, f.y, f.z, 0.0f);
       }
     }
@@ -1453,7 +1473,6 @@ k_angular_f12(const ModelParams p, int N, const Box* __restrict__ box,
   const Site me = sites[i];
   const double xi = me.x, yi = me.y, zi = me.z;
   const int t1 = static_cast<int>(me.type);
-  const float ra1 = p.rc_a[t1];
   const int na = nn_a[i];
   const int* arow = nl_a + static_cast<size_t>(i) * mn_a;
   const float* ai = acoef + static_cast<size_t>(i) * nA * num_lm<LMAX>();
@@ -1469,9 +1488,10 @@ k_angular_f12(const ModelParams p, int N, const Box* __restrict__ box,
     } else {
       site_displacement(b, sites, xi, yi, zi, arow[k], dx, dy, dz, t2);
     }
-    const float rc = (ra1 + p.rc_a[t2]) * 0.5f;
+    float rc, rcinv;
+    pair_cutoff<FAST>(p, 1, t1, t2, rc, rcinv);
     const float3 f = angular_edge_force<KM, NAM, LMAX, true, FAST>(
-      p, sm + (t1 * T + t2) * nA * KP, ai, rc, dx, dy, dz);
+      p, sm + (t1 * T + t2) * nA * KP, ai, rc, rcinv, dx, dy, dz);
     f12[static_cast<size_t>(i) * mn_a + k] = make_float4(f.x, f.y, f.z, 0.0f);
   }
 }
@@ -1520,7 +1540,6 @@ k_gather(const ModelParams p, int N, const Box* __restrict__ box,
     const Site me = sites[i];
     const double xi = me.x, yi = me.y, zi = me.z;
     const int t1 = static_cast<int>(me.type);
-    const float rr1 = p.rc_r[t1];
     const float* ali = alpha + static_cast<size_t>(i) * T * kpr;
     // radial pairs: both site energies through the alpha coefficients
     const int nr = nn_r[i];
@@ -1549,8 +1568,8 @@ k_gather(const ModelParams p, int N, const Box* __restrict__ box,
       }
       float d, dinv;
       edge_length<FAST>(dx * dx + dy * dy + dz * dz, d, dinv);
-      const float rc = (rr1 + p.rc_r[t2]) * 0.5f;
-      const float rcinv = recip<FAST>(rc);
+      float rc, rcinv;
+      pair_cutoff<FAST>(p, 0, t1, t2, rc, rcinv);
       float fc, fcp;
       cutoff_fc<FAST>(rc, rcinv, d, fc, fcp);
       float fn[KP], fnp[KP];
@@ -1619,15 +1638,16 @@ k_gather(const ModelParams p, int N, const Box* __restrict__ box,
             atomicOr(&st->overflow, 4);
           }
         } else {
-          const float rc = (p.rc_a[t1] + p.rc_a[t2]) * 0.5f;
+          float rc, rcinv;
+          pair_cutoff<FAST>(p, 1, t1, t2, rc, rcinv);
           const int nA = p.nA;
           constexpr int NLM = num_lm<LMAX>();
           const float3 fij = angular_edge_force<KM, NAM, LMAX, true, FAST>(
-            p, sm + (t1 * T + t2) * nA * KP, acoef + static_cast<size_t>(i) * nA * NLM, rc, dx,
-            dy, dz);
+            p, sm + (t1 * T + t2) * nA * KP, acoef + static_cast<size_t>(i) * nA * NLM, rc,
+            rcinv, dx, dy, dz);
           const float3 fji = angular_edge_force<KM, NAM, LMAX, true, FAST>(
-            p, sm + (t2 * T + t1) * nA * KP, acoef + static_cast<size_t>(j) * nA * NLM, rc, -dx,
-            -dy, -dz);
+            p, sm + (t2 * T + t1) * nA * KP, acoef + static_cast<size_t>(j) * nA * NLM, rc,
+            rcinv, -dx, -dy, -dz);
           a12 = make_float4(fij.x, fij.y, fij.z, 0.0f);
           a21 = make_float4(fji.x, fji.y, fji.z, 0.0f);
         }
