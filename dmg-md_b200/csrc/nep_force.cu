@@ -1883,9 +1883,13 @@ void launch_gather_t(Engine& e, int N, double* pe, double* force, double* virial
 {
   if constexpr (KM == kSmallK && LMAX == 4) {
     if (fast_math(e)) {
-      // the explicit-row FAST build is held to two CTAs per SM
-      launch_gather_tf<G, KM, NAM, XR, LMAX, (XR ? 2 : GMINB), true>(e, N, pe, force, virial,
-                                                                      accumulate, s);
+      // the FAST builds are held to their occupancy: two CTAs per SM on
+      // explicit rows, three for the uncapped Verlet-row build (it takes 84
+      // registers unheld, which the 8-register allocation unit rounds to 88:
+      // two CTAs of 256, and 1.5x the time)
+      constexpr int fast_minb = XR ? 2 : (GMINB == 0 ? 3 : GMINB);
+      launch_gather_tf<G, KM, NAM, XR, LMAX, fast_minb, true>(e, N, pe, force, virial,
+                                                              accumulate, s);
       return;
     }
   }
