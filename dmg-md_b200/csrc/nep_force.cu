@@ -786,9 +786,10 @@ __device__ void tc_ann(const ModelParams& p, const FusedLayout& Lay, float* sm, 
 // instead of the nR x kR contraction.  Kept apart from k_nep_fused so this
 // latency-bound sweep runs at the occupancy of its own register count.
 // FAST: the mixed-precision build (hardware sqrt / reciprocal / sine-cosine
-// approximations, see cutoff_fc).
+// approximations, see cutoff_fc), held to seven CTAs per SM (72 registers,
+// as the exact build takes; it would take 78, rounded to 80: six CTAs).
 template <int G, int NRM, int KM, bool BIN, bool FAST>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, (FAST ? 7 : 0))
 k_filter_radial(const ModelParams p, int N, const Box* __restrict__ box,
                 const Site* __restrict__ sites, NeighborState* st,
                 const int* __restrict__ nn_v, const int* __restrict__ nl_v, int mn_v,
@@ -1449,8 +1450,10 @@ __device__ __forceinline__ void load_angular_tables(const ModelParams& p, float*
 // every edge of the center's angular row, f12[i][k] (float4, w unused).
 // XR: explicit rows of a batch; only the centers of structures that are not
 // small (each neighbour once in their rows) take this scheme.
+// FAST builds held to four CTAs per SM (128 registers, as the exact build
+// takes; they would take 142, rounded to 144: three CTAs).
 template <int G, int KM, int NAM, bool XR, int LMAX, bool FAST>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, (FAST ? 4 : 0))
 k_angular_f12(const ModelParams p, int N, const Box* __restrict__ box,
               const Site* __restrict__ sites,
               const int* __restrict__ nn_a, const int* __restrict__ nl_a, int mn_a,
