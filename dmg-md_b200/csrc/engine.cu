@@ -328,19 +328,20 @@ void engine_autotune(Engine& e, int N, const double* pos, const int* type, cudaS
   if (!e.use_xr) {
     float best = 1e30f;
     int pick = e.filter_group;
+    // each grouping: one untimed launch, then the median of five
     for (int g : groups) {
       e.filter_group = g;
-      float t[3];
-      for (int r = 0; r < 3; ++r) {
+      float t[6];
+      for (int r = 0; r < 6; ++r) {
         cudaEventRecord(a, stream);
         launch_filter(e, N, stream);
         cudaEventRecord(b, stream);
         cudaEventSynchronize(b);
         cudaEventElapsedTime(&t[r], a, b);
       }
-      std::sort(t, t + 3);
-      if (t[1] < best) {
-        best = t[1];
+      std::sort(t + 1, t + 6);
+      if (t[3] < best) {
+        best = t[3];
         pick = g;
       }
     }
