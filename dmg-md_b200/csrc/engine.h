@@ -119,7 +119,7 @@ struct Engine {
   int filter_group = 8;      // lanes per center in the typewise filter (autotuned)
   int f12_group = 4;         // lanes per center in the angular-force kernel (autotuned)
   int gather_group = 8;      // lanes per center in the gather (autotuned)
-  int gather_minb = 3;       // CTAs per SM the Verlet-row gather is built for (autotuned)
+  int gather_minb = 3;       // Verlet-row gather build: 3 unheld, 4 held to four CTAs (autotuned)
   bool fuse_f12 = false;     // the descriptor kernel evaluates f12 itself (autotuned)
   bool tuned = false;
   std::string error;

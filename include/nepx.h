@@ -328,8 +328,9 @@ int nepx_set_precision(nepx_t* handle, int mode);
  *   [5] 1: the descriptor kernel evaluates the angular partial forces itself
  *       (models with n_max <= 4, basis <= 8, l_max <= 4, on the Verlet-row
  *       path), 0: k_angular_f12 does
- *   [6] CTAs of 256 per SM the Verlet-row gather is built for (3 or 4; models
- *       with l_max <= 4)
+ *   [6] the Verlet-row gather's build (models with l_max <= 4): 3 = unheld
+ *       (about 80 registers, three CTAs of 256 per SM), 4 = held to four CTAs
+ *       (64 registers, some spills, a third more warps)
  * The first compute of a handle times the variants and keeps the fastest
  * (the autotuner; its picks are shared by the handles of the process and,
  * with NEPX_TUNE_FILE set, kept in that file).  nepx_get_tuning reports the
