@@ -77,15 +77,15 @@ import workloads  # noqa: E402
 
 K_B = 8.617343e-5
 # DRAM bytes per atom and force call of the force kernels (k_filter_radial,
-# k_nep_fused with the angular partial forces inside, k_gather: the form the
-# autotuner picks for this model), dram__bytes_read.sum +
-# dram__bytes_write.sum of one ncu-captured launch each on the large-carbon
+# k_nep_fused with the angular partial forces inside, k_gather at four CTAs
+# per SM: the builds the autotuner picks for this model), dram__bytes_read.sum
+# + dram__bytes_write.sum of one ncu-captured launch each on the large-carbon
 # system at 1,000,000 atoms (--ncell 50), divided by its atoms (traffic grows
 # with the atoms processed).  Keyed by workload and the kernel list; another
 # form reports no traffic.
 TRAFFIC_PER_ATOM = {
     ("carbon8m", ("k_filter_radial", "k_nep_fused", "k_gather")):
-        (694.4 + 402.8 + 349.1 + 567.1 + 1349.8 + 99.0) * 1e6 / 1.0e6}
+        (701.6 + 412.2 + 349.1 + 567.1 + 1359.3 + 292.3) * 1e6 / 1.0e6}
 FP32_LANES = 148 * 128          # B200: SMs x FP32 lanes
 SM_MAX_MHZ = 1965.0
 L2_NOTE = "flushed by a 512 MiB write before every %d-step chunk"
